@@ -1,0 +1,230 @@
+/*
+ * pism_ssa_gpu.h — C-ABI of the B200 finite-difference SSA (SSAFD) solver.
+ *
+ * This is the boundary a PISM host binds to in place of SSAFD's PETSc path.
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (0 = success, see PISM_GPU_SSA_E*); nothing throws across this boundary.
+ * The message of the last failure of a handle is pism_gpu_ssa_last_error().
+ *
+ * Field layout (all FP64 unless stated): a scalar field is Mx*My values indexed
+ * [i][j] with j (the y index) contiguous, i.e. element i*My + j — the layout of a
+ * PETSc DMDA local array without ghosts (src/base/util/IceGrid.cc:800-823).  A
+ * vector field (velocity, boundary values, driving stress) interleaves (u, v)
+ * per cell (2*Mx*My values, IceModelVec2V); a staggered field stores
+ * (east face i+1/2, north face j+1/2) per cell (IceModelVec2Stag).  Neighbour
+ * accesses wrap periodically at every domain edge, as the reference's DMDA does.
+ *
+ * Units are SI: m, m/s, Pa, Pa s m, J/kg.
+ */
+#ifndef PISM_SSA_GPU_H
+#define PISM_SSA_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PISM_GPU_SSA_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+  PISM_GPU_SSA_OK = 0,
+  PISM_GPU_SSA_EINVAL = 1,          /* bad argument (null pointer, size, enum)          */
+  PISM_GPU_SSA_ECUDA = 2,           /* CUDA runtime error; context may be unusable      */
+  PISM_GPU_SSA_ENOMEM = 3,          /* device allocation failed                         */
+  PISM_GPU_SSA_EKSP = 4,            /* KSPFailure: Krylov solve failed (SSAFD.hh:115)   */
+  PISM_GPU_SSA_EPICARD = 5,         /* PicardFailure (SSAFD.hh:120)                     */
+  PISM_GPU_SSA_EZERODIAG = 6,       /* zero diagonal at a regular location (SSAFD.cc:766-776) */
+  PISM_GPU_SSA_ENAN = 7,            /* non-finite value in a residual / inputs          */
+  PISM_GPU_SSA_ESTATE = 8           /* call order violated (e.g. solve before inputs)   */
+};
+
+/* ---- enumerations -------------------------------------------------------- */
+/* flow laws accepted by the SSA (src/base/rheology/flowlaw_factory.hh:31-37,
+ * Goldsby-Kohlstedt excluded as in SSA.cc:107-109) */
+enum {
+  PISM_FLOW_LAW_ISOTHERMAL_GLEN = 0,
+  PISM_FLOW_LAW_PB = 1,
+  PISM_FLOW_LAW_GPBLD = 2,
+  PISM_FLOW_LAW_ARR = 3,
+  PISM_FLOW_LAW_ARRWARM = 4,
+  PISM_FLOW_LAW_HOOKE = 5
+};
+
+/* grid periodicity (IceGrid.hh, Periodicity) */
+enum { PISM_NOT_PERIODIC = 0, PISM_X_PERIODIC = 1, PISM_Y_PERIODIC = 2, PISM_XY_PERIODIC = 3 };
+
+/* Krylov method (replaces PETSc KSPSolve, SSAFD.cc:1018) */
+enum { PISM_KSP_BICGSTAB = 0, PISM_KSP_GMRES = 1 };
+
+/* preconditioner (replaces PCBJACOBI/ILU(0) and PCASM/LU, SSAFD.cc:136-219) */
+enum { PISM_PC_BLOCK_JACOBI = 0, PISM_PC_MULTIGRID = 1 };
+
+/* arithmetic of the inner Krylov iterations */
+enum { PISM_PRECISION_FP64 = 0, PISM_PRECISION_MIXED = 1 };
+
+/* where the pointers handed to set_inputs / solve live */
+enum { PISM_MEM_HOST = 0, PISM_MEM_DEVICE = 1 };
+
+/* ---- grid -------------------------------------------------------------- */
+typedef struct pism_gpu_grid {
+  int Mx, My;            /* points in x (i) and y (j); both >= 3                  */
+  double dx, dy;         /* spacing (IceGrid::dx(), dy())                          */
+  int periodicity;       /* PISM_*_PERIODIC; only affects the one-sided edge
+                            differences of compute_surf_grad_inward_ssa            */
+  int Mz;                /* vertical levels of the enthalpy columns (0 = none)     */
+  const double *z;       /* host array of Mz levels, z[0] = 0 (IceGrid::z())       */
+} pism_gpu_grid;
+
+/* ---- SSA configuration: the pism_config.cdl parameters the path reads ---- */
+typedef struct pism_gpu_ssa_config {
+  double ice_density, sea_water_density, standard_gravity, sea_level;
+  double epsilon_ssa;                              /* nu*H regularisation            */
+  double ssafd_relative_convergence;               /* Picard tolerance (-ssa_rtol)   */
+  int    max_iterations_ssafd;                     /* -ssa_maxi                      */
+  double ssafd_nuH_iter_failure_underrelaxation;
+  double min_thickness_strength_extension_ssa;
+  double constant_nu_strength_extension_ssa;
+  double plastic_regularization;                   /* m/s                            */
+  int    do_pseudo_plastic_till;
+  double pseudo_plastic_q, pseudo_plastic_uthreshold, sliding_scale_factor_reduces_tauc;
+  double beta_ice_free_bedrock;
+  int    calving_front_stress_boundary_condition;  /* -cfbc                          */
+  int    ssa_dirichlet_bc;
+  int    sub_groundingline;
+  int    nu_bedrock_set;
+  double nu_bedrock;
+  int    surface_gradient_eta;                     /* surface_gradient_method == eta */
+  int    compute_surf_grad_inward_ssa;
+  int    flow_law;                                 /* PISM_FLOW_LAW_*                */
+  double ssa_Glen_exponent, ssa_enhancement_factor, ice_softness;
+  double Schoof_regularizing_length, Schoof_regularizing_velocity;   /* m, m/s     */
+  double Paterson_Budd_A_cold, Paterson_Budd_A_warm, Paterson_Budd_Q_cold, Paterson_Budd_Q_warm;
+  double Paterson_Budd_critical_temperature, ideal_gas_constant;
+  double gpbld_water_frac_coeff, gpbld_water_frac_observed_limit;
+  double Hooke_A, Hooke_Q, Hooke_C, Hooke_k, Hooke_Tr;
+  double beta_CC, ice_specific_heat_capacity, water_latent_heat_fusion, surface_pressure;
+  double water_melting_point_temperature, enthalpy_converter_reference_temperature;
+  int    do_fracture_density;
+  double fracture_density_softening_lower_limit;
+  int    brutal_sliding;
+  double brutal_sliding_scale;
+  /* linear solver: the -ssafd_ksp_* / -ssafd_pc_* options of the reference */
+  int    ksp_type;                                 /* PISM_KSP_*                     */
+  int    pc_type;                                  /* PISM_PC_*                      */
+  double ksp_rtol;                                 /* -ssafd_ksp_rtol (PETSc 1e-5)   */
+  int    ksp_max_it;                               /* PETSc default 10000            */
+  int    gmres_restart;                            /* PETSc default 30               */
+  int    precision;                                /* PISM_PRECISION_*               */
+  double mixed_inner_rtol;                         /* inner FP32 solve tolerance     */
+  int    verbosity;                                /* 0 silent .. 3 per-iteration    */
+} pism_gpu_ssa_config;
+
+/* ---- input fields (SSA::init_impl, SSA.cc:134-184; SSAFD::update) -------- */
+typedef struct pism_gpu_ssa_inputs {
+  int where;                      /* PISM_MEM_HOST or PISM_MEM_DEVICE                  */
+  const double *thickness;        /* land_ice_thickness                    (required) */
+  const double *surface;          /* surface_altitude                      (required) */
+  const double *bed;              /* bedrock_altitude                      (required) */
+  const double *mask;             /* mask, doubles rounded by as_int()     (required) */
+  const double *tauc;             /* tauc (yield stress)                   (required) */
+  const double *bc_mask;          /* bc_mask; NULL = no Dirichlet locations          */
+  const double *bc_values;        /* vel_ssa_bc, interleaved; NULL with bc_mask NULL */
+  const double *melange;          /* melange back pressure fraction; NULL = 0        */
+  const double *gl_mask;          /* gl_mask; required if sub_groundingline          */
+  const double *enthalpy;         /* Mx*My*Mz, [i][j][k]; required unless the flow
+                                     law is isothermal_glen or hardness is given     */
+  const double *hardness_stag;    /* optional precomputed staggered hardness (2*Mx*My);
+                                     replaces compute_hardav_staggered when non-NULL */
+  const double *fracture_density; /* required if do_fracture_density                 */
+} pism_gpu_ssa_inputs;
+
+/* ---- per-solve statistics (the SSAFD stdout report, SSAFD.cc:994-1118) ---- */
+typedef struct pism_gpu_ssa_stats {
+  int    status;                   /* PISM_GPU_SSA_* of the solve                     */
+  int    converged;                /* 1 if a Picard strategy met the tolerance        */
+  int    strategy;                 /* 0 default, 1 under-relaxation, 2 regularisation */
+  int    picard_iterations;        /* outer iterations of the accepted strategy       */
+  int    ksp_iterations;           /* Krylov iterations, all strategies               */
+  int    ksp_failures;             /* KSP failures that switched the solver           */
+  int    refinement_steps;         /* FP64 refinement steps (mixed precision)         */
+  double nuH_norm, nuH_norm_change;
+  double final_linear_residual;    /* ||b - A x|| / ||b|| of the last linear solve    */
+  double solve_ms;                 /* wall time of pism_gpu_ssa_solve                 */
+  double kernel_ms;                /* device time (CUDA events) of the solve          */
+} pism_gpu_ssa_stats;
+
+typedef struct pism_gpu_ssa pism_gpu_ssa;   /* opaque handle: owns device scratch */
+
+/* Fill *cfg with the pism_config.cdl defaults.  Replaces Config::get_* reads. */
+int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *cfg);
+
+/* Create a solver for one grid on CUDA device `device`.  Replaces the SSAFD
+ * constructor + SSAFD::init_impl (SSAFD.cc:59-129, 221-258) and the factory
+ * SSAFDFactory (SSAFD.cc:47-49, typedef SSAFactory SSA.hh:77). */
+int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cfg,
+                        int device, pism_gpu_ssa **out);
+
+/* Destroy a handle and free its device memory. */
+int pism_gpu_ssa_destroy(pism_gpu_ssa *h);
+
+/* Last error message of the handle ("" if none); valid until the next call. */
+const char *pism_gpu_ssa_last_error(const pism_gpu_ssa *h);
+
+/* Run the handle's work on a caller-owned cudaStream_t (NULL = the handle's own). */
+int pism_gpu_ssa_set_stream(pism_gpu_ssa *h, void *cuda_stream);
+
+/* Replace the configuration (e.g. epsilon_ssa set after init, as ssa_testi.cc:99-100). */
+int pism_gpu_ssa_set_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *cfg);
+
+/* Copy the input fields (borrowed for the duration of the call).  Replaces the
+ * m_grid->variables() lookups of SSA::init_impl (SSA.cc:134-184), the
+ * ShallowStressBalance::set_boundary_conditions call and the melange pointer of
+ * SSAFD::update (SSAFD.cc:260-264). */
+int pism_gpu_ssa_set_inputs(pism_gpu_ssa *h, const pism_gpu_ssa_inputs *in);
+
+/* SSA::set_initial_guess (SSA.cc:361-363): velocity (2*Mx*My, host or device per
+ * `where`). */
+int pism_gpu_ssa_set_initial_guess(pism_gpu_ssa *h, const double *velocity, int where);
+
+/* SSAFD::solve (SSAFD.cc:869-924) with the Picard strategy ladder, followed by
+ * compute_basal_frictional_heating as in SSA::update (SSA.cc:188-196).  Writes the
+ * velocity (2*Mx*My) to velocity_out (host or device per `where`; may be NULL)
+ * and fills *stats (may be NULL).  Blocks until the solve is done. */
+int pism_gpu_ssa_solve(pism_gpu_ssa *h, double *velocity_out, int where,
+                       pism_gpu_ssa_stats *stats);
+
+/* Field getters (host or device destination per `where`). */
+enum {
+  PISM_FIELD_VELOCITY = 0,        /* 2N  m_velocity                                   */
+  PISM_FIELD_TAUD = 1,            /* 2N  driving stress (SSA_taud, SSA.cc:402-432)    */
+  PISM_FIELD_RHS = 2,             /* 2N  m_b (SSAFD::assemble_rhs)                    */
+  PISM_FIELD_HARDNESS = 3,        /* 2N  staggered hardness                           */
+  PISM_FIELD_NUH = 4,             /* 2N  nu*H (SSAFD_nuH diagnostic, SSAFD.cc:1790)   */
+  PISM_FIELD_BETA = 5,            /* N   basal drag coefficient of the last assembly  */
+  PISM_FIELD_BFRICT = 6           /* N   basal frictional heating                     */
+};
+int pism_gpu_ssa_get_field(pism_gpu_ssa *h, int field, double *out, int where);
+
+/* Stage entry points, each the device restatement of one reference method, for
+ * stage-by-stage checking:
+ *   assemble_rhs       -> SSA::compute_driving_stress + SSAFD::assemble_rhs
+ *   compute_hardness   -> SSAFD::compute_hardav_staggered (+ fracture softening)
+ *   compute_nuH        -> SSAFD::compute_nuH_staggered[_cfbc] at the current
+ *                         velocity, with regularisation `reg`; also refreshes beta
+ *   apply              -> y = A x with the matrix SSAFD::assemble_matrix would
+ *                         build from the current nu*H and beta (device pointers) */
+int pism_gpu_ssa_assemble_rhs(pism_gpu_ssa *h);
+int pism_gpu_ssa_compute_hardness(pism_gpu_ssa *h);
+int pism_gpu_ssa_compute_nuH(pism_gpu_ssa *h, double reg);
+int pism_gpu_ssa_apply(pism_gpu_ssa *h, const double *x_dev, double *y_dev);
+
+/* One linear solve A x = b at the current nu*H / beta with the configured
+ * Krylov method (the body of KSPSolve, SSAFD.cc:1018).  x (device, 2N) holds the
+ * initial guess on entry.  *iterations and *rel_residual may be NULL. */
+int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations,
+                              double *rel_residual);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PISM_SSA_GPU_H */
