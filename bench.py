@@ -1,0 +1,313 @@
+"""Benchmark: one SSAFD solve on the seeded synthetic 801 x 801 ice sheet (5 km grid).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size M]
+
+A step is one complete SSA solve (SSAFD::solve: driving stress, hardness, the
+Picard loop with its linear solves) from a zero initial guess, with the inputs
+of the plain-FP64 configuration: plastic till, Picard nu*H tolerance 1e-4,
+KSP rtol 1e-8.  The metric is milliseconds per solve (lower is better); with N
+GPUs every rank solves its own replica (no data-path collective: the solve
+does not shard) and ``value`` is the job's time per solve = max-over-ranks step
+time / N.
+
+``--impl reference`` times the CPU restatement of the reference's own path
+(numpy assembly of the SSAFD matrix + PETSc-style GMRES(30) / block-Jacobi
+ILU(0) with one block per host thread, oracle/) on a bounded sample of the same
+solve: the first few Picard iterations, scaled to a full solve by the GPU run's
+Picard count for the same input.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(REPO, "pismv0.7.3_b200")
+METRIC = "SSA solve ms at 801² to rel resid 1e-6: learned+FP32 vs plain FP64, 1 B200"
+# Picard iterations of the GPU FP64 solve of the 801^2 seed-0 case (used to scale the
+# CPU sample to a whole solve when the GPU arm has not run in this process)
+DEFAULT_PICARD_801 = None
+
+
+def _package():
+    if "pism_b200" in sys.modules:
+        return sys.modules["pism_b200"]
+    spec = importlib.util.spec_from_file_location("pism_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pism_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return p.get("hbm_gbs", 6650.0), "measured"
+    except OSError:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[2 + k]
+                          and not s[2 + k].startswith("Not")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_case(M):
+    _package()
+    from pism_b200 import synthetic as S
+    dx = 4000e3 / (M - 1)
+    g, c, f, meta = S.build_synthetic(M, dx, seed=0)
+    c.ksp_rtol = 1e-8
+    c.ssafd_relative_convergence = 1e-4
+    return g, c, f, meta
+
+
+def cpu_reference_sample(M, picard_sample, picard_full, nthreads):
+    """The oracle port on the host cores: `picard_sample` Picard iterations of the
+    reference algorithm (PETSc-style GMRES(30) + block Jacobi ILU(0), one block
+    per thread), scaled to `picard_full` iterations."""
+    sys.path.insert(0, REPO)
+    from oracle import ssafd_oracle as O
+    g, c, f, _ = build_case(M)
+    G, Cc, I = O.from_case(g, c, f)
+    o = O.SSAFDOracle(G, Cc, I, linear="petsc", ksp_rtol=c.ksp_rtol, nranks=nthreads, nthreads=nthreads)
+    Cc.max_iterations_ssafd = picard_sample
+    t0 = time.perf_counter()
+    try:
+        o.prepare()
+        o.picard_manager(Cc.epsilon_ssa, 1.0)
+    except O.PicardFailure:
+        pass
+    dt = time.perf_counter() - t0
+    done = max(1, o.stats.picard_iterations)
+    return dt * 1e3 / done * picard_full, done, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    picard_full = args.picard_full or 160
+    vals = []
+    sample = None
+    for k in range(args.warmup + args.steps):
+        ms, done, dt = cpu_reference_sample(args.size, args.cpu_picard, picard_full, nthreads)
+        if k >= args.warmup:
+            vals.append(ms)
+            sample = f"first {done} Picard iterations of the {args.size}^2 seed-0 solve ({dt:.1f} s), " \
+                     f"scaled to {picard_full} Picard iterations"
+    v = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"SSAFD solve, synthetic ice sheet {args.size}x{args.size} at "
+                               f"{4000 / (args.size - 1):.0f} km, plastic till, Picard 1e-4, KSP 1e-8",
+                   "grid": [args.size, args.size], "seed": 0},
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--size", type=int, default=801)
+    ap.add_argument("--cpu-picard", type=int, default=2, help="Picard iterations in the CPU sample")
+    ap.add_argument("--picard-full", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--apply-launches", type=int, default=50)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    _package()
+    from pism_b200.ssa import SSAFD
+
+    g, c, f, meta = build_case(args.size)
+    M = args.size
+    N = M * M
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)      # a real stream: the solver and the events share it
+    torch.cuda.set_stream(stream)
+    names = ("thickness", "surface", "bed", "mask", "tauc", "melange")
+    dfields = {k: torch.tensor(f[k], dtype=torch.float64, device=dev) for k in names}
+    zero = torch.zeros((M, M, 2), dtype=torch.float64, device=dev)
+    out = torch.empty((M, M, 2), dtype=torch.float64, device=dev)
+    s = SSAFD(g, c, device=local)
+    s.set_stream(stream.cuda_stream)
+    s.set_inputs(**dfields)
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)   # > L2 (126 MB)
+
+    def step():
+        s.set_initial_guess(zero)
+        s.solve(out=out)
+
+    for _ in range(args.warmup):
+        step()
+    st = s.stats()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    launches = 0
+    picard = []
+    ksp = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        st = s.stats()
+        launches += st["kernel_launches"]
+        picard.append(st["picard_iterations"])
+        ksp.append(st["ksp_iterations"])
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t.item()) / args.steps
+    value = ms_per_step / world
+
+    # end to end through the C-ABI with pinned host buffers: H2D inputs, solve, D2H velocity
+    hfields = {k: torch.tensor(f[k], dtype=torch.float64).pin_memory() for k in names}
+    hzero = torch.zeros((M, M, 2), dtype=torch.float64).pin_memory()
+    hout = torch.empty((M, M, 2), dtype=torch.float64).pin_memory()
+    h2d = sum(v.numel() * 8 for v in hfields.values()) + hzero.numel() * 8
+    d2h = hout.numel() * 8
+    e2e_ms = 0.0
+    for _ in range(max(1, min(args.steps, 2))):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.set_inputs(**{k: v.numpy() for k, v in hfields.items()})
+        s.set_initial_guess(hzero.numpy())
+        s.solve(out=hout.numpy())
+        torch.cuda.synchronize()
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+    e2e_ms /= max(1, min(args.steps, 2))
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = float(te.item()) / world
+
+    # roofline of the dominant kernel: the matrix-free SSAFD apply at the final nu*H
+    x = torch.randn((M, M, 2), dtype=torch.float64, device=dev) * 1e-5
+    y = torch.empty_like(x)
+    for _ in range(5):
+        s.apply(x, y)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    flush.fill_(1.0)
+    ev[0].record(stream)
+    for _ in range(args.apply_launches):
+        s.apply(x, y)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    apply_ms = ev[0].elapsed_time(ev[1]) / args.apply_launches
+    # algorithmic bytes per cell: x 16, nu*H 16, beta 8, flags 4, y 16 (neighbours counted once)
+    apply_bytes = 60 * N
+    achieved = apply_bytes / (apply_ms * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"SSAFD solve, synthetic ice sheet {M}x{M} at {4000 / (M - 1):.0f} km, plastic till, "
+                               "Picard 1e-4, KSP 1e-8 (plain FP64: BiCGStab + block Jacobi)",
+                   "grid": [M, M], "seed": 0, "precision": "fp64", "l2": "flushed (256 MB write) between steps",
+                   "parallelism": f"replicas x{world}"},
+        "solver": {"picard_iterations": picard, "ksp_iterations": ksp, "converged": st["converged"],
+                   "strategy": st["strategy"], "final_linear_residual": st["final_linear_residual"]},
+        "roofline": {"bound": "hbm", "kernel": "k_apply (SSAFD stencil, matrix-free)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind, "bytes_per_launch": apply_bytes, "launch_ms": apply_ms},
+        "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        cms, done, dt = cpu_reference_sample(M, args.cpu_picard, picard[-1], nthreads)
+        line["cpu_baseline"] = {"value": cms, "unit": "ms", "cores": nthreads, "kind": "port",
+                                "sample": f"first {done} Picard iterations of the same solve ({dt:.1f} s), "
+                                          f"scaled to the GPU run's {picard[-1]} Picard iterations"}
+    if rank == 0:
+        print(json.dumps(line))
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

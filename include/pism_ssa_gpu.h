@@ -151,6 +151,7 @@ typedef struct pism_gpu_ssa_stats {
   double final_linear_residual;    /* ||b - A x|| / ||b|| of the last linear solve    */
   double solve_ms;                 /* wall time of pism_gpu_ssa_solve                 */
   double kernel_ms;                /* device time (CUDA events) of the solve          */
+  long long kernel_launches;       /* kernels launched by the solve                   */
 } pism_gpu_ssa_stats;
 
 typedef struct pism_gpu_ssa pism_gpu_ssa;   /* opaque handle: owns device scratch */

@@ -160,7 +160,7 @@ class CStats(C.Structure):
     _fields_ = [("status", _I), ("converged", _I), ("strategy", _I), ("picard_iterations", _I),
                 ("ksp_iterations", _I), ("ksp_failures", _I), ("refinement_steps", _I),
                 ("nuH_norm", _D), ("nuH_norm_change", _D), ("final_linear_residual", _D),
-                ("solve_ms", _D), ("kernel_ms", _D)]
+                ("solve_ms", _D), ("kernel_ms", _D), ("kernel_launches", C.c_longlong)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

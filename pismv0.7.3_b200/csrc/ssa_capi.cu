@@ -1,0 +1,612 @@
+// ssa_capi.cu — the C-ABI of the B200 SSAFD solver (include/pism_ssa_gpu.h) and its
+// host-side driver: the Picard loop and the strategy ladder of SSAFD::solve
+// (src/base/stressbalance/ssa/SSAFD.cc:869-1155), driving the kernels of
+// ssa_kernels.cu on one CUDA stream.  Host <-> device traffic per Picard
+// iteration is one small read-back (the Krylov state and the two nu*H norms).
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ssa_internal.h"
+
+using namespace pism_gpu;
+
+struct pism_gpu_ssa {
+  pism_gpu_grid grid{};
+  std::vector<double> z_host;
+  pism_gpu_ssa_config cfg{};
+  int device = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  GridDev g{};
+  int N = 0;
+  Launch L{};
+  // inputs
+  double *H = nullptr, *srf = nullptr, *bed = nullptr, *tauc = nullptr, *melange = nullptr, *gl_mask = nullptr;
+  double *enthalpy = nullptr, *fracture = nullptr, *z_dev = nullptr, *stage = nullptr, *stage2 = nullptr;
+  int8_t *mask = nullptr;
+  uint8_t *bc = nullptr;
+  double2 *bcv = nullptr;
+  // derived / state
+  double2 *taud = nullptr, *rhs = nullptr, *hardness = nullptr, *nuH = nullptr, *vel = nullptr, *vel_old = nullptr;
+  double *beta = nullptr, *bfrict = nullptr;
+  uint32_t *flags = nullptr;
+  Krylov K{};
+  double *partials = nullptr;
+  unsigned *ticket = nullptr;
+  double *norm_dev = nullptr;
+  int *zd_dev = nullptr;
+  // pinned host mirrors
+  KState *st_host = nullptr;
+  double *norm_host = nullptr;
+  int *zd_host = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool inputs_set = false, have_melange = false, have_gl = false, have_enthalpy = false, have_hardness = false,
+       have_fracture = false, prepared = false;
+  int default_pc_failure_count = 0;   // SSAFD.cc:252-253 (m_default_pc_failure_*)
+  int use_fallback = 0;
+  int last_ksp_its = 0;
+  std::string err;
+  pism_gpu_ssa_stats stats{};
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int fail(pism_gpu_ssa *h, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  return code;
+}
+
+#define CK(h, call)                                                                                  \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return fail((h), e_ == cudaErrorMemoryAllocation ? PISM_GPU_SSA_ENOMEM : PISM_GPU_SSA_ECUDA,   \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);       \
+  } while (0)
+
+#define RET(x)                      \
+  do {                              \
+    int r_ = (x);                   \
+    if (r_ != PISM_GPU_SSA_OK) return r_; \
+  } while (0)
+
+template <class T>
+int dalloc(pism_gpu_ssa *h, T **p, size_t count) {
+  CK(h, cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T)));
+  return PISM_GPU_SSA_OK;
+}
+
+Fields fields_of(pism_gpu_ssa *h) {
+  Fields f;
+  f.H = h->H; f.srf = h->srf; f.bed = h->bed; f.tauc = h->tauc;
+  f.melange = h->have_melange ? h->melange : nullptr;
+  f.gl_mask = h->gl_mask;
+  f.enthalpy = h->have_enthalpy ? h->enthalpy : nullptr;
+  f.fracture = h->have_fracture ? h->fracture : nullptr;
+  f.bcv = h->bcv; f.mask = h->mask; f.bc = h->bc;
+  f.taud = h->taud; f.rhs = h->rhs; f.hardness = h->hardness; f.nuH = h->nuH; f.vel = h->vel;
+  f.beta = h->beta; f.flags = h->flags;
+  return f;
+}
+
+int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
+  if (!c) return fail(h, PISM_GPU_SSA_EINVAL, "config is NULL");
+  if (c->flow_law < PISM_FLOW_LAW_ISOTHERMAL_GLEN || c->flow_law > PISM_FLOW_LAW_HOOKE)
+    return fail(h, PISM_GPU_SSA_EINVAL, "unknown flow law %d", c->flow_law);
+  if (c->ksp_type != PISM_KSP_BICGSTAB && c->ksp_type != PISM_KSP_GMRES)
+    return fail(h, PISM_GPU_SSA_EINVAL, "unknown ksp_type %d", c->ksp_type);
+  if (c->pc_type != PISM_PC_BLOCK_JACOBI && c->pc_type != PISM_PC_MULTIGRID)
+    return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
+  if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
+    return fail(h, PISM_GPU_SSA_EINVAL, "ksp_rtol, ksp_max_it and max_iterations_ssafd must be positive");
+  if (!(c->ssa_Glen_exponent > 0.0) || !(c->min_thickness_strength_extension_ssa > 0.0))
+    return fail(h, PISM_GPU_SSA_EINVAL, "Glen exponent and strength-extension thickness must be positive");
+  return PISM_GPU_SSA_OK;
+}
+
+// ---- one linear solve: BiCGStab on the device, host reads the state per chunk ----
+int linear_solve(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
+  const GridDev &g = h->g;
+  Fields f = fields_of(h);
+  KState init{};
+  init.rtol = h->cfg.ksp_rtol;
+  init.maxit = h->use_fallback ? 4 * h->cfg.ksp_max_it : h->cfg.ksp_max_it;
+  *h->st_host = init;
+  CK(h, cudaMemcpyAsync(h->K.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
+  launch_bicg_init(h->L, g, f, h->K, h->rhs, x);
+  int launched = 0;
+  int chunk = std::max(8, (int)(0.8 * h->last_ksp_its));
+  while (true) {
+    for (int q = 0; q < chunk; ++q) launch_bicg_iteration(h->L, g, f, h->K, x);
+    launched += chunk;
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(h->st_host, h->K.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (h->st_host->done) break;
+    chunk = std::max(4, std::min(64, launched / 8));
+  }
+  h->last_ksp_its = h->st_host->iter;
+  *its_out = h->st_host->iter;
+  *status_out = h->st_host->status;
+  h->stats.final_linear_residual =
+      h->st_host->bnorm2 > 0 ? sqrt(h->st_host->rnorm2 / h->st_host->bnorm2) : sqrt(h->st_host->rnorm2);
+  return PISM_GPU_SSA_OK;
+}
+
+// SSAFD::picard_manager, SSAFD.cc:962-1119
+int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
+  const pism_gpu_ssa_config &c = h->cfg;
+  Fields f = fields_of(h);
+  launch_nuH(h->L, h->g, c, f, reg, 1.0, false, h->norm_dev);
+  for (int k = 0; k < c.max_iterations_ssafd; ++k) {
+    *h->zd_host = INT_MAX;
+    CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    launch_diag_setup(h->L, h->g, f, h->K.dinv, h->zd_dev);
+    int its = 0, status = 0;
+    RET(linear_solve(h, h->vel, &its, &status));
+    CK(h, cudaMemcpyAsync(h->zd_host, h->zd_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->stats.ksp_iterations += its;
+    if (*h->zd_host != INT_MAX) {
+      const int cidx = *h->zd_host;
+      return fail(h, PISM_GPU_SSA_EZERODIAG,
+                  "SSAFD system: zero diagonal entry at a regular (not Dirichlet B.C.) location: i = %d, j = %d",
+                  cidx / h->g.My, cidx % h->g.My);
+    }
+    if (status != KSP_OK)
+      return fail(h, PISM_GPU_SSA_EKSP, "SSAFD KSP (linear solver) failed: reason %d after %d iterations",
+                  status, its);
+    launch_nuH(h->L, h->g, c, f, reg, underrelax, true, h->norm_dev);
+    CK(h, cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const double norm = h->norm_host[0], change = h->norm_host[1];
+    h->stats.picard_iterations = k + 1;
+    h->stats.nuH_norm = norm;
+    h->stats.nuH_norm_change = change;
+    if (c.verbosity > 2)
+      fprintf(stderr, "  %2d: S:%d,%d: |nu|_2, |Delta nu|_2/|nu|_2 = %10.3e %10.3e\n", k, its, status, norm,
+              change / norm);
+    if (!std::isfinite(norm) || !std::isfinite(change))
+      return fail(h, PISM_GPU_SSA_ENAN, "non-finite nu*H norm at Picard iteration %d", k);
+    if (norm == 0 || change / norm < c.ssafd_relative_convergence) return PISM_GPU_SSA_OK;
+  }
+  return fail(h, PISM_GPU_SSA_EPICARD,
+              "SSAFD Picard iterations failed: effective viscosity not converged after %d iterations with "
+              "nuH_regularization=%8.2e.",
+              c.max_iterations_ssafd, reg);
+}
+
+// SSAFD::picard_iteration, SSAFD.cc:926-959: a KSP failure switches to the fallback
+// solver (the reference's ASM + LU) and restarts from the previous velocity.
+int picard_iteration(pism_gpu_ssa *h, double reg, double underrelax) {
+  if (h->default_pc_failure_count < 5) {
+    h->use_fallback = 0;
+    int rc = picard_manager(h, reg, underrelax);
+    if (rc != PISM_GPU_SSA_EKSP) return rc;
+    h->default_pc_failure_count += 1;
+    h->stats.ksp_failures += 1;
+    if (h->cfg.verbosity > 0) fprintf(stderr, "  re-trying using the fallback linear solver...\n");
+    h->use_fallback = 1;
+    CK(h, cudaMemcpyAsync(h->vel, h->vel_old, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
+    return picard_manager(h, reg, underrelax);
+  }
+  h->use_fallback = 1;
+  return picard_manager(h, reg, underrelax);
+}
+
+// SSAFD::picard_strategy_regularization, SSAFD.cc:1122-1155
+int picard_strategy_regularization(pism_gpu_ssa *h) {
+  double reg = h->cfg.epsilon_ssa;
+  if (reg <= 0.0)
+    return fail(h, PISM_GPU_SSA_EPICARD,
+                "SSAFD Picard iterations failed: will not attempt over-regularization of nuH because "
+                "nuH_regularization == 0.0.");
+  for (int k = 0; k < 5; ++k) {
+    CK(h, cudaMemcpyAsync(h->vel, h->vel_old, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->cfg.verbosity > 0) fprintf(stderr, "  re-trying with nuH_regularization multiplied by %8.2f...\n", 4.0);
+    reg *= 4.0;
+    int rc = picard_iteration(h, reg, 1.0);
+    if (rc == PISM_GPU_SSA_OK) return rc;
+    if (rc != PISM_GPU_SSA_EPICARD) return rc;
+  }
+  return fail(h, PISM_GPU_SSA_EPICARD,
+              "SSAFD Picard iterations failed: exceeded the max. number of nuH over-regularization attempts");
+}
+
+int prepare(pism_gpu_ssa *h) {
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  Fields f = fields_of(h);
+  launch_prepare(h->L, h->g, h->cfg, h->grid.periodicity, f);
+  if (!h->have_hardness) {
+    if (h->cfg.flow_law != PISM_FLOW_LAW_ISOTHERMAL_GLEN && !h->have_enthalpy)
+      return fail(h, PISM_GPU_SSA_EINVAL, "the flow law needs enthalpy (or a precomputed hardness)");
+    launch_hardness(h->L, h->g, h->cfg, f, (int)h->z_host.size(), h->z_dev);
+  }
+  CK(h, cudaGetLastError());
+  h->prepared = true;
+  return PISM_GPU_SSA_OK;
+}
+
+int copy_in(pism_gpu_ssa *h, void *dst, const void *src, size_t bytes, int where) {
+  CK(h, cudaMemcpyAsync(dst, src, bytes, where == PISM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int copy_out(pism_gpu_ssa *h, void *dst, const void *src, size_t bytes, int where) {
+  CK(h, cudaMemcpyAsync(dst, src, bytes, where == PISM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *c) {
+  if (!c) return PISM_GPU_SSA_EINVAL;
+  const double secpera = 31556925.9747;   // UDUNITS-2 year
+  memset(c, 0, sizeof(*c));
+  // src/pism_config.cdl
+  c->ice_density = 910.0;
+  c->sea_water_density = 1028.0;
+  c->standard_gravity = 9.81;
+  c->sea_level = 0.0;
+  c->epsilon_ssa = 1.0e13;
+  c->ssafd_relative_convergence = 1.0e-4;
+  c->max_iterations_ssafd = 300;
+  c->ssafd_nuH_iter_failure_underrelaxation = 0.8;
+  c->min_thickness_strength_extension_ssa = 50.0;
+  c->constant_nu_strength_extension_ssa = 9.48680701906572e14;
+  c->plastic_regularization = 0.01 / secpera;
+  c->do_pseudo_plastic_till = 0;
+  c->pseudo_plastic_q = 0.25;
+  c->pseudo_plastic_uthreshold = 100.0 / secpera;
+  c->sliding_scale_factor_reduces_tauc = -1.0;
+  c->beta_ice_free_bedrock = 1.8e9;
+  c->nu_bedrock = 5.0e15;
+  c->flow_law = PISM_FLOW_LAW_GPBLD;
+  c->ssa_Glen_exponent = 3.0;
+  c->ssa_enhancement_factor = 1.0;
+  c->ice_softness = 3.1689e-24;
+  c->Schoof_regularizing_length = 1000.0e3;
+  c->Schoof_regularizing_velocity = 1.0 / secpera;
+  c->Paterson_Budd_A_cold = 3.61e-13;
+  c->Paterson_Budd_A_warm = 1.73e3;
+  c->Paterson_Budd_Q_cold = 6.0e4;
+  c->Paterson_Budd_Q_warm = 13.9e4;
+  c->Paterson_Budd_critical_temperature = 263.15;
+  c->ideal_gas_constant = 8.31441;
+  c->gpbld_water_frac_coeff = 181.25;
+  c->gpbld_water_frac_observed_limit = 0.01;
+  c->Hooke_A = 4.42165e-9;
+  c->Hooke_Q = 7.88e4;
+  c->Hooke_C = 0.16612;
+  c->Hooke_k = 1.17;
+  c->Hooke_Tr = 273.39;
+  c->beta_CC = 7.9e-8;
+  c->ice_specific_heat_capacity = 2009.0;
+  c->water_latent_heat_fusion = 3.34e5;
+  c->surface_pressure = 0.0;
+  c->water_melting_point_temperature = 273.15;
+  c->enthalpy_converter_reference_temperature = 223.15;
+  c->fracture_density_softening_lower_limit = 1.0;
+  c->brutal_sliding_scale = 1.0;
+  // PETSc KSP defaults
+  c->ksp_type = PISM_KSP_BICGSTAB;
+  c->pc_type = PISM_PC_BLOCK_JACOBI;
+  c->ksp_rtol = 1.0e-5;
+  c->ksp_max_it = 10000;
+  c->gmres_restart = 30;
+  c->precision = PISM_PRECISION_FP64;
+  c->mixed_inner_rtol = 1.0e-3;
+  c->verbosity = 0;
+  return PISM_GPU_SSA_OK;
+}
+
+const char *pism_gpu_ssa_last_error(const pism_gpu_ssa *h) { return h ? h->err.c_str() : "null handle"; }
+
+int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cfg, int device, pism_gpu_ssa **out) {
+  if (!grid || !cfg || !out) return PISM_GPU_SSA_EINVAL;
+  *out = nullptr;
+  if (grid->Mx < 3 || grid->My < 3 || !(grid->dx > 0) || !(grid->dy > 0) || grid->Mz < 0 ||
+      (grid->Mz > 0 && !grid->z) || (long long)grid->Mx * grid->My > (1LL << 30))
+    return PISM_GPU_SSA_EINVAL;
+  pism_gpu_ssa *h = new pism_gpu_ssa();
+  if (check_config(h, cfg) != PISM_GPU_SSA_OK) {
+    delete h;
+    return PISM_GPU_SSA_EINVAL;
+  }
+  h->grid = *grid;
+  if (grid->Mz > 0) h->z_host.assign(grid->z, grid->z + grid->Mz);
+  h->grid.z = nullptr;
+  h->cfg = *cfg;
+  h->device = device;
+  h->g.Mx = grid->Mx;
+  h->g.My = grid->My;
+  h->g.dx = grid->dx;
+  h->g.dy = grid->dy;
+  h->N = grid->Mx * grid->My;
+  DeviceGuard dg(device);
+  auto bail = [&](int rc) {
+    pism_gpu_ssa_destroy(h);
+    return rc;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(PISM_GPU_SSA_ECUDA);
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return bail(PISM_GPU_SSA_ECUDA);
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PISM_GPU_SSA_ECUDA);
+  h->stream = h->own_stream;
+  const size_t N = h->N;
+  int rc = PISM_GPU_SSA_OK;
+#define AL(p, n) \
+  if ((rc = dalloc(h, &p, n)) != PISM_GPU_SSA_OK) return bail(rc)
+  AL(h->H, N); AL(h->srf, N); AL(h->bed, N); AL(h->tauc, N); AL(h->melange, N); AL(h->gl_mask, N);
+  AL(h->fracture, N); AL(h->stage, N); AL(h->stage2, N);
+  AL(h->enthalpy, N * std::max(1, grid->Mz)); AL(h->z_dev, std::max(1, grid->Mz));
+  AL(h->mask, N); AL(h->bc, N); AL(h->bcv, N);
+  AL(h->taud, N); AL(h->rhs, N); AL(h->hardness, N); AL(h->nuH, N); AL(h->vel, N); AL(h->vel_old, N);
+  AL(h->beta, N); AL(h->bfrict, N); AL(h->flags, N);
+  AL(h->K.r, N); AL(h->K.rhat, N); AL(h->K.p, N); AL(h->K.v, N); AL(h->K.s, N); AL(h->K.t, N);
+  AL(h->K.phat, N); AL(h->K.shat, N); AL(h->K.dinv, N); AL(h->K.st, 1);
+  h->L.max_blocks = sms * 8;
+  AL(h->partials, (size_t)h->L.max_blocks * 8); AL(h->ticket, 1); AL(h->norm_dev, 2); AL(h->zd_dev, 1);
+#undef AL
+  if (cudaMallocHost((void **)&h->st_host, sizeof(KState)) != cudaSuccess ||
+      cudaMallocHost((void **)&h->norm_host, 2 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void **)&h->zd_host, sizeof(int)) != cudaSuccess)
+    return bail(PISM_GPU_SSA_ENOMEM);
+  if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
+    return bail(PISM_GPU_SSA_ECUDA);
+  if (cudaMemsetAsync(h->ticket, 0, sizeof(unsigned), h->stream) != cudaSuccess ||
+      cudaMemsetAsync(h->vel, 0, sizeof(double2) * N, h->stream) != cudaSuccess ||     // SSA.cc:178
+      cudaMemsetAsync(h->nuH, 0, sizeof(double2) * N, h->stream) != cudaSuccess)
+    return bail(PISM_GPU_SSA_ECUDA);
+  if (grid->Mz > 0 &&
+      cudaMemcpyAsync(h->z_dev, h->z_host.data(), sizeof(double) * grid->Mz, cudaMemcpyHostToDevice, h->stream) !=
+          cudaSuccess)
+    return bail(PISM_GPU_SSA_ECUDA);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(PISM_GPU_SSA_ECUDA);
+  h->L.stream = h->stream;
+  h->L.partials = h->partials;
+  h->L.ticket = h->ticket;
+  h->L.count = &h->stats.kernel_launches;
+  *out = h;
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
+  if (!h) return PISM_GPU_SSA_OK;
+  DeviceGuard dg(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  void *dev[] = {h->H, h->srf, h->bed, h->tauc, h->melange, h->gl_mask, h->fracture, h->stage, h->stage2,
+                 h->enthalpy, h->z_dev, h->mask, h->bc, h->bcv, h->taud, h->rhs, h->hardness, h->nuH, h->vel,
+                 h->vel_old, h->beta, h->bfrict, h->flags, h->K.r, h->K.rhat, h->K.p, h->K.v, h->K.s, h->K.t,
+                 h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev};
+  for (void *p : dev)
+    if (p) cudaFree(p);
+  if (h->st_host) cudaFreeHost(h->st_host);
+  if (h->norm_host) cudaFreeHost(h->norm_host);
+  if (h->zd_host) cudaFreeHost(h->zd_host);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_set_stream(pism_gpu_ssa *h, void *s) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  h->L.stream = h->stream;
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_set_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *cfg) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  RET(check_config(h, cfg));
+  h->cfg = *cfg;
+  h->prepared = false;
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_set_inputs(pism_gpu_ssa *h, const pism_gpu_ssa_inputs *in) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  if (!in || !in->thickness || !in->surface || !in->bed || !in->mask || !in->tauc)
+    return fail(h, PISM_GPU_SSA_EINVAL, "thickness, surface, bed, mask and tauc are required");
+  if ((in->bc_mask == nullptr) != (in->bc_values == nullptr))
+    return fail(h, PISM_GPU_SSA_EINVAL, "bc_mask and bc_values must be given together");
+  if (h->cfg.sub_groundingline && !in->gl_mask)
+    return fail(h, PISM_GPU_SSA_EINVAL, "sub_groundingline needs gl_mask");
+  if (h->cfg.do_fracture_density && !in->fracture_density)
+    return fail(h, PISM_GPU_SSA_EINVAL, "do_fracture_density needs fracture_density");
+  if (in->enthalpy && h->z_host.empty())
+    return fail(h, PISM_GPU_SSA_EINVAL, "enthalpy given but the grid has no vertical levels (Mz = 0)");
+  DeviceGuard dg(h->device);
+  const size_t N = h->N, B = N * sizeof(double);
+  const int w = in->where;
+  RET(copy_in(h, h->H, in->thickness, B, w));
+  RET(copy_in(h, h->srf, in->surface, B, w));
+  RET(copy_in(h, h->bed, in->bed, B, w));
+  RET(copy_in(h, h->tauc, in->tauc, B, w));
+  RET(copy_in(h, h->stage, in->mask, B, w));
+  if (in->bc_mask) {
+    RET(copy_in(h, h->stage2, in->bc_mask, B, w));
+    RET(copy_in(h, h->bcv, in->bc_values, 2 * B, w));
+  }
+  h->have_melange = in->melange != nullptr;
+  if (in->melange) RET(copy_in(h, h->melange, in->melange, B, w));
+  h->have_gl = in->gl_mask != nullptr;
+  if (in->gl_mask) RET(copy_in(h, h->gl_mask, in->gl_mask, B, w));
+  h->have_enthalpy = in->enthalpy != nullptr;
+  if (in->enthalpy) RET(copy_in(h, h->enthalpy, in->enthalpy, B * h->z_host.size(), w));
+  h->have_hardness = in->hardness_stag != nullptr;
+  if (in->hardness_stag) RET(copy_in(h, h->hardness, in->hardness_stag, 2 * B, w));
+  h->have_fracture = in->fracture_density != nullptr;
+  if (in->fracture_density) RET(copy_in(h, h->fracture, in->fracture_density, B, w));
+  launch_convert_masks(h->L, h->N, h->stage, in->bc_mask ? h->stage2 : nullptr, h->mask, h->bc);
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->inputs_set = true;
+  h->prepared = false;
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_set_initial_guess(pism_gpu_ssa *h, const double *velocity, int where) {
+  if (!h || !velocity) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  RET(copy_in(h, h->vel, velocity, sizeof(double2) * h->N, where));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_solve(pism_gpu_ssa *h, double *velocity_out, int where, pism_gpu_ssa_stats *stats) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  auto t0 = std::chrono::steady_clock::now();
+  h->stats = pism_gpu_ssa_stats{};
+  h->err.clear();
+  h->L.count = &h->stats.kernel_launches;
+  CK(h, cudaEventRecord(h->ev0, h->stream));
+  // SSAFD::solve, SSAFD.cc:869-924
+  CK(h, cudaMemcpyAsync(h->vel_old, h->vel, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
+  int rc = prepare(h);
+  if (rc == PISM_GPU_SSA_OK) {
+    for (int k = 0; k < 3; ++k) {
+      h->stats.strategy = k;
+      if (k == 0)
+        rc = picard_iteration(h, h->cfg.epsilon_ssa, 1.0);
+      else if (k == 1) {
+        if (h->cfg.verbosity > 0)
+          fprintf(stderr, "  re-trying with effective viscosity under-relaxation (parameter = %.2f) ...\n",
+                  h->cfg.ssafd_nuH_iter_failure_underrelaxation);
+        rc = picard_iteration(h, h->cfg.epsilon_ssa, h->cfg.ssafd_nuH_iter_failure_underrelaxation);
+      } else {
+        rc = picard_strategy_regularization(h);
+      }
+      if (rc == PISM_GPU_SSA_OK) {
+        h->stats.converged = 1;
+        break;
+      }
+      if (rc != PISM_GPU_SSA_EPICARD) break;
+    }
+    // the reference's strategy loop ends silently when every strategy failed
+    // (SSAFD.cc:882-911: the k == 3 branch is unreachable); stats.converged = 0 says so
+    if (rc == PISM_GPU_SSA_EPICARD) rc = PISM_GPU_SSA_OK;
+  }
+  if (rc == PISM_GPU_SSA_OK) {
+    if (h->cfg.brutal_sliding) launch_scale(h->L, 2 * h->N, h->cfg.brutal_sliding_scale, (double *)h->vel);
+    Fields f = fields_of(h);
+    launch_bfrict(h->L, h->N, h->cfg, f, h->bfrict);   // SSA::update, SSA.cc:193-194
+    CK(h, cudaGetLastError());
+  }
+  CK(h, cudaEventRecord(h->ev1, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->stats.kernel_ms = ms;
+  h->stats.status = rc;
+  h->stats.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (stats) *stats = h->stats;
+  if (rc != PISM_GPU_SSA_OK) return rc;
+  if (velocity_out) RET(copy_out(h, velocity_out, h->vel, sizeof(double2) * h->N, where));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_get_field(pism_gpu_ssa *h, int field, double *out, int where) {
+  if (!h || !out) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  const size_t N = h->N;
+  switch (field) {
+    case PISM_FIELD_VELOCITY: return copy_out(h, out, h->vel, 16 * N, where);
+    case PISM_FIELD_TAUD: return copy_out(h, out, h->taud, 16 * N, where);
+    case PISM_FIELD_RHS: return copy_out(h, out, h->rhs, 16 * N, where);
+    case PISM_FIELD_HARDNESS: return copy_out(h, out, h->hardness, 16 * N, where);
+    case PISM_FIELD_NUH: return copy_out(h, out, h->nuH, 16 * N, where);
+    case PISM_FIELD_BETA: return copy_out(h, out, h->beta, 8 * N, where);
+    case PISM_FIELD_BFRICT: return copy_out(h, out, h->bfrict, 8 * N, where);
+    default: return fail(h, PISM_GPU_SSA_EINVAL, "unknown field %d", field);
+  }
+}
+
+int pism_gpu_ssa_assemble_rhs(pism_gpu_ssa *h) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  launch_prepare(h->L, h->g, h->cfg, h->grid.periodicity, fields_of(h));
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_compute_hardness(pism_gpu_ssa *h) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  if (h->have_hardness) return PISM_GPU_SSA_OK;
+  if (h->cfg.flow_law != PISM_FLOW_LAW_ISOTHERMAL_GLEN && !h->have_enthalpy)
+    return fail(h, PISM_GPU_SSA_EINVAL, "the flow law needs enthalpy (or a precomputed hardness)");
+  launch_hardness(h->L, h->g, h->cfg, fields_of(h), (int)h->z_host.size(), h->z_dev);
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_compute_nuH(pism_gpu_ssa *h, double reg) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  launch_nuH(h->L, h->g, h->cfg, fields_of(h), reg, 1.0, false, h->norm_dev);
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_apply(pism_gpu_ssa *h, const double *x_dev, double *y_dev) {
+  if (!h || !x_dev || !y_dev) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  launch_apply(h->L, h->g, fields_of(h), (const double2 *)x_dev, (double2 *)y_dev);
+  CK(h, cudaGetLastError());
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, double *rel_residual) {
+  if (!h || !x_dev) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  *h->zd_host = INT_MAX;
+  CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  launch_diag_setup(h->L, h->g, fields_of(h), h->K.dinv, h->zd_dev);
+  int its = 0, status = 0;
+  RET(linear_solve(h, (double2 *)x_dev, &its, &status));
+  if (iterations) *iterations = its;
+  if (rel_residual) *rel_residual = h->stats.final_linear_residual;
+  if (status != KSP_OK)
+    return fail(h, PISM_GPU_SSA_EKSP, "SSAFD KSP (linear solver) failed: reason %d after %d iterations", status, its);
+  return PISM_GPU_SSA_OK;
+}
+
+}  // extern "C"

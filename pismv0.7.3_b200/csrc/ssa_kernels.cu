@@ -1,0 +1,897 @@
+// ssa_kernels.cu — sm_100a kernels of the B200 SSAFD solver.
+//
+// Every kernel restates one piece of the reference's SSAFD arithmetic (file:line
+// in each comment).  All are HBM-bound stencil / vector kernels: cells are mapped
+// to 32 (j, contiguous) x 8 (i) tiles so that a warp reads 32 consecutive double2
+// values (512 B) and the i +- 1 rows of the stencil are re-read from L1 by the
+// neighbouring warps of the same block; blocks loop over tiles (grid = a multiple
+// of the SM count).  Reductions are fused into the producing kernel: each block
+// writes its partial sums, and the last block to finish (atomic ticket) adds them
+// in block order — deterministic — and updates the solver scalars on the device,
+// so no kernel boundary or host round trip is spent on a dot product.
+#include <cstdio>
+
+#include "ssa_internal.h"
+
+namespace pism_gpu {
+
+constexpr int TJ = 32;  // tile width along j (contiguous)
+constexpr int TI = 8;   // tile height along i
+constexpr int NT = TJ * TI;
+
+struct TileMap {
+  int tiles_j, tiles;
+  __device__ __forceinline__ bool cell_of(const GridDev &g, int t, int &i, int &j) const {
+    int ti = t / tiles_j, tj = t - ti * tiles_j;
+    j = tj * TJ + (threadIdx.x & (TJ - 1));
+    i = ti * TI + (threadIdx.x >> 5);
+    return i < g.Mx && j < g.My;
+  }
+};
+
+static TileMap make_tiles(const GridDev &g) {
+  TileMap m;
+  m.tiles_j = (g.My + TJ - 1) / TJ;
+  m.tiles = m.tiles_j * ((g.Mx + TI - 1) / TI);
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// block reduction with last-block finalisation
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Reduce NV values over the grid.  Returns true in thread 0 of the last block,
+// with the grid totals in tot[].
+template <int NV>
+__device__ __forceinline__ bool grid_reduce(double (&val)[NV], double *partials, unsigned *ticket,
+                                            double (&tot)[NV]) {
+  __shared__ double sh[NV][NT / 32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double s = warp_sum(val[v]);
+    if (lane == 0) sh[v][warp] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double s = 0.0;
+      for (int w = 0; w < NT / 32; ++w) s += sh[v][w];
+      partials[blockIdx.x * NV + v] = s;
+    }
+    __threadfence();
+    unsigned t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  // the last block adds all partials in block order (deterministic)
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) s += __ldcg(&partials[b * NV + v]);
+    s = warp_sum(s);
+    if (lane == 0) sh[v][warp] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return false;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double s = 0.0;
+    for (int w = 0; w < NT / 32; ++w) s += sh[v][w];
+    tot[v] = s;
+  }
+  *ticket = 0u;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// input conversion: masks stored as doubles -> integers (IceModelVec2Int::as_int,
+// IceModelVec_inline.hh:94-100)
+// ---------------------------------------------------------------------------
+__global__ void k_convert_masks(int N, const double *mask, const double *bc_mask, int8_t *mask_i,
+                                uint8_t *bc_i) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    mask_i[k] = (int8_t)(int)floor(mask[k] + 0.5);
+    bc_i[k] = bc_mask ? (uint8_t)((int)floor(bc_mask[k] + 0.5) == 1) : (uint8_t)0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// driving stress + right-hand side + stencil flags (once per solve)
+//   SSA::compute_driving_stress  SSA.cc:211-353
+//   SSAFD::assemble_rhs          SSAFD.cc:282-417
+//   SSAFD::is_marginal           SSAFD.cc:1657-1682, CFBC weights SSAFD.cc:594-684
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_prepare(GridDev g, TileMap tm, pism_gpu_ssa_config c, int periodicity,
+                                                const double *__restrict__ H, const double *__restrict__ srf,
+                                                const double *__restrict__ bed, const int8_t *__restrict__ mask,
+                                                const uint8_t *__restrict__ bc, const double2 *__restrict__ bcv,
+                                                const double *__restrict__ melange, double2 *__restrict__ taud,
+                                                double2 *__restrict__ rhs, uint32_t *__restrict__ flags) {
+  const double dx = g.dx, dy = g.dy;
+  const bool cfbc = c.calving_front_stress_boundary_condition != 0;
+  const bool bb = c.ssa_dirichlet_bc != 0;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const int kE = nbr(g, i, j, 1, 0), kW = nbr(g, i, j, -1, 0), kN = nbr(g, i, j, 0, 1), kS = nbr(g, i, j, 0, -1);
+    const int M = mask[k], Me = mask[kE], Mw = mask[kW], Mn = mask[kN], Ms = mask[kS];
+    const int Mne = mask[nbr(g, i, j, 1, 1)], Mse = mask[nbr(g, i, j, 1, -1)], Mnw = mask[nbr(g, i, j, -1, 1)],
+              Msw = mask[nbr(g, i, j, -1, -1)];
+    const double Hc = H[k];
+
+    // ---- driving stress (SSA.cc:234-352) ----
+    const double n = c.ssa_Glen_exponent;
+    const double pressure = ec_pressure(c, Hc);
+    double2 td = make_double2(0.0, 0.0);
+    if (pressure > 0.0) {
+      double h_x = 0.0, h_y = 0.0;
+      if (m_grounded(M) && c.surface_gradient_eta) {
+        const double etapow = (2.0 * n + 2.0) / n, invpow = 1.0 / etapow, dinvpow = (-n - 2.0) / (2.0 * n + 2.0);
+        const double minThickEtaTransform = 5.0;
+        if (Hc > 0.0) {
+          const double myH = (Hc < minThickEtaTransform ? minThickEtaTransform : Hc);
+          const double eta = pow(myH, etapow), factor = invpow * pow(eta, dinvpow);
+          h_x = factor * (pow(H[kE], etapow) - pow(H[kW], etapow)) / (2 * dx);
+          h_y = factor * (pow(H[kN], etapow) - pow(H[kS], etapow)) / (2 * dy);
+        }
+        h_x += (bed[kE] - bed[kW]) / (2 * dx);
+        h_y += (bed[kN] - bed[kS]) / (2 * dy);
+      } else if (c.compute_surf_grad_inward_ssa) {
+        // IceModelVec2S::diff_x_p / diff_y_p (iceModelVec2.cc:501-530)
+        if ((periodicity & PISM_X_PERIODIC) || (i != 0 && i != g.Mx - 1))
+          h_x = (srf[kE] - srf[kW]) / (2 * dx);
+        else if (i == 0)
+          h_x = (srf[kE] - srf[k]) / dx;
+        else
+          h_x = (srf[k] - srf[kW]) / dx;
+        if ((periodicity & PISM_Y_PERIODIC) || (j != 0 && j != g.My - 1))
+          h_y = (srf[kN] - srf[kS]) / (2 * dy);
+        else if (j == 0)
+          h_y = (srf[kN] - srf[k]) / dy;
+        else
+          h_y = (srf[k] - srf[kS]) / dy;
+      } else {
+        double west = 1, east = 1, south = 1, north = 1;
+        if ((m_grounded(M) && m_floating_ice(Me)) || (m_floating_ice(M) && m_grounded(Me)) ||
+            (m_floating_ice(M) && m_ice_free_ocean(Me)))
+          east = 0;
+        if ((m_grounded(M) && m_floating_ice(Mw)) || (m_floating_ice(M) && m_grounded(Mw)) ||
+            (m_floating_ice(M) && m_ice_free_ocean(Mw)))
+          west = 0;
+        if ((m_grounded(M) && m_floating_ice(Mn)) || (m_floating_ice(M) && m_grounded(Mn)) ||
+            (m_floating_ice(M) && m_ice_free_ocean(Mn)))
+          north = 0;
+        if ((m_grounded(M) && m_floating_ice(Ms)) || (m_floating_ice(M) && m_grounded(Ms)) ||
+            (m_floating_ice(M) && m_ice_free_ocean(Ms)))
+          south = 0;
+        if (cfbc) {
+          if (m_icy(M) && m_ice_free(Me)) east = 0;
+          if (m_icy(M) && m_ice_free(Mw)) west = 0;
+          if (m_icy(M) && m_ice_free(Mn)) north = 0;
+          if (m_icy(M) && m_ice_free(Ms)) south = 0;
+        }
+        const double s0 = srf[k];
+        if (east + west > 0)
+          h_x = 1.0 / (west + east) * (west * ((s0 - srf[kW]) / dx) + east * ((srf[kE] - s0) / dx));
+        if (north + south > 0)
+          h_y = 1.0 / (south + north) * (south * ((s0 - srf[kS]) / dy) + north * ((srf[kN] - s0) / dy));
+      }
+      td.x = -pressure * h_x;
+      td.y = -pressure * h_y;
+    }
+    taud[k] = td;
+
+    // ---- flags and right-hand side ----
+    const bool is_bc = bc[k] != 0;
+    uint32_t f = F_WEIGHTS | ((uint32_t)(M & 7) << F_MASK_SHIFT);
+    double2 b = td;
+    if (cfbc) {
+      bool marginal;
+      if (bb)
+        marginal = m_icy(M) && (m_ice_free(Me) || m_ice_free(Mw) || m_ice_free(Mn) || m_ice_free(Ms) ||
+                                m_ice_free(Mne) || m_ice_free(Mse) || m_ice_free(Mnw) || m_ice_free(Msw));
+      else
+        marginal = m_icy(M) && (m_ice_free_ocean(Me) || m_ice_free_ocean(Mw) || m_ice_free_ocean(Mn) ||
+                                m_ice_free_ocean(Ms) || m_ice_free_ocean(Mne) || m_ice_free_ocean(Mse) ||
+                                m_ice_free_ocean(Mnw) || m_ice_free_ocean(Msw));
+      if (m_ice_free(M)) {
+        f |= F_DIAG_ONLY;
+        b = make_double2(0.0, 0.0);   // m_scaling * ice_free_default_velocity (= 0)
+      } else if (marginal) {
+        auto fr = [&](int Mq) { return bb ? m_ice_free_ocean(Mq) : m_ice_free(Mq); };
+        const bool e = fr(Me), w = fr(Mw), nn = fr(Mn), s = fr(Ms), ne = fr(Mne), se = fr(Mse), nw = fr(Mnw),
+                   sw = fr(Msw);
+        if (e) f &= ~F_aPP;
+        if (w) f &= ~F_aMM;
+        if (nn) f &= ~F_bPP;
+        if (s) f &= ~F_bMM;
+        if (nn || ne) f &= ~F_aPn;
+        if (e || ne) f &= ~F_bPe;
+        if (e || se) f &= ~F_bMe;
+        if (s || se) f &= ~F_aPs;
+        if (s || sw) f &= ~F_aMs;
+        if (w || sw) f &= ~F_bMw;
+        if (w || nw) f &= ~F_bPw;
+        if (nn || nw) f &= ~F_aMn;
+        // ocean pressure imbalance (SSAFD.cc:370-403)
+        const double H2 = Hc * Hc, bcell = bed[k], rho_g = c.ice_density * c.standard_gravity;
+        double op;
+        if (m_ocean(M))
+          op = 0.5 * rho_g * (1.0 - (c.ice_density / c.sea_water_density)) * H2;
+        else if (bcell >= c.sea_level)
+          op = 0.5 * rho_g * H2;
+        else
+          op = 0.5 * rho_g * (H2 - (c.sea_water_density / c.ice_density) * pow(c.sea_level - bcell, 2.0));
+        if (melange) op *= (1.0 - melange[k]);
+        const int aMM = w ? 0 : 1, aPP = e ? 0 : 1, bMM = s ? 0 : 1, bPP = nn ? 0 : 1;
+        b.x = td.x + (aMM - aPP) * op / dx;
+        b.y = td.y + (bMM - bPP) * op / dy;
+      }
+    }
+    if (is_bc) {
+      f |= F_DIAG_ONLY | F_BC;
+      const double2 v = bcv[k];
+      b = make_double2(1.0e9 * v.x, 1.0e9 * v.y);
+    }
+    rhs[k] = b;
+    flags[k] = f;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// staggered vertically averaged hardness (SSAFD::compute_hardav_staggered,
+// SSAFD.cc:1192-1246; FlowLaw::averaged_hardness, flowlaws.cc:141-185;
+// fracture_induced_softening, SSAFD.cc:1282-1310)
+// ---------------------------------------------------------------------------
+__device__ double averaged_hardness(const pism_gpu_ssa_config &c, double thickness, int kb, const double *z,
+                                    const double *E0, const double *E1) {
+  double B = 0;
+  if (kb > 0) {
+    double h0 = hardness_parameter(c, 0.5 * (E0[0] + E1[0]), ec_pressure(c, thickness));
+    for (int q = 1; q <= kb; ++q) {
+      double h1 = hardness_parameter(c, 0.5 * (E0[q] + E1[q]), ec_pressure(c, thickness - z[q]));
+      B += (z[q] - z[q - 1]) * (h0 + h1);
+      h0 = h1;
+    }
+  }
+  B *= 0.5;
+  double depth = thickness - z[kb];
+  B += depth * hardness_parameter(c, 0.5 * (E0[kb] + E1[kb]), ec_pressure(c, depth));
+  return thickness > 0 ? B / thickness : 0.0;
+}
+
+__global__ void k_hardness(GridDev g, int N, pism_gpu_ssa_config c, const double *__restrict__ H,
+                           const int8_t *__restrict__ mask, const double *__restrict__ enthalpy, int Mz,
+                           const double *__restrict__ z, const double *__restrict__ fracture,
+                           double2 *__restrict__ hardness) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const int i = k / g.My, j = k - i * g.My;
+    double out[2];
+    for (int o = 0; o < 2; ++o) {
+      const int oi = 1 - o, oj = o;
+      const int kn = nbr(g, i, j, oi, oj);
+      const bool ic = m_icy(mask[k]), in = m_icy(mask[kn]);
+      double Hf;
+      if (ic && in)
+        Hf = 0.5 * (H[k] + H[kn]);
+      else if (ic)
+        Hf = H[k];
+      else
+        Hf = H[kn];
+      if (Hf == 0) {
+        out[o] = -1e6;
+        continue;
+      }
+      if (c.flow_law == PISM_FLOW_LAW_ISOTHERMAL_GLEN) {
+        out[o] = pow(c.ice_softness, -1.0 / c.ssa_Glen_exponent);   // flowlaws.cc:239-240
+      } else {
+        // IceGrid::kBelowHeight: largest q in [0, Mz-2] with z[q] <= Hf (gsl_interp_accel_find)
+        int lo = 0, hi = Mz - 1;
+        while (hi > lo + 1) {
+          int mid = (lo + hi) / 2;
+          if (z[mid] > Hf) hi = mid; else lo = mid;
+        }
+        out[o] = averaged_hardness(c, Hf, lo, z, enthalpy + (size_t)k * Mz, enthalpy + (size_t)kn * Mz);
+      }
+    }
+    if (c.do_fracture_density && fracture) {
+      const double n = c.ssa_Glen_exponent, eps = c.fracture_density_softening_lower_limit;
+      for (int o = 0; o < 2; ++o) {
+        const int kn = nbr(g, i, j, 1 - o, o);
+        const double phi = 0.5 * (fracture[k] + fracture[kn]);
+        const double soft = pow((1.0 - (1.0 - eps) * phi), -n);
+        out[o] *= pow(soft, -1.0 / n);
+      }
+    }
+    hardness[k] = make_double2(out[0], out[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// nu*H on the staggered grid, beta, under-relaxation and the L1 norms — fused.
+//   SSAFD::compute_nuH_staggered       SSAFD.cc:1359-1421
+//   SSAFD::compute_nuH_staggered_cfbc  SSAFD.cc:1441-1582 (m_work recomputed on the fly)
+//   under-relaxation                   SSAFD.cc:1061-1064
+//   SSAFD::compute_nuH_norm            SSAFD.cc:1170-1189 (L1 over the ghosted local
+//                                      vectors: interior + one periodic ghost ring)
+//   basal drag of the next assembly    SSAFD.cc:744-759
+// ---------------------------------------------------------------------------
+struct NuHParams {
+  double reg, underrelax, Hmin, notional, schoof_reg, visc_power, enh_scaling, B_area;
+  int with_norm;
+};
+
+struct WorkVal {  // one entry of the reference's m_work: derivative pair + weight
+  double u, v, w;
+};
+
+template <bool CFBC>
+__global__ void __launch_bounds__(NT) k_nuH(GridDev g, TileMap tm, pism_gpu_ssa_config c, NuHParams p,
+                                            const double2 *__restrict__ vel, const double *__restrict__ H,
+                                            const double2 *__restrict__ hardness, const int8_t *__restrict__ mask,
+                                            const double *__restrict__ tauc, const double *__restrict__ gl_mask,
+                                            double2 *__restrict__ nuH, double *__restrict__ beta,
+                                            double *partials, unsigned *ticket, double *norm_out) {
+  const double dx = g.dx, dy = g.dy;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const int kE = nbr(g, i, j, 1, 0), kN = nbr(g, i, j, 0, 1), kS = nbr(g, i, j, 0, -1), kW = nbr(g, i, j, -1, 0);
+    const int kNE = nbr(g, i, j, 1, 1), kSE = nbr(g, i, j, 1, -1), kNW = nbr(g, i, j, -1, 1);
+    const double2 uc = vel[k], ue = vel[kE], un = vel[kN], us = vel[kS], uw = vel[kW], une = vel[kNE],
+                  use = vel[kSE], unw = vel[kNW];
+    const double Hc = H[k], He = H[kE], Hn = H[kN];
+    const double2 B = hardness[k];
+    double r0, r1;
+    if (!CFBC) {
+      // east face (o = 0)
+      double Hf = 0.5 * (Hc + He);
+      if (Hf < p.Hmin) {
+        r0 = p.notional;
+      } else {
+        double u_x = (ue.x - uc.x) / dx, u_y = (un.x + une.x - us.x - use.x) / (4 * dy);
+        double v_x = (ue.y - uc.y) / dx, v_y = (un.y + une.y - us.y - use.y) / (4 * dy);
+        double nu = 0.5 * B.x * pow(p.schoof_reg + second_invariant_2d(u_x, u_y, v_x, v_y), p.visc_power);
+        r0 = nu * Hf;
+        r0 *= p.enh_scaling;
+        r0 += p.reg;
+      }
+      // north face (o = 1)
+      Hf = 0.5 * (Hc + Hn);
+      if (Hf < p.Hmin) {
+        r1 = p.notional;
+      } else {
+        double u_x = (ue.x + une.x - uw.x - unw.x) / (4 * dx), u_y = (un.x - uc.x) / dy;
+        double v_x = (ue.y + une.y - uw.y - unw.y) / (4 * dx), v_y = (un.y - uc.y) / dy;
+        double nu = 0.5 * B.y * pow(p.schoof_reg + second_invariant_2d(u_x, u_y, v_x, v_y), p.visc_power);
+        r1 = nu * Hf;
+        r1 *= p.enh_scaling;
+        r1 += p.reg;
+      }
+    } else {
+      const int Mc = mask[k], Me = mask[kE], Mn = mask[kN], Ms = mask[kS], Mw = mask[kW], Mse = mask[kSE],
+                Mnw = mask[kNW], Mne = mask[kNE];
+      const bool ic = m_icy(Mc), ie = m_icy(Me), in = m_icy(Mn), is = m_icy(Ms), iw = m_icy(Mw), ise = m_icy(Mse),
+                 inw = m_icy(Mnw), ine = m_icy(Mne);
+      // m_work entries (SSAFD.cc:1463-1491), W_I at (a) between a and a+1 in i, W_J in j
+      auto WI = [&](bool a, bool b, double2 va, double2 vb) {
+        return (a && b) ? WorkVal{(vb.x - va.x) / dx, (vb.y - va.y) / dx, 1.0} : WorkVal{0.0, 0.0, 0.0};
+      };
+      auto WJ = [&](bool a, bool b, double2 va, double2 vb) {
+        return (a && b) ? WorkVal{(vb.x - va.x) / dy, (vb.y - va.y) / dy, 1.0} : WorkVal{0.0, 0.0, 0.0};
+      };
+      const WorkVal wi_c = WI(ic, ie, uc, ue), wi_w = WI(iw, ic, uw, uc), wi_nw = WI(inw, in, unw, un),
+                    wi_n = WI(in, ine, un, une);
+      const WorkVal wj_c = WJ(ic, in, uc, un), wj_s = WJ(is, ic, us, uc), wj_se = WJ(ise, ie, use, ue),
+                    wj_e = WJ(ie, ine, ue, une);
+      // i-offset
+      double Hf = (ic && ie) ? 0.5 * (Hc + He) : (ic ? Hc : He);
+      if (Hf >= p.Hmin) {
+        double u_x = wi_c.u, v_x = wi_c.v, u_y = 0.0, v_y = 0.0;
+        double W = wj_c.w + wj_s.w + wj_se.w + wj_e.w;
+        if (W > 0) {
+          u_y = 1.0 / W * (wj_c.u + wj_s.u + wj_se.u + wj_e.u);
+          v_y = 1.0 / W * (wj_c.v + wj_s.v + wj_se.v + wj_e.v);
+        }
+        double nu = 0.5 * B.x * pow(p.schoof_reg + second_invariant_2d(u_x, u_y, v_x, v_y), p.visc_power);
+        r0 = nu * Hf;
+      } else {
+        r0 = p.notional;
+      }
+      // j-offset
+      Hf = (ic && in) ? 0.5 * (Hc + Hn) : (ic ? Hc : Hn);
+      if (Hf >= p.Hmin) {
+        double u_y = wj_c.u, v_y = wj_c.v, u_x = 0.0, v_x = 0.0;
+        double W = wi_c.w + wi_w.w + wi_nw.w + wi_n.w;
+        if (W > 0.0) {
+          u_x = 1.0 / W * (wi_c.u + wi_w.u + wi_nw.u + wi_n.u);
+          v_x = 1.0 / W * (wi_c.v + wi_w.v + wi_nw.v + wi_n.v);
+        }
+        double nu = 0.5 * B.y * pow(p.schoof_reg + second_invariant_2d(u_x, u_y, v_x, v_y), p.visc_power);
+        r1 = nu * Hf;
+      } else {
+        r1 = p.notional;
+      }
+      r0 *= p.enh_scaling;
+      r0 += p.reg;
+      r1 *= p.enh_scaling;
+      r1 += p.reg;
+    }
+    const double2 old = nuH[k];
+    if (p.underrelax != 1.0) {
+      r0 *= p.underrelax;
+      r0 += (1.0 - p.underrelax) * old.x;
+      r1 *= p.underrelax;
+      r1 += (1.0 - p.underrelax) * old.y;
+    }
+    nuH[k] = make_double2(r0, r1);
+    if (p.with_norm) {
+      const double wi = (i == 0 ? 1.0 : 0.0) + (i == g.Mx - 1 ? 1.0 : 0.0) + 1.0;
+      const double wj = (j == 0 ? 1.0 : 0.0) + (j == g.My - 1 ? 1.0 : 0.0) + 1.0;
+      const double w = wi * wj;
+      acc[0] += fabs(r0) * w;
+      acc[1] += fabs(r1) * w;
+      acc[2] += fabs(old.x - r0) * w;
+      acc[3] += fabs(old.y - r1) * w;
+    }
+    // basal drag for the next assembly (SSAFD.cc:744-759)
+    const int Mc = mask[k];
+    double bta = 0.0;
+    if (m_grounded_ice(Mc))
+      bta = basal_drag(c, tauc[k], uc.x, uc.y);
+    else if (m_ice_free_land(Mc))
+      bta = c.beta_ice_free_bedrock;
+    if (c.sub_groundingline && m_icy(Mc)) bta = gl_mask[k] * basal_drag(c, tauc[k], uc.x, uc.y);
+    beta[k] = bta;
+  }
+  if (p.with_norm) {
+    double tot[4];
+    if (grid_reduce<4>(acc, partials, ticket, tot)) {
+      const double a = p.B_area;
+      const double n0 = tot[0] * a, n1 = tot[1] * a, c0 = tot[2] * a, c1 = tot[3] * a;
+      norm_out[0] = sqrt(n0 * n0 + n1 * n1);
+      norm_out[1] = sqrt(c0 * c0 + c1 * c1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the SSAFD stencil (SSAFD::assemble_matrix, SSAFD.cc:540-796), matrix-free
+// ---------------------------------------------------------------------------
+struct StencilConst {
+  double rdx2, rdy2, r2, r4, scaling;   // 1/dx^2, 1/dy^2, 1/(2 dx dy), 1/(4 dx dy), m_scaling
+};
+
+// the 36 row coefficients of one cell; eq1 = u-row, eq2 = v-row; positions
+// NW N NE / W C E / SW S SE
+struct Row2 {
+  double uNW, uN, uNE, uW, uC, uE, uSW, uS, uSE;
+  double vNW, vN, vNE, vW, vC, vE, vSW, vS, vSE;
+};
+
+__device__ __forceinline__ void stencil_rows(const StencilConst &s, uint32_t f, double c_w, double c_e, double c_s,
+                                             double c_n, double bta, Row2 &e1, Row2 &e2) {
+  const double aMn = (f & F_aMn) ? 1.0 : 0.0, aPn = (f & F_aPn) ? 1.0 : 0.0, aMM = (f & F_aMM) ? 1.0 : 0.0,
+               aPP = (f & F_aPP) ? 1.0 : 0.0, aMs = (f & F_aMs) ? 1.0 : 0.0, aPs = (f & F_aPs) ? 1.0 : 0.0;
+  const double bPw = (f & F_bPw) ? 1.0 : 0.0, bPP = (f & F_bPP) ? 1.0 : 0.0, bPe = (f & F_bPe) ? 1.0 : 0.0,
+               bMw = (f & F_bMw) ? 1.0 : 0.0, bMM = (f & F_bMM) ? 1.0 : 0.0, bMe = (f & F_bMe) ? 1.0 : 0.0;
+  // products of a staggered coefficient with its weights (exact: weights are 0 or 1)
+  const double w = c_w * aMM, e = c_e * aPP, sS = c_s * bMM, n = c_n * bPP;
+  const double wPw = w * bPw, wMw = w * bMw, wPP = w * bPP, wMM = w * bMM;
+  const double ePe = e * bPe, eMe = e * bMe, ePP = e * bPP, eMM = e * bMM;
+  const double nMn = n * aMn, nPn = n * aPn, nPP = n * aPP, nMM = n * aMM;
+  const double sMs = sS * aMs, sPs = sS * aPs, sPP = sS * aPP, sMM = sS * aMM;
+  const double r2 = s.r2, r4 = s.r4;
+  // first equation, u part
+  e1.uNW = 0.0; e1.uN = -n * s.rdy2; e1.uNE = 0.0;
+  e1.uW = -4 * w * s.rdx2;
+  e1.uC = (n + sS) * s.rdy2 + (4 * e + 4 * w) * s.rdx2 + bta;
+  e1.uE = -4 * e * s.rdx2;
+  e1.uSW = 0.0; e1.uS = -sS * s.rdy2; e1.uSE = 0.0;
+  // first equation, v part
+  e1.vNW = wPw * r2 + nMn * r4;
+  e1.vN = (nPn - nMn) * r4 + (wPP - ePP) * r2;
+  e1.vNE = -ePe * r2 - nPn * r4;
+  e1.vW = (wMw - wPw) * r2 + (nMM - sMM) * r4;
+  e1.vC = (nPP - nMM - sPP + sMM) * r4 + (ePP - wPP - eMM + wMM) * r2;
+  e1.vE = (ePe - eMe) * r2 + (sPP - nPP) * r4;
+  e1.vSW = -wMw * r2 - sMs * r4;
+  e1.vS = (sMs - sPs) * r4 + (eMM - wMM) * r2;
+  e1.vSE = eMe * r2 + sPs * r4;
+  // second equation, u part (cross terms with 1/d2 and 1/d4 swapped)
+  e2.uNW = wPw * r4 + nMn * r2;
+  e2.uN = (nPn - nMn) * r2 + (wPP - ePP) * r4;
+  e2.uNE = -ePe * r4 - nPn * r2;
+  e2.uW = (wMw - wPw) * r4 + (nMM - sMM) * r2;
+  e2.uC = (nPP - nMM - sPP + sMM) * r2 + (ePP - wPP - eMM + wMM) * r4;
+  e2.uE = (ePe - eMe) * r4 + (sPP - nPP) * r2;
+  e2.uSW = -wMw * r4 - sMs * r2;
+  e2.uS = (sMs - sPs) * r2 + (eMM - wMM) * r4;
+  e2.uSE = eMe * r4 + sPs * r2;
+  // second equation, v part
+  e2.vNW = 0.0; e2.vN = -4 * n * s.rdy2; e2.vNE = 0.0;
+  e2.vW = -w * s.rdx2;
+  e2.vC = (4 * n + 4 * sS) * s.rdy2 + (e + w) * s.rdx2 + bta;
+  e2.vE = -e * s.rdx2;
+  e2.vSW = 0.0; e2.vS = -4 * sS * s.rdy2; e2.vSE = 0.0;
+}
+
+// y(i, j) = (A x)(i, j)
+__device__ __forceinline__ double2 apply_cell(const GridDev &g, const StencilConst &s, int i, int j, uint32_t f,
+                                              const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                              const double2 *__restrict__ x) {
+  const int k = cell(g, i, j);
+  if (f & F_DIAG_ONLY) {
+    const double2 xc = x[k];
+    return make_double2(s.scaling * xc.x, s.scaling * xc.y);
+  }
+  const int ip = wrap(i + 1, g.Mx), im = wrap(i - 1, g.Mx), jp = wrap(j + 1, g.My), jm = wrap(j - 1, g.My);
+  const int rC = i * g.My, rE = ip * g.My, rW = im * g.My;
+  const double2 nC = nuH[k];
+  const double c_w = nuH[rW + j].x, c_s = nuH[rC + jm].y;
+  Row2 e1, e2;
+  stencil_rows(s, f, c_w, nC.x, c_s, nC.y, beta[k], e1, e2);
+  const double2 xNW = x[rW + jp], xN = x[rC + jp], xNE = x[rE + jp];
+  const double2 xW = x[rW + j], xC = x[k], xE = x[rE + j];
+  const double2 xSW = x[rW + jm], xS = x[rC + jm], xSE = x[rE + jm];
+  double y1 = e1.uN * xN.x + e1.uW * xW.x + e1.uC * xC.x + e1.uE * xE.x + e1.uS * xS.x;
+  y1 += e1.vNW * xNW.y + e1.vN * xN.y + e1.vNE * xNE.y + e1.vW * xW.y + e1.vC * xC.y + e1.vE * xE.y +
+        e1.vSW * xSW.y + e1.vS * xS.y + e1.vSE * xSE.y;
+  double y2 = e2.uNW * xNW.x + e2.uN * xN.x + e2.uNE * xNE.x + e2.uW * xW.x + e2.uC * xC.x + e2.uE * xE.x +
+              e2.uSW * xSW.x + e2.uS * xS.x + e2.uSE * xSE.x;
+  y2 += e2.vN * xN.y + e2.vW * xW.y + e2.vC * xC.y + e2.vE * xE.y + e2.vS * xS.y;
+  return make_double2(y1, y2);
+}
+
+// y = A x (plain apply, for checking and for the residual of the refinement)
+__global__ void __launch_bounds__(NT) k_apply(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
+                                              const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                              const double2 *__restrict__ x, double2 *__restrict__ y) {
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    y[k] = apply_cell(g, s, i, j, flags[k], nuH, beta, x);
+  }
+}
+
+// block-diagonal (2x2) inverse for the point-block Jacobi preconditioner, and the
+// zero-diagonal check of SSAFD.cc:766-776 (first offending cell index reported)
+__global__ void __launch_bounds__(NT) k_diag_setup(GridDev g, TileMap tm, StencilConst s,
+                                                   const uint32_t *__restrict__ flags,
+                                                   const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                                   double4 *__restrict__ dinv, int *zero_diag_cell) {
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const uint32_t f = flags[k];
+    if (f & F_DIAG_ONLY) {
+      dinv[k] = make_double4(1.0 / s.scaling, 0.0, 0.0, 1.0 / s.scaling);
+      continue;
+    }
+    const double2 nC = nuH[k];
+    const double c_w = nuH[nbr(g, i, j, -1, 0)].x, c_s = nuH[nbr(g, i, j, 0, -1)].y;
+    Row2 e1, e2;
+    stencil_rows(s, f, c_w, nC.x, c_s, nC.y, beta[k], e1, e2);
+    const double a11 = e1.uC, a12 = e1.vC, a21 = e2.uC, a22 = e2.vC;
+    if (fabs(a11) < 1e-16 || fabs(a22) < 1e-16) atomicMin(zero_diag_cell, k);
+    const double det = a11 * a22 - a12 * a21;
+    if (det != 0.0 && isfinite(det)) {
+      const double r = 1.0 / det;
+      dinv[k] = make_double4(a22 * r, -a12 * r, -a21 * r, a11 * r);
+    } else {
+      dinv[k] = make_double4(a11 != 0.0 ? 1.0 / a11 : 0.0, 0.0, 0.0, a22 != 0.0 ? 1.0 / a22 : 0.0);
+    }
+  }
+}
+
+__device__ __forceinline__ double2 dmul(const double4 &m, const double2 &v) {
+  return make_double2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
+}
+__device__ __forceinline__ double dot2(const double2 &a, const double2 &b) { return a.x * b.x + a.y * b.y; }
+
+// ---------------------------------------------------------------------------
+// BiCGStab, right preconditioned by M^-1 = block-Jacobi (van der Vorst 1992),
+// five kernels per iteration with all dot products fused into them.
+// Stop: ||b - A x||_2 <= rtol ||b||_2 (the unpreconditioned norm of the
+// reference's ASM path, SSAFD.cc:181-187).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_bicg_init(GridDev g, TileMap tm, StencilConst s,
+                                                  const uint32_t *__restrict__ flags,
+                                                  const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                                  const double2 *__restrict__ b, const double2 *__restrict__ x,
+                                                  double2 *__restrict__ r, double2 *__restrict__ rhat,
+                                                  double2 *__restrict__ p, double2 *__restrict__ v,
+                                                  double *partials, unsigned *ticket, KState *st) {
+  double acc[2] = {0.0, 0.0};
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const double2 ax = apply_cell(g, s, i, j, flags[k], nuH, beta, x);
+    const double2 bk = b[k];
+    const double2 rk = make_double2(bk.x - ax.x, bk.y - ax.y);
+    r[k] = rk;
+    rhat[k] = rk;
+    p[k] = make_double2(0.0, 0.0);
+    v[k] = make_double2(0.0, 0.0);
+    acc[0] += dot2(rk, rk);
+    acc[1] += dot2(bk, bk);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) {
+    st->rnorm2 = tot[0];
+    st->bnorm2 = tot[1];
+    st->rnorm0 = sqrt(tot[0]);
+    st->rho = tot[0];
+    st->alpha = 1.0;
+    st->omega = 1.0;
+    st->beta = 0.0;
+    st->iter = 0;
+    st->status = 0;
+    const double tol = st->rtol * sqrt(tot[1]);
+    st->done = (sqrt(tot[0]) <= tol || tot[1] == 0.0) ? 1 : 0;
+    if (!isfinite(tot[0])) { st->done = 1; st->status = KSP_NAN; }
+  }
+}
+
+// p = r + beta (p - omega v);  phat = M^-1 p
+__global__ void __launch_bounds__(NT) k_bicg_p(int N, const double2 *__restrict__ r, const double2 *__restrict__ v,
+                                               const double4 *__restrict__ dinv, double2 *__restrict__ p,
+                                               double2 *__restrict__ phat, const KState *st) {
+  if (st->done) return;
+  const double bta = st->beta, om = st->omega;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 rk = r[k], pk = p[k], vk = v[k];
+    const double2 pn = make_double2(rk.x + bta * (pk.x - om * vk.x), rk.y + bta * (pk.y - om * vk.y));
+    p[k] = pn;
+    phat[k] = dmul(dinv[k], pn);
+  }
+}
+
+// v = A phat; alpha = rho / (rhat . v)
+__global__ void __launch_bounds__(NT) k_bicg_v(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
+                                               const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                               const double2 *__restrict__ phat, const double2 *__restrict__ rhat,
+                                               double2 *__restrict__ v, double *partials, unsigned *ticket,
+                                               KState *st) {
+  if (st->done) return;
+  double acc[1] = {0.0};
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const double2 vk = apply_cell(g, s, i, j, flags[k], nuH, beta, phat);
+    v[k] = vk;
+    acc[0] += dot2(rhat[k], vk);
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, partials, ticket, tot)) {
+    if (tot[0] == 0.0 || !isfinite(tot[0])) {
+      st->done = 1;
+      st->status = isfinite(tot[0]) ? KSP_BREAKDOWN : KSP_NAN;
+    } else {
+      st->alpha = st->rho / tot[0];
+    }
+  }
+}
+
+// s = r - alpha v;  shat = M^-1 s
+__global__ void __launch_bounds__(NT) k_bicg_s(int N, const double2 *__restrict__ r, const double2 *__restrict__ v,
+                                               const double4 *__restrict__ dinv, double2 *__restrict__ sv,
+                                               double2 *__restrict__ shat, const KState *st) {
+  if (st->done) return;
+  const double al = st->alpha;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 rk = r[k], vk = v[k];
+    const double2 sk = make_double2(rk.x - al * vk.x, rk.y - al * vk.y);
+    sv[k] = sk;
+    shat[k] = dmul(dinv[k], sk);
+  }
+}
+
+// t = A shat; omega = (t . s) / (t . t)
+__global__ void __launch_bounds__(NT) k_bicg_t(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
+                                               const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                               const double2 *__restrict__ shat, const double2 *__restrict__ sv,
+                                               double2 *__restrict__ tv, double *partials, unsigned *ticket,
+                                               KState *st) {
+  if (st->done) return;
+  double acc[2] = {0.0, 0.0};
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tm.cell_of(g, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const double2 tk = apply_cell(g, s, i, j, flags[k], nuH, beta, shat);
+    tv[k] = tk;
+    acc[0] += dot2(tk, sv[k]);
+    acc[1] += dot2(tk, tk);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) st->omega = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
+}
+
+// x += alpha phat + omega shat;  r = s - omega t;  convergence test
+__global__ void __launch_bounds__(NT) k_bicg_x(int N, const double2 *__restrict__ phat, const double2 *__restrict__ shat,
+                                               const double2 *__restrict__ sv, const double2 *__restrict__ tv,
+                                               const double2 *__restrict__ rhat, double2 *__restrict__ x,
+                                               double2 *__restrict__ r, double *partials, unsigned *ticket,
+                                               KState *st) {
+  if (st->done) return;
+  const double al = st->alpha, om = st->omega;
+  double acc[2] = {0.0, 0.0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 ph = phat[k], sh = shat[k], sk = sv[k], tk = tv[k];
+    double2 xk = x[k];
+    xk.x += al * ph.x + om * sh.x;
+    xk.y += al * ph.y + om * sh.y;
+    x[k] = xk;
+    const double2 rk = make_double2(sk.x - om * tk.x, sk.y - om * tk.y);
+    r[k] = rk;
+    acc[0] += dot2(rhat[k], rk);
+    acc[1] += dot2(rk, rk);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) {
+    const double rho_new = tot[0];
+    st->rnorm2 = tot[1];
+    st->iter += 1;
+    const double rn = sqrt(tot[1]), tol = st->rtol * sqrt(st->bnorm2);
+    if (!isfinite(rn)) {
+      st->done = 1; st->status = KSP_NAN;
+    } else if (rn <= tol) {
+      st->done = 1; st->status = 0;
+    } else if (st->iter >= st->maxit) {
+      st->done = 1; st->status = KSP_MAXIT;
+    } else if (om == 0.0 || rho_new == 0.0) {
+      st->done = 1; st->status = KSP_BREAKDOWN;
+    } else {
+      st->beta = (rho_new / st->rho) * (al / om);
+      st->rho = rho_new;
+    }
+  }
+}
+
+// basal frictional heating (ShallowStressBalance.cc:179-205)
+__global__ void k_bfrict(int N, pism_gpu_ssa_config c, const double2 *__restrict__ vel, const double *__restrict__ tauc,
+                         const int8_t *__restrict__ mask, double *__restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    if (m_ocean(mask[k])) {
+      out[k] = 0.0;
+    } else {
+      const double2 V = vel[k];
+      const double C = basal_drag(c, tauc[k], V.x, V.y);
+      const double bx = -C * V.x, by = -C * V.y;
+      out[k] = -bx * V.x - by * V.y;
+    }
+  }
+}
+
+__global__ void k_scale(int n, double a, double *x) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] *= a;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int grid_for_tiles(const Launch &L, int tiles) { return tiles < L.max_blocks ? tiles : L.max_blocks; }
+static int grid_for(const Launch &L, int n) {
+  int b = (n + NT - 1) / NT;
+  return b < L.max_blocks ? b : L.max_blocks;
+}
+
+static StencilConst stencil_const(const GridDev &g) {
+  StencilConst s;
+  s.rdx2 = 1.0 / (g.dx * g.dx);
+  s.rdy2 = 1.0 / (g.dy * g.dy);
+  s.r2 = 1.0 / (2 * g.dx * g.dy);
+  s.r4 = 1.0 / (4 * g.dx * g.dy);
+  s.scaling = 1.0e9;
+  return s;
+}
+
+void launch_convert_masks(const Launch &L, int N, const double *mask, const double *bc_mask, int8_t *mask_i,
+                          uint8_t *bc_i) {
+  L.tick();
+  k_convert_masks<<<grid_for(L, N), NT, 0, L.stream>>>(N, mask, bc_mask, mask_i, bc_i);
+}
+
+void launch_prepare(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int periodicity, const Fields &f) {
+  L.tick();
+  TileMap tm = make_tiles(g);
+  k_prepare<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, c, periodicity, f.H, f.srf, f.bed, f.mask,
+                                                              f.bc, f.bcv, f.melange, f.taud, f.rhs, f.flags);
+}
+
+void launch_hardness(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, const Fields &f, int Mz,
+                     const double *z) {
+  L.tick();
+  int N = g.Mx * g.My;
+  k_hardness<<<grid_for(L, N), NT, 0, L.stream>>>(g, N, c, f.H, f.mask, f.enthalpy, Mz, z, f.fracture, f.hardness);
+}
+
+void launch_nuH(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, const Fields &f, double reg,
+                double underrelax, bool with_norm, double *norm_out) {
+  L.tick();
+  TileMap tm = make_tiles(g);
+  NuHParams p;
+  const double n = c.ssa_Glen_exponent;
+  p.reg = reg;
+  p.underrelax = underrelax;
+  p.Hmin = c.min_thickness_strength_extension_ssa;
+  p.notional = c.constant_nu_strength_extension_ssa * c.min_thickness_strength_extension_ssa;
+  p.schoof_reg = (c.Schoof_regularizing_velocity / c.Schoof_regularizing_length) *
+                 (c.Schoof_regularizing_velocity / c.Schoof_regularizing_length);
+  p.visc_power = (1.0 - n) / (2.0 * n);
+  p.enh_scaling = 1.0 / pow(c.ssa_enhancement_factor, 1.0 / n);
+  p.B_area = g.dx * g.dy;
+  p.with_norm = with_norm ? 1 : 0;
+  int blocks = grid_for_tiles(L, tm.tiles);
+  if (c.calving_front_stress_boundary_condition)
+    k_nuH<true><<<blocks, NT, 0, L.stream>>>(g, tm, c, p, f.vel, f.H, f.hardness, f.mask, f.tauc, f.gl_mask, f.nuH,
+                                             f.beta, L.partials, L.ticket, norm_out);
+  else
+    k_nuH<false><<<blocks, NT, 0, L.stream>>>(g, tm, c, p, f.vel, f.H, f.hardness, f.mask, f.tauc, f.gl_mask, f.nuH,
+                                              f.beta, L.partials, L.ticket, norm_out);
+}
+
+void launch_apply(const Launch &L, const GridDev &g, const Fields &f, const double2 *x, double2 *y) {
+  L.tick();
+  TileMap tm = make_tiles(g);
+  k_apply<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g), f.flags, f.nuH, f.beta, x, y);
+}
+
+void launch_diag_setup(const Launch &L, const GridDev &g, const Fields &f, double4 *dinv, int *zero_diag_cell) {
+  L.tick();
+  TileMap tm = make_tiles(g);
+  k_diag_setup<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g), f.flags, f.nuH, f.beta,
+                                                                 dinv, zero_diag_cell);
+}
+
+void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, const double2 *b,
+                      const double2 *x) {
+  L.tick();
+  TileMap tm = make_tiles(g);
+  k_bicg_init<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g), f.flags, f.nuH, f.beta, b,
+                                                                x, K.r, K.rhat, K.p, K.v, L.partials, L.ticket, K.st);
+}
+
+void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x) {
+  L.tick(5);
+  TileMap tm = make_tiles(g);
+  const int N = g.Mx * g.My;
+  const StencilConst s = stencil_const(g);
+  const int bt = grid_for_tiles(L, tm.tiles), bv = grid_for(L, N);
+  k_bicg_p<<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
+  k_bicg_v<<<bt, NT, 0, L.stream>>>(g, tm, s, f.flags, f.nuH, f.beta, K.phat, K.rhat, K.v, L.partials, L.ticket,
+                                    K.st);
+  k_bicg_s<<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
+  k_bicg_t<<<bt, NT, 0, L.stream>>>(g, tm, s, f.flags, f.nuH, f.beta, K.shat, K.s, K.t, L.partials, L.ticket, K.st);
+  k_bicg_x<<<bv, NT, 0, L.stream>>>(N, K.phat, K.shat, K.s, K.t, K.rhat, x, K.r, L.partials, L.ticket, K.st);
+}
+
+void launch_bfrict(const Launch &L, int N, const pism_gpu_ssa_config &c, const Fields &f, double *out) {
+  L.tick();
+  k_bfrict<<<grid_for(L, N), NT, 0, L.stream>>>(N, c, f.vel, f.tauc, f.mask, out);
+}
+
+void launch_scale(const Launch &L, int n, double a, double *x) {
+  L.tick();
+  k_scale<<<grid_for(L, n), NT, 0, L.stream>>>(n, a, x);
+}
+
+}  // namespace pism_gpu

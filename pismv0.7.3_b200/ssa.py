@@ -1,0 +1,250 @@
+"""Host-side mirror of PISM's SSA interface over the B200 C-ABI.
+
+``SSAFD`` keeps the names, argument meaning and error behaviour of the
+reference's ``pism::stressbalance::SSAFD`` (src/base/stressbalance/ssa/SSAFD.hh,
+SSA.hh:110-156, ShallowStressBalance.hh:39-99): ``init``, ``update(fast,
+melange_back_pressure)``, ``solve``, ``set_boundary_conditions``,
+``set_initial_guess``, ``velocity``, ``basal_frictional_heating``,
+``stdout_report``, and the stage methods ``assemble_rhs``,
+``compute_hardav_staggered``, ``compute_nuH_staggered``.  Failures raise
+``RuntimeError`` subclasses named as in the reference (``KSPFailure``,
+``PicardFailure``, SSAFD.hh:115-123).
+
+Arrays are numpy FP64 arrays indexed ``[i, j]`` (``[..., 2]`` for vectors) or,
+to keep data on the device, CUDA tensors of the same shape (``torch.float64``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from .config import CInputs, CStats, GridDesc, SSAConfig
+
+_D = C.POINTER(C.c_double)
+
+
+class SSAError(RuntimeError):
+    """RuntimeError raised by the solver (pism::RuntimeError)."""
+
+
+class KSPFailure(SSAError):
+    """SSAFD::KSPFailure (SSAFD.hh:115-118)."""
+
+
+class PicardFailure(SSAError):
+    """SSAFD::PicardFailure (SSAFD.hh:120-123)."""
+
+
+class ZeroDiagonal(SSAError):
+    """Zero diagonal entry at a regular location (SSAFD.cc:766-776)."""
+
+
+_EXC = {_capi.EKSP: KSPFailure, _capi.EPICARD: PicardFailure, _capi.EZERODIAG: ZeroDiagonal}
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+class _Buf:
+    """Pointer + keep-alive for a host numpy array or a CUDA tensor."""
+
+    def __init__(self, a, shape):
+        if a is None:
+            self.ptr, self.keep, self.device = None, None, None
+            return
+        if _is_device(a):
+            import torch
+            t = a.to(torch.float64).contiguous()
+            if tuple(t.shape) != tuple(shape):
+                t = t.reshape(shape)
+            self.keep, self.device = t, True
+            self.ptr = C.cast(C.c_void_p(t.data_ptr()), _D)
+        else:
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+            self.keep, self.device = arr, False
+            self.ptr = arr.ctypes.data_as(_D)
+
+
+class SSAFD:
+    """B200 finite-difference SSA solver with the reference's SSAFD interface."""
+
+    def __init__(self, grid: GridDesc, config: SSAConfig | None = None, device: int = 0):
+        self.lib = _capi.load()
+        self.grid = grid
+        self.config = (config or SSAConfig()).copy()
+        self.device = device
+        self._h = C.c_void_p()
+        cgrid, self._z = grid.to_c()
+        ccfg = self.config.to_c()
+        rc = self.lib.pism_gpu_ssa_create(C.byref(cgrid), C.byref(ccfg), device, C.byref(self._h))
+        if rc != _capi.OK:
+            raise SSAError(f"pism_gpu_ssa_create failed with status {rc}")
+        self._stats = CStats()
+        self._bc = (None, None)
+        self._fields = {}
+        self._stdout = ""
+
+    # ---- lifetime ----
+    def close(self):
+        if self._h:
+            self.lib.pism_gpu_ssa_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != _capi.OK:
+            msg = self.lib.pism_gpu_ssa_last_error(self._h).decode() or what
+            raise _EXC.get(rc, SSAError)(f"{what}: {msg} (status {rc})")
+
+    @property
+    def shape(self):
+        return (self.grid.Mx, self.grid.My)
+
+    # ---- configuration and inputs ----
+    def set_config(self, config: SSAConfig):
+        self.config = config.copy()
+        ccfg = self.config.to_c()
+        self._check(self.lib.pism_gpu_ssa_set_config(self._h, C.byref(ccfg)), "set_config")
+
+    def set_stream(self, cuda_stream_ptr: int | None):
+        self._check(self.lib.pism_gpu_ssa_set_stream(self._h, C.c_void_p(cuda_stream_ptr or 0)), "set_stream")
+
+    def init(self):
+        """SSAFD::init_impl: nothing to fetch; inputs come through set_inputs."""
+
+    def set_boundary_conditions(self, locations, velocities):
+        """ShallowStressBalance::set_boundary_conditions(bc_mask, vel_ssa_bc)."""
+        self._bc = (locations, velocities)
+        if self._fields:
+            self._upload()
+
+    def set_inputs(self, thickness, surface, bed, mask, tauc, melange=None, gl_mask=None, enthalpy=None,
+                   hardness=None, fracture_density=None, bc_mask=None, bc_values=None):
+        """Hand over the fields SSA::init_impl fetches by name (SSA.cc:134-184)."""
+        self._fields = dict(thickness=thickness, surface=surface, bed=bed, mask=mask, tauc=tauc,
+                            melange=melange, gl_mask=gl_mask, enthalpy=enthalpy, hardness=hardness,
+                            fracture_density=fracture_density)
+        if bc_mask is not None:
+            self._bc = (bc_mask, bc_values)
+        self._upload()
+
+    def _upload(self):
+        f = self._fields
+        Mx, My = self.shape
+        Mz = 0 if self.grid.z is None else len(self.grid.z)
+        s2, s3 = (Mx, My), (Mx, My, 2)
+        bufs = {
+            "thickness": _Buf(f["thickness"], s2), "surface": _Buf(f["surface"], s2),
+            "bed": _Buf(f["bed"], s2), "mask": _Buf(f["mask"], s2), "tauc": _Buf(f["tauc"], s2),
+            "bc_mask": _Buf(self._bc[0], s2), "bc_values": _Buf(self._bc[1], s3),
+            "melange": _Buf(f.get("melange"), s2), "gl_mask": _Buf(f.get("gl_mask"), s2),
+            "enthalpy": _Buf(f.get("enthalpy"), (Mx, My, Mz)), "hardness_stag": _Buf(f.get("hardness"), s3),
+            "fracture_density": _Buf(f.get("fracture_density"), s2),
+        }
+        kinds = {b.device for b in bufs.values() if b.ptr is not None}
+        if len(kinds) > 1:
+            raise ValueError("inputs must be all host arrays or all CUDA tensors")
+        ci = CInputs()
+        ci.where = _capi.MEM_DEVICE if kinds == {True} else _capi.MEM_HOST
+        for name, b in bufs.items():
+            setattr(ci, name, b.ptr)
+        self._check(self.lib.pism_gpu_ssa_set_inputs(self._h, C.byref(ci)), "set_inputs")
+
+    def set_initial_guess(self, guess):
+        """SSA::set_initial_guess (SSA.cc:361-363)."""
+        b = _Buf(guess, (*self.shape, 2))
+        where = _capi.MEM_DEVICE if b.device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_set_initial_guess(self._h, b.ptr, where), "set_initial_guess")
+
+    # ---- the solve ----
+    def update(self, fast: bool = False, melange_back_pressure=None):
+        """SSA::update (SSA.cc:188-196) / SSAFD::update (SSAFD.cc:260-264)."""
+        if melange_back_pressure is not None:
+            self._fields["melange"] = melange_back_pressure
+            self._upload()
+        if not fast:
+            self.solve()
+
+    def solve(self, out=None):
+        """SSAFD::solve (SSAFD.cc:869-924). Returns the velocity ([Mx, My, 2])."""
+        if out is None:
+            out = np.empty((*self.shape, 2))
+        b = _Buf(out, (*self.shape, 2))
+        where = _capi.MEM_DEVICE if b.device else _capi.MEM_HOST
+        rc = self.lib.pism_gpu_ssa_solve(self._h, b.ptr, where, C.byref(self._stats))
+        self._check(rc, "SSAFD solve")
+        s = self._stats
+        self._stdout = "%5d outer iterations, ~%3.1f KSP iterations each\n" % (
+            s.picard_iterations, s.ksp_iterations / max(1, s.picard_iterations))
+        return b.keep if b.device else out
+
+    def stats(self) -> dict:
+        return self._stats.as_dict()
+
+    def stdout_report(self) -> str:
+        return self._stdout
+
+    # ---- fields ----
+    def _get(self, field, shape, out=None):
+        if out is None:
+            out = np.empty(shape)
+        b = _Buf(out, shape)
+        where = _capi.MEM_DEVICE if b.device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_get_field(self._h, field, b.ptr, where), "get_field")
+        return b.keep if b.device else out
+
+    def velocity(self, out=None):
+        return self._get(_capi.FIELD_VELOCITY, (*self.shape, 2), out)
+
+    def driving_stress(self, out=None):
+        return self._get(_capi.FIELD_TAUD, (*self.shape, 2), out)
+
+    def rhs(self, out=None):
+        return self._get(_capi.FIELD_RHS, (*self.shape, 2), out)
+
+    def hardness(self, out=None):
+        return self._get(_capi.FIELD_HARDNESS, (*self.shape, 2), out)
+
+    def nuH(self, out=None):
+        return self._get(_capi.FIELD_NUH, (*self.shape, 2), out)
+
+    def beta(self, out=None):
+        return self._get(_capi.FIELD_BETA, self.shape, out)
+
+    def basal_frictional_heating(self, out=None):
+        return self._get(_capi.FIELD_BFRICT, self.shape, out)
+
+    # ---- stage methods (one reference method each) ----
+    def assemble_rhs(self):
+        self._check(self.lib.pism_gpu_ssa_assemble_rhs(self._h), "assemble_rhs")
+
+    def compute_hardav_staggered(self):
+        self._check(self.lib.pism_gpu_ssa_compute_hardness(self._h), "compute_hardav_staggered")
+
+    def compute_nuH_staggered(self, nuH_regularization: float):
+        self._check(self.lib.pism_gpu_ssa_compute_nuH(self._h, nuH_regularization), "compute_nuH_staggered")
+
+    def apply(self, x_dev, y_dev):
+        """y = A x on device tensors ([Mx, My, 2] float64 CUDA)."""
+        self._check(self.lib.pism_gpu_ssa_apply(self._h, C.c_void_p(x_dev.data_ptr()),
+                                                C.c_void_p(y_dev.data_ptr())), "apply")
+
+    def linear_solve(self, x_dev):
+        its = C.c_int(0)
+        res = C.c_double(0)
+        self._check(self.lib.pism_gpu_ssa_linear_solve(self._h, C.c_void_p(x_dev.data_ptr()), C.byref(its),
+                                                       C.byref(res)), "KSPSolve")
+        return its.value, res.value
+
+
+def SSAFD_GPUFactory(grid: GridDesc, config: SSAConfig | None = None) -> SSAFD:
+    """The SSAFactory of this solver (typedef SSAFactory, SSA.hh:77; SSAFDFactory SSAFD.cc:47-49)."""
+    return SSAFD(grid, config)

@@ -1,0 +1,228 @@
+"""GPU parity: every stage of the CUDA SSAFD path against the CPU oracle, through the C-ABI.
+
+Tolerances: FP64 stage values agree to 1e-12 relative (the GPU multiplies by
+reciprocals of dx^2, dy^2, 2 dx dy, 4 dx dy and contracts to FMA where the oracle
+divides); converged velocities agree to the north-star bar of 1e-8 relative L2
+with tight Picard / KSP tolerances.
+"""
+import numpy as np
+import pytest
+
+from pism_b200 import verification as V, synthetic as S
+from pism_b200.config import SSAConfig, GridDesc, X_PERIODIC, Y_PERIODIC
+from oracle import ssafd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from pism_b200.ssa import SSAFD, ZeroDiagonal  # noqa: E402
+
+FIELDS = ("thickness", "surface", "bed", "mask", "tauc", "melange", "gl_mask", "enthalpy", "fracture_density")
+
+
+def make_solver(g, c, f):
+    s = SSAFD(g, c)
+    kw = {k: f[k] for k in FIELDS if f.get(k) is not None}
+    s.set_inputs(**kw, bc_mask=f.get("bc_mask"), bc_values=f.get("bc_values"))
+    return s
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def random_case(seed, Mx=23, My=19, cfbc=False, dirichlet_bc=False, bc=True, periodicity=0, pseudo=False,
+                sub_gl=False, eta=False, flow_law="isothermal_glen", nu_bedrock=False):
+    """Random inputs exercising every mask configuration of a 3x3 neighbourhood."""
+    rng = np.random.default_rng(seed)
+    g = GridDesc(Mx, My, 0.5 * (Mx - 1) * 7e3, 0.5 * (My - 1) * 9e3, periodicity=periodicity,
+                 z=np.linspace(0, 4000, 11))
+    c = SSAConfig(calving_front_stress_boundary_condition=cfbc, ssa_dirichlet_bc=dirichlet_bc,
+                  do_pseudo_plastic_till=pseudo, sub_groundingline=sub_gl,
+                  surface_gradient_method="eta" if eta else "haseloff", flow_law=flow_law,
+                  nu_bedrock_set=nu_bedrock)
+    mask = rng.choice([0.0, 2.0, 3.0, 4.0], size=(Mx, My)) + rng.uniform(-0.3, 0.3, (Mx, My))
+    Mi = np.floor(mask + 0.5)
+    H = np.where((Mi == 2) | (Mi == 3), rng.uniform(20, 3000, (Mx, My)), rng.uniform(0, 30, (Mx, My)))
+    H[rng.random((Mx, My)) < 0.05] = 0.0
+    bed = rng.uniform(-1500, 1500, (Mx, My))
+    f = {
+        "thickness": H, "bed": bed, "surface": bed + H + rng.uniform(-5, 5, (Mx, My)), "mask": mask,
+        "tauc": rng.uniform(1e3, 2e5, (Mx, My)), "melange": rng.uniform(0, 0.5, (Mx, My)),
+        "gl_mask": rng.uniform(0, 1, (Mx, My)) if sub_gl else None,
+        "enthalpy": rng.uniform(1.0e5, 2.0e5, (Mx, My, 11)) if flow_law != "isothermal_glen" else None,
+    }
+    if bc:
+        bm = (rng.random((Mx, My)) < 0.1).astype(float)
+        f["bc_mask"] = bm
+        f["bc_values"] = rng.normal(0, 1e-5, (Mx, My, 2))
+    return g, c, f
+
+
+CASES = {
+    "plain": dict(),
+    "cfbc": dict(cfbc=True),
+    "cfbc_dirichlet": dict(cfbc=True, dirichlet_bc=True),
+    "no_bc": dict(bc=False),
+    "pseudo_subgl": dict(pseudo=True, sub_gl=True),
+    "eta": dict(eta=True),
+    "xperiodic": dict(periodicity=X_PERIODIC),
+    "yperiodic_inward": dict(periodicity=Y_PERIODIC),
+    "nu_bedrock": dict(nu_bedrock=True),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_stage_parity(name):
+    g, c, f = random_case(sum(map(ord, name)), **CASES[name])
+    if name == "yperiodic_inward":
+        c.compute_surf_grad_inward_ssa = True
+    G, Cc, I = O.from_case(g, c, f)
+    s = make_solver(g, c, f)
+    s.assemble_rhs()
+    s.compute_hardav_staggered()
+    taud = O.driving_stress(G, Cc, I)
+    np.testing.assert_allclose(s.driving_stress(), taud, rtol=1e-12, atol=1e-9 * np.abs(taud).max())
+    b = O.assemble_rhs(G, Cc, I, taud)
+    np.testing.assert_allclose(s.rhs(), b, rtol=1e-12, atol=1e-9 * np.abs(b).max())
+    hard = O.hardness_staggered(G, Cc, I)
+    np.testing.assert_allclose(s.hardness(), hard, rtol=1e-12)
+    rng = np.random.default_rng(1)
+    vel = rng.normal(0, 3e-6, (g.Mx, g.My, 2))
+    s.set_initial_guess(vel)
+    s.compute_nuH_staggered(1e13)
+    nuH = O.compute_nuH(G, Cc, I, hard, vel, 1e13)
+    np.testing.assert_allclose(s.nuH(), nuH, rtol=1e-12)
+    beta = O.beta_field(Cc, I, vel)
+    np.testing.assert_allclose(s.beta(), beta, rtol=1e-12)
+    # operator: GPU matrix-free apply vs the assembled 18-column matrix
+    x = rng.normal(0, 1e-5, (g.Mx, g.My, 2))
+    A = O.assemble_matrix(G, Cc, I, s.nuH(), s.beta(), check_diagonal=False)
+    y_ref = (A @ x.ravel()).reshape(x.shape)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    s.apply(xd, yd)
+    torch.cuda.synchronize()
+    y = yd.cpu().numpy()
+    scale = (abs(A) @ np.abs(x).ravel()).reshape(x.shape)      # sum_m |a_m x_m| per row
+    assert np.all(np.abs(y - y_ref) <= 1e-12 * scale + 1e-300), np.max(np.abs(y - y_ref) / (scale + 1e-300))
+    s.close()
+
+
+@pytest.mark.parametrize("law", ["gpbld", "pb", "arr", "arrwarm", "hooke"])
+def test_hardness_from_enthalpy(law):
+    g, c, f = random_case(7, flow_law=law)
+    G, Cc, I = O.from_case(g, c, f)
+    s = make_solver(g, c, f)
+    s.compute_hardav_staggered()
+    np.testing.assert_allclose(s.hardness(), O.hardness_staggered(G, Cc, I), rtol=1e-12)
+    s.close()
+
+
+def test_linear_solve_matches_direct():
+    g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=3)
+    c.ksp_rtol = 1e-12
+    G, Cc, I = O.from_case(g, c, f)
+    s = make_solver(g, c, f)
+    s.assemble_rhs()
+    s.compute_hardav_staggered()
+    vel = np.zeros((g.Mx, g.My, 2))
+    s.set_initial_guess(vel)
+    s.compute_nuH_staggered(c.epsilon_ssa)
+    A = O.assemble_matrix(G, Cc, I, s.nuH(), s.beta())
+    x_ref = O.linear_solve(A, s.rhs().ravel(), None, "direct").reshape(vel.shape)
+    xd = torch.zeros((g.Mx, g.My, 2), dtype=torch.float64, device="cuda")
+    its, res = s.linear_solve(xd)
+    assert res <= 1e-12
+    assert rel(xd.cpu().numpy(), x_ref) < 1e-8
+    s.close()
+
+
+def test_picard_iterates_match_oracle():
+    """Iterate-by-iterate: nu*H -> linear solve, five Picard steps on a synthetic sheet."""
+    g, c, f, _ = S.build_synthetic(33, 4000e3 / 32, seed=5)
+    c.ksp_rtol = 1e-13
+    G, Cc, I = O.from_case(g, c, f)
+    s = make_solver(g, c, f)
+    o = O.SSAFDOracle(G, Cc, I)
+    o.prepare()
+    s.assemble_rhs()
+    s.compute_hardav_staggered()
+    vel_ref = np.zeros((g.Mx, g.My, 2))
+    xd = torch.zeros((g.Mx, g.My, 2), dtype=torch.float64, device="cuda")
+    s.set_initial_guess(xd)
+    for _ in range(5):
+        s.compute_nuH_staggered(c.epsilon_ssa)
+        nuH = O.compute_nuH(G, Cc, I, o.hardness, vel_ref, c.epsilon_ssa)
+        np.testing.assert_allclose(s.nuH(), nuH, rtol=1e-8)
+        A = O.assemble_matrix(G, Cc, I, nuH, O.beta_field(Cc, I, vel_ref))
+        vel_ref = O.linear_solve(A, o.b.ravel(), None, "direct").reshape(vel_ref.shape)
+        s.linear_solve(xd)
+        s.set_initial_guess(xd)
+        assert rel(xd.cpu().numpy(), vel_ref) < 1e-8
+    s.close()
+
+
+def _solve_case(g, c, f):
+    s = make_solver(g, c, f)
+    vel = s.solve()
+    st = s.stats()
+    s.close()
+    return vel, st
+
+
+@pytest.mark.parametrize("My", [61, 121])
+def test_verification_i(goldens, My):
+    g, c, f = V.build_test_i(My=My)
+    c.ssafd_relative_convergence = 5e-7
+    c.ksp_rtol = 1e-12
+    vel, st = _solve_case(g, c, f)
+    assert st["converged"] == 1
+    case = [k for k in goldens["test_i_fd"]["cases"] if k["My"] == My][0]
+    r = V.report(vel, V.exact_velocity_i(g))
+    for key, d in (("maxvector", 4), ("prcntavvec", 5), ("maxu", 4), ("maxv", 4), ("avu", 4), ("avv", 4)):
+        assert round(r[key], d) == pytest.approx(case[key], abs=0.6 * 10 ** -d), key
+    ref = O.SSAFDOracle(*O.from_case(g, c, f)).solve()
+    assert rel(vel, ref) < 1e-8
+
+
+@pytest.mark.parametrize("Mx", [201, 401])
+def test_verification_v_cfbc(goldens, Mx):
+    g, c, f = V.build_test_v(Mx)
+    c.ksp_rtol = 1e-13
+    vel, st = _solve_case(g, c, f)
+    case = [k for k in goldens["test_v_cfbc"]["cases"] if k["Mx"] == Mx][0]
+    r = V.report(vel, V.exact_velocity_v(g))
+    for key, d in (("maxvector", 4), ("prcntavvec", 5), ("maxu", 4), ("avu", 4)):
+        assert round(r[key], d) == pytest.approx(case[key], abs=0.6 * 10 ** -d), key
+    ref = O.SSAFDOracle(*O.from_case(g, c, f)).solve()
+    assert rel(vel, ref) < 1e-8
+
+
+@pytest.mark.parametrize("M", [61, 121])
+def test_verification_j(M):
+    """Test J with a tight KSP equals the oracle's direct solve (the golden itself
+    records PETSc's rtol-1e-5 iterate; the CPU suite pins that)."""
+    g, c, f = V.build_test_j(M, M)
+    c.ksp_rtol = 1e-13
+    vel, st = _solve_case(g, c, f)
+    ref = O.SSAFDOracle(*O.from_case(g, c, f)).solve()
+    assert rel(vel, ref) < 1e-8
+
+
+def test_zero_diagonal_is_reported():
+    """A regular cell with no coupling and no drag: the reference throws (SSAFD.cc:766-776)."""
+    M = 9
+    g = GridDesc(M, M, 40e3, 40e3, periodicity=0)
+    c = SSAConfig(flow_law="isothermal_glen")
+    f = {"thickness": np.zeros((M, M)), "surface": np.zeros((M, M)), "bed": np.full((M, M), -500.0),
+         "mask": np.full((M, M), 4.0), "tauc": np.zeros((M, M))}
+    c.constant_nu_strength_extension_ssa = 0.0
+    c.epsilon_ssa = 0.0
+    s = make_solver(g, c, f)
+    with pytest.raises(ZeroDiagonal):
+        s.solve()
+    s.close()
