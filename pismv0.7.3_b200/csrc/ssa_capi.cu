@@ -109,6 +109,7 @@ Fields fields_of(pism_gpu_ssa *h) {
   f.bcv = h->bcv; f.mask = h->mask; f.bc = h->bc;
   f.taud = h->taud; f.rhs = h->rhs; f.hardness = h->hardness; f.nuH = h->nuH; f.vel = h->vel;
   f.beta = h->beta; f.flags = h->flags;
+  f.nu_bedrock = h->cfg.nu_bedrock;
   return f;
 }
 

@@ -34,7 +34,10 @@ enum : uint32_t {
   F_WEIGHTS = 0xFFFu,
   F_DIAG_ONLY = 1u << 12,   // Dirichlet or CFBC ice-free row: m_scaling on the diagonal only
   F_BC = 1u << 13,          // Dirichlet location (bc_mask == 1)
-  F_MASK_SHIFT = 16         // bits 16-18: the integer mask value
+  F_MASK_SHIFT = 16,        // bits 16-18: the integer mask value
+  // nu_bedrock_set overrides of c_w, c_e, c_n, c_s (SSAFD.cc:561-585)
+  F_NB_W = 1u << 20, F_NB_E = 1u << 21, F_NB_N = 1u << 22, F_NB_S = 1u << 23,
+  F_NB_ANY = F_NB_W | F_NB_E | F_NB_N | F_NB_S
 };
 __host__ __device__ __forceinline__ int flag_mask(uint32_t f) { return (int)((f >> F_MASK_SHIFT) & 7u); }
 

@@ -28,6 +28,7 @@ struct Fields {
   double2 *taud, *rhs, *hardness, *nuH, *vel;
   double *beta;
   uint32_t *flags;
+  double nu_bedrock;
 };
 
 // Krylov work vectors (BiCGStab)

@@ -239,6 +239,13 @@ __global__ void __launch_bounds__(NT) k_prepare(GridDev g, TileMap tm, pism_gpu_
         b.y = td.y + (bMM - bPP) * op / dy;
       }
     }
+    if (c.nu_bedrock_set && Hc > 0.0) {   // HminFrozen = 0 (SSAFD.cc:535, 571-584)
+      const double s0 = srf[k];
+      if (bed[kW] > s0 && m_ice_free_land(Mw)) f |= F_NB_W;
+      if (bed[kE] > s0 && m_ice_free_land(Me)) f |= F_NB_E;
+      if (bed[kN] > s0 && m_ice_free_land(Mn)) f |= F_NB_N;
+      if (bed[kS] > s0 && m_ice_free_land(Ms)) f |= F_NB_S;
+    }
     if (is_bc) {
       f |= F_DIAG_ONLY | F_BC;
       const double2 v = bcv[k];
@@ -473,7 +480,28 @@ __global__ void __launch_bounds__(NT) k_nuH(GridDev g, TileMap tm, pism_gpu_ssa_
 // ---------------------------------------------------------------------------
 struct StencilConst {
   double rdx2, rdy2, r2, r4, scaling;   // 1/dx^2, 1/dy^2, 1/(2 dx dy), 1/(4 dx dy), m_scaling
+  double nu_bedrock;                    // nu_bedrock (used where F_NB_* flags are set)
+  const double *H;                      // thickness, read only where F_NB_* flags are set
 };
+
+// staggered coefficients of row (i, j): c_w, c_e, c_s, c_n (SSAFD.cc:556-585)
+__device__ __forceinline__ void row_coefficients(const GridDev &g, const StencilConst &s, int i, int j, uint32_t f,
+                                                 const double2 *__restrict__ nuH, double &c_w, double &c_e,
+                                                 double &c_s, double &c_n) {
+  const int k = cell(g, i, j);
+  const double2 nC = nuH[k];
+  c_w = nuH[nbr(g, i, j, -1, 0)].x;
+  c_e = nC.x;
+  c_s = nuH[nbr(g, i, j, 0, -1)].y;
+  c_n = nC.y;
+  if (f & F_NB_ANY) {
+    const double Hc = s.H[k], HE = s.H[nbr(g, i, j, 1, 0)];
+    if (f & F_NB_W) c_w = s.nu_bedrock * 0.5 * (Hc + s.H[nbr(g, i, j, -1, 0)]);
+    if (f & F_NB_E) c_e = s.nu_bedrock * 0.5 * (Hc + HE);
+    if (f & F_NB_N) c_n = s.nu_bedrock * 0.5 * (Hc + s.H[nbr(g, i, j, 0, 1)]);
+    if (f & F_NB_S) c_s = s.nu_bedrock * 0.5 * (Hc + HE);   // thickness(i+1, j), as SSAFD.cc:582
+  }
+}
 
 // the 36 row coefficients of one cell; eq1 = u-row, eq2 = v-row; positions
 // NW N NE / W C E / SW S SE
@@ -540,10 +568,10 @@ __device__ __forceinline__ double2 apply_cell(const GridDev &g, const StencilCon
   }
   const int ip = wrap(i + 1, g.Mx), im = wrap(i - 1, g.Mx), jp = wrap(j + 1, g.My), jm = wrap(j - 1, g.My);
   const int rC = i * g.My, rE = ip * g.My, rW = im * g.My;
-  const double2 nC = nuH[k];
-  const double c_w = nuH[rW + j].x, c_s = nuH[rC + jm].y;
+  double c_w, c_e, c_s, c_n;
+  row_coefficients(g, s, i, j, f, nuH, c_w, c_e, c_s, c_n);
   Row2 e1, e2;
-  stencil_rows(s, f, c_w, nC.x, c_s, nC.y, beta[k], e1, e2);
+  stencil_rows(s, f, c_w, c_e, c_s, c_n, beta[k], e1, e2);
   const double2 xNW = x[rW + jp], xN = x[rC + jp], xNE = x[rE + jp];
   const double2 xW = x[rW + j], xC = x[k], xE = x[rE + j];
   const double2 xSW = x[rW + jm], xS = x[rC + jm], xSE = x[rE + jm];
@@ -583,10 +611,10 @@ __global__ void __launch_bounds__(NT) k_diag_setup(GridDev g, TileMap tm, Stenci
       dinv[k] = make_double4(1.0 / s.scaling, 0.0, 0.0, 1.0 / s.scaling);
       continue;
     }
-    const double2 nC = nuH[k];
-    const double c_w = nuH[nbr(g, i, j, -1, 0)].x, c_s = nuH[nbr(g, i, j, 0, -1)].y;
+    double c_w, c_e, c_s, c_n;
+    row_coefficients(g, s, i, j, f, nuH, c_w, c_e, c_s, c_n);
     Row2 e1, e2;
-    stencil_rows(s, f, c_w, nC.x, c_s, nC.y, beta[k], e1, e2);
+    stencil_rows(s, f, c_w, c_e, c_s, c_n, beta[k], e1, e2);
     const double a11 = e1.uC, a12 = e1.vC, a21 = e2.uC, a22 = e2.vC;
     if (fabs(a11) < 1e-16 || fabs(a22) < 1e-16) atomicMin(zero_diag_cell, k);
     const double det = a11 * a22 - a12 * a21;
@@ -794,8 +822,10 @@ static int grid_for(const Launch &L, int n) {
   return b < L.max_blocks ? b : L.max_blocks;
 }
 
-static StencilConst stencil_const(const GridDev &g) {
+static StencilConst stencil_const(const GridDev &g, const Fields &f) {
   StencilConst s;
+  s.nu_bedrock = f.nu_bedrock;
+  s.H = f.H;
   s.rdx2 = 1.0 / (g.dx * g.dx);
   s.rdy2 = 1.0 / (g.dy * g.dy);
   s.r2 = 1.0 / (2 * g.dx * g.dy);
@@ -852,13 +882,13 @@ void launch_nuH(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c,
 void launch_apply(const Launch &L, const GridDev &g, const Fields &f, const double2 *x, double2 *y) {
   L.tick();
   TileMap tm = make_tiles(g);
-  k_apply<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g), f.flags, f.nuH, f.beta, x, y);
+  k_apply<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta, x, y);
 }
 
 void launch_diag_setup(const Launch &L, const GridDev &g, const Fields &f, double4 *dinv, int *zero_diag_cell) {
   L.tick();
   TileMap tm = make_tiles(g);
-  k_diag_setup<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g), f.flags, f.nuH, f.beta,
+  k_diag_setup<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta,
                                                                  dinv, zero_diag_cell);
 }
 
@@ -866,7 +896,7 @@ void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const 
                       const double2 *x) {
   L.tick();
   TileMap tm = make_tiles(g);
-  k_bicg_init<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g), f.flags, f.nuH, f.beta, b,
+  k_bicg_init<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta, b,
                                                                 x, K.r, K.rhat, K.p, K.v, L.partials, L.ticket, K.st);
 }
 
@@ -874,7 +904,7 @@ void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, c
   L.tick(5);
   TileMap tm = make_tiles(g);
   const int N = g.Mx * g.My;
-  const StencilConst s = stencil_const(g);
+  const StencilConst s = stencil_const(g, f);
   const int bt = grid_for_tiles(L, tm.tiles), bv = grid_for(L, N);
   k_bicg_p<<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
   k_bicg_v<<<bt, NT, 0, L.stream>>>(g, tm, s, f.flags, f.nuH, f.beta, K.phat, K.rhat, K.v, L.partials, L.ticket,
