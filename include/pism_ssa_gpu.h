@@ -35,7 +35,8 @@ enum {
   PISM_GPU_SSA_EPICARD = 5,         /* PicardFailure (SSAFD.hh:120)                     */
   PISM_GPU_SSA_EZERODIAG = 6,       /* zero diagonal at a regular location (SSAFD.cc:766-776) */
   PISM_GPU_SSA_ENAN = 7,            /* non-finite value in a residual / inputs          */
-  PISM_GPU_SSA_ESTATE = 8           /* call order violated (e.g. solve before inputs)   */
+  PISM_GPU_SSA_ESTATE = 8,          /* call order violated (e.g. solve before inputs)   */
+  PISM_GPU_SSA_ETOOLARGE = 9        /* grid exceeds PISM_GPU_SSA_NOALLOC_MAX_CELLS      */
 };
 
 /* ---- enumerations -------------------------------------------------------- */
@@ -224,6 +225,39 @@ int pism_gpu_ssa_apply(pism_gpu_ssa *h, const double *x_dev, double *y_dev);
  * initial guess on entry.  *iterations and *rel_residual may be NULL. */
 int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations,
                               double *rel_residual);
+
+/* ---- allocation-free entry point ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * hosts that route every device allocation through their own pool or arena,
+ * code that runs while the caller captures a CUDA graph or works under a memory
+ * budget that forbids new allocations, and bindings without access to the CUDA
+ * allocator.  It computes what pism_gpu_ssa_compute_nuH computes for the plain
+ * (non-CFBC) stencil — nu*H on the staggered grid, under-relaxed against the
+ * values in `nuH` when underrelax != 1 (SSAFD.cc:1061-1064), and the basal drag
+ * coefficient of the next assembly — and writes the two L1 norms of the Picard
+ * test, |nuH| and |nuH_before - nuH| (SSAFD.cc:1170-1189), to norms[0..1].
+ *
+ * All pointers are device memory: velocity (2N), thickness (N), hardness_stag
+ * (2N), mask (N, doubles rounded as IceModelVec2Int::as_int does), tauc (N),
+ * gl_mask (N; only read with sub_groundingline), nuH (2N, in: the previous
+ * values, out: the new ones), beta (N, out), norms (2, out).  The work is
+ * enqueued on `cuda_stream` (NULL = the legacy default stream) and the call
+ * returns without waiting for it.
+ *
+ * It allocates nothing: its scratch is a fixed 512 KiB device array inside the
+ * library, which every GPU that loads the library holds until the process exits.
+ * So the grid may have at most PISM_GPU_SSA_NOALLOC_MAX_CELLS cells (larger grids
+ * return PISM_GPU_SSA_ETOOLARGE), and because every call shares that array, calls
+ * whose work overlaps on the GPU (other streams, other host threads) race: order
+ * them on one stream.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.
+ * CFBC configurations return PISM_GPU_SSA_EINVAL (use the handle API). */
+#define PISM_GPU_SSA_NOALLOC_MAX_CELLS (2048 * 2048)
+int pism_gpu_ssa_nuH_noalloc(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cfg,
+                             const double *velocity, const double *thickness, const double *hardness_stag,
+                             const double *mask, const double *tauc, const double *gl_mask,
+                             double nuH_regularization, double underrelax, double *nuH, double *beta,
+                             double *norms, void *cuda_stream);
 
 #ifdef __cplusplus
 }

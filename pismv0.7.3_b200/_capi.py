@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libpism_ssa_gpu.so")
 
 # status codes (PISM_GPU_SSA_*)
-OK, EINVAL, ECUDA, ENOMEM, EKSP, EPICARD, EZERODIAG, ENAN, ESTATE = range(9)
+OK, EINVAL, ECUDA, ENOMEM, EKSP, EPICARD, EZERODIAG, ENAN, ESTATE, ETOOLARGE = range(10)
+NOALLOC_MAX_CELLS = 2048 * 2048
 # fields (PISM_FIELD_*)
 FIELD_VELOCITY, FIELD_TAUD, FIELD_RHS, FIELD_HARDNESS, FIELD_NUH, FIELD_BETA, FIELD_BFRICT = range(7)
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -24,7 +25,7 @@ EXPORTS = [
     "pism_gpu_ssa_set_stream", "pism_gpu_ssa_set_config", "pism_gpu_ssa_set_inputs",
     "pism_gpu_ssa_set_initial_guess", "pism_gpu_ssa_solve", "pism_gpu_ssa_get_field",
     "pism_gpu_ssa_assemble_rhs", "pism_gpu_ssa_compute_hardness", "pism_gpu_ssa_compute_nuH",
-    "pism_gpu_ssa_apply", "pism_gpu_ssa_linear_solve",
+    "pism_gpu_ssa_apply", "pism_gpu_ssa_linear_solve", "pism_gpu_ssa_nuH_noalloc",
 ]
 
 _lib = None
@@ -55,6 +56,7 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_compute_nuH": (I, [V, D]),
         "pism_gpu_ssa_apply": (I, [V, V, V]),
         "pism_gpu_ssa_linear_solve": (I, [V, V, P(I), P(D)]),
+        "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
