@@ -100,13 +100,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_case(M):
+def build_case(M, pc="mg"):
     _package()
     from pism_b200 import synthetic as S
     dx = 4000e3 / (M - 1)
     g, c, f, meta = S.build_synthetic(M, dx, seed=0)
     c.ksp_rtol = 1e-8
     c.ssafd_relative_convergence = 1e-4
+    c.pc_type = pc
     return g, c, f, meta
 
 
@@ -171,6 +172,7 @@ def main():
     ap.add_argument("--picard-full", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--apply-launches", type=int, default=50)
+    ap.add_argument("--pc", default="mg", choices=["mg", "bjacobi"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -187,7 +189,7 @@ def main():
     _package()
     from pism_b200.ssa import SSAFD
 
-    g, c, f, meta = build_case(args.size)
+    g, c, f, meta = build_case(args.size, args.pc)
     M = args.size
     N = M * M
     dev = torch.device("cuda", local)
@@ -283,7 +285,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"SSAFD solve, synthetic ice sheet {M}x{M} at {4000 / (M - 1):.0f} km, plastic till, "
-                               "Picard 1e-4, KSP 1e-8 (plain FP64: BiCGStab + block Jacobi)",
+                               f"Picard 1e-4, KSP 1e-8 (plain FP64: BiCGStab + {'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'})",
                    "grid": [M, M], "seed": 0, "precision": "fp64", "l2": "flushed (256 MB write) between steps",
                    "parallelism": f"replicas x{world}"},
         "solver": {"picard_iterations": picard, "ksp_iterations": ksp, "converged": st["converged"],

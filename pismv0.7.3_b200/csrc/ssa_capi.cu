@@ -36,6 +36,7 @@ struct pism_gpu_ssa {
   double *beta = nullptr, *bfrict = nullptr;
   uint32_t *flags = nullptr;
   Krylov K{};
+  MGHierarchy mg{};
   double *partials = nullptr;
   unsigned *ticket = nullptr;
   double *norm_dev = nullptr;
@@ -113,6 +114,25 @@ Fields fields_of(pism_gpu_ssa *h) {
   return f;
 }
 
+// the multigrid hierarchy when it is the active preconditioner; a KSP failure switches
+// between multigrid and block Jacobi (the reference switches BJacobi -> ASM, SSAFD.cc:929-958)
+const MGHierarchy *active_mg(pism_gpu_ssa *h) {
+  bool want = h->cfg.pc_type == PISM_PC_MULTIGRID;
+  if (h->use_fallback) want = !want;
+  return (want && h->mg.nlev > 0) ? &h->mg : nullptr;
+}
+
+// preconditioner set-up after nu*H / beta changed (replaces PCSetUp)
+int pc_setup(pism_gpu_ssa *h) {
+  Fields f = fields_of(h);
+  *h->zd_host = INT_MAX;
+  CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  launch_diag_setup(h->L, h->g, f, h->K.dinv, h->zd_dev);
+  if (active_mg(h)) mg_setup(h->L, h->g, f, h->K.dinv, h->mg);
+  CK(h, cudaGetLastError());
+  return PISM_GPU_SSA_OK;
+}
+
 int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
   if (!c) return fail(h, PISM_GPU_SSA_EINVAL, "config is NULL");
   if (c->flow_law < PISM_FLOW_LAW_ISOTHERMAL_GLEN || c->flow_law > PISM_FLOW_LAW_HOOKE)
@@ -141,7 +161,8 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
   int launched = 0;
   int chunk = std::max(8, (int)(0.8 * h->last_ksp_its));
   while (true) {
-    for (int q = 0; q < chunk; ++q) launch_bicg_iteration(h->L, g, f, h->K, x);
+    const MGHierarchy *mg = active_mg(h);
+    for (int q = 0; q < chunk; ++q) launch_bicg_iteration(h->L, g, f, h->K, x, mg);
     launched += chunk;
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(h->st_host, h->K.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
@@ -163,9 +184,7 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
   Fields f = fields_of(h);
   launch_nuH(h->L, h->g, c, f, reg, 1.0, false, h->norm_dev);
   for (int k = 0; k < c.max_iterations_ssafd; ++k) {
-    *h->zd_host = INT_MAX;
-    CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    launch_diag_setup(h->L, h->g, f, h->K.dinv, h->zd_dev);
+    RET(pc_setup(h));
     int its = 0, status = 0;
     RET(linear_solve(h, h->vel, &its, &status));
     CK(h, cudaMemcpyAsync(h->zd_host, h->zd_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -375,6 +394,10 @@ int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cf
   AL(h->K.r, N); AL(h->K.rhat, N); AL(h->K.p, N); AL(h->K.v, N); AL(h->K.s, N); AL(h->K.t, N);
   AL(h->K.phat, N); AL(h->K.shat, N); AL(h->K.dinv, N); AL(h->K.st, 1);
   h->L.max_blocks = sms * 8;
+  if (mg_plan(grid->Mx, grid->My, h->mg) > 0) {
+    if (mg_allocate(h->mg, h->N) != 0) return bail(PISM_GPU_SSA_ENOMEM);
+    if (cudaMemsetAsync(h->mg.singular, 0, sizeof(int), h->stream) != cudaSuccess) return bail(PISM_GPU_SSA_ECUDA);
+  }
   AL(h->partials, (size_t)h->L.max_blocks * 8); AL(h->ticket, 1); AL(h->norm_dev, 2); AL(h->zd_dev, 1);
 #undef AL
   if (cudaMallocHost((void **)&h->st_host, sizeof(KState)) != cudaSuccess ||
@@ -415,6 +438,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
   if (h->zd_host) cudaFreeHost(h->zd_host);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  mg_free(h->mg);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return PISM_GPU_SSA_OK;
@@ -598,9 +622,7 @@ int pism_gpu_ssa_apply(pism_gpu_ssa *h, const double *x_dev, double *y_dev) {
 int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, double *rel_residual) {
   if (!h || !x_dev) return PISM_GPU_SSA_EINVAL;
   DeviceGuard dg(h->device);
-  *h->zd_host = INT_MAX;
-  CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-  launch_diag_setup(h->L, h->g, fields_of(h), h->K.dinv, h->zd_dev);
+  RET(pc_setup(h));
   int its = 0, status = 0;
   RET(linear_solve(h, (double2 *)x_dev, &its, &status));
   if (iterations) *iterations = its;

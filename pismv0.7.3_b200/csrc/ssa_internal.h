@@ -49,6 +49,38 @@ struct Launch {
   }
 };
 
+// ---- aggregation multigrid (ssa_mg.cu) ----
+constexpr int MG_MAX_LEVELS = 16;
+constexpr int MG_COARSE_DIM = 8;                 // the coarsest level has <= 8 x 8 cells
+constexpr int MG_MAX_COARSE_CELLS = MG_COARSE_DIM * MG_COARSE_DIM;
+constexpr double MG_OMEGA = 0.7;                 // damping of the block-Jacobi smoother
+constexpr double MG_CORRECTION = 1.5;            // scaling of the coarse-grid correction
+constexpr int MG_CTA_CELLS = 4096;               // levels this small are cycled by one CTA
+
+struct MGLevel {
+  int Mx = 0, My = 0, N = 0;
+  int ax = 1, ay = 1;                            // aggregation factors towards the next level
+  float4 *A = nullptr;                           // 9 stencil blocks x N (block b of cell k at b*N+k)
+  float4 *dinv = nullptr;                        // inverse 2x2 diagonal blocks
+  float2 *b = nullptr, *x = nullptr;
+};
+
+struct MGHierarchy {
+  int nlev = 0;                                  // coarse levels (level 1 .. nlev)
+  int fine_ax = 1, fine_ay = 1;                  // aggregation of the fine grid
+  MGLevel lev[MG_MAX_LEVELS];
+  int small_first = 0;                           // first level cycled by one CTA
+  double *cinv = nullptr;                        // dense inverse of the coarsest operator (transposed)
+  int *singular = nullptr;
+  float2 *nuHf = nullptr;                        // FP32 copies of the fine nu*H, beta, D^-1
+  float *betaf = nullptr;
+  float4 *dinvf = nullptr;
+};
+
+int mg_plan(int Mx, int My, MGHierarchy &H);
+int mg_allocate(MGHierarchy &H, int fine_cells);
+void mg_free(MGHierarchy &H);
+
 void launch_convert_masks(const Launch &L, int N, const double *mask, const double *bc_mask, int8_t *mask_i,
                           uint8_t *bc_i);
 void launch_prepare(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int periodicity,
@@ -61,7 +93,11 @@ void launch_apply(const Launch &L, const GridDev &g, const Fields &f, const doub
 void launch_diag_setup(const Launch &L, const GridDev &g, const Fields &f, double4 *dinv, int *zero_diag_cell);
 void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, const double2 *b,
                       const double2 *x);
-void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x);
+void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x,
+                           const MGHierarchy *mg);
+void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
+void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b,
+               double2 *z, const KState *st);
 void launch_bfrict(const Launch &L, int N, const pism_gpu_ssa_config &c, const Fields &f, double *out);
 void launch_scale(const Launch &L, int n, double a, double *x);
 

@@ -12,6 +12,7 @@
 #include <cstdio>
 
 #include "ssa_internal.h"
+#include "ssa_stencil.cuh"
 
 namespace pism_gpu {
 
@@ -475,115 +476,6 @@ __global__ void __launch_bounds__(NT) k_nuH(GridDev g, TileMap tm, pism_gpu_ssa_
   }
 }
 
-// ---------------------------------------------------------------------------
-// the SSAFD stencil (SSAFD::assemble_matrix, SSAFD.cc:540-796), matrix-free
-// ---------------------------------------------------------------------------
-struct StencilConst {
-  double rdx2, rdy2, r2, r4, scaling;   // 1/dx^2, 1/dy^2, 1/(2 dx dy), 1/(4 dx dy), m_scaling
-  double nu_bedrock;                    // nu_bedrock (used where F_NB_* flags are set)
-  const double *H;                      // thickness, read only where F_NB_* flags are set
-};
-
-// staggered coefficients of row (i, j): c_w, c_e, c_s, c_n (SSAFD.cc:556-585)
-__device__ __forceinline__ void row_coefficients(const GridDev &g, const StencilConst &s, int i, int j, uint32_t f,
-                                                 const double2 *__restrict__ nuH, double &c_w, double &c_e,
-                                                 double &c_s, double &c_n) {
-  const int k = cell(g, i, j);
-  const double2 nC = nuH[k];
-  c_w = nuH[nbr(g, i, j, -1, 0)].x;
-  c_e = nC.x;
-  c_s = nuH[nbr(g, i, j, 0, -1)].y;
-  c_n = nC.y;
-  if (f & F_NB_ANY) {
-    const double Hc = s.H[k], HE = s.H[nbr(g, i, j, 1, 0)];
-    if (f & F_NB_W) c_w = s.nu_bedrock * 0.5 * (Hc + s.H[nbr(g, i, j, -1, 0)]);
-    if (f & F_NB_E) c_e = s.nu_bedrock * 0.5 * (Hc + HE);
-    if (f & F_NB_N) c_n = s.nu_bedrock * 0.5 * (Hc + s.H[nbr(g, i, j, 0, 1)]);
-    if (f & F_NB_S) c_s = s.nu_bedrock * 0.5 * (Hc + HE);   // thickness(i+1, j), as SSAFD.cc:582
-  }
-}
-
-// the 36 row coefficients of one cell; eq1 = u-row, eq2 = v-row; positions
-// NW N NE / W C E / SW S SE
-struct Row2 {
-  double uNW, uN, uNE, uW, uC, uE, uSW, uS, uSE;
-  double vNW, vN, vNE, vW, vC, vE, vSW, vS, vSE;
-};
-
-__device__ __forceinline__ void stencil_rows(const StencilConst &s, uint32_t f, double c_w, double c_e, double c_s,
-                                             double c_n, double bta, Row2 &e1, Row2 &e2) {
-  const double aMn = (f & F_aMn) ? 1.0 : 0.0, aPn = (f & F_aPn) ? 1.0 : 0.0, aMM = (f & F_aMM) ? 1.0 : 0.0,
-               aPP = (f & F_aPP) ? 1.0 : 0.0, aMs = (f & F_aMs) ? 1.0 : 0.0, aPs = (f & F_aPs) ? 1.0 : 0.0;
-  const double bPw = (f & F_bPw) ? 1.0 : 0.0, bPP = (f & F_bPP) ? 1.0 : 0.0, bPe = (f & F_bPe) ? 1.0 : 0.0,
-               bMw = (f & F_bMw) ? 1.0 : 0.0, bMM = (f & F_bMM) ? 1.0 : 0.0, bMe = (f & F_bMe) ? 1.0 : 0.0;
-  // products of a staggered coefficient with its weights (exact: weights are 0 or 1)
-  const double w = c_w * aMM, e = c_e * aPP, sS = c_s * bMM, n = c_n * bPP;
-  const double wPw = w * bPw, wMw = w * bMw, wPP = w * bPP, wMM = w * bMM;
-  const double ePe = e * bPe, eMe = e * bMe, ePP = e * bPP, eMM = e * bMM;
-  const double nMn = n * aMn, nPn = n * aPn, nPP = n * aPP, nMM = n * aMM;
-  const double sMs = sS * aMs, sPs = sS * aPs, sPP = sS * aPP, sMM = sS * aMM;
-  const double r2 = s.r2, r4 = s.r4;
-  // first equation, u part
-  e1.uNW = 0.0; e1.uN = -n * s.rdy2; e1.uNE = 0.0;
-  e1.uW = -4 * w * s.rdx2;
-  e1.uC = (n + sS) * s.rdy2 + (4 * e + 4 * w) * s.rdx2 + bta;
-  e1.uE = -4 * e * s.rdx2;
-  e1.uSW = 0.0; e1.uS = -sS * s.rdy2; e1.uSE = 0.0;
-  // first equation, v part
-  e1.vNW = wPw * r2 + nMn * r4;
-  e1.vN = (nPn - nMn) * r4 + (wPP - ePP) * r2;
-  e1.vNE = -ePe * r2 - nPn * r4;
-  e1.vW = (wMw - wPw) * r2 + (nMM - sMM) * r4;
-  e1.vC = (nPP - nMM - sPP + sMM) * r4 + (ePP - wPP - eMM + wMM) * r2;
-  e1.vE = (ePe - eMe) * r2 + (sPP - nPP) * r4;
-  e1.vSW = -wMw * r2 - sMs * r4;
-  e1.vS = (sMs - sPs) * r4 + (eMM - wMM) * r2;
-  e1.vSE = eMe * r2 + sPs * r4;
-  // second equation, u part (cross terms with 1/d2 and 1/d4 swapped)
-  e2.uNW = wPw * r4 + nMn * r2;
-  e2.uN = (nPn - nMn) * r2 + (wPP - ePP) * r4;
-  e2.uNE = -ePe * r4 - nPn * r2;
-  e2.uW = (wMw - wPw) * r4 + (nMM - sMM) * r2;
-  e2.uC = (nPP - nMM - sPP + sMM) * r2 + (ePP - wPP - eMM + wMM) * r4;
-  e2.uE = (ePe - eMe) * r4 + (sPP - nPP) * r2;
-  e2.uSW = -wMw * r4 - sMs * r2;
-  e2.uS = (sMs - sPs) * r2 + (eMM - wMM) * r4;
-  e2.uSE = eMe * r4 + sPs * r2;
-  // second equation, v part
-  e2.vNW = 0.0; e2.vN = -4 * n * s.rdy2; e2.vNE = 0.0;
-  e2.vW = -w * s.rdx2;
-  e2.vC = (4 * n + 4 * sS) * s.rdy2 + (e + w) * s.rdx2 + bta;
-  e2.vE = -e * s.rdx2;
-  e2.vSW = 0.0; e2.vS = -4 * sS * s.rdy2; e2.vSE = 0.0;
-}
-
-// y(i, j) = (A x)(i, j)
-__device__ __forceinline__ double2 apply_cell(const GridDev &g, const StencilConst &s, int i, int j, uint32_t f,
-                                              const double2 *__restrict__ nuH, const double *__restrict__ beta,
-                                              const double2 *__restrict__ x) {
-  const int k = cell(g, i, j);
-  if (f & F_DIAG_ONLY) {
-    const double2 xc = x[k];
-    return make_double2(s.scaling * xc.x, s.scaling * xc.y);
-  }
-  const int ip = wrap(i + 1, g.Mx), im = wrap(i - 1, g.Mx), jp = wrap(j + 1, g.My), jm = wrap(j - 1, g.My);
-  const int rC = i * g.My, rE = ip * g.My, rW = im * g.My;
-  double c_w, c_e, c_s, c_n;
-  row_coefficients(g, s, i, j, f, nuH, c_w, c_e, c_s, c_n);
-  Row2 e1, e2;
-  stencil_rows(s, f, c_w, c_e, c_s, c_n, beta[k], e1, e2);
-  const double2 xNW = x[rW + jp], xN = x[rC + jp], xNE = x[rE + jp];
-  const double2 xW = x[rW + j], xC = x[k], xE = x[rE + j];
-  const double2 xSW = x[rW + jm], xS = x[rC + jm], xSE = x[rE + jm];
-  double y1 = e1.uN * xN.x + e1.uW * xW.x + e1.uC * xC.x + e1.uE * xE.x + e1.uS * xS.x;
-  y1 += e1.vNW * xNW.y + e1.vN * xN.y + e1.vNE * xNE.y + e1.vW * xW.y + e1.vC * xC.y + e1.vE * xE.y +
-        e1.vSW * xSW.y + e1.vS * xS.y + e1.vSE * xSE.y;
-  double y2 = e2.uNW * xNW.x + e2.uN * xN.x + e2.uNE * xNE.x + e2.uW * xW.x + e2.uC * xC.x + e2.uE * xE.x +
-              e2.uSW * xSW.x + e2.uS * xS.x + e2.uSE * xSE.x;
-  y2 += e2.vN * xN.y + e2.vW * xW.y + e2.vC * xC.y + e2.vE * xE.y + e2.vS * xS.y;
-  return make_double2(y1, y2);
-}
-
 // y = A x (plain apply, for checking and for the residual of the refinement)
 __global__ void __launch_bounds__(NT) k_apply(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
                                               const double2 *__restrict__ nuH, const double *__restrict__ beta,
@@ -626,11 +518,6 @@ __global__ void __launch_bounds__(NT) k_diag_setup(GridDev g, TileMap tm, Stenci
     }
   }
 }
-
-__device__ __forceinline__ double2 dmul(const double4 &m, const double2 &v) {
-  return make_double2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
-}
-__device__ __forceinline__ double dot2(const double2 &a, const double2 &b) { return a.x * b.x + a.y * b.y; }
 
 // ---------------------------------------------------------------------------
 // BiCGStab, right preconditioned by M^-1 = block-Jacobi (van der Vorst 1992),
@@ -677,7 +564,9 @@ __global__ void __launch_bounds__(NT) k_bicg_init(GridDev g, TileMap tm, Stencil
   }
 }
 
-// p = r + beta (p - omega v);  phat = M^-1 p
+// p = r + beta (p - omega v);  phat = M^-1 p (block Jacobi; with multigrid phat is
+// written by the V-cycle instead)
+template <bool JAC>
 __global__ void __launch_bounds__(NT) k_bicg_p(int N, const double2 *__restrict__ r, const double2 *__restrict__ v,
                                                const double4 *__restrict__ dinv, double2 *__restrict__ p,
                                                double2 *__restrict__ phat, const KState *st) {
@@ -687,7 +576,7 @@ __global__ void __launch_bounds__(NT) k_bicg_p(int N, const double2 *__restrict_
     const double2 rk = r[k], pk = p[k], vk = v[k];
     const double2 pn = make_double2(rk.x + bta * (pk.x - om * vk.x), rk.y + bta * (pk.y - om * vk.y));
     p[k] = pn;
-    phat[k] = dmul(dinv[k], pn);
+    if (JAC) phat[k] = dmul(dinv[k], pn);
   }
 }
 
@@ -719,6 +608,7 @@ __global__ void __launch_bounds__(NT) k_bicg_v(GridDev g, TileMap tm, StencilCon
 }
 
 // s = r - alpha v;  shat = M^-1 s
+template <bool JAC>
 __global__ void __launch_bounds__(NT) k_bicg_s(int N, const double2 *__restrict__ r, const double2 *__restrict__ v,
                                                const double4 *__restrict__ dinv, double2 *__restrict__ sv,
                                                double2 *__restrict__ shat, const KState *st) {
@@ -728,7 +618,7 @@ __global__ void __launch_bounds__(NT) k_bicg_s(int N, const double2 *__restrict_
     const double2 rk = r[k], vk = v[k];
     const double2 sk = make_double2(rk.x - al * vk.x, rk.y - al * vk.y);
     sv[k] = sk;
-    shat[k] = dmul(dinv[k], sk);
+    if (JAC) shat[k] = dmul(dinv[k], sk);
   }
 }
 
@@ -822,17 +712,6 @@ static int grid_for(const Launch &L, int n) {
   return b < L.max_blocks ? b : L.max_blocks;
 }
 
-static StencilConst stencil_const(const GridDev &g, const Fields &f) {
-  StencilConst s;
-  s.nu_bedrock = f.nu_bedrock;
-  s.H = f.H;
-  s.rdx2 = 1.0 / (g.dx * g.dx);
-  s.rdy2 = 1.0 / (g.dy * g.dy);
-  s.r2 = 1.0 / (2 * g.dx * g.dy);
-  s.r4 = 1.0 / (4 * g.dx * g.dy);
-  s.scaling = 1.0e9;
-  return s;
-}
 
 void launch_convert_masks(const Launch &L, int N, const double *mask, const double *bc_mask, int8_t *mask_i,
                           uint8_t *bc_i) {
@@ -900,16 +779,27 @@ void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const 
                                                                 x, K.r, K.rhat, K.p, K.v, L.partials, L.ticket, K.st);
 }
 
-void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x) {
+void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x,
+                           const MGHierarchy *mg) {
   L.tick(5);
   TileMap tm = make_tiles(g);
   const int N = g.Mx * g.My;
   const StencilConst s = stencil_const(g, f);
   const int bt = grid_for_tiles(L, tm.tiles), bv = grid_for(L, N);
-  k_bicg_p<<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
+  if (mg) {
+    k_bicg_p<false><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
+    mg_vcycle(L, g, f, *mg, K.p, K.phat, K.st);
+  } else {
+    k_bicg_p<true><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
+  }
   k_bicg_v<<<bt, NT, 0, L.stream>>>(g, tm, s, f.flags, f.nuH, f.beta, K.phat, K.rhat, K.v, L.partials, L.ticket,
                                     K.st);
-  k_bicg_s<<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
+  if (mg) {
+    k_bicg_s<false><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
+    mg_vcycle(L, g, f, *mg, K.s, K.shat, K.st);
+  } else {
+    k_bicg_s<true><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
+  }
   k_bicg_t<<<bt, NT, 0, L.stream>>>(g, tm, s, f.flags, f.nuH, f.beta, K.shat, K.s, K.t, L.partials, L.ticket, K.st);
   k_bicg_x<<<bv, NT, 0, L.stream>>>(N, K.phat, K.shat, K.s, K.t, K.rhat, x, K.r, L.partials, L.ticket, K.st);
 }

@@ -1,0 +1,729 @@
+// ssa_mg.cu — aggregation multigrid preconditioner for the SSAFD system (replaces the
+// reference's PETSc block-Jacobi / ILU(0) and ASM / LU preconditioners,
+// SSAFD.cc:136-219, inside the Krylov solve).  It runs in FP32: it only has to
+// approximate A^-1; the Krylov method around it, the operator and the residuals stay FP64.
+//
+// Hierarchy: level 0 is the fine SSAFD operator, applied matrix-free from an FP32 copy of
+// nu*H and beta (refreshed once per Picard iteration) and the flag word.  Level l+1
+// aggregates 2 x 2 cells of level l (1 in a direction that is already <= 8 cells) and
+// carries the Galerkin operator R A P with piecewise-constant P (R = P^T): the sum, over
+// the aggregate, of the fine 2 x 2 blocks grouped by the neighbouring aggregate they
+// couple to.  With a 3 x 3 fine stencil this is again a 3 x 3 stencil of 2 x 2 blocks,
+// stored as 9 float4 arrays (one per block) so that a warp reads 512 contiguous bytes per
+// block.  The coarsest level (<= 8 x 8 cells) is inverted densely in FP64.
+//
+// Cycle (a V(1,1) cycle used as a fixed preconditioner z = M^-1 b):
+//   x_l = omega D_l^-1 b_l                       (computed on the fly, never stored)
+//   b_{l+1} = R (b_l - A_l x_l)                  (restriction kernel)
+//   ...  x_L = A_L^-1 b_L                        (dense inverse)
+//   x_l <- x_l + s P x_{l+1};  x_l <- x_l + omega D_l^-1 (b_l - A_l x_l)   (post kernel)
+// so each level costs two stencil passes.  Levels of <= MG_CTA_CELLS cells are cycled by
+// one CTA in one launch (their kernels would be launch- and latency-bound).
+// omega = 0.7 and s = 1.5 (over-correction, compensating the piecewise-constant
+// interpolation) were chosen on SSA matrices of the synthetic ice sheet at 201^2 and
+// 401^2 (BiCGStab iterations 108 -> 15 and 190 -> 19 against point-block Jacobi).
+#include <algorithm>
+#include <cstdio>
+
+#include "ssa_internal.h"
+#include "ssa_stencil.cuh"
+
+namespace pism_gpu {
+
+namespace {
+
+constexpr int TJm = 32, TIm = 8, NTm = TJm * TIm;
+constexpr int CTA_THREADS = 1024;
+
+struct TileM {
+  int tiles_j, tiles;
+};
+
+TileM tiles_of(int Mx, int My) {
+  TileM t;
+  t.tiles_j = (My + TJm - 1) / TJm;
+  t.tiles = t.tiles_j * ((Mx + TIm - 1) / TIm);
+  return t;
+}
+
+__device__ __forceinline__ bool tile_cell(const TileM &tm, int Mx, int My, int t, int &i, int &j) {
+  const int ti = t / tm.tiles_j, tj = t - ti * tm.tiles_j;
+  j = tj * TJm + (threadIdx.x & (TJm - 1));
+  i = ti * TIm + (threadIdx.x >> 5);
+  return i < Mx && j < My;
+}
+
+__device__ __forceinline__ int wdiff(int a, int b, int n) {
+  int d = a - b;
+  if (d > 1) d -= n;
+  if (d < -1) d += n;
+  return d;
+}
+
+// stencil block index of the offset (di, dj): NW N NE / W C E / SW S SE
+__host__ __device__ __forceinline__ int blk_of(int di, int dj) { return (1 - dj) * 3 + (di + 1); }
+
+__device__ __forceinline__ float4 inv2x2(float a11, float a12, float a21, float a22) {
+  const float det = a11 * a22 - a12 * a21;
+  if (det != 0.0f && isfinite(det)) {
+    const float r = 1.0f / det;
+    return make_float4(a22 * r, -a12 * r, -a21 * r, a11 * r);
+  }
+  return make_float4(a11 != 0.0f ? 1.0f / a11 : 0.0f, 0.0f, 0.0f, a22 != 0.0f ? 1.0f / a22 : 0.0f);
+}
+
+__device__ __forceinline__ float2 fmul4(const float4 &m, const float2 &v) {
+  return make_float2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
+}
+
+struct LevelView {
+  int Mx, My, N, ax, ay;
+  const float4 *A;     // 9 blocks x N: block b of cell k at A[b * N + k]
+  const float4 *dinv;
+  float2 *b, *x;
+};
+
+// y = A_l x at (i, j), x read through xa(i', j')
+template <class XA>
+__device__ __forceinline__ float2 coarse_apply(const LevelView &L, int i, int j, const XA &xa) {
+  const int k = i * L.My + j;
+  const int ip = wrap(i + 1, L.Mx), im = wrap(i - 1, L.Mx), jp = wrap(j + 1, L.My), jm = wrap(j - 1, L.My);
+  const int ii[9] = {im, i, ip, im, i, ip, im, i, ip};
+  const int jj[9] = {jp, jp, jp, j, j, j, jm, jm, jm};
+  float4 a[9];
+#pragma unroll
+  for (int b = 0; b < 9; ++b) a[b] = L.A[b * L.N + k];
+  float y1 = 0.0f, y2 = 0.0f;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const float2 xv = xa(ii[b], jj[b]);
+    y1 += a[b].x * xv.x + a[b].y * xv.y;
+    y2 += a[b].z * xv.x + a[b].w * xv.y;
+  }
+  return make_float2(y1, y2);
+}
+
+// ---------------------------------------------------------------------------
+// fine-level FP32 data (once per Picard iteration)
+// ---------------------------------------------------------------------------
+struct FineF {
+  GridDev g;
+  float rdx2, rdy2, r2, r4, scaling, nu_bedrock;
+  const uint32_t *flags;
+  const float2 *nuH;    // FP32 nu*H
+  const float *beta;    // FP32 beta
+  const float4 *dinv;   // FP32 inverse diagonal blocks
+  const double *H;      // thickness, read only where F_NB_* flags are set
+};
+
+__global__ void k_mg0_compact(int N, const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                              const double4 *__restrict__ dinv, float2 *__restrict__ nuHf, float *__restrict__ betaf,
+                              float4 *__restrict__ dinvf) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 n = nuH[k];
+    const double4 d = dinv[k];
+    nuHf[k] = make_float2((float)n.x, (float)n.y);
+    betaf[k] = (float)beta[k];
+    dinvf[k] = make_float4((float)d.x, (float)d.y, (float)d.z, (float)d.w);
+  }
+}
+
+// the two FP32 rows of fine cell (i, j); false for a diagonal-only row
+__device__ __forceinline__ bool fine_rows(const FineF &F, int i, int j, uint32_t f, Row2T<float> &e1,
+                                          Row2T<float> &e2) {
+  if (f & F_DIAG_ONLY) return false;
+  const GridDev &g = F.g;
+  const int k = cell(g, i, j);
+  const float2 nC = F.nuH[k];
+  float c_w = F.nuH[nbr(g, i, j, -1, 0)].x, c_e = nC.x, c_s = F.nuH[nbr(g, i, j, 0, -1)].y, c_n = nC.y;
+  if (f & F_NB_ANY) {   // nu_bedrock_set overrides, SSAFD.cc:561-585
+    const double Hc = F.H[k], HE = F.H[nbr(g, i, j, 1, 0)];
+    if (f & F_NB_W) c_w = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, -1, 0)]));
+    if (f & F_NB_E) c_e = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
+    if (f & F_NB_N) c_n = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, 0, 1)]));
+    if (f & F_NB_S) c_s = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
+  }
+  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, F.beta[k], e1, e2);
+  return true;
+}
+
+template <class XA>
+__device__ __forceinline__ float2 fine_apply(const FineF &F, int i, int j, const XA &xa) {
+  const uint32_t f = F.flags[cell(F.g, i, j)];
+  Row2T<float> e1, e2;
+  if (!fine_rows(F, i, j, f, e1, e2)) {
+    const float2 xc = xa(i, j);
+    return make_float2(F.scaling * xc.x, F.scaling * xc.y);
+  }
+  const int ip = wrap(i + 1, F.g.Mx), im = wrap(i - 1, F.g.Mx), jp = wrap(j + 1, F.g.My), jm = wrap(j - 1, F.g.My);
+  const float2 xNW = xa(im, jp), xN = xa(i, jp), xNE = xa(ip, jp);
+  const float2 xW = xa(im, j), xC = xa(i, j), xE = xa(ip, j);
+  const float2 xSW = xa(im, jm), xS = xa(i, jm), xSE = xa(ip, jm);
+  float y1 = e1.uN * xN.x + e1.uW * xW.x + e1.uC * xC.x + e1.uE * xE.x + e1.uS * xS.x;
+  y1 += e1.vNW * xNW.y + e1.vN * xN.y + e1.vNE * xNE.y + e1.vW * xW.y + e1.vC * xC.y + e1.vE * xE.y +
+        e1.vSW * xSW.y + e1.vS * xS.y + e1.vSE * xSE.y;
+  float y2 = e2.uNW * xNW.x + e2.uN * xN.x + e2.uNE * xNE.x + e2.uW * xW.x + e2.uC * xC.x + e2.uE * xE.x +
+             e2.uSW * xSW.x + e2.uS * xS.x + e2.uSE * xSE.x;
+  y2 += e2.vN * xN.y + e2.vW * xW.y + e2.vC * xC.y + e2.vE * xE.y + e2.vS * xS.y;
+  return make_float2(y1, y2);
+}
+
+// ---------------------------------------------------------------------------
+// set-up: Galerkin coarse operators
+// ---------------------------------------------------------------------------
+// level 1 from the fine operator (FP64 rows, FP64 accumulation in shared memory)
+__global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, const uint32_t *__restrict__ flags,
+                                                   const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                                   int ax, int ay, int Mxc, int Myc, TileM tm, float4 *Ac,
+                                                   float4 *dinvc) {
+  extern __shared__ double acc_sh[];   // [36][NTm]
+  double *acc = acc_sh + threadIdx.x;
+  const int Nc = Mxc * Myc;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int I, J;
+    if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
+    for (int q = 0; q < 36; ++q) acc[q * NTm] = 0.0;
+    for (int pi = 0; pi < ax; ++pi)
+      for (int pj = 0; pj < ay; ++pj) {
+        const int i = I * ax + pi, j = J * ay + pj;
+        if (i >= g.Mx || j >= g.My) continue;
+        const uint32_t f = flags[cell(g, i, j)];
+        Row2 e1, e2;
+        if (!cell_rows(g, s, i, j, f, nuH, beta, e1, e2)) {
+          const int cb = blk_of(0, 0);
+          acc[(4 * cb + 0) * NTm] += s.scaling;
+          acc[(4 * cb + 3) * NTm] += s.scaling;
+          continue;
+        }
+        const double r1u[9] = {e1.uNW, e1.uN, e1.uNE, e1.uW, e1.uC, e1.uE, e1.uSW, e1.uS, e1.uSE};
+        const double r1v[9] = {e1.vNW, e1.vN, e1.vNE, e1.vW, e1.vC, e1.vE, e1.vSW, e1.vS, e1.vSE};
+        const double r2u[9] = {e2.uNW, e2.uN, e2.uNE, e2.uW, e2.uC, e2.uE, e2.uSW, e2.uS, e2.uSE};
+        const double r2v[9] = {e2.vNW, e2.vN, e2.vNE, e2.vW, e2.vC, e2.vE, e2.vSW, e2.vS, e2.vSE};
+#pragma unroll
+        for (int b = 0; b < 9; ++b) {
+          const int di = (b % 3) - 1, dj = 1 - (b / 3);
+          const int ni = wrap(i + di, g.Mx), nj = wrap(j + dj, g.My);
+          const int cb = blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc));
+          acc[(4 * cb + 0) * NTm] += r1u[b];
+          acc[(4 * cb + 1) * NTm] += r1v[b];
+          acc[(4 * cb + 2) * NTm] += r2u[b];
+          acc[(4 * cb + 3) * NTm] += r2v[b];
+        }
+      }
+    const int kc = I * Myc + J;
+    for (int b = 0; b < 9; ++b)
+      Ac[b * Nc + kc] = make_float4((float)acc[(4 * b) * NTm], (float)acc[(4 * b + 1) * NTm],
+                                    (float)acc[(4 * b + 2) * NTm], (float)acc[(4 * b + 3) * NTm]);
+    dinvc[kc] = inv2x2((float)acc[16 * NTm], (float)acc[17 * NTm], (float)acc[18 * NTm], (float)acc[19 * NTm]);
+  }
+}
+
+// level l+1 from the stored operator of level l
+__global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc, TileM tm, float4 *Ac, float4 *dinvc) {
+  extern __shared__ double acc_sh[];
+  double *acc = acc_sh + threadIdx.x;
+  const int Nc = Mxc * Myc, ax = F.ax, ay = F.ay;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int I, J;
+    if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
+    for (int q = 0; q < 36; ++q) acc[q * NTm] = 0.0;
+    for (int pi = 0; pi < ax; ++pi)
+      for (int pj = 0; pj < ay; ++pj) {
+        const int i = I * ax + pi, j = J * ay + pj;
+        if (i >= F.Mx || j >= F.My) continue;
+        const int k = i * F.My + j;
+#pragma unroll
+        for (int b = 0; b < 9; ++b) {
+          const int di = (b % 3) - 1, dj = 1 - (b / 3);
+          const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
+          const int cb = blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc));
+          const float4 a = F.A[b * F.N + k];
+          acc[(4 * cb + 0) * NTm] += (double)a.x;
+          acc[(4 * cb + 1) * NTm] += (double)a.y;
+          acc[(4 * cb + 2) * NTm] += (double)a.z;
+          acc[(4 * cb + 3) * NTm] += (double)a.w;
+        }
+      }
+    const int kc = I * Myc + J;
+    for (int b = 0; b < 9; ++b)
+      Ac[b * Nc + kc] = make_float4((float)acc[(4 * b) * NTm], (float)acc[(4 * b + 1) * NTm],
+                                    (float)acc[(4 * b + 2) * NTm], (float)acc[(4 * b + 3) * NTm]);
+    dinvc[kc] = inv2x2((float)acc[16 * NTm], (float)acc[17 * NTm], (float)acc[18 * NTm], (float)acc[19 * NTm]);
+  }
+}
+
+// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial
+// pivoting, in place in shared memory (n <= 2 * 64), one CTA; written transposed so
+// that the per-cycle product reads it coalesced.  Rows are spread over 8-lane groups.
+__global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
+  extern __shared__ double a[];   // n * n, row-major
+  const int n = 2 * L.N;
+  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
+  __shared__ int piv_row;
+  const int t = threadIdx.x, lane8 = t & 7, grp = t >> 3, ngrp = CTA_THREADS >> 3;
+  for (int q = t; q < n * n; q += CTA_THREADS) a[q] = 0.0;
+  __syncthreads();
+  if (t < L.N) {   // each cell's two rows are written by one thread
+    const int k = t, i = k / L.My, j = k % L.My;
+    for (int b = 0; b < 9; ++b) {
+      const int di = (b % 3) - 1, dj = 1 - (b / 3);
+      const int kn = wrap(i + di, L.Mx) * L.My + wrap(j + dj, L.My);
+      const float4 v = L.A[b * L.N + k];
+      a[(2 * k + 0) * n + 2 * kn + 0] += (double)v.x;
+      a[(2 * k + 0) * n + 2 * kn + 1] += (double)v.y;
+      a[(2 * k + 1) * n + 2 * kn + 0] += (double)v.z;
+      a[(2 * k + 1) * n + 2 * kn + 1] += (double)v.w;
+    }
+  }
+  __syncthreads();
+  for (int col = 0; col < n; ++col) {
+    if (t < 32) {   // pivot search by warp 0
+      double best = -1.0;
+      int bi = col;
+      for (int r = col + t; r < n; r += 32) {
+        const double v = fabs(a[r * n + col]);
+        if (v > best) { best = v; bi = r; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (t == 0) {
+        piv_row = bi;
+        perm[col] = bi;
+        if (!(best > 0.0)) *singular = 1;
+      }
+    }
+    __syncthreads();
+    const int p = piv_row;
+    if (p != col)
+      for (int q = t; q < n; q += CTA_THREADS) {
+        const double tmp = a[col * n + q];
+        a[col * n + q] = a[p * n + q];
+        a[p * n + q] = tmp;
+      }
+    __syncthreads();
+    const double pv = a[col * n + col];
+    const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
+    __syncthreads();
+    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
+    for (int q = t; q < n; q += CTA_THREADS) a[col * n + q] = (q == col ? 1.0 : a[col * n + q]) * pinv;
+    __syncthreads();
+    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
+    for (int r = grp; r < n; r += ngrp) {
+      if (r == col) continue;
+      const double f = a[r * n + col];
+      for (int q = lane8; q < n; q += 8)
+        if (q != col) a[r * n + q] -= f * a[col * n + q];
+    }
+    __syncthreads();
+    for (int r = t; r < n; r += CTA_THREADS)
+      if (r != col) a[r * n + col] = -a[r * n + col] * a[col * n + col];
+    __syncthreads();
+  }
+  // undo the row interchanges as column interchanges, in reverse order
+  for (int col = n - 1; col >= 0; --col) {
+    const int p = perm[col];
+    if (p != col)
+      for (int r = t; r < n; r += CTA_THREADS) {
+        const double tmp = a[r * n + col];
+        a[r * n + col] = a[r * n + p];
+        a[r * n + p] = tmp;
+      }
+    __syncthreads();
+  }
+  for (int q = t; q < n * n; q += CTA_THREADS) {
+    const int r = q / n, c = q - r * n;
+    invT_out[c * n + r] = a[q];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle kernels
+// ---------------------------------------------------------------------------
+// fine level: b_1 = R (b - A x0), x0 = omega D^-1 b on the fly; one thread per aggregate
+template <int AX, int AY>
+__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__restrict__ b, float omega, int Mxc,
+                                                      int Myc, TileM tm, float2 *__restrict__ bc, const KState *st) {
+  if (st && st->done) return;
+  const GridDev &g = F.g;
+  auto xa = [&](int ii, int jj) {
+    const int q = ii * g.My + jj;
+    const double2 bd = b[q];
+    const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
+    return make_float2(omega * v.x, omega * v.y);
+  };
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int I, J;
+    if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
+    float ru = 0.0f, rv = 0.0f;
+#pragma unroll
+    for (int pi = 0; pi < AX; ++pi)
+#pragma unroll
+      for (int pj = 0; pj < AY; ++pj) {
+        const int i = I * AX + pi, j = J * AY + pj;
+        if (i < g.Mx && j < g.My) {
+          const float2 y = fine_apply(F, i, j, xa);
+          const double2 bk = b[i * g.My + j];
+          ru += (float)bk.x - y.x;
+          rv += (float)bk.y - y.y;
+        }
+      }
+    bc[I * Myc + J] = make_float2(ru, rv);
+  }
+}
+
+// fine level: x = omega D^-1 b + s P x_1;  z = x + omega D^-1 (b - A x)
+template <int AX, int AY>
+__global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const double2 *__restrict__ b, float omega, float corr,
+                                                  int Myc, const float2 *__restrict__ xc, TileM tm,
+                                                  double2 *__restrict__ z, const KState *st) {
+  if (st && st->done) return;
+  const GridDev &g = F.g;
+  auto xa = [&](int ii, int jj) {
+    const int q = ii * g.My + jj;
+    const double2 bd = b[q];
+    const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
+    const float2 c = xc[(ii / AX) * Myc + jj / AY];
+    return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+  };
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tile_cell(tm, g.Mx, g.My, t, i, j)) continue;
+    const int k = cell(g, i, j);
+    const float2 xk = xa(i, j);
+    const float2 y = fine_apply(F, i, j, xa);
+    const double2 bk = b[k];
+    const float2 d = fmul4(F.dinv[k], make_float2((float)bk.x - y.x, (float)bk.y - y.y));
+    z[k] = make_double2((double)(xk.x + omega * d.x), (double)(xk.y + omega * d.y));
+  }
+}
+
+// coarse level l: b_{l+1} = R (b_l - A_l x0), x0 = omega D^-1 b_l
+template <int AX, int AY>
+__global__ void __launch_bounds__(NTm) k_mgc_restrict(LevelView L, float omega, int Mxc, int Myc, TileM tm,
+                                                      float2 *__restrict__ bc, const KState *st) {
+  if (st && st->done) return;
+  auto xa = [&](int ii, int jj) {
+    const int q = ii * L.My + jj;
+    const float2 v = fmul4(L.dinv[q], L.b[q]);
+    return make_float2(omega * v.x, omega * v.y);
+  };
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int I, J;
+    if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
+    float ru = 0.0f, rv = 0.0f;
+#pragma unroll
+    for (int pi = 0; pi < AX; ++pi)
+#pragma unroll
+      for (int pj = 0; pj < AY; ++pj) {
+        const int i = I * AX + pi, j = J * AY + pj;
+        if (i < L.Mx && j < L.My) {
+          const float2 y = coarse_apply(L, i, j, xa);
+          const float2 bk = L.b[i * L.My + j];
+          ru += bk.x - y.x;
+          rv += bk.y - y.y;
+        }
+      }
+    bc[I * Myc + J] = make_float2(ru, rv);
+  }
+}
+
+// coarse level l: x = omega D^-1 b + s P x_{l+1};  x <- x + omega D^-1 (b - A x)
+template <int AX, int AY>
+__global__ void __launch_bounds__(NTm) k_mgc_post(LevelView L, float omega, float corr, int Myc,
+                                                  const float2 *__restrict__ xc, TileM tm, const KState *st) {
+  if (st && st->done) return;
+  auto xa = [&](int ii, int jj) {
+    const int q = ii * L.My + jj;
+    const float2 v = fmul4(L.dinv[q], L.b[q]);
+    const float2 c = xc[(ii / AX) * Myc + jj / AY];
+    return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+  };
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!tile_cell(tm, L.Mx, L.My, t, i, j)) continue;
+    const int k = i * L.My + j;
+    const float2 xk = xa(i, j);
+    const float2 y = coarse_apply(L, i, j, xa);
+    const float2 bk = L.b[k];
+    const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+    L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+  }
+}
+
+// The small levels (first .. last, <= MG_CTA_CELLS cells each) in one CTA: restrictions
+// down, the dense solve, post-smoothing up; __syncthreads between the steps.
+struct SmallLevels {
+  int first, last;   // level indices into lev[]
+  LevelView lev[MG_MAX_LEVELS];
+  const double *invT;
+  int n;             // unknowns of the coarsest level
+};
+
+__global__ void __launch_bounds__(CTA_THREADS) k_mg_small_cycle(SmallLevels S, float omega, float corr,
+                                                                const KState *st) {
+  if (st && st->done) return;
+  __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
+  // down
+  for (int l = S.first; l < S.last; ++l) {
+    const LevelView &L = S.lev[l], &C = S.lev[l + 1];
+    auto xa = [&](int ii, int jj) {
+      const int q = ii * L.My + jj;
+      const float2 v = fmul4(L.dinv[q], L.b[q]);
+      return make_float2(omega * v.x, omega * v.y);
+    };
+    for (int kc = threadIdx.x; kc < C.N; kc += CTA_THREADS) {
+      const int I = kc / C.My, J = kc - I * C.My;
+      float ru = 0.0f, rv = 0.0f;
+      for (int pi = 0; pi < L.ax; ++pi)
+        for (int pj = 0; pj < L.ay; ++pj) {
+          const int i = I * L.ax + pi, j = J * L.ay + pj;
+          if (i >= L.Mx || j >= L.My) continue;
+          const float2 y = coarse_apply(L, i, j, xa);
+          const float2 bk = L.b[i * L.My + j];
+          ru += bk.x - y.x;
+          rv += bk.y - y.y;
+        }
+      C.b[kc] = make_float2(ru, rv);
+    }
+    __syncthreads();
+  }
+  // coarsest: x = A^-1 b
+  {
+    const LevelView &C = S.lev[S.last];
+    for (int q = threadIdx.x; q < C.N; q += CTA_THREADS) {
+      const float2 v = C.b[q];
+      bsh[2 * q] = v.x;
+      bsh[2 * q + 1] = v.y;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < S.n; r += CTA_THREADS) {
+      double acc = 0.0;
+      for (int c = 0; c < S.n; ++c) acc += S.invT[c * S.n + r] * (double)bsh[c];
+      reinterpret_cast<float *>(C.x)[r] = (float)acc;
+    }
+    __syncthreads();
+  }
+  // up
+  for (int l = S.last - 1; l >= S.first; --l) {
+    const LevelView &L = S.lev[l], &C = S.lev[l + 1];
+    auto xa = [&](int ii, int jj) {
+      const int q = ii * L.My + jj;
+      const float2 v = fmul4(L.dinv[q], L.b[q]);
+      const float2 c = C.x[(ii / L.ax) * C.My + jj / L.ay];
+      return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+    };
+    for (int k = threadIdx.x; k < L.N; k += CTA_THREADS) {
+      const int i = k / L.My, j = k - i * L.My;
+      const float2 xk = xa(i, j);
+      const float2 y = coarse_apply(L, i, j, xa);
+      const float2 bk = L.b[k];
+      const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+      L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int mg_plan(int Mx, int My, MGHierarchy &H) {
+  H.nlev = 0;
+  int mx = Mx, my = My;
+  if (mx <= MG_COARSE_DIM && my <= MG_COARSE_DIM) return 0;   // too small for a hierarchy
+  H.fine_ax = mx > MG_COARSE_DIM ? 2 : 1;
+  H.fine_ay = my > MG_COARSE_DIM ? 2 : 1;
+  mx = (mx + H.fine_ax - 1) / H.fine_ax;
+  my = (my + H.fine_ay - 1) / H.fine_ay;
+  while (H.nlev < MG_MAX_LEVELS) {
+    MGLevel &L = H.lev[H.nlev++];
+    L.Mx = mx;
+    L.My = my;
+    L.N = mx * my;
+    if (mx <= MG_COARSE_DIM && my <= MG_COARSE_DIM) break;
+    L.ax = mx > MG_COARSE_DIM ? 2 : 1;
+    L.ay = my > MG_COARSE_DIM ? 2 : 1;
+    mx = (mx + L.ax - 1) / L.ax;
+    my = (my + L.ay - 1) / L.ay;
+  }
+  MGLevel &C = H.lev[H.nlev - 1];
+  if (C.Mx > MG_COARSE_DIM || C.My > MG_COARSE_DIM) {   // ran out of levels
+    H.nlev = 0;
+    return 0;
+  }
+  C.ax = C.ay = 1;
+  // the levels cycled by one CTA: the trailing run of levels with <= MG_CTA_CELLS cells
+  H.small_first = H.nlev - 1;
+  while (H.small_first > 0 && H.lev[H.small_first - 1].N <= MG_CTA_CELLS) --H.small_first;
+  return H.nlev;
+}
+
+int mg_allocate(MGHierarchy &H, int fine_cells) {
+  for (int l = 0; l < H.nlev; ++l) {
+    MGLevel &L = H.lev[l];
+    if (cudaMalloc(&L.A, sizeof(float4) * 9 * L.N) != cudaSuccess) return 1;
+    if (cudaMalloc(&L.dinv, sizeof(float4) * L.N) != cudaSuccess) return 1;
+    if (cudaMalloc(&L.b, sizeof(float2) * L.N) != cudaSuccess) return 1;
+    if (cudaMalloc(&L.x, sizeof(float2) * L.N) != cudaSuccess) return 1;
+  }
+  if (cudaMalloc(&H.nuHf, sizeof(float2) * fine_cells) != cudaSuccess) return 1;
+  if (cudaMalloc(&H.betaf, sizeof(float) * fine_cells) != cudaSuccess) return 1;
+  if (cudaMalloc(&H.dinvf, sizeof(float4) * fine_cells) != cudaSuccess) return 1;
+  const int n = 2 * H.lev[H.nlev - 1].N;
+  if (cudaMalloc(&H.cinv, sizeof(double) * n * n) != cudaSuccess) return 1;
+  if (cudaMalloc(&H.singular, sizeof(int)) != cudaSuccess) return 1;
+  if (cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(double) * n * n)) != cudaSuccess)
+    return 1;
+  if (cudaFuncSetAttribute(k_mg_build1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(double) * 36 * NTm)) != cudaSuccess)
+    return 1;
+  if (cudaFuncSetAttribute(k_mg_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(double) * 36 * NTm)) != cudaSuccess)
+    return 1;
+  return 0;
+}
+
+void mg_free(MGHierarchy &H) {
+  for (int l = 0; l < MG_MAX_LEVELS; ++l) {
+    MGLevel &L = H.lev[l];
+    cudaFree(L.A);
+    cudaFree(L.dinv);
+    cudaFree(L.b);
+    cudaFree(L.x);
+    L.A = nullptr;
+    L.dinv = nullptr;
+    L.b = L.x = nullptr;
+  }
+  cudaFree(H.nuHf);
+  cudaFree(H.betaf);
+  cudaFree(H.dinvf);
+  cudaFree(H.cinv);
+  cudaFree(H.singular);
+  H.nuHf = nullptr;
+  H.betaf = nullptr;
+  H.dinvf = nullptr;
+  H.cinv = nullptr;
+  H.singular = nullptr;
+  H.nlev = 0;
+}
+
+static LevelView view(const MGLevel &L) { return LevelView{L.Mx, L.My, L.N, L.ax, L.ay, L.A, L.dinv, L.b, L.x}; }
+
+static int blocks_for(const Launch &Lc, int tiles) { return std::min(tiles, Lc.max_blocks); }
+
+static FineF fine_view(const GridDev &g, const Fields &f, const MGHierarchy &H) {
+  FineF F;
+  F.g = g;
+  F.rdx2 = (float)(1.0 / (g.dx * g.dx));
+  F.rdy2 = (float)(1.0 / (g.dy * g.dy));
+  F.r2 = (float)(1.0 / (2 * g.dx * g.dy));
+  F.r4 = (float)(1.0 / (4 * g.dx * g.dy));
+  F.scaling = 1.0e9f;
+  F.nu_bedrock = (float)f.nu_bedrock;
+  F.flags = f.flags;
+  F.nuH = H.nuHf;
+  F.beta = H.betaf;
+  F.dinv = H.dinvf;
+  F.H = f.H;
+  return F;
+}
+
+void mg_setup(const Launch &Lc, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H) {
+  const StencilConst s = stencil_const(g, f);
+  const size_t smem = sizeof(double) * 36 * NTm;
+  const int N = g.Mx * g.My;
+  k_mg0_compact<<<std::min((N + NTm - 1) / NTm, Lc.max_blocks), NTm, 0, Lc.stream>>>(N, f.nuH, f.beta, dinv0, H.nuHf,
+                                                                                     H.betaf, H.dinvf);
+  {
+    const MGLevel &C = H.lev[0];
+    const TileM tm = tiles_of(C.Mx, C.My);
+    k_mg_build1<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(g, s, f.flags, f.nuH, f.beta, H.fine_ax,
+                                                                     H.fine_ay, C.Mx, C.My, tm, C.A, C.dinv);
+  }
+  for (int l = 0; l + 1 < H.nlev; ++l) {
+    const MGLevel &F = H.lev[l], &C = H.lev[l + 1];
+    const TileM tm = tiles_of(C.Mx, C.My);
+    k_mg_build<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(view(F), C.Mx, C.My, tm, C.A, C.dinv);
+  }
+  const MGLevel &C = H.lev[H.nlev - 1];
+  const int n = 2 * C.N;
+  k_mg_coarse_invert<<<1, CTA_THREADS, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
+  Lc.tick(H.nlev + 2);
+}
+
+template <class F22, class F21, class F12, class F11>
+static void dispatch_ax(int ax, int ay, F22 f22, F21 f21, F12 f12, F11 f11) {
+  if (ax == 2 && ay == 2) f22();
+  else if (ax == 2) f21();
+  else if (ay == 2) f12();
+  else f11();
+}
+
+void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b, double2 *z,
+               const KState *st) {
+  const FineF F = fine_view(g, f, H);
+  const float omega = (float)MG_OMEGA, corr = (float)MG_CORRECTION;
+  int launches = 0;
+  // down: fine -> level 1
+  {
+    const MGLevel &C = H.lev[0];
+    const TileM tm = tiles_of(C.Mx, C.My);
+    const int nb = blocks_for(Lc, tm.tiles);
+#define MG0R(AX, AY) [&] { k_mg0_restrict<AX, AY><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, C.Mx, C.My, tm, C.b, st); }
+    dispatch_ax(H.fine_ax, H.fine_ay, MG0R(2, 2), MG0R(2, 1), MG0R(1, 2), MG0R(1, 1));
+#undef MG0R
+    ++launches;
+  }
+  // down through the large coarse levels
+  for (int l = 0; l < H.small_first; ++l) {
+    const MGLevel &L = H.lev[l], &C = H.lev[l + 1];
+    const LevelView V = view(L);
+    const TileM tm = tiles_of(C.Mx, C.My);
+    const int nb = blocks_for(Lc, tm.tiles);
+#define MGCR(AX, AY) [&] { k_mgc_restrict<AX, AY><<<nb, NTm, 0, Lc.stream>>>(V, omega, C.Mx, C.My, tm, C.b, st); }
+    dispatch_ax(L.ax, L.ay, MGCR(2, 2), MGCR(2, 1), MGCR(1, 2), MGCR(1, 1));
+#undef MGCR
+    ++launches;
+  }
+  // the small levels in one CTA
+  {
+    SmallLevels S;
+    S.first = H.small_first;
+    S.last = H.nlev - 1;
+    for (int l = 0; l < H.nlev; ++l) S.lev[l] = view(H.lev[l]);
+    S.invT = H.cinv;
+    S.n = 2 * H.lev[H.nlev - 1].N;
+    k_mg_small_cycle<<<1, CTA_THREADS, 0, Lc.stream>>>(S, omega, corr, st);
+    ++launches;
+  }
+  // up through the large coarse levels
+  for (int l = H.small_first - 1; l >= 0; --l) {
+    const MGLevel &L = H.lev[l], &C = H.lev[l + 1];
+    const LevelView V = view(L);
+    const TileM tm = tiles_of(L.Mx, L.My);
+    const int nb = blocks_for(Lc, tm.tiles);
+#define MGCP(AX, AY) [&] { k_mgc_post<AX, AY><<<nb, NTm, 0, Lc.stream>>>(V, omega, corr, C.My, C.x, tm, st); }
+    dispatch_ax(L.ax, L.ay, MGCP(2, 2), MGCP(2, 1), MGCP(1, 2), MGCP(1, 1));
+#undef MGCP
+    ++launches;
+  }
+  // fine level
+  {
+    const MGLevel &C = H.lev[0];
+    const TileM tm = tiles_of(g.Mx, g.My);
+    const int nb = blocks_for(Lc, tm.tiles);
+#define MG0P(AX, AY) [&] { k_mg0_post<AX, AY><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, st); }
+    dispatch_ax(H.fine_ax, H.fine_ay, MG0P(2, 2), MG0P(2, 1), MG0P(1, 2), MG0P(1, 1));
+#undef MG0P
+    ++launches;
+  }
+  Lc.tick(launches);
+}
+
+}  // namespace pism_gpu

@@ -122,11 +122,13 @@ def test_hardness_from_enthalpy(law):
     s.close()
 
 
-def test_linear_solve_matches_direct():
+@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
+def test_linear_solve_matches_direct(pc):
     """One KSPSolve at the first Picard step (zero velocity: plastic drag 1e14, the worst
     conditioning of the solve).  Both answers must have tiny true residuals and agree."""
     g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=3)
     c.ksp_rtol = 1e-14
+    c.pc_type = pc
     G, Cc, I = O.from_case(g, c, f)
     s = make_solver(g, c, f)
     s.assemble_rhs()
@@ -181,9 +183,11 @@ def _solve_case(g, c, f):
     return vel, st
 
 
+@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
 @pytest.mark.parametrize("My", [61, 121])
-def test_verification_i(goldens, My):
+def test_verification_i(goldens, My, pc):
     g, c, f = V.build_test_i(My=My)
+    c.pc_type = pc
     c.ssafd_relative_convergence = 5e-7
     c.ksp_rtol = 1e-12
     vel, st = _solve_case(g, c, f)
@@ -196,9 +200,11 @@ def test_verification_i(goldens, My):
     assert rel(vel, ref) < 1e-8
 
 
+@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
 @pytest.mark.parametrize("Mx", [201, 401])
-def test_verification_v_cfbc(goldens, Mx):
+def test_verification_v_cfbc(goldens, Mx, pc):
     g, c, f = V.build_test_v(Mx)
+    c.pc_type = pc
     c.ksp_rtol = 1e-13
     vel, st = _solve_case(g, c, f)
     case = [k for k in goldens["test_v_cfbc"]["cases"] if k["Mx"] == Mx][0]
@@ -209,11 +215,13 @@ def test_verification_v_cfbc(goldens, Mx):
     assert rel(vel, ref) < 1e-8
 
 
+@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
 @pytest.mark.parametrize("M", [61, 121])
-def test_verification_j(M):
+def test_verification_j(M, pc):
     """Test J with a tight KSP equals the oracle's direct solve (the golden itself
     records PETSc's rtol-1e-5 iterate; the CPU suite pins that)."""
     g, c, f = V.build_test_j(M, M)
+    c.pc_type = pc
     c.ksp_rtol = 1e-13
     vel, st = _solve_case(g, c, f)
     ref = O.SSAFDOracle(*O.from_case(g, c, f)).solve()
@@ -233,3 +241,23 @@ def test_zero_diagonal_is_reported():
     with pytest.raises(ZeroDiagonal):
         s.solve()
     s.close()
+
+
+@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
+@pytest.mark.parametrize("M", [45, 64])
+def test_synthetic_solve_matches_oracle(M, pc):
+    """A whole SSAFD::solve of the synthetic sheet against the oracle, odd and even grid sizes
+    (the multigrid aggregates wrap differently).  Pseudo-plastic till: its Picard iteration
+    contracts ~25 % per step, so both solvers stop at the same iteration; with plastic till
+    the nu*H change decreases ~1 % per step near 1e-4 and the stopping step is ill-posed."""
+    g, c, f, _ = S.build_synthetic(M, 4000e3 / (M - 1), seed=2)
+    c.do_pseudo_plastic_till = True
+    c.ssafd_relative_convergence = 1e-7
+    c.ksp_rtol = 1e-12
+    c.pc_type = pc
+    vel, st = _solve_case(g, c, f)
+    o = O.SSAFDOracle(*O.from_case(g, c, f))
+    ref = o.solve()
+    assert st["converged"] == 1 and st["strategy"] == o.stats.strategy
+    assert abs(st["picard_iterations"] - o.stats.picard_iterations) <= 1
+    assert rel(vel, ref) < 1e-8
