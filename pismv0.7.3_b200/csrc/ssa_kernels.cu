@@ -476,15 +476,56 @@ __global__ void __launch_bounds__(NT) k_nuH(GridDev g, TileMap tm, pism_gpu_ssa_
   }
 }
 
+// y = A x at cell (i, j) = tile position (ti, tj), x and nu*H staged in halo tiles
+__device__ __forceinline__ double2 apply_cell_tile(const GridDev &g, const StencilConst &s, int i, int j, uint32_t f,
+                                                   const HaloTile<double2> &xT, const HaloTile<double2> &nT,
+                                                   const double *__restrict__ beta, int ti, int tj) {
+  if (f & F_DIAG_ONLY) {
+    const double2 xc = xT[ti + 1][tj + 1];
+    return make_double2(s.scaling * xc.x, s.scaling * xc.y);
+  }
+  double c_w = nT[ti][tj + 1].x, c_e = nT[ti + 1][tj + 1].x, c_s = nT[ti + 1][tj].y, c_n = nT[ti + 1][tj + 1].y;
+  if (f & F_NB_ANY) {   // nu_bedrock_set overrides (SSAFD.cc:561-585), from global memory
+    const int k = cell(g, i, j);
+    const double Hc = s.H[k], HE = s.H[nbr(g, i, j, 1, 0)];
+    if (f & F_NB_W) c_w = s.nu_bedrock * 0.5 * (Hc + s.H[nbr(g, i, j, -1, 0)]);
+    if (f & F_NB_E) c_e = s.nu_bedrock * 0.5 * (Hc + HE);
+    if (f & F_NB_N) c_n = s.nu_bedrock * 0.5 * (Hc + s.H[nbr(g, i, j, 0, 1)]);
+    if (f & F_NB_S) c_s = s.nu_bedrock * 0.5 * (Hc + HE);   // thickness(i+1, j), as SSAFD.cc:582
+  }
+  auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
+  const double bta = beta[cell(g, i, j)];
+  if ((f & F_WEIGHTS) == F_WEIGHTS)
+    return apply_regular<double, double2>(s.rdx2, s.rdy2, s.r2, s.r4, c_w, c_e, c_s, c_n, bta, xr);
+  Row2 e1, e2;
+  stencil_rows(s, f, c_w, c_e, c_s, c_n, bta, e1, e2);
+  return apply_rows_rel<double, double2>(e1, e2, xr);
+}
+
+// stage the x and nu*H halo tiles of tile t; returns this thread's cell
+__device__ __forceinline__ bool stage_tile(const GridDev &g, const TileMap &tm, int t, const double2 *__restrict__ x,
+                                           const double2 *__restrict__ nuH, HaloTile<double2> &xT,
+                                           HaloTile<double2> &nT, int &i, int &j) {
+  const int i0 = (t / tm.tiles_j) * TI, j0 = (t % tm.tiles_j) * TJ;
+  __syncthreads();
+  load_halo_tile<double2>(xT, i0, j0, g.Mx, g.My, [&](int a, int b) { return x[a * g.My + b]; });
+  load_halo_tile<double2>(nT, i0, j0, g.Mx, g.My, [&](int a, int b) { return nuH[a * g.My + b]; });
+  __syncthreads();
+  i = i0 + (threadIdx.x >> 5);
+  j = j0 + (threadIdx.x & 31);
+  return i < g.Mx && j < g.My;
+}
+
 // y = A x (plain apply, for checking and for the residual of the refinement)
-__global__ void __launch_bounds__(NT) k_apply(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
+__global__ void __launch_bounds__(NT, 4) k_apply(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
                                               const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                               const double2 *__restrict__ x, double2 *__restrict__ y) {
+  __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int i, j;
-    if (!tm.cell_of(g, t, i, j)) continue;
+    if (!stage_tile(g, tm, t, x, nuH, xT, nT, i, j)) continue;
     const int k = cell(g, i, j);
-    y[k] = apply_cell(g, s, i, j, flags[k], nuH, beta, x);
+    y[k] = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
   }
 }
 
@@ -525,7 +566,7 @@ __global__ void __launch_bounds__(NT) k_diag_setup(GridDev g, TileMap tm, Stenci
 // Stop: ||b - A x||_2 <= rtol ||b||_2 (the unpreconditioned norm of the
 // reference's ASM path, SSAFD.cc:181-187).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) k_bicg_init(GridDev g, TileMap tm, StencilConst s,
+__global__ void __launch_bounds__(NT, 4) k_bicg_init(GridDev g, TileMap tm, StencilConst s,
                                                   const uint32_t *__restrict__ flags,
                                                   const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                                   const double2 *__restrict__ b, const double2 *__restrict__ x,
@@ -533,11 +574,12 @@ __global__ void __launch_bounds__(NT) k_bicg_init(GridDev g, TileMap tm, Stencil
                                                   double2 *__restrict__ p, double2 *__restrict__ v,
                                                   double *partials, unsigned *ticket, KState *st) {
   double acc[2] = {0.0, 0.0};
+  __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int i, j;
-    if (!tm.cell_of(g, t, i, j)) continue;
+    if (!stage_tile(g, tm, t, x, nuH, xT, nT, i, j)) continue;
     const int k = cell(g, i, j);
-    const double2 ax = apply_cell(g, s, i, j, flags[k], nuH, beta, x);
+    const double2 ax = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
     const double2 bk = b[k];
     const double2 rk = make_double2(bk.x - ax.x, bk.y - ax.y);
     r[k] = rk;
@@ -581,18 +623,19 @@ __global__ void __launch_bounds__(NT) k_bicg_p(int N, const double2 *__restrict_
 }
 
 // v = A phat; alpha = rho / (rhat . v)
-__global__ void __launch_bounds__(NT) k_bicg_v(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
+__global__ void __launch_bounds__(NT, 4) k_bicg_v(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
                                                const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                                const double2 *__restrict__ phat, const double2 *__restrict__ rhat,
                                                double2 *__restrict__ v, double *partials, unsigned *ticket,
                                                KState *st) {
   if (st->done) return;
   double acc[1] = {0.0};
+  __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int i, j;
-    if (!tm.cell_of(g, t, i, j)) continue;
+    if (!stage_tile(g, tm, t, phat, nuH, xT, nT, i, j)) continue;
     const int k = cell(g, i, j);
-    const double2 vk = apply_cell(g, s, i, j, flags[k], nuH, beta, phat);
+    const double2 vk = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
     v[k] = vk;
     acc[0] += dot2(rhat[k], vk);
   }
@@ -623,18 +666,19 @@ __global__ void __launch_bounds__(NT) k_bicg_s(int N, const double2 *__restrict_
 }
 
 // t = A shat; omega = (t . s) / (t . t)
-__global__ void __launch_bounds__(NT) k_bicg_t(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
+__global__ void __launch_bounds__(NT, 4) k_bicg_t(GridDev g, TileMap tm, StencilConst s, const uint32_t *__restrict__ flags,
                                                const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                                const double2 *__restrict__ shat, const double2 *__restrict__ sv,
                                                double2 *__restrict__ tv, double *partials, unsigned *ticket,
                                                KState *st) {
   if (st->done) return;
   double acc[2] = {0.0, 0.0};
+  __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int i, j;
-    if (!tm.cell_of(g, t, i, j)) continue;
+    if (!stage_tile(g, tm, t, shat, nuH, xT, nT, i, j)) continue;
     const int k = cell(g, i, j);
-    const double2 tk = apply_cell(g, s, i, j, flags[k], nuH, beta, shat);
+    const double2 tk = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
     tv[k] = tk;
     acc[0] += dot2(tk, sv[k]);
     acc[1] += dot2(tk, tk);

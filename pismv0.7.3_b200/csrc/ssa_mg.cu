@@ -25,6 +25,8 @@
 #include <algorithm>
 #include <cstdio>
 
+#include <cooperative_groups.h>
+
 #include "ssa_internal.h"
 #include "ssa_stencil.cuh"
 
@@ -34,6 +36,7 @@ namespace {
 
 constexpr int TJm = 32, TIm = 8, NTm = TJm * TIm;
 constexpr int CTA_THREADS = 1024;
+constexpr int SMALL_CLUSTER = 8;   // CTAs (SMs) of the cluster that cycles the small levels
 
 struct TileM {
   int tiles_j, tiles;
@@ -126,46 +129,6 @@ __global__ void k_mg0_compact(int N, const double2 *__restrict__ nuH, const doub
     betaf[k] = (float)beta[k];
     dinvf[k] = make_float4((float)d.x, (float)d.y, (float)d.z, (float)d.w);
   }
-}
-
-// the two FP32 rows of fine cell (i, j); false for a diagonal-only row
-__device__ __forceinline__ bool fine_rows(const FineF &F, int i, int j, uint32_t f, Row2T<float> &e1,
-                                          Row2T<float> &e2) {
-  if (f & F_DIAG_ONLY) return false;
-  const GridDev &g = F.g;
-  const int k = cell(g, i, j);
-  const float2 nC = F.nuH[k];
-  float c_w = F.nuH[nbr(g, i, j, -1, 0)].x, c_e = nC.x, c_s = F.nuH[nbr(g, i, j, 0, -1)].y, c_n = nC.y;
-  if (f & F_NB_ANY) {   // nu_bedrock_set overrides, SSAFD.cc:561-585
-    const double Hc = F.H[k], HE = F.H[nbr(g, i, j, 1, 0)];
-    if (f & F_NB_W) c_w = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, -1, 0)]));
-    if (f & F_NB_E) c_e = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
-    if (f & F_NB_N) c_n = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, 0, 1)]));
-    if (f & F_NB_S) c_s = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
-  }
-  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, F.beta[k], e1, e2);
-  return true;
-}
-
-template <class XA>
-__device__ __forceinline__ float2 fine_apply(const FineF &F, int i, int j, const XA &xa) {
-  const uint32_t f = F.flags[cell(F.g, i, j)];
-  Row2T<float> e1, e2;
-  if (!fine_rows(F, i, j, f, e1, e2)) {
-    const float2 xc = xa(i, j);
-    return make_float2(F.scaling * xc.x, F.scaling * xc.y);
-  }
-  const int ip = wrap(i + 1, F.g.Mx), im = wrap(i - 1, F.g.Mx), jp = wrap(j + 1, F.g.My), jm = wrap(j - 1, F.g.My);
-  const float2 xNW = xa(im, jp), xN = xa(i, jp), xNE = xa(ip, jp);
-  const float2 xW = xa(im, j), xC = xa(i, j), xE = xa(ip, j);
-  const float2 xSW = xa(im, jm), xS = xa(i, jm), xSE = xa(ip, jm);
-  float y1 = e1.uN * xN.x + e1.uW * xW.x + e1.uC * xC.x + e1.uE * xE.x + e1.uS * xS.x;
-  y1 += e1.vNW * xNW.y + e1.vN * xN.y + e1.vNE * xNE.y + e1.vW * xW.y + e1.vC * xC.y + e1.vE * xE.y +
-        e1.vSW * xSW.y + e1.vS * xS.y + e1.vSE * xSE.y;
-  float y2 = e2.uNW * xNW.x + e2.uN * xN.x + e2.uNE * xNE.x + e2.uW * xW.x + e2.uC * xC.x + e2.uE * xE.x +
-             e2.uSW * xSW.x + e2.uS * xS.x + e2.uSE * xSE.x;
-  y2 += e2.vN * xN.y + e2.vW * xW.y + e2.vC * xC.y + e2.vE * xE.y + e2.vS * xS.y;
-  return make_float2(y1, y2);
 }
 
 // ---------------------------------------------------------------------------
@@ -342,35 +305,115 @@ __global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, d
 // ---------------------------------------------------------------------------
 // V-cycle kernels
 // ---------------------------------------------------------------------------
-// fine level: b_1 = R (b - A x0), x0 = omega D^-1 b on the fly; one thread per aggregate
-template <int AX, int AY>
-__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__restrict__ b, float omega, int Mxc,
-                                                      int Myc, TileM tm, float2 *__restrict__ bc, const KState *st) {
-  if (st && st->done) return;
+// Stencil passes of the cycle.  A block stages the 34 x 10 halo tile of x (computed
+// from b, D^-1 and, after the coarse solve, the prolonged correction) in shared memory once,
+// so each x value is formed once per block instead of once per neighbour.
+
+// the two FP32 rows of fine cell (i, j) from a staged tile of FP32 nu*H; false for a
+// diagonal-only row
+__device__ __forceinline__ bool fine_rows_tile(const FineF &F, int i, int j, uint32_t f, const HaloTile<float2> &nT,
+                                               int ti, int tj, Row2T<float> &e1, Row2T<float> &e2) {
+  if (f & F_DIAG_ONLY) return false;
   const GridDev &g = F.g;
-  auto xa = [&](int ii, int jj) {
-    const int q = ii * g.My + jj;
-    const double2 bd = b[q];
-    const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
-    return make_float2(omega * v.x, omega * v.y);
-  };
-  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int I, J;
-    if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
+  float c_w = nT[ti][tj + 1].x, c_e = nT[ti + 1][tj + 1].x, c_s = nT[ti + 1][tj].y, c_n = nT[ti + 1][tj + 1].y;
+  if (f & F_NB_ANY) {   // nu_bedrock_set overrides, SSAFD.cc:561-585
+    const int k = cell(g, i, j);
+    const double Hc = F.H[k], HE = F.H[nbr(g, i, j, 1, 0)];
+    if (f & F_NB_W) c_w = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, -1, 0)]));
+    if (f & F_NB_E) c_e = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
+    if (f & F_NB_N) c_n = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, 0, 1)]));
+    if (f & F_NB_S) c_s = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
+  }
+  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, F.beta[cell(g, i, j)], e1, e2);
+  return true;
+}
+
+// y = A x at fine cell (i, j) = tile position (ti, tj), x and nu*H from tiles
+__device__ __forceinline__ float2 fine_apply_tile(const FineF &F, int i, int j, const HaloTile<float2> &xT,
+                                                  const HaloTile<float2> &nT, int ti, int tj) {
+  const uint32_t f = F.flags[cell(F.g, i, j)];
+  if ((f & (F_WEIGHTS | F_DIAG_ONLY | F_NB_ANY)) == F_WEIGHTS) {
+    auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
+    return apply_regular<float, float2>(F.rdx2, F.rdy2, F.r2, F.r4, nT[ti][tj + 1].x, nT[ti + 1][tj + 1].x,
+                                        nT[ti + 1][tj].y, nT[ti + 1][tj + 1].y, F.beta[cell(F.g, i, j)], xr);
+  }
+  Row2T<float> e1, e2;
+  if (!fine_rows_tile(F, i, j, f, nT, ti, tj, e1, e2)) {
+    const float2 xc = xT[ti + 1][tj + 1];
+    return make_float2(F.scaling * xc.x, F.scaling * xc.y);
+  }
+  auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
+  return apply_rows_rel<float, float2>(e1, e2, xr);
+}
+
+// y = A_l x at coarse cell (i, j) = tile position (ti, tj), x from a tile
+__device__ __forceinline__ float2 coarse_apply_tile(const LevelView &L, int k, const HaloTile<float2> &xT, int ti,
+                                                    int tj) {
+  float4 a[9];
+#pragma unroll
+  for (int b = 0; b < 9; ++b) a[b] = L.A[b * L.N + k];
+  float y1 = 0.0f, y2 = 0.0f;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const int di = (b % 3) - 1, dj = 1 - (b / 3);
+    const float2 xv = xT[ti + 1 + di][tj + 1 + dj];
+    y1 += a[b].x * xv.x + a[b].y * xv.y;
+    y2 += a[b].z * xv.x + a[b].w * xv.y;
+  }
+  return make_float2(y1, y2);
+}
+
+// 2 x 2 (AX x AY) aggregate sums of the residuals staged in rsh, written to bc
+template <int AX, int AY>
+__device__ __forceinline__ void store_aggregates(float2 (&rsh)[TILE_I][TILE_J], int i0, int j0, int Mxc, int Myc,
+                                                 float2 *__restrict__ bc) {
+  constexpr int CJ = TILE_J / AY, CI = TILE_I / AX;
+  if (threadIdx.x < CI * CJ) {
+    const int ci = threadIdx.x / CJ, cj = threadIdx.x - ci * CJ;
     float ru = 0.0f, rv = 0.0f;
 #pragma unroll
     for (int pi = 0; pi < AX; ++pi)
 #pragma unroll
       for (int pj = 0; pj < AY; ++pj) {
-        const int i = I * AX + pi, j = J * AY + pj;
-        if (i < g.Mx && j < g.My) {
-          const float2 y = fine_apply(F, i, j, xa);
-          const double2 bk = b[i * g.My + j];
-          ru += (float)bk.x - y.x;
-          rv += (float)bk.y - y.y;
-        }
+        const float2 r = rsh[ci * AX + pi][cj * AY + pj];
+        ru += r.x;
+        rv += r.y;
       }
-    bc[I * Myc + J] = make_float2(ru, rv);
+    const int I = i0 / AX + ci, J = j0 / AY + cj;
+    if (I < Mxc && J < Myc) bc[I * Myc + J] = make_float2(ru, rv);
+  }
+}
+
+// fine level: b_1 = R (b - A x0), x0 = omega D^-1 b
+template <int AX, int AY>
+__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__restrict__ b, float omega, int Mxc,
+                                                      int Myc, TileM tm, float2 *__restrict__ bc, const KState *st) {
+  if (st && st->done) return;
+  __shared__ HaloTile<float2> xT, nT;
+  __shared__ float2 rsh[TILE_I][TILE_J];
+  const GridDev &g = F.g;
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    __syncthreads();
+    load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) {
+      const int q = i * g.My + j;
+      const double2 bd = b[q];
+      const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
+      return make_float2(omega * v.x, omega * v.y);
+    });
+    load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
+    __syncthreads();
+    const int i = i0 + ti, j = j0 + tj;
+    float2 r = make_float2(0.0f, 0.0f);
+    if (i < g.Mx && j < g.My) {
+      const float2 y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
+      const double2 bk = b[i * g.My + j];
+      r = make_float2((float)bk.x - y.x, (float)bk.y - y.y);
+    }
+    rsh[ti][tj] = r;
+    __syncthreads();
+    store_aggregates<AX, AY>(rsh, i0, j0, Mxc, Myc, bc);
   }
 }
 
@@ -380,23 +423,30 @@ __global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const double2 *__rest
                                                   int Myc, const float2 *__restrict__ xc, TileM tm,
                                                   double2 *__restrict__ z, const KState *st) {
   if (st && st->done) return;
+  __shared__ HaloTile<float2> xT, nT;
   const GridDev &g = F.g;
-  auto xa = [&](int ii, int jj) {
-    const int q = ii * g.My + jj;
-    const double2 bd = b[q];
-    const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
-    const float2 c = xc[(ii / AX) * Myc + jj / AY];
-    return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
-  };
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!tile_cell(tm, g.Mx, g.My, t, i, j)) continue;
-    const int k = cell(g, i, j);
-    const float2 xk = xa(i, j);
-    const float2 y = fine_apply(F, i, j, xa);
-    const double2 bk = b[k];
-    const float2 d = fmul4(F.dinv[k], make_float2((float)bk.x - y.x, (float)bk.y - y.y));
-    z[k] = make_double2((double)(xk.x + omega * d.x), (double)(xk.y + omega * d.y));
+    const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    __syncthreads();
+    load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) {
+      const int q = i * g.My + j;
+      const double2 bd = b[q];
+      const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
+      const float2 c = xc[(i / AX) * Myc + j / AY];
+      return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+    });
+    load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
+    __syncthreads();
+    const int i = i0 + ti, j = j0 + tj;
+    if (i < g.Mx && j < g.My) {
+      const int k = i * g.My + j;
+      const float2 xk = xT[ti + 1][tj + 1];
+      const float2 y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
+      const double2 bk = b[k];
+      const float2 d = fmul4(F.dinv[k], make_float2((float)bk.x - y.x, (float)bk.y - y.y));
+      z[k] = make_double2((double)(xk.x + omega * d.x), (double)(xk.y + omega * d.y));
+    }
   }
 }
 
@@ -405,28 +455,29 @@ template <int AX, int AY>
 __global__ void __launch_bounds__(NTm) k_mgc_restrict(LevelView L, float omega, int Mxc, int Myc, TileM tm,
                                                       float2 *__restrict__ bc, const KState *st) {
   if (st && st->done) return;
-  auto xa = [&](int ii, int jj) {
-    const int q = ii * L.My + jj;
-    const float2 v = fmul4(L.dinv[q], L.b[q]);
-    return make_float2(omega * v.x, omega * v.y);
-  };
+  __shared__ HaloTile<float2> xT;
+  __shared__ float2 rsh[TILE_I][TILE_J];
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int I, J;
-    if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
-    float ru = 0.0f, rv = 0.0f;
-#pragma unroll
-    for (int pi = 0; pi < AX; ++pi)
-#pragma unroll
-      for (int pj = 0; pj < AY; ++pj) {
-        const int i = I * AX + pi, j = J * AY + pj;
-        if (i < L.Mx && j < L.My) {
-          const float2 y = coarse_apply(L, i, j, xa);
-          const float2 bk = L.b[i * L.My + j];
-          ru += bk.x - y.x;
-          rv += bk.y - y.y;
-        }
-      }
-    bc[I * Myc + J] = make_float2(ru, rv);
+    const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    __syncthreads();
+    load_halo_tile<float2>(xT, i0, j0, L.Mx, L.My, [&](int i, int j) {
+      const int q = i * L.My + j;
+      const float2 v = fmul4(L.dinv[q], L.b[q]);
+      return make_float2(omega * v.x, omega * v.y);
+    });
+    __syncthreads();
+    const int i = i0 + ti, j = j0 + tj;
+    float2 r = make_float2(0.0f, 0.0f);
+    if (i < L.Mx && j < L.My) {
+      const int k = i * L.My + j;
+      const float2 y = coarse_apply_tile(L, k, xT, ti, tj);
+      const float2 bk = L.b[k];
+      r = make_float2(bk.x - y.x, bk.y - y.y);
+    }
+    rsh[ti][tj] = r;
+    __syncthreads();
+    store_aggregates<AX, AY>(rsh, i0, j0, Mxc, Myc, bc);
   }
 }
 
@@ -435,21 +486,27 @@ template <int AX, int AY>
 __global__ void __launch_bounds__(NTm) k_mgc_post(LevelView L, float omega, float corr, int Myc,
                                                   const float2 *__restrict__ xc, TileM tm, const KState *st) {
   if (st && st->done) return;
-  auto xa = [&](int ii, int jj) {
-    const int q = ii * L.My + jj;
-    const float2 v = fmul4(L.dinv[q], L.b[q]);
-    const float2 c = xc[(ii / AX) * Myc + jj / AY];
-    return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
-  };
+  __shared__ HaloTile<float2> xT;
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!tile_cell(tm, L.Mx, L.My, t, i, j)) continue;
-    const int k = i * L.My + j;
-    const float2 xk = xa(i, j);
-    const float2 y = coarse_apply(L, i, j, xa);
-    const float2 bk = L.b[k];
-    const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
-    L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+    const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    __syncthreads();
+    load_halo_tile<float2>(xT, i0, j0, L.Mx, L.My, [&](int i, int j) {
+      const int q = i * L.My + j;
+      const float2 v = fmul4(L.dinv[q], L.b[q]);
+      const float2 c = xc[(i / AX) * Myc + j / AY];
+      return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+    });
+    __syncthreads();
+    const int i = i0 + ti, j = j0 + tj;
+    if (i < L.Mx && j < L.My) {
+      const int k = i * L.My + j;
+      const float2 xk = xT[ti + 1][tj + 1];
+      const float2 y = coarse_apply_tile(L, k, xT, ti, tj);
+      const float2 bk = L.b[k];
+      const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+      L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+    }
   }
 }
 
@@ -462,19 +519,28 @@ struct SmallLevels {
   int n;             // unknowns of the coarsest level
 };
 
-__global__ void __launch_bounds__(CTA_THREADS) k_mg_small_cycle(SmallLevels S, float omega, float corr,
-                                                                const KState *st) {
+// The small levels run on one thread-block cluster of SMALL_CLUSTER CTAs: every CTA
+// stages the whole level's x in its shared memory, computes its share of the cells, and the
+// cluster barrier (release / acquire at cluster scope) orders the steps.
+namespace cg = cooperative_groups;
+
+__global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THREADS)
+    k_mg_small_cycle(SmallLevels S, float omega, float corr, const KState *st) {
   if (st && st->done) return;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = cluster.block_rank() * CTA_THREADS + threadIdx.x, nthr = SMALL_CLUSTER * CTA_THREADS;
+  __shared__ float2 xs[MG_CTA_CELLS];
   __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
   // down
   for (int l = S.first; l < S.last; ++l) {
     const LevelView &L = S.lev[l], &C = S.lev[l + 1];
-    auto xa = [&](int ii, int jj) {
-      const int q = ii * L.My + jj;
+    for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
       const float2 v = fmul4(L.dinv[q], L.b[q]);
-      return make_float2(omega * v.x, omega * v.y);
-    };
-    for (int kc = threadIdx.x; kc < C.N; kc += CTA_THREADS) {
+      xs[q] = make_float2(omega * v.x, omega * v.y);
+    }
+    __syncthreads();
+    auto xa = [&](int ii, int jj) { return xs[ii * L.My + jj]; };
+    for (int kc = rank; kc < C.N; kc += nthr) {
       const int I = kc / C.My, J = kc - I * C.My;
       float ru = 0.0f, rv = 0.0f;
       for (int pi = 0; pi < L.ax; ++pi)
@@ -488,7 +554,7 @@ __global__ void __launch_bounds__(CTA_THREADS) k_mg_small_cycle(SmallLevels S, f
         }
       C.b[kc] = make_float2(ru, rv);
     }
-    __syncthreads();
+    cluster.sync();
   }
   // coarsest: x = A^-1 b
   {
@@ -499,31 +565,38 @@ __global__ void __launch_bounds__(CTA_THREADS) k_mg_small_cycle(SmallLevels S, f
       bsh[2 * q + 1] = v.y;
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < S.n; r += CTA_THREADS) {
+    // one warp per row, the lanes split the columns (the row-major transpose keeps a
+    // column's entries of consecutive rows adjacent; here each lane reads its own column)
+    const int lane = threadIdx.x & 31, warp = rank >> 5, nwarp = nthr >> 5;
+    for (int r = warp; r < S.n; r += nwarp) {
       double acc = 0.0;
-      for (int c = 0; c < S.n; ++c) acc += S.invT[c * S.n + r] * (double)bsh[c];
-      reinterpret_cast<float *>(C.x)[r] = (float)acc;
+      for (int c = lane; c < S.n; c += 32) acc += S.invT[c * S.n + r] * (double)bsh[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) reinterpret_cast<float *>(C.x)[r] = (float)acc;
     }
-    __syncthreads();
+    cluster.sync();
   }
   // up
   for (int l = S.last - 1; l >= S.first; --l) {
     const LevelView &L = S.lev[l], &C = S.lev[l + 1];
-    auto xa = [&](int ii, int jj) {
-      const int q = ii * L.My + jj;
+    for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
+      const int i = q / L.My, j = q - i * L.My;
       const float2 v = fmul4(L.dinv[q], L.b[q]);
-      const float2 c = C.x[(ii / L.ax) * C.My + jj / L.ay];
-      return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
-    };
-    for (int k = threadIdx.x; k < L.N; k += CTA_THREADS) {
+      const float2 c = C.x[(i / L.ax) * C.My + j / L.ay];
+      xs[q] = make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+    }
+    __syncthreads();
+    auto xa = [&](int ii, int jj) { return xs[ii * L.My + jj]; };
+    for (int k = rank; k < L.N; k += nthr) {
       const int i = k / L.My, j = k - i * L.My;
-      const float2 xk = xa(i, j);
+      const float2 xk = xs[k];
       const float2 y = coarse_apply(L, i, j, xa);
       const float2 bk = L.b[k];
       const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
       L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
     }
-    __syncthreads();
+    cluster.sync();
   }
 }
 
@@ -673,7 +746,7 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
   // down: fine -> level 1
   {
     const MGLevel &C = H.lev[0];
-    const TileM tm = tiles_of(C.Mx, C.My);
+    const TileM tm = tiles_of(g.Mx, g.My);
     const int nb = blocks_for(Lc, tm.tiles);
 #define MG0R(AX, AY) [&] { k_mg0_restrict<AX, AY><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, C.Mx, C.My, tm, C.b, st); }
     dispatch_ax(H.fine_ax, H.fine_ay, MG0R(2, 2), MG0R(2, 1), MG0R(1, 2), MG0R(1, 1));
@@ -684,7 +757,7 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
   for (int l = 0; l < H.small_first; ++l) {
     const MGLevel &L = H.lev[l], &C = H.lev[l + 1];
     const LevelView V = view(L);
-    const TileM tm = tiles_of(C.Mx, C.My);
+    const TileM tm = tiles_of(L.Mx, L.My);
     const int nb = blocks_for(Lc, tm.tiles);
 #define MGCR(AX, AY) [&] { k_mgc_restrict<AX, AY><<<nb, NTm, 0, Lc.stream>>>(V, omega, C.Mx, C.My, tm, C.b, st); }
     dispatch_ax(L.ax, L.ay, MGCR(2, 2), MGCR(2, 1), MGCR(1, 2), MGCR(1, 1));
@@ -699,7 +772,7 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
     for (int l = 0; l < H.nlev; ++l) S.lev[l] = view(H.lev[l]);
     S.invT = H.cinv;
     S.n = 2 * H.lev[H.nlev - 1].N;
-    k_mg_small_cycle<<<1, CTA_THREADS, 0, Lc.stream>>>(S, omega, corr, st);
+    k_mg_small_cycle<<<SMALL_CLUSTER, CTA_THREADS, 0, Lc.stream>>>(S, omega, corr, st);
     ++launches;
   }
   // up through the large coarse levels

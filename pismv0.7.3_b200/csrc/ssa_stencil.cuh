@@ -97,6 +97,85 @@ __device__ __forceinline__ void stencil_rows(const StencilConst &s, uint32_t f, 
   stencil_rows_t<double>(s.rdx2, s.rdy2, s.r2, s.r4, f, c_w, c_e, c_s, c_n, bta, e1, e2);
 }
 
+// y = the two rows applied to x, with x at the offset (di, dj) read through xr(di, dj)
+template <class T, class V, class XR>
+__device__ __forceinline__ V apply_rows_rel(const Row2T<T> &e1, const Row2T<T> &e2, const XR &xr) {
+  const V xNW = xr(-1, 1), xN = xr(0, 1), xNE = xr(1, 1);
+  const V xW = xr(-1, 0), xC = xr(0, 0), xE = xr(1, 0);
+  const V xSW = xr(-1, -1), xS = xr(0, -1), xSE = xr(1, -1);
+  T y1 = e1.uN * xN.x + e1.uW * xW.x + e1.uC * xC.x + e1.uE * xE.x + e1.uS * xS.x;
+  y1 += e1.vNW * xNW.y + e1.vN * xN.y + e1.vNE * xNE.y + e1.vW * xW.y + e1.vC * xC.y + e1.vE * xE.y +
+        e1.vSW * xSW.y + e1.vS * xS.y + e1.vSE * xSE.y;
+  T y2 = e2.uNW * xNW.x + e2.uN * xN.x + e2.uNE * xNE.x + e2.uW * xW.x + e2.uC * xC.x + e2.uE * xE.x +
+         e2.uSW * xSW.x + e2.uS * xS.x + e2.uSE * xSE.x;
+  y2 += e2.vN * xN.y + e2.vW * xW.y + e2.vC * xC.y + e2.vE * xE.y + e2.vS * xS.y;
+  V y;
+  y.x = y1;
+  y.y = y2;
+  return y;
+}
+
+// y = A x for a regular row whose CFBC weights are all 1 (every cell without -cfbc): the
+// rows of stencil_rows_t with the weights substituted, written in difference form
+// (about 40 flops instead of forming 36 coefficients); xr(di, dj) reads x at the offset.
+template <class T, class V, class XR>
+__device__ __forceinline__ V apply_regular(T rdx2, T rdy2, T r2, T r4, T c_w, T c_e, T c_s, T c_n, T bta,
+                                           const XR &xr) {
+  const V xNW = xr(-1, 1), xN = xr(0, 1), xNE = xr(1, 1);
+  const V xW = xr(-1, 0), xC = xr(0, 0), xE = xr(1, 0);
+  const V xSW = xr(-1, -1), xS = xr(0, -1), xSE = xr(1, -1);
+  // d/dy (c du/dy), d/dx (4 c du/dx) and the mixed terms of the first equation
+  const T uy = c_n * (xC.x - xN.x) + c_s * (xC.x - xS.x);
+  const T ux = c_e * (xC.x - xE.x) + c_w * (xC.x - xW.x);
+  const T vA = c_w * (xNW.y + xN.y - xSW.y - xS.y) + c_e * (xSE.y + xS.y - xNE.y - xN.y);
+  const T vB = c_n * (xNW.y - xNE.y + xW.y - xE.y) + c_s * (xSE.y - xSW.y - xW.y + xE.y);
+  // and of the second equation
+  const T vy = c_n * (xC.y - xN.y) + c_s * (xC.y - xS.y);
+  const T vx = c_e * (xC.y - xE.y) + c_w * (xC.y - xW.y);
+  const T uA = c_w * (xNW.x + xN.x - xSW.x - xS.x) + c_e * (xSE.x + xS.x - xNE.x - xN.x);
+  const T uB = c_n * (xNW.x - xNE.x + xW.x - xE.x) + c_s * (xSE.x - xSW.x - xW.x + xE.x);
+  V y;
+  y.x = rdy2 * uy + 4 * rdx2 * ux + r2 * vA + r4 * vB + bta * xC.x;
+  y.y = 4 * rdy2 * vy + rdx2 * vx + r4 * uA + r2 * uB + bta * xC.y;
+  return y;
+}
+
+// Tiles of 32 (j) x 8 (i) cells with a one-cell halo, staged in shared memory.  Element
+// [a][b] holds the value at (i0 - 1 + a, j0 - 1 + b), indices wrapped periodically (a true
+// modulo: grids may be narrower than a tile).
+constexpr int TILE_J = 32, TILE_I = 8, TILE_THREADS = TILE_J * TILE_I;
+template <class T>
+using HaloTile = T[TILE_I + 2][TILE_J + 2];
+
+__device__ __forceinline__ int pmod(int a, int n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+// One load round: thread (ti, tj) loads its own cell; threads of rows 0-5 also load one
+// halo element each (top / bottom rows, the two corner pairs, left / right columns).
+template <class T, class LOAD>
+__device__ __forceinline__ void load_halo_tile(HaloTile<T> &tile, int i0, int j0, int Mx, int My, const LOAD &load) {
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
+  const int i = i0 + ti, j = j0 + tj;
+  const T own = load(i < Mx ? i : pmod(i, Mx), j < My ? j : pmod(j, My));
+  T halo;
+  int ha = -1, hb = 0;
+  if (ti < 2) {                       // top (a = 0) / bottom (a = 9) row, b = 0..31
+    ha = ti == 0 ? 0 : TILE_I + 1;
+    hb = tj;
+  } else if (ti < 4 && tj < 2) {      // the same rows, b = 32, 33
+    ha = ti == 2 ? 0 : TILE_I + 1;
+    hb = 32 + tj;
+  } else if (ti < 6 && tj < TILE_I) { // left (b = 0) / right (b = 33) column, a = 1..8
+    ha = tj + 1;
+    hb = ti == 4 ? 0 : TILE_J + 1;
+  }
+  if (ha >= 0) halo = load(pmod(i0 - 1 + ha, Mx), pmod(j0 - 1 + hb, My));
+  tile[ti + 1][tj + 1] = own;
+  if (ha >= 0) tile[ha][hb] = halo;
+}
+
 // y(i, j) = sum over the 9 neighbours of the two rows applied to x, read through an
 // accessor xa(i', j') (i', j' already wrapped)
 template <class XA>
