@@ -173,6 +173,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--apply-launches", type=int, default=50)
     ap.add_argument("--pc", default="mg", choices=["mg", "bjacobi"])
+    ap.add_argument("--mg-omega", type=float, default=None)
+    ap.add_argument("--mg-correction", type=float, default=None)
+    ap.add_argument("--verbosity", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -190,6 +193,11 @@ def main():
     from pism_b200.ssa import SSAFD
 
     g, c, f, meta = build_case(args.size, args.pc)
+    if args.mg_omega is not None:
+        c.mg_omega = args.mg_omega
+    if args.mg_correction is not None:
+        c.mg_correction = args.mg_correction
+    c.verbosity = args.verbosity
     M = args.size
     N = M * M
     dev = torch.device("cuda", local)

@@ -117,6 +117,8 @@ typedef struct pism_gpu_ssa_config {
   int    gmres_restart;                            /* PETSc default 30               */
   int    precision;                                /* PISM_PRECISION_*               */
   double mixed_inner_rtol;                         /* inner FP32 solve tolerance     */
+  double mg_omega;                                 /* multigrid smoother damping     */
+  double mg_correction;                            /* coarse-correction scaling      */
   int    verbosity;                                /* 0 silent .. 3 per-iteration    */
 } pism_gpu_ssa_config;
 

@@ -87,6 +87,8 @@ class SSAConfig:
     gmres_restart: int = 30
     precision: str = "fp64"
     mixed_inner_rtol: float = 1.0e-3
+    mg_omega: float = 0.9
+    mg_correction: float = 1.2
     verbosity: int = 0
     # geometry helpers (not part of the C struct)
     mask_icefree_thickness_standard: float = 0.01
@@ -141,7 +143,7 @@ class CConfig(C.Structure):
         ("fracture_density_softening_lower_limit", _D), ("brutal_sliding", _I),
         ("brutal_sliding_scale", _D), ("ksp_type", _I), ("pc_type", _I), ("ksp_rtol", _D),
         ("ksp_max_it", _I), ("gmres_restart", _I), ("precision", _I), ("mixed_inner_rtol", _D),
-        ("verbosity", _I),
+        ("mg_omega", _D), ("mg_correction", _D), ("verbosity", _I),
     ]
 
 

@@ -128,6 +128,8 @@ int pc_setup(pism_gpu_ssa *h) {
   *h->zd_host = INT_MAX;
   CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
   launch_diag_setup(h->L, h->g, f, h->K.dinv, h->zd_dev);
+  h->mg.omega = (float)h->cfg.mg_omega;
+  h->mg.correction = (float)h->cfg.mg_correction;
   if (active_mg(h)) mg_setup(h->L, h->g, f, h->K.dinv, h->mg);
   CK(h, cudaGetLastError());
   return PISM_GPU_SSA_OK;
@@ -344,6 +346,8 @@ int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *c) {
   c->gmres_restart = 30;
   c->precision = PISM_PRECISION_FP64;
   c->mixed_inner_rtol = 1.0e-3;
+  c->mg_omega = 0.9;
+  c->mg_correction = 1.2;
   c->verbosity = 0;
   return PISM_GPU_SSA_OK;
 }

@@ -53,8 +53,6 @@ struct Launch {
 constexpr int MG_MAX_LEVELS = 16;
 constexpr int MG_COARSE_DIM = 8;                 // the coarsest level has <= 8 x 8 cells
 constexpr int MG_MAX_COARSE_CELLS = MG_COARSE_DIM * MG_COARSE_DIM;
-constexpr double MG_OMEGA = 0.7;                 // damping of the block-Jacobi smoother
-constexpr double MG_CORRECTION = 1.5;            // scaling of the coarse-grid correction
 constexpr int MG_CTA_CELLS = 4096;               // levels this small are cycled by one CTA
 
 struct MGLevel {
@@ -70,11 +68,14 @@ struct MGHierarchy {
   int fine_ax = 1, fine_ay = 1;                  // aggregation of the fine grid
   MGLevel lev[MG_MAX_LEVELS];
   int small_first = 0;                           // first level cycled by one CTA
+  float omega = 0.9f;                            // damping of the block-Jacobi smoother
+  float correction = 1.2f;                       // scaling of the coarse-grid correction
   double *cinv = nullptr;                        // dense inverse of the coarsest operator (transposed)
   int *singular = nullptr;
   float2 *nuHf = nullptr;                        // FP32 copies of the fine nu*H, beta, D^-1
   float *betaf = nullptr;
   float4 *dinvf = nullptr;
+  void *views = nullptr;                         // device copy of the level views
 };
 
 int mg_plan(int Mx, int My, MGHierarchy &H);

@@ -19,9 +19,10 @@
 //   x_l <- x_l + s P x_{l+1};  x_l <- x_l + omega D_l^-1 (b_l - A_l x_l)   (post kernel)
 // so each level costs two stencil passes.  Levels of <= MG_CTA_CELLS cells are cycled by
 // one CTA in one launch (their kernels would be launch- and latency-bound).
-// omega = 0.7 and s = 1.5 (over-correction, compensating the piecewise-constant
-// interpolation) were chosen on SSA matrices of the synthetic ice sheet at 201^2 and
-// 401^2 (BiCGStab iterations 108 -> 15 and 190 -> 19 against point-block Jacobi).
+// The defaults omega = 0.9 and s = 1.2 (mg_omega, mg_correction; s > 1 over-corrects to
+// compensate the piecewise-constant interpolation) come from a sweep of whole 801^2
+// synthetic solves: 7115 BiCGStab iterations against 9558 at (0.7, 1.5) and 8042 at
+// (0.85, 1.5); omega >= 1 makes the damped block-Jacobi smoother unstable (> 1e5).
 #include <algorithm>
 #include <cstdio>
 
@@ -513,10 +514,10 @@ __global__ void __launch_bounds__(NTm) k_mgc_post(LevelView L, float omega, floa
 // The small levels (first .. last, <= MG_CTA_CELLS cells each) in one CTA: restrictions
 // down, the dense solve, post-smoothing up; __syncthreads between the steps.
 struct SmallLevels {
-  int first, last;   // level indices into lev[]
-  LevelView lev[MG_MAX_LEVELS];
+  int first, last;        // level indices into lev[]
+  const LevelView *lev;   // device array of the level views (read through L1, no local copy)
   const double *invT;
-  int n;             // unknowns of the coarsest level
+  int n;                  // unknowns of the coarsest level
 };
 
 // The small levels run on one thread-block cluster of SMALL_CLUSTER CTAs: every CTA
@@ -529,6 +530,17 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   if (st && st->done) return;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = cluster.block_rank() * CTA_THREADS + threadIdx.x, nthr = SMALL_CLUSTER * CTA_THREADS;
+  // the small levels' operators are evicted from L2 by the fine-level passes between
+  // cycles; pull all of them back in at once instead of one dependent round per step
+  for (int l = S.first; l <= S.last; ++l) {
+    const LevelView &L = S.lev[l];
+    const char *A = reinterpret_cast<const char *>(L.A), *D = reinterpret_cast<const char *>(L.dinv);
+    const int lines_A = (9 * L.N * (int)sizeof(float4) + 127) / 128, lines_D = (L.N * (int)sizeof(float4) + 127) / 128;
+    for (int q = rank; q < lines_A + lines_D; q += nthr) {
+      const char *p = q < lines_A ? A + 128 * (size_t)q : D + 128 * (size_t)(q - lines_A);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
+  }
   __shared__ float2 xs[MG_CTA_CELLS];
   __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
   // down
@@ -650,6 +662,14 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
   const int n = 2 * H.lev[H.nlev - 1].N;
   if (cudaMalloc(&H.cinv, sizeof(double) * n * n) != cudaSuccess) return 1;
   if (cudaMalloc(&H.singular, sizeof(int)) != cudaSuccess) return 1;
+  {
+    LevelView v[MG_MAX_LEVELS];
+    for (int l = 0; l < H.nlev; ++l)
+      v[l] = LevelView{H.lev[l].Mx, H.lev[l].My, H.lev[l].N, H.lev[l].ax, H.lev[l].ay, H.lev[l].A, H.lev[l].dinv,
+                       H.lev[l].b, H.lev[l].x};
+    if (cudaMalloc(&H.views, sizeof(LevelView) * MG_MAX_LEVELS) != cudaSuccess) return 1;
+    if (cudaMemcpy(H.views, v, sizeof(LevelView) * H.nlev, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
+  }
   if (cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(double) * n * n)) != cudaSuccess)
     return 1;
@@ -678,6 +698,8 @@ void mg_free(MGHierarchy &H) {
   cudaFree(H.dinvf);
   cudaFree(H.cinv);
   cudaFree(H.singular);
+  cudaFree(H.views);
+  H.views = nullptr;
   H.nuHf = nullptr;
   H.betaf = nullptr;
   H.dinvf = nullptr;
@@ -741,7 +763,7 @@ static void dispatch_ax(int ax, int ay, F22 f22, F21 f21, F12 f12, F11 f11) {
 void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b, double2 *z,
                const KState *st) {
   const FineF F = fine_view(g, f, H);
-  const float omega = (float)MG_OMEGA, corr = (float)MG_CORRECTION;
+  const float omega = H.omega, corr = H.correction;
   int launches = 0;
   // down: fine -> level 1
   {
@@ -769,7 +791,7 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
     SmallLevels S;
     S.first = H.small_first;
     S.last = H.nlev - 1;
-    for (int l = 0; l < H.nlev; ++l) S.lev[l] = view(H.lev[l]);
+    S.lev = reinterpret_cast<const LevelView *>(H.views);
     S.invT = H.cinv;
     S.n = 2 * H.lev[H.nlev - 1].N;
     k_mg_small_cycle<<<SMALL_CLUSTER, CTA_THREADS, 0, Lc.stream>>>(S, omega, corr, st);
