@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--mg-omega", type=float, default=None)
     ap.add_argument("--mg-correction", type=float, default=None)
     ap.add_argument("--verbosity", type=int, default=0)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--inner-rtol", type=float, default=None)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -198,6 +200,9 @@ def main():
     if args.mg_correction is not None:
         c.mg_correction = args.mg_correction
     c.verbosity = args.verbosity
+    c.precision = args.precision
+    if args.inner_rtol is not None:
+        c.mixed_inner_rtol = args.inner_rtol
     M = args.size
     N = M * M
     dev = torch.device("cuda", local)
@@ -294,9 +299,10 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"SSAFD solve, synthetic ice sheet {M}x{M} at {4000 / (M - 1):.0f} km, plastic till, "
                                f"Picard 1e-4, KSP 1e-8 (plain FP64: BiCGStab + {'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'})",
-                   "grid": [M, M], "seed": 0, "precision": "fp64", "l2": "flushed (256 MB write) between steps",
+                   "grid": [M, M], "seed": 0, "precision": args.precision, "l2": "flushed (256 MB write) between steps",
                    "parallelism": f"replicas x{world}"},
         "solver": {"picard_iterations": picard, "ksp_iterations": ksp, "converged": st["converged"],
+                   "refinement_steps": st["refinement_steps"],
                    "strategy": st["strategy"], "final_linear_residual": st["final_linear_residual"]},
         "roofline": {"bound": "hbm", "kernel": "k_apply (SSAFD stencil, matrix-free)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,

@@ -36,6 +36,9 @@ struct pism_gpu_ssa {
   double *beta = nullptr, *bfrict = nullptr;
   uint32_t *flags = nullptr;
   Krylov K{};
+  Krylov32 K32{};
+  double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
+  double *res_host = nullptr;
   MGHierarchy mg{};
   double *partials = nullptr;
   unsigned *ticket = nullptr;
@@ -141,6 +144,10 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown flow law %d", c->flow_law);
   if (c->ksp_type != PISM_KSP_BICGSTAB && c->ksp_type != PISM_KSP_GMRES)
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown ksp_type %d", c->ksp_type);
+  if (c->precision != PISM_PRECISION_FP64 && c->precision != PISM_PRECISION_MIXED)
+    return fail(h, PISM_GPU_SSA_EINVAL, "unknown precision %d", c->precision);
+  if (c->precision == PISM_PRECISION_MIXED && !(c->mixed_inner_rtol > 0.0 && c->mixed_inner_rtol < 1.0))
+    return fail(h, PISM_GPU_SSA_EINVAL, "mixed_inner_rtol must be in (0, 1)");
   if (c->pc_type != PISM_PC_BLOCK_JACOBI && c->pc_type != PISM_PC_MULTIGRID)
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
   if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
@@ -180,6 +187,50 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
   return PISM_GPU_SSA_OK;
 }
 
+// Mixed precision: FP64 iterative refinement around FP32 BiCGStab + FP32 multigrid.  The
+// convergence test ||b - A x|| <= ksp_rtol ||b|| is evaluated in FP64 each refinement step.
+int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
+  const GridDev &g = h->g;
+  Fields f = fields_of(h);
+  const MGHierarchy *mg = active_mg(h);
+  const int max_refine = 60;
+  int inner_total = 0, status = KSP_OK;
+  for (int refine = 0;; ++refine) {
+    launch_residual32(h->L, g, f, h->rhs, x, h->K32.rhs, h->res_dev);
+    CK(h, cudaMemcpyAsync(h->res_host, h->res_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const double rn = sqrt(h->res_host[0]), bn = sqrt(h->res_host[1]);
+    h->stats.final_linear_residual = bn > 0 ? rn / bn : rn;
+    if (!std::isfinite(rn)) { status = KSP_NAN; break; }
+    if (rn <= h->cfg.ksp_rtol * bn || bn == 0.0) break;
+    if (refine >= max_refine) { status = KSP_MAXIT; break; }
+    KState init{};
+    init.rtol = h->cfg.mixed_inner_rtol;
+    init.maxit = h->cfg.ksp_max_it;
+    *h->st_host = init;
+    CK(h, cudaMemcpyAsync(h->K32.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
+    launch_mixed_init(h->L, g.Mx * g.My, h->K32);
+    int launched = 0, chunk = 8;
+    while (true) {
+      for (int q = 0; q < chunk; ++q) launch_mixed_iteration(h->L, g, f, *mg, h->K32);
+      launched += chunk;
+      CK(h, cudaGetLastError());
+      CK(h, cudaMemcpyAsync(h->st_host, h->K32.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
+      CK(h, cudaStreamSynchronize(h->stream));
+      if (h->st_host->done) break;
+      chunk = std::max(4, std::min(32, launched / 4));
+    }
+    inner_total += h->st_host->iter;
+    h->stats.refinement_steps += 1;
+    if (h->st_host->status == KSP_NAN) { status = KSP_NAN; break; }
+    if (h->st_host->iter == 0) { status = KSP_BREAKDOWN; break; }   // no progress possible
+    launch_axpy32(h->L, g.Mx * g.My, h->K32.d, x);
+  }
+  *its_out = inner_total;
+  *status_out = status;
+  return PISM_GPU_SSA_OK;
+}
+
 // SSAFD::picard_manager, SSAFD.cc:962-1119
 int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
   const pism_gpu_ssa_config &c = h->cfg;
@@ -188,7 +239,10 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
   for (int k = 0; k < c.max_iterations_ssafd; ++k) {
     RET(pc_setup(h));
     int its = 0, status = 0;
-    RET(linear_solve(h, h->vel, &its, &status));
+    if (h->cfg.precision == PISM_PRECISION_MIXED && active_mg(h))
+      RET(linear_solve_mixed(h, h->vel, &its, &status));
+    else
+      RET(linear_solve(h, h->vel, &its, &status));
     CK(h, cudaMemcpyAsync(h->zd_host, h->zd_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     h->stats.ksp_iterations += its;
@@ -397,6 +451,9 @@ int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cf
   AL(h->beta, N); AL(h->bfrict, N); AL(h->flags, N);
   AL(h->K.r, N); AL(h->K.rhat, N); AL(h->K.p, N); AL(h->K.v, N); AL(h->K.s, N); AL(h->K.t, N);
   AL(h->K.phat, N); AL(h->K.shat, N); AL(h->K.dinv, N); AL(h->K.st, 1);
+  AL(h->K32.rhs, N); AL(h->K32.r, N); AL(h->K32.rhat, N); AL(h->K32.p, N); AL(h->K32.v, N);
+  AL(h->K32.s, N); AL(h->K32.t, N); AL(h->K32.phat, N); AL(h->K32.shat, N); AL(h->K32.d, N); AL(h->K32.st, 1);
+  AL(h->res_dev, 2);
   h->L.max_blocks = sms * 8;
   if (mg_plan(grid->Mx, grid->My, h->mg) > 0) {
     if (mg_allocate(h->mg, h->N) != 0) return bail(PISM_GPU_SSA_ENOMEM);
@@ -406,7 +463,8 @@ int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cf
 #undef AL
   if (cudaMallocHost((void **)&h->st_host, sizeof(KState)) != cudaSuccess ||
       cudaMallocHost((void **)&h->norm_host, 2 * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost((void **)&h->zd_host, sizeof(int)) != cudaSuccess)
+      cudaMallocHost((void **)&h->zd_host, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void **)&h->res_host, 2 * sizeof(double)) != cudaSuccess)
     return bail(PISM_GPU_SSA_ENOMEM);
   if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
     return bail(PISM_GPU_SSA_ECUDA);
@@ -434,12 +492,15 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
   void *dev[] = {h->H, h->srf, h->bed, h->tauc, h->melange, h->gl_mask, h->fracture, h->stage, h->stage2,
                  h->enthalpy, h->z_dev, h->mask, h->bc, h->bcv, h->taud, h->rhs, h->hardness, h->nuH, h->vel,
                  h->vel_old, h->beta, h->bfrict, h->flags, h->K.r, h->K.rhat, h->K.p, h->K.v, h->K.s, h->K.t,
-                 h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev};
+                 h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev,
+                 h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.s, h->K32.t, h->K32.phat,
+                 h->K32.shat, h->K32.d, h->K32.st, h->res_dev};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
   if (h->norm_host) cudaFreeHost(h->norm_host);
   if (h->zd_host) cudaFreeHost(h->zd_host);
+  if (h->res_host) cudaFreeHost(h->res_host);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   mg_free(h->mg);
@@ -628,7 +689,10 @@ int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, d
   DeviceGuard dg(h->device);
   RET(pc_setup(h));
   int its = 0, status = 0;
-  RET(linear_solve(h, (double2 *)x_dev, &its, &status));
+  if (h->cfg.precision == PISM_PRECISION_MIXED && active_mg(h))
+    RET(linear_solve_mixed(h, (double2 *)x_dev, &its, &status));
+  else
+    RET(linear_solve(h, (double2 *)x_dev, &its, &status));
   if (iterations) *iterations = its;
   if (rel_residual) *rel_residual = h->stats.final_linear_residual;
   if (status != KSP_OK)

@@ -38,6 +38,12 @@ struct Krylov {
   KState *st;
 };
 
+// FP32 work vectors of the inner solve of the mixed-precision path
+struct Krylov32 {
+  float2 *rhs, *r, *rhat, *p, *v, *s, *t, *phat, *shat, *d;
+  KState *st;
+};
+
 struct Launch {
   cudaStream_t stream;
   int max_blocks;        // resident blocks (SM count x blocks per SM)
@@ -99,6 +105,16 @@ void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, c
 void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b,
                double2 *z, const KState *st);
+void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
+               const KState *st);
+void launch_mixed_init(const Launch &L, int N, const Krylov32 &K);
+void launch_mixed_iteration(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H,
+                            const Krylov32 &K);
+// r32 = (float) (b - A x) with FP64 arithmetic; out2 = {||b - A x||^2, ||b||^2}
+void launch_residual32(const Launch &L, const GridDev &g, const Fields &f, const double2 *b, const double2 *x,
+                       float2 *r32, double *out2);
+// x += d
+void launch_axpy32(const Launch &L, int N, const float2 *d, double2 *x);
 void launch_bfrict(const Launch &L, int N, const pism_gpu_ssa_config &c, const Fields &f, double *out);
 void launch_scale(const Launch &L, int n, double a, double *x);
 

@@ -13,6 +13,7 @@
 
 #include "ssa_internal.h"
 #include "ssa_stencil.cuh"
+#include "ssa_reduce.cuh"
 
 namespace pism_gpu {
 
@@ -35,63 +36,6 @@ static TileMap make_tiles(const GridDev &g) {
   m.tiles_j = (g.My + TJ - 1) / TJ;
   m.tiles = m.tiles_j * ((g.Mx + TI - 1) / TI);
   return m;
-}
-
-// ---------------------------------------------------------------------------
-// block reduction with last-block finalisation
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Reduce NV values over the grid.  Returns true in thread 0 of the last block,
-// with the grid totals in tot[].
-template <int NV>
-__device__ __forceinline__ bool grid_reduce(double (&val)[NV], double *partials, unsigned *ticket,
-                                            double (&tot)[NV]) {
-  __shared__ double sh[NV][NT / 32];
-  __shared__ bool last;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    double s = warp_sum(val[v]);
-    if (lane == 0) sh[v][warp] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      double s = 0.0;
-      for (int w = 0; w < NT / 32; ++w) s += sh[v][w];
-      partials[blockIdx.x * NV + v] = s;
-    }
-    __threadfence();
-    unsigned t = atomicAdd(ticket, 1u);
-    last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return false;
-  __threadfence();
-  // the last block adds all partials in block order (deterministic)
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) s += __ldcg(&partials[b * NV + v]);
-    s = warp_sum(s);
-    if (lane == 0) sh[v][warp] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return false;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    double s = 0.0;
-    for (int w = 0; w < NT / 32; ++w) s += sh[v][w];
-    tot[v] = s;
-  }
-  *ticket = 0u;
-  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -728,6 +672,44 @@ __global__ void __launch_bounds__(NT) k_bicg_x(int N, const double2 *__restrict_
   }
 }
 
+// the outer residual of the mixed-precision refinement: r = b - A x in FP64, handed to the
+// inner FP32 solve; the two norms feed the FP64 convergence test
+__global__ void __launch_bounds__(NT, 4) k_residual32(GridDev g, TileMap tm, StencilConst s,
+                                                      const uint32_t *__restrict__ flags,
+                                                      const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                                      const double2 *__restrict__ b, const double2 *__restrict__ x,
+                                                      float2 *__restrict__ r32, double *partials, unsigned *ticket,
+                                                      double *out2) {
+  double acc[2] = {0.0, 0.0};
+  __shared__ HaloTile<double2> xT, nT;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j;
+    if (!stage_tile(g, tm, t, x, nuH, xT, nT, i, j)) continue;
+    const int k = cell(g, i, j);
+    const double2 ax = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
+    const double2 bk = b[k];
+    const double2 rk = make_double2(bk.x - ax.x, bk.y - ax.y);
+    r32[k] = make_float2((float)rk.x, (float)rk.y);
+    acc[0] += dot2(rk, rk);
+    acc[1] += dot2(bk, bk);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) {
+    out2[0] = tot[0];
+    out2[1] = tot[1];
+  }
+}
+
+__global__ void k_axpy32(int N, const float2 *__restrict__ d, double2 *__restrict__ x) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const float2 dk = d[k];
+    double2 xk = x[k];
+    xk.x += (double)dk.x;
+    xk.y += (double)dk.y;
+    x[k] = xk;
+  }
+}
+
 // basal frictional heating (ShallowStressBalance.cc:179-205)
 __global__ void k_bfrict(int N, pism_gpu_ssa_config c, const double2 *__restrict__ vel, const double *__restrict__ tauc,
                          const int8_t *__restrict__ mask, double *__restrict__ out) {
@@ -846,6 +828,19 @@ void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, c
   }
   k_bicg_t<<<bt, NT, 0, L.stream>>>(g, tm, s, f.flags, f.nuH, f.beta, K.shat, K.s, K.t, L.partials, L.ticket, K.st);
   k_bicg_x<<<bv, NT, 0, L.stream>>>(N, K.phat, K.shat, K.s, K.t, K.rhat, x, K.r, L.partials, L.ticket, K.st);
+}
+
+void launch_residual32(const Launch &L, const GridDev &g, const Fields &f, const double2 *b, const double2 *x,
+                       float2 *r32, double *out2) {
+  L.tick();
+  TileMap tm = make_tiles(g);
+  k_residual32<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta, b,
+                                                                 x, r32, L.partials, L.ticket, out2);
+}
+
+void launch_axpy32(const Launch &L, int N, const float2 *d, double2 *x) {
+  L.tick();
+  k_axpy32<<<grid_for(L, N), NT, 0, L.stream>>>(N, d, x);
 }
 
 void launch_bfrict(const Launch &L, int N, const pism_gpu_ssa_config &c, const Fields &f, double *out) {

@@ -28,8 +28,7 @@
 
 #include <cooperative_groups.h>
 
-#include "ssa_internal.h"
-#include "ssa_stencil.cuh"
+#include "ssa_fine32.cuh"
 
 namespace pism_gpu {
 
@@ -67,19 +66,6 @@ __device__ __forceinline__ int wdiff(int a, int b, int n) {
 // stencil block index of the offset (di, dj): NW N NE / W C E / SW S SE
 __host__ __device__ __forceinline__ int blk_of(int di, int dj) { return (1 - dj) * 3 + (di + 1); }
 
-__device__ __forceinline__ float4 inv2x2(float a11, float a12, float a21, float a22) {
-  const float det = a11 * a22 - a12 * a21;
-  if (det != 0.0f && isfinite(det)) {
-    const float r = 1.0f / det;
-    return make_float4(a22 * r, -a12 * r, -a21 * r, a11 * r);
-  }
-  return make_float4(a11 != 0.0f ? 1.0f / a11 : 0.0f, 0.0f, 0.0f, a22 != 0.0f ? 1.0f / a22 : 0.0f);
-}
-
-__device__ __forceinline__ float2 fmul4(const float4 &m, const float2 &v) {
-  return make_float2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
-}
-
 struct LevelView {
   int Mx, My, N, ax, ay;
   const float4 *A;     // 9 blocks x N: block b of cell k at A[b * N + k]
@@ -107,19 +93,7 @@ __device__ __forceinline__ float2 coarse_apply(const LevelView &L, int i, int j,
   return make_float2(y1, y2);
 }
 
-// ---------------------------------------------------------------------------
-// fine-level FP32 data (once per Picard iteration)
-// ---------------------------------------------------------------------------
-struct FineF {
-  GridDev g;
-  float rdx2, rdy2, r2, r4, scaling, nu_bedrock;
-  const uint32_t *flags;
-  const float2 *nuH;    // FP32 nu*H
-  const float *beta;    // FP32 beta
-  const float4 *dinv;   // FP32 inverse diagonal blocks
-  const double *H;      // thickness, read only where F_NB_* flags are set
-};
-
+// FP32 copies of nu*H, beta and D^-1 for the fine-level passes (once per Picard iteration)
 __global__ void k_mg0_compact(int N, const double2 *__restrict__ nuH, const double *__restrict__ beta,
                               const double4 *__restrict__ dinv, float2 *__restrict__ nuHf, float *__restrict__ betaf,
                               float4 *__restrict__ dinvf) {
@@ -306,47 +280,6 @@ __global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, d
 // ---------------------------------------------------------------------------
 // V-cycle kernels
 // ---------------------------------------------------------------------------
-// Stencil passes of the cycle.  A block stages the 34 x 10 halo tile of x (computed
-// from b, D^-1 and, after the coarse solve, the prolonged correction) in shared memory once,
-// so each x value is formed once per block instead of once per neighbour.
-
-// the two FP32 rows of fine cell (i, j) from a staged tile of FP32 nu*H; false for a
-// diagonal-only row
-__device__ __forceinline__ bool fine_rows_tile(const FineF &F, int i, int j, uint32_t f, const HaloTile<float2> &nT,
-                                               int ti, int tj, Row2T<float> &e1, Row2T<float> &e2) {
-  if (f & F_DIAG_ONLY) return false;
-  const GridDev &g = F.g;
-  float c_w = nT[ti][tj + 1].x, c_e = nT[ti + 1][tj + 1].x, c_s = nT[ti + 1][tj].y, c_n = nT[ti + 1][tj + 1].y;
-  if (f & F_NB_ANY) {   // nu_bedrock_set overrides, SSAFD.cc:561-585
-    const int k = cell(g, i, j);
-    const double Hc = F.H[k], HE = F.H[nbr(g, i, j, 1, 0)];
-    if (f & F_NB_W) c_w = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, -1, 0)]));
-    if (f & F_NB_E) c_e = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
-    if (f & F_NB_N) c_n = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, 0, 1)]));
-    if (f & F_NB_S) c_s = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
-  }
-  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, F.beta[cell(g, i, j)], e1, e2);
-  return true;
-}
-
-// y = A x at fine cell (i, j) = tile position (ti, tj), x and nu*H from tiles
-__device__ __forceinline__ float2 fine_apply_tile(const FineF &F, int i, int j, const HaloTile<float2> &xT,
-                                                  const HaloTile<float2> &nT, int ti, int tj) {
-  const uint32_t f = F.flags[cell(F.g, i, j)];
-  if ((f & (F_WEIGHTS | F_DIAG_ONLY | F_NB_ANY)) == F_WEIGHTS) {
-    auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
-    return apply_regular<float, float2>(F.rdx2, F.rdy2, F.r2, F.r4, nT[ti][tj + 1].x, nT[ti + 1][tj + 1].x,
-                                        nT[ti + 1][tj].y, nT[ti + 1][tj + 1].y, F.beta[cell(F.g, i, j)], xr);
-  }
-  Row2T<float> e1, e2;
-  if (!fine_rows_tile(F, i, j, f, nT, ti, tj, e1, e2)) {
-    const float2 xc = xT[ti + 1][tj + 1];
-    return make_float2(F.scaling * xc.x, F.scaling * xc.y);
-  }
-  auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
-  return apply_rows_rel<float, float2>(e1, e2, xr);
-}
-
 // y = A_l x at coarse cell (i, j) = tile position (ti, tj), x from a tile
 __device__ __forceinline__ float2 coarse_apply_tile(const LevelView &L, int k, const HaloTile<float2> &xT, int ti,
                                                     int tj) {
@@ -386,8 +319,8 @@ __device__ __forceinline__ void store_aggregates(float2 (&rsh)[TILE_I][TILE_J], 
 }
 
 // fine level: b_1 = R (b - A x0), x0 = omega D^-1 b
-template <int AX, int AY>
-__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__restrict__ b, float omega, int Mxc,
+template <int AX, int AY, class BV>
+__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const BV *__restrict__ b, float omega, int Mxc,
                                                       int Myc, TileM tm, float2 *__restrict__ bc, const KState *st) {
   if (st && st->done) return;
   __shared__ HaloTile<float2> xT, nT;
@@ -399,8 +332,7 @@ __global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__
     __syncthreads();
     load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) {
       const int q = i * g.My + j;
-      const double2 bd = b[q];
-      const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
+      const float2 v = fmul4(F.dinv[q], to_f2(b[q]));
       return make_float2(omega * v.x, omega * v.y);
     });
     load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
@@ -409,8 +341,8 @@ __global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__
     float2 r = make_float2(0.0f, 0.0f);
     if (i < g.Mx && j < g.My) {
       const float2 y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
-      const double2 bk = b[i * g.My + j];
-      r = make_float2((float)bk.x - y.x, (float)bk.y - y.y);
+      const float2 bk = to_f2(b[i * g.My + j]);
+      r = make_float2(bk.x - y.x, bk.y - y.y);
     }
     rsh[ti][tj] = r;
     __syncthreads();
@@ -419,10 +351,10 @@ __global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const double2 *__
 }
 
 // fine level: x = omega D^-1 b + s P x_1;  z = x + omega D^-1 (b - A x)
-template <int AX, int AY>
-__global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const double2 *__restrict__ b, float omega, float corr,
+template <int AX, int AY, class BV, class ZV>
+__global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const BV *__restrict__ b, float omega, float corr,
                                                   int Myc, const float2 *__restrict__ xc, TileM tm,
-                                                  double2 *__restrict__ z, const KState *st) {
+                                                  ZV *__restrict__ z, const KState *st) {
   if (st && st->done) return;
   __shared__ HaloTile<float2> xT, nT;
   const GridDev &g = F.g;
@@ -432,8 +364,7 @@ __global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const double2 *__rest
     __syncthreads();
     load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) {
       const int q = i * g.My + j;
-      const double2 bd = b[q];
-      const float2 v = fmul4(F.dinv[q], make_float2((float)bd.x, (float)bd.y));
+      const float2 v = fmul4(F.dinv[q], to_f2(b[q]));
       const float2 c = xc[(i / AX) * Myc + j / AY];
       return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
     });
@@ -444,9 +375,9 @@ __global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const double2 *__rest
       const int k = i * g.My + j;
       const float2 xk = xT[ti + 1][tj + 1];
       const float2 y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
-      const double2 bk = b[k];
-      const float2 d = fmul4(F.dinv[k], make_float2((float)bk.x - y.x, (float)bk.y - y.y));
-      z[k] = make_double2((double)(xk.x + omega * d.x), (double)(xk.y + omega * d.y));
+      const float2 bk = to_f2(b[k]);
+      const float2 d = fmul4(F.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+      z[k] = from_f2<ZV>(make_float2(xk.x + omega * d.x, xk.y + omega * d.y));
     }
   }
 }
@@ -712,7 +643,7 @@ static LevelView view(const MGLevel &L) { return LevelView{L.Mx, L.My, L.N, L.ax
 
 static int blocks_for(const Launch &Lc, int tiles) { return std::min(tiles, Lc.max_blocks); }
 
-static FineF fine_view(const GridDev &g, const Fields &f, const MGHierarchy &H) {
+FineF fine_view(const GridDev &g, const Fields &f, const MGHierarchy &H) {
   FineF F;
   F.g = g;
   F.rdx2 = (float)(1.0 / (g.dx * g.dx));
@@ -760,8 +691,9 @@ static void dispatch_ax(int ax, int ay, F22 f22, F21 f21, F12 f12, F11 f11) {
   else f11();
 }
 
-void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b, double2 *z,
-               const KState *st) {
+template <class BV, class ZV>
+static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const BV *b, ZV *z,
+                   const KState *st) {
   const FineF F = fine_view(g, f, H);
   const float omega = H.omega, corr = H.correction;
   int launches = 0;
@@ -770,7 +702,7 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(g.Mx, g.My);
     const int nb = blocks_for(Lc, tm.tiles);
-#define MG0R(AX, AY) [&] { k_mg0_restrict<AX, AY><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, C.Mx, C.My, tm, C.b, st); }
+#define MG0R(AX, AY) [&] { k_mg0_restrict<AX, AY, BV><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, C.Mx, C.My, tm, C.b, st); }
     dispatch_ax(H.fine_ax, H.fine_ay, MG0R(2, 2), MG0R(2, 1), MG0R(1, 2), MG0R(1, 1));
 #undef MG0R
     ++launches;
@@ -813,12 +745,22 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(g.Mx, g.My);
     const int nb = blocks_for(Lc, tm.tiles);
-#define MG0P(AX, AY) [&] { k_mg0_post<AX, AY><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, st); }
+#define MG0P(AX, AY) [&] { k_mg0_post<AX, AY, BV, ZV><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, st); }
     dispatch_ax(H.fine_ax, H.fine_ay, MG0P(2, 2), MG0P(2, 1), MG0P(1, 2), MG0P(1, 1));
 #undef MG0P
     ++launches;
   }
   Lc.tick(launches);
+}
+
+void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b, double2 *z,
+               const KState *st) {
+  vcycle(Lc, g, f, H, b, z, st);
+}
+
+void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
+               const KState *st) {
+  vcycle(Lc, g, f, H, b, z, st);
 }
 
 }  // namespace pism_gpu

@@ -1,0 +1,210 @@
+// ssa_mixed.cu — the mixed-precision linear solve: FP64 iterative refinement around an FP32
+// BiCGStab preconditioned by the (FP32) multigrid V-cycle.
+//
+//   r = b - A x            FP64 operator, FP64 vectors; stop when ||r|| <= rtol ||b||
+//   A d = r  (approx.)     FP32 operator from FP32 nu*H / beta, FP32 vectors, FP64 dots;
+//                          to the relative tolerance mixed_inner_rtol
+//   x <- x + d             FP64
+//
+// The outer residual, the convergence test and the solution stay FP64, so the accepted
+// answer meets the same ||b - A x|| <= rtol ||b|| as the plain FP64 solve; the FP32 stencil
+// reads 32 B per cell (x 8, nu*H 8, beta 4, flags 4, y 8) instead of 60.
+#include "ssa_fine32.cuh"
+#include "ssa_reduce.cuh"
+
+namespace pism_gpu {
+
+namespace {
+
+constexpr int NT32 = TILE_THREADS;
+
+struct Tile32 {
+  int tiles_j, tiles;
+};
+
+Tile32 tiles32(const GridDev &g) {
+  Tile32 t;
+  t.tiles_j = (g.My + TILE_J - 1) / TILE_J;
+  t.tiles = t.tiles_j * ((g.Mx + TILE_I - 1) / TILE_I);
+  return t;
+}
+
+// y = A x at this thread's cell of tile t (FP32); false outside the grid
+__device__ __forceinline__ bool apply32(const FineF &F, const Tile32 &tm, int t, const float2 *__restrict__ x,
+                                        HaloTile<float2> &xT, HaloTile<float2> &nT, int &k, float2 &y) {
+  const GridDev &g = F.g;
+  const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+  __syncthreads();
+  load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) { return x[i * g.My + j]; });
+  load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
+  __syncthreads();
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31, i = i0 + ti, j = j0 + tj;
+  if (i >= g.Mx || j >= g.My) return false;
+  k = i * g.My + j;
+  y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
+  return true;
+}
+
+__device__ __forceinline__ double dotf(const float2 &a, const float2 &b) {
+  return (double)a.x * (double)b.x + (double)a.y * (double)b.y;
+}
+
+// start of an inner solve with d0 = 0: r = rhat = rhs, p = v = d = 0
+__global__ void __launch_bounds__(NT32) k32_init(int N, const float2 *__restrict__ rhs, float2 *__restrict__ r,
+                                                 float2 *__restrict__ rhat, float2 *__restrict__ p,
+                                                 float2 *__restrict__ v, float2 *__restrict__ d, double *partials,
+                                                 unsigned *ticket, KState *st) {
+  double acc[1] = {0.0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const float2 b = rhs[k], z = make_float2(0.0f, 0.0f);
+    r[k] = b;
+    rhat[k] = b;
+    p[k] = z;
+    v[k] = z;
+    d[k] = z;
+    acc[0] += dotf(b, b);
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, partials, ticket, tot)) {
+    st->rnorm2 = tot[0];
+    st->bnorm2 = tot[0];
+    st->rnorm0 = sqrt(tot[0]);
+    st->rho = tot[0];
+    st->alpha = 1.0;
+    st->omega = 1.0;
+    st->beta = 0.0;
+    st->iter = 0;
+    st->status = 0;
+    st->done = (tot[0] == 0.0) ? 1 : 0;
+    if (!isfinite(tot[0])) { st->done = 1; st->status = KSP_NAN; }
+  }
+}
+
+__global__ void __launch_bounds__(NT32) k32_p(int N, const float2 *__restrict__ r, const float2 *__restrict__ v,
+                                              float2 *__restrict__ p, const KState *st) {
+  if (st->done) return;
+  const float bta = (float)st->beta, om = (float)st->omega;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const float2 rk = r[k], pk = p[k], vk = v[k];
+    p[k] = make_float2(rk.x + bta * (pk.x - om * vk.x), rk.y + bta * (pk.y - om * vk.y));
+  }
+}
+
+__global__ void __launch_bounds__(NT32) k32_v(FineF F, Tile32 tm, const float2 *__restrict__ phat,
+                                              const float2 *__restrict__ rhat, float2 *__restrict__ v,
+                                              double *partials, unsigned *ticket, KState *st) {
+  if (st->done) return;
+  __shared__ HaloTile<float2> xT, nT;
+  double acc[1] = {0.0};
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int k;
+    float2 y;
+    if (!apply32(F, tm, t, phat, xT, nT, k, y)) continue;
+    v[k] = y;
+    acc[0] += dotf(rhat[k], y);
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, partials, ticket, tot)) {
+    if (tot[0] == 0.0 || !isfinite(tot[0])) {
+      st->done = 1;
+      st->status = isfinite(tot[0]) ? KSP_BREAKDOWN : KSP_NAN;
+    } else {
+      st->alpha = st->rho / tot[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT32) k32_s(int N, const float2 *__restrict__ r, const float2 *__restrict__ v,
+                                              float2 *__restrict__ s, const KState *st) {
+  if (st->done) return;
+  const float al = (float)st->alpha;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const float2 rk = r[k], vk = v[k];
+    s[k] = make_float2(rk.x - al * vk.x, rk.y - al * vk.y);
+  }
+}
+
+__global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *__restrict__ shat,
+                                              const float2 *__restrict__ s, float2 *__restrict__ tv, double *partials,
+                                              unsigned *ticket, KState *st) {
+  if (st->done) return;
+  __shared__ HaloTile<float2> xT, nT;
+  double acc[2] = {0.0, 0.0};
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int k;
+    float2 y;
+    if (!apply32(F, tm, t, shat, xT, nT, k, y)) continue;
+    tv[k] = y;
+    acc[0] += dotf(y, s[k]);
+    acc[1] += dotf(y, y);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) st->omega = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
+}
+
+__global__ void __launch_bounds__(NT32) k32_x(int N, const float2 *__restrict__ phat, const float2 *__restrict__ shat,
+                                              const float2 *__restrict__ s, const float2 *__restrict__ tv,
+                                              const float2 *__restrict__ rhat, float2 *__restrict__ d,
+                                              float2 *__restrict__ r, double *partials, unsigned *ticket,
+                                              KState *st) {
+  if (st->done) return;
+  const float al = (float)st->alpha, om = (float)st->omega;
+  double acc[2] = {0.0, 0.0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const float2 ph = phat[k], sh = shat[k], sk = s[k], tk = tv[k];
+    float2 dk = d[k];
+    dk.x += al * ph.x + om * sh.x;
+    dk.y += al * ph.y + om * sh.y;
+    d[k] = dk;
+    const float2 rk = make_float2(sk.x - om * tk.x, sk.y - om * tk.y);
+    r[k] = rk;
+    acc[0] += dotf(rhat[k], rk);
+    acc[1] += dotf(rk, rk);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) {
+    const double rho_new = tot[0];
+    st->rnorm2 = tot[1];
+    st->iter += 1;
+    const double rn = sqrt(tot[1]), tol = st->rtol * sqrt(st->bnorm2);
+    if (!isfinite(rn)) {
+      st->done = 1; st->status = KSP_NAN;
+    } else if (rn <= tol) {
+      st->done = 1; st->status = 0;
+    } else if (st->iter >= st->maxit) {
+      st->done = 1; st->status = KSP_MAXIT;
+    } else if (om == 0.0f || rho_new == 0.0) {
+      st->done = 1; st->status = KSP_BREAKDOWN;
+    } else {
+      st->beta = (rho_new / st->rho) * ((double)al / (double)om);
+      st->rho = rho_new;
+    }
+  }
+}
+
+int blocks_n(const Launch &L, int n) { return std::min((n + NT32 - 1) / NT32, L.max_blocks); }
+
+}  // namespace
+
+void launch_mixed_init(const Launch &L, int N, const Krylov32 &K) {
+  k32_init<<<blocks_n(L, N), NT32, 0, L.stream>>>(N, K.rhs, K.r, K.rhat, K.p, K.v, K.d, L.partials, L.ticket, K.st);
+  L.tick();
+}
+
+void launch_mixed_iteration(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H,
+                            const Krylov32 &K) {
+  const int N = g.Mx * g.My;
+  const FineF F = fine_view(g, f, H);
+  const Tile32 tm = tiles32(g);
+  const int bv = blocks_n(L, N), bt = std::min(tm.tiles, L.max_blocks);
+  k32_p<<<bv, NT32, 0, L.stream>>>(N, K.r, K.v, K.p, K.st);
+  mg_vcycle(L, g, f, H, K.p, K.phat, K.st);
+  k32_v<<<bt, NT32, 0, L.stream>>>(F, tm, K.phat, K.rhat, K.v, L.partials, L.ticket, K.st);
+  k32_s<<<bv, NT32, 0, L.stream>>>(N, K.r, K.v, K.s, K.st);
+  mg_vcycle(L, g, f, H, K.s, K.shat, K.st);
+  k32_t<<<bt, NT32, 0, L.stream>>>(F, tm, K.shat, K.s, K.t, L.partials, L.ticket, K.st);
+  k32_x<<<bv, NT32, 0, L.stream>>>(N, K.phat, K.shat, K.s, K.t, K.rhat, K.d, K.r, L.partials, L.ticket, K.st);
+  L.tick(5);
+}
+
+}  // namespace pism_gpu

@@ -122,13 +122,14 @@ def test_hardness_from_enthalpy(law):
     s.close()
 
 
-@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
-def test_linear_solve_matches_direct(pc):
+@pytest.mark.parametrize("pc,precision", [("bjacobi", "fp64"), ("mg", "fp64"), ("mg", "mixed")])
+def test_linear_solve_matches_direct(pc, precision):
     """One KSPSolve at the first Picard step (zero velocity: plastic drag 1e14, the worst
     conditioning of the solve).  Both answers must have tiny true residuals and agree."""
     g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=3)
     c.ksp_rtol = 1e-14
     c.pc_type = pc
+    c.precision = precision
     G, Cc, I = O.from_case(g, c, f)
     s = make_solver(g, c, f)
     s.assemble_rhs()
@@ -183,11 +184,12 @@ def _solve_case(g, c, f):
     return vel, st
 
 
-@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
+@pytest.mark.parametrize("pc,precision", [("bjacobi", "fp64"), ("mg", "fp64"), ("mg", "mixed")])
 @pytest.mark.parametrize("My", [61, 121])
-def test_verification_i(goldens, My, pc):
+def test_verification_i(goldens, My, pc, precision):
     g, c, f = V.build_test_i(My=My)
     c.pc_type = pc
+    c.precision = precision
     c.ssafd_relative_convergence = 5e-7
     c.ksp_rtol = 1e-12
     vel, st = _solve_case(g, c, f)
@@ -243,9 +245,9 @@ def test_zero_diagonal_is_reported():
     s.close()
 
 
-@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
+@pytest.mark.parametrize("pc,precision", [("bjacobi", "fp64"), ("mg", "fp64"), ("mg", "mixed")])
 @pytest.mark.parametrize("M", [45, 64])
-def test_synthetic_solve_matches_oracle(M, pc):
+def test_synthetic_solve_matches_oracle(M, pc, precision):
     """A whole SSAFD::solve of the synthetic sheet against the oracle, odd and even grid sizes
     (the multigrid aggregates wrap differently).  Pseudo-plastic till: its Picard iteration
     contracts ~25 % per step, so both solvers stop at the same iteration; with plastic till
@@ -255,6 +257,7 @@ def test_synthetic_solve_matches_oracle(M, pc):
     c.ssafd_relative_convergence = 1e-7
     c.ksp_rtol = 1e-12
     c.pc_type = pc
+    c.precision = precision
     vel, st = _solve_case(g, c, f)
     o = O.SSAFDOracle(*O.from_case(g, c, f))
     ref = o.solve()
