@@ -39,8 +39,9 @@ struct FineF {
 // rows / apply of a fine cell from staged tiles
 // the two FP32 rows of fine cell (i, j) from a staged tile of FP32 nu*H; false for a
 // diagonal-only row
-__device__ __forceinline__ bool fine_rows_tile(const FineF &F, int i, int j, uint32_t f, const HaloTile<float2> &nT,
-                                               int ti, int tj, Row2T<float> &e1, Row2T<float> &e2) {
+__device__ __forceinline__ bool fine_rows_tile(const FineF &F, int i, int j, uint32_t f, float bta,
+                                               const HaloTile<float2> &nT, int ti, int tj, Row2T<float> &e1,
+                                               Row2T<float> &e2) {
   if (f & F_DIAG_ONLY) return false;
   const GridDev &g = F.g;
   float c_w = nT[ti][tj + 1].x, c_e = nT[ti + 1][tj + 1].x, c_s = nT[ti + 1][tj].y, c_n = nT[ti + 1][tj + 1].y;
@@ -52,21 +53,23 @@ __device__ __forceinline__ bool fine_rows_tile(const FineF &F, int i, int j, uin
     if (f & F_NB_N) c_n = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, 0, 1)]));
     if (f & F_NB_S) c_s = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
   }
-  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, F.beta[cell(g, i, j)], e1, e2);
+  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, bta, e1, e2);
   return true;
 }
 
 // y = A x at fine cell (i, j) = tile position (ti, tj), x and nu*H from tiles
-__device__ __forceinline__ float2 fine_apply_tile(const FineF &F, int i, int j, const HaloTile<float2> &xT,
-                                                  const HaloTile<float2> &nT, int ti, int tj) {
-  const uint32_t f = F.flags[cell(F.g, i, j)];
+// f and bta (the cell's flag word and beta) are loaded by the caller together with the
+// halo tiles, so that a tile costs one round trip to memory
+__device__ __forceinline__ float2 fine_apply_tile(const FineF &F, int i, int j, uint32_t f, float bta,
+                                                  const HaloTile<float2> &xT, const HaloTile<float2> &nT, int ti,
+                                                  int tj) {
   if ((f & (F_WEIGHTS | F_DIAG_ONLY | F_NB_ANY)) == F_WEIGHTS) {
     auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
     return apply_regular<float, float2>(F.rdx2, F.rdy2, F.r2, F.r4, nT[ti][tj + 1].x, nT[ti + 1][tj + 1].x,
-                                        nT[ti + 1][tj].y, nT[ti + 1][tj + 1].y, F.beta[cell(F.g, i, j)], xr);
+                                        nT[ti + 1][tj].y, nT[ti + 1][tj + 1].y, bta, xr);
   }
   Row2T<float> e1, e2;
-  if (!fine_rows_tile(F, i, j, f, nT, ti, tj, e1, e2)) {
+  if (!fine_rows_tile(F, i, j, f, bta, nT, ti, tj, e1, e2)) {
     const float2 xc = xT[ti + 1][tj + 1];
     return make_float2(F.scaling * xc.x, F.scaling * xc.y);
   }

@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(NT) k_nuH(GridDev g, TileMap tm, pism_gpu_ssa_
 // y = A x at cell (i, j) = tile position (ti, tj), x and nu*H staged in halo tiles
 __device__ __forceinline__ double2 apply_cell_tile(const GridDev &g, const StencilConst &s, int i, int j, uint32_t f,
                                                    const HaloTile<double2> &xT, const HaloTile<double2> &nT,
-                                                   const double *__restrict__ beta, int ti, int tj) {
+                                                   double bta, int ti, int tj) {
   if (f & F_DIAG_ONLY) {
     const double2 xc = xT[ti + 1][tj + 1];
     return make_double2(s.scaling * xc.x, s.scaling * xc.y);
@@ -438,7 +438,6 @@ __device__ __forceinline__ double2 apply_cell_tile(const GridDev &g, const Stenc
     if (f & F_NB_S) c_s = s.nu_bedrock * 0.5 * (Hc + HE);   // thickness(i+1, j), as SSAFD.cc:582
   }
   auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
-  const double bta = beta[cell(g, i, j)];
   if ((f & F_WEIGHTS) == F_WEIGHTS)
     return apply_regular<double, double2>(s.rdx2, s.rdy2, s.r2, s.r4, c_w, c_e, c_s, c_n, bta, xr);
   Row2 e1, e2;
@@ -446,18 +445,27 @@ __device__ __forceinline__ double2 apply_cell_tile(const GridDev &g, const Stenc
   return apply_rows_rel<double, double2>(e1, e2, xr);
 }
 
-// stage the x and nu*H halo tiles of tile t; returns this thread's cell
+// Stage the x and nu*H halo tiles of tile t and load this thread's flags, beta and
+// (optionally) one more vector entry `extra`, all in the same round trip to memory.
+// Returns whether this thread's cell (i, j) lies inside the grid.
 __device__ __forceinline__ bool stage_tile(const GridDev &g, const TileMap &tm, int t, const double2 *__restrict__ x,
-                                           const double2 *__restrict__ nuH, HaloTile<double2> &xT,
-                                           HaloTile<double2> &nT, int &i, int &j) {
+                                           const double2 *__restrict__ nuH, const uint32_t *__restrict__ flags,
+                                           const double *__restrict__ beta, const double2 *__restrict__ extra,
+                                           HaloTile<double2> &xT, HaloTile<double2> &nT, int &i, int &j, int &k,
+                                           uint32_t &f, double &bta, double2 &ex) {
   const int i0 = (t / tm.tiles_j) * TI, j0 = (t % tm.tiles_j) * TJ;
+  i = i0 + (threadIdx.x >> 5);
+  j = j0 + (threadIdx.x & 31);
+  const bool inside = i < g.Mx && j < g.My;
+  k = inside ? i * g.My + j : 0;
+  f = flags[k];
+  bta = beta[k];
+  if (extra) ex = extra[k];
   __syncthreads();
   load_halo_tile<double2>(xT, i0, j0, g.Mx, g.My, [&](int a, int b) { return x[a * g.My + b]; });
   load_halo_tile<double2>(nT, i0, j0, g.Mx, g.My, [&](int a, int b) { return nuH[a * g.My + b]; });
   __syncthreads();
-  i = i0 + (threadIdx.x >> 5);
-  j = j0 + (threadIdx.x & 31);
-  return i < g.Mx && j < g.My;
+  return inside;
 }
 
 // y = A x (plain apply, for checking and for the residual of the refinement)
@@ -466,10 +474,12 @@ __global__ void __launch_bounds__(NT, 4) k_apply(GridDev g, TileMap tm, StencilC
                                               const double2 *__restrict__ x, double2 *__restrict__ y) {
   __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!stage_tile(g, tm, t, x, nuH, xT, nT, i, j)) continue;
-    const int k = cell(g, i, j);
-    y[k] = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
+    int i, j, k;
+    uint32_t f;
+    double bta;
+    double2 ex;
+    if (!stage_tile(g, tm, t, x, nuH, flags, beta, nullptr, xT, nT, i, j, k, f, bta, ex)) continue;
+    y[k] = apply_cell_tile(g, s, i, j, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
   }
 }
 
@@ -520,11 +530,12 @@ __global__ void __launch_bounds__(NT, 4) k_bicg_init(GridDev g, TileMap tm, Sten
   double acc[2] = {0.0, 0.0};
   __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!stage_tile(g, tm, t, x, nuH, xT, nT, i, j)) continue;
-    const int k = cell(g, i, j);
-    const double2 ax = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
-    const double2 bk = b[k];
+    int i, j, k;
+    uint32_t f;
+    double bta;
+    double2 bk;
+    if (!stage_tile(g, tm, t, x, nuH, flags, beta, b, xT, nT, i, j, k, f, bta, bk)) continue;
+    const double2 ax = apply_cell_tile(g, s, i, j, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
     const double2 rk = make_double2(bk.x - ax.x, bk.y - ax.y);
     r[k] = rk;
     rhat[k] = rk;
@@ -576,10 +587,12 @@ __global__ void __launch_bounds__(NT, 4) k_bicg_v(GridDev g, TileMap tm, Stencil
   double acc[1] = {0.0};
   __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!stage_tile(g, tm, t, phat, nuH, xT, nT, i, j)) continue;
-    const int k = cell(g, i, j);
-    const double2 vk = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
+    int i, j, k;
+    uint32_t f;
+    double bta;
+    double2 ex;
+    if (!stage_tile(g, tm, t, phat, nuH, flags, beta, nullptr, xT, nT, i, j, k, f, bta, ex)) continue;
+    const double2 vk = apply_cell_tile(g, s, i, j, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
     v[k] = vk;
     acc[0] += dot2(rhat[k], vk);
   }
@@ -619,10 +632,12 @@ __global__ void __launch_bounds__(NT, 4) k_bicg_t(GridDev g, TileMap tm, Stencil
   double acc[2] = {0.0, 0.0};
   __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!stage_tile(g, tm, t, shat, nuH, xT, nT, i, j)) continue;
-    const int k = cell(g, i, j);
-    const double2 tk = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
+    int i, j, k;
+    uint32_t f;
+    double bta;
+    double2 ex;
+    if (!stage_tile(g, tm, t, shat, nuH, flags, beta, nullptr, xT, nT, i, j, k, f, bta, ex)) continue;
+    const double2 tk = apply_cell_tile(g, s, i, j, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
     tv[k] = tk;
     acc[0] += dot2(tk, sv[k]);
     acc[1] += dot2(tk, tk);
@@ -683,11 +698,12 @@ __global__ void __launch_bounds__(NT, 4) k_residual32(GridDev g, TileMap tm, Ste
   double acc[2] = {0.0, 0.0};
   __shared__ HaloTile<double2> xT, nT;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int i, j;
-    if (!stage_tile(g, tm, t, x, nuH, xT, nT, i, j)) continue;
-    const int k = cell(g, i, j);
-    const double2 ax = apply_cell_tile(g, s, i, j, flags[k], xT, nT, beta, threadIdx.x >> 5, threadIdx.x & 31);
-    const double2 bk = b[k];
+    int i, j, k;
+    uint32_t f;
+    double bta;
+    double2 bk;
+    if (!stage_tile(g, tm, t, x, nuH, flags, beta, b, xT, nT, i, j, k, f, bta, bk)) continue;
+    const double2 ax = apply_cell_tile(g, s, i, j, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
     const double2 rk = make_double2(bk.x - ax.x, bk.y - ax.y);
     r32[k] = make_float2((float)rk.x, (float)rk.y);
     acc[0] += dot2(rk, rk);

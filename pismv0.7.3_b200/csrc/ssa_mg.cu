@@ -280,12 +280,9 @@ __global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, d
 // ---------------------------------------------------------------------------
 // V-cycle kernels
 // ---------------------------------------------------------------------------
-// y = A_l x at coarse cell (i, j) = tile position (ti, tj), x from a tile
-__device__ __forceinline__ float2 coarse_apply_tile(const LevelView &L, int k, const HaloTile<float2> &xT, int ti,
-                                                    int tj) {
-  float4 a[9];
-#pragma unroll
-  for (int b = 0; b < 9; ++b) a[b] = L.A[b * L.N + k];
+// y = A_l x at coarse cell = tile position (ti, tj); a[] = the cell's 9 stencil blocks,
+// loaded by the caller together with the tile
+__device__ __forceinline__ float2 coarse_apply_tile(const float4 (&a)[9], const HaloTile<float2> &xT, int ti, int tj) {
   float y1 = 0.0f, y2 = 0.0f;
 #pragma unroll
   for (int b = 0; b < 9; ++b) {
@@ -329,19 +326,23 @@ __global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const BV *__restr
   const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    const int i = i0 + ti, j = j0 + tj;
+    const bool inside = i < g.Mx && j < g.My;
+    const int k = inside ? i * g.My + j : 0;
+    const uint32_t f = F.flags[k];   // issued with the tile loads: one round trip per tile
+    const float bta = F.beta[k];
+    const float2 bk = to_f2(b[k]);
     __syncthreads();
-    load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) {
-      const int q = i * g.My + j;
+    load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int ii, int jj) {
+      const int q = ii * g.My + jj;
       const float2 v = fmul4(F.dinv[q], to_f2(b[q]));
       return make_float2(omega * v.x, omega * v.y);
     });
-    load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
+    load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int ii, int jj) { return F.nuH[ii * g.My + jj]; });
     __syncthreads();
-    const int i = i0 + ti, j = j0 + tj;
     float2 r = make_float2(0.0f, 0.0f);
-    if (i < g.Mx && j < g.My) {
-      const float2 y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
-      const float2 bk = to_f2(b[i * g.My + j]);
+    if (inside) {
+      const float2 y = fine_apply_tile(F, i, j, f, bta, xT, nT, ti, tj);
       r = make_float2(bk.x - y.x, bk.y - y.y);
     }
     rsh[ti][tj] = r;
@@ -361,22 +362,26 @@ __global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const BV *__restrict_
   const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    const int i = i0 + ti, j = j0 + tj;
+    const bool inside = i < g.Mx && j < g.My;
+    const int k = inside ? i * g.My + j : 0;
+    const uint32_t f = F.flags[k];   // issued with the tile loads: one round trip per tile
+    const float bta = F.beta[k];
+    const float2 bk = to_f2(b[k]);
+    const float4 dk = F.dinv[k];
     __syncthreads();
-    load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) {
-      const int q = i * g.My + j;
+    load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int ii, int jj) {
+      const int q = ii * g.My + jj;
       const float2 v = fmul4(F.dinv[q], to_f2(b[q]));
-      const float2 c = xc[(i / AX) * Myc + j / AY];
+      const float2 c = xc[(ii / AX) * Myc + jj / AY];
       return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
     });
-    load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
+    load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int ii, int jj) { return F.nuH[ii * g.My + jj]; });
     __syncthreads();
-    const int i = i0 + ti, j = j0 + tj;
-    if (i < g.Mx && j < g.My) {
-      const int k = i * g.My + j;
+    if (inside) {
       const float2 xk = xT[ti + 1][tj + 1];
-      const float2 y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
-      const float2 bk = to_f2(b[k]);
-      const float2 d = fmul4(F.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+      const float2 y = fine_apply_tile(F, i, j, f, bta, xT, nT, ti, tj);
+      const float2 d = fmul4(dk, make_float2(bk.x - y.x, bk.y - y.y));
       z[k] = from_f2<ZV>(make_float2(xk.x + omega * d.x, xk.y + omega * d.y));
     }
   }
@@ -392,19 +397,23 @@ __global__ void __launch_bounds__(NTm) k_mgc_restrict(LevelView L, float omega, 
   const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    const int i = i0 + ti, j = j0 + tj;
+    const bool inside = i < L.Mx && j < L.My;
+    const int k = inside ? i * L.My + j : 0;
+    float4 a[9];   // issued with the tile loads: one round trip per tile
+#pragma unroll
+    for (int q = 0; q < 9; ++q) a[q] = L.A[q * L.N + k];
+    const float2 bk = L.b[k];
     __syncthreads();
-    load_halo_tile<float2>(xT, i0, j0, L.Mx, L.My, [&](int i, int j) {
-      const int q = i * L.My + j;
+    load_halo_tile<float2>(xT, i0, j0, L.Mx, L.My, [&](int ii, int jj) {
+      const int q = ii * L.My + jj;
       const float2 v = fmul4(L.dinv[q], L.b[q]);
       return make_float2(omega * v.x, omega * v.y);
     });
     __syncthreads();
-    const int i = i0 + ti, j = j0 + tj;
     float2 r = make_float2(0.0f, 0.0f);
-    if (i < L.Mx && j < L.My) {
-      const int k = i * L.My + j;
-      const float2 y = coarse_apply_tile(L, k, xT, ti, tj);
-      const float2 bk = L.b[k];
+    if (inside) {
+      const float2 y = coarse_apply_tile(a, xT, ti, tj);
       r = make_float2(bk.x - y.x, bk.y - y.y);
     }
     rsh[ti][tj] = r;
@@ -422,21 +431,26 @@ __global__ void __launch_bounds__(NTm) k_mgc_post(LevelView L, float omega, floa
   const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    const int i = i0 + ti, j = j0 + tj;
+    const bool inside = i < L.Mx && j < L.My;
+    const int k = inside ? i * L.My + j : 0;
+    float4 a[9];   // issued with the tile loads: one round trip per tile
+#pragma unroll
+    for (int q = 0; q < 9; ++q) a[q] = L.A[q * L.N + k];
+    const float2 bk = L.b[k];
+    const float4 dk = L.dinv[k];
     __syncthreads();
-    load_halo_tile<float2>(xT, i0, j0, L.Mx, L.My, [&](int i, int j) {
-      const int q = i * L.My + j;
+    load_halo_tile<float2>(xT, i0, j0, L.Mx, L.My, [&](int ii, int jj) {
+      const int q = ii * L.My + jj;
       const float2 v = fmul4(L.dinv[q], L.b[q]);
-      const float2 c = xc[(i / AX) * Myc + j / AY];
+      const float2 c = xc[(ii / AX) * Myc + jj / AY];
       return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
     });
     __syncthreads();
-    const int i = i0 + ti, j = j0 + tj;
-    if (i < L.Mx && j < L.My) {
-      const int k = i * L.My + j;
+    if (inside) {
       const float2 xk = xT[ti + 1][tj + 1];
-      const float2 y = coarse_apply_tile(L, k, xT, ti, tj);
-      const float2 bk = L.b[k];
-      const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+      const float2 y = coarse_apply_tile(a, xT, ti, tj);
+      const float2 d = fmul4(dk, make_float2(bk.x - y.x, bk.y - y.y));
       L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
     }
   }

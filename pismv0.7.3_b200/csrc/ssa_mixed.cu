@@ -30,18 +30,22 @@ Tile32 tiles32(const GridDev &g) {
 }
 
 // y = A x at this thread's cell of tile t (FP32); false outside the grid
+// (the cell's flags and beta are issued with the tile loads: one round trip per tile)
 __device__ __forceinline__ bool apply32(const FineF &F, const Tile32 &tm, int t, const float2 *__restrict__ x,
                                         HaloTile<float2> &xT, HaloTile<float2> &nT, int &k, float2 &y) {
   const GridDev &g = F.g;
   const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
-  __syncthreads();
-  load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int i, int j) { return x[i * g.My + j]; });
-  load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int i, int j) { return F.nuH[i * g.My + j]; });
-  __syncthreads();
   const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31, i = i0 + ti, j = j0 + tj;
-  if (i >= g.Mx || j >= g.My) return false;
-  k = i * g.My + j;
-  y = fine_apply_tile(F, i, j, xT, nT, ti, tj);
+  const bool inside = i < g.Mx && j < g.My;
+  k = inside ? i * g.My + j : 0;
+  const uint32_t f = F.flags[k];
+  const float bta = F.beta[k];
+  __syncthreads();
+  load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int ii, int jj) { return x[ii * g.My + jj]; });
+  load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int ii, int jj) { return F.nuH[ii * g.My + jj]; });
+  __syncthreads();
+  if (!inside) return false;
+  y = fine_apply_tile(F, i, j, f, bta, xT, nT, ti, tj);
   return true;
 }
 
