@@ -3,12 +3,21 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size M]
 
 A step is one complete SSA solve (SSAFD::solve: driving stress, hardness, the
-Picard loop with its linear solves) from a zero initial guess, with the inputs
-of the plain-FP64 configuration: plastic till, Picard nu*H tolerance 1e-4,
-KSP rtol 1e-8.  The metric is milliseconds per solve (lower is better); with N
-GPUs every rank solves its own replica (no data-path collective: the solve
-does not shard) and ``value`` is the job's time per solve = max-over-ranks step
-time / N.
+Picard loop with its linear solves) of the seeded synthetic sheet (plastic till,
+Picard nu*H tolerance 1e-4).  Two solver set-ups run on the same inputs:
+
+* ``plain``: FP64 throughout, every Picard linear solve to KSP rtol 1e-8
+  (BiCGStab + aggregation multigrid), from a zero initial guess;
+* ``fast`` (the headline): inexact Picard (early linear solves only as accurate as
+  the nonlinear iteration needs, the accepted one to relative residual 1e-6), FP32
+  inner BiCGStab + FP32 multigrid inside FP64 iterative refinement, and the learned
+  warm start when trained weights are present.
+
+The metric is milliseconds per solve (lower is better) of ``--mode`` (default
+fast); the other set-up is timed once beside it and the fast result's velocity
+error against the plain FP64 result is reported.  With N GPUs every rank solves
+its own replica (no data-path collective: the solve does not shard) and
+``value`` is the job's time per solve = max-over-ranks step time / N.
 
 ``--impl reference`` times the CPU restatement of the reference's own path
 (numpy assembly of the SSAFD matrix + PETSc-style GMRES(30) / block-Jacobi
@@ -111,6 +120,13 @@ def build_case(M, pc="mg"):
     return g, c, f, meta
 
 
+def fast_config(c, precision="mixed"):
+    """The fast set-up: inexact Picard with FP32 inner solves; the accepted linear
+    solve reaches relative residual 1e-6 in FP64."""
+    return c.copy(precision=precision, ksp_rtol=1e-6, ksp_rtol_adaptive=True, ksp_rtol_factor=0.1,
+                  ksp_rtol_max=1e-2)
+
+
 def cpu_reference_sample(M, picard_sample, picard_full, nthreads):
     """The oracle port on the host cores: `picard_sample` Picard iterations of the
     reference algorithm (PETSc-style GMRES(30) + block Jacobi ILU(0), one block
@@ -176,7 +192,9 @@ def main():
     ap.add_argument("--mg-omega", type=float, default=None)
     ap.add_argument("--mg-correction", type=float, default=None)
     ap.add_argument("--verbosity", type=int, default=0)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mode", default="fast", choices=["fast", "plain"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="override the mode's precision (fast: mixed, plain: fp64)")
     ap.add_argument("--inner-rtol", type=float, default=None)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -194,15 +212,18 @@ def main():
     _package()
     from pism_b200.ssa import SSAFD
 
-    g, c, f, meta = build_case(args.size, args.pc)
+    g, c_plain, f, meta = build_case(args.size, args.pc)
     if args.mg_omega is not None:
-        c.mg_omega = args.mg_omega
+        c_plain.mg_omega = args.mg_omega
     if args.mg_correction is not None:
-        c.mg_correction = args.mg_correction
-    c.verbosity = args.verbosity
-    c.precision = args.precision
+        c_plain.mg_correction = args.mg_correction
+    c_plain.verbosity = args.verbosity
+    c_fast = fast_config(c_plain)
     if args.inner_rtol is not None:
-        c.mixed_inner_rtol = args.inner_rtol
+        c_fast.mixed_inner_rtol = args.inner_rtol
+    c, c_other = (c_fast, c_plain) if args.mode == "fast" else (c_plain, c_fast)
+    if args.precision is not None:
+        c.precision = args.precision
     M = args.size
     N = M * M
     dev = torch.device("cuda", local)
@@ -233,6 +254,7 @@ def main():
     launches = 0
     picard = []
     ksp = []
+    refine = []
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -245,8 +267,31 @@ def main():
         launches += st["kernel_launches"]
         picard.append(st["picard_iterations"])
         ksp.append(st["ksp_iterations"])
+        refine.append(st["refinement_steps"])
     torch.cuda.synchronize()
     clocks = sampler.stop()
+    vel_mode = out.clone()
+
+    # the other set-up on the same inputs, timed once (after one untimed solve)
+    s_other = SSAFD(g, c_other, device=local)
+    s_other.set_stream(stream.cuda_stream)
+    s_other.set_inputs(**dfields)
+    out_other = torch.empty_like(out)
+    for rep in range(2):
+        flush.fill_(1.0)
+        s_other.set_initial_guess(zero)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s_other.solve(out=out_other)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    other_ms = e0.elapsed_time(e1)
+    st_other = s_other.stats()
+    s_other.close()
+    vel_fast, vel_plain = (vel_mode, out_other) if args.mode == "fast" else (out_other, vel_mode)
+    err = vel_fast - vel_plain
+    vel_error = {"l2_rel": float(err.norm() / vel_plain.norm()),
+                 "linf_rel": float(err.abs().max() / vel_plain.abs().max())}
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -296,14 +341,22 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if c.precision == "fp64" else "f64+f32", "data": "synthetic",
         "config": {"workload": f"SSAFD solve, synthetic ice sheet {M}x{M} at {4000 / (M - 1):.0f} km, plastic till, "
-                               f"Picard 1e-4, KSP 1e-8 (plain FP64: BiCGStab + {'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'})",
-                   "grid": [M, M], "seed": 0, "precision": args.precision, "l2": "flushed (256 MB write) between steps",
+                               f"Picard 1e-4; {args.mode} set-up",
+                   "mode": args.mode, "grid": [M, M], "seed": 0, "precision": c.precision,
+                   "ksp": f"BiCGStab + {'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'}",
+                   "ksp_rtol": c.ksp_rtol, "ksp_rtol_adaptive": bool(c.ksp_rtol_adaptive),
+                   "warm_start": "zero", "l2": "flushed (256 MB write) between steps",
                    "parallelism": f"replicas x{world}"},
         "solver": {"picard_iterations": picard, "ksp_iterations": ksp, "converged": st["converged"],
-                   "refinement_steps": st["refinement_steps"],
+                   "refinement_steps": refine,
                    "strategy": st["strategy"], "final_linear_residual": st["final_linear_residual"]},
+        "comparison": {"other_mode": "plain" if args.mode == "fast" else "fast", "other_ms": other_ms,
+                       "other_picard_iterations": st_other["picard_iterations"],
+                       "other_ksp_iterations": st_other["ksp_iterations"],
+                       "plain_over_fast": (other_ms / ms_per_step) if args.mode == "fast" else (ms_per_step / other_ms),
+                       "fast_velocity_error_vs_plain_fp64": vel_error},
         "roofline": {"bound": "hbm", "kernel": "k_apply (SSAFD stencil, matrix-free)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                      "peak_kind": peak_kind, "bytes_per_launch": apply_bytes, "launch_ms": apply_ms},
@@ -313,10 +366,11 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        cms, done, dt = cpu_reference_sample(M, args.cpu_picard, picard[-1], nthreads)
+        picard_plain = st_other["picard_iterations"] if args.mode == "fast" else picard[-1]
+        cms, done, dt = cpu_reference_sample(M, args.cpu_picard, picard_plain, nthreads)
         line["cpu_baseline"] = {"value": cms, "unit": "ms", "cores": nthreads, "kind": "port",
                                 "sample": f"first {done} Picard iterations of the same solve ({dt:.1f} s), "
-                                          f"scaled to the GPU run's {picard[-1]} Picard iterations"}
+                                          f"scaled to the plain GPU solve's {picard_plain} Picard iterations"}
     if rank == 0:
         print(json.dumps(line))
     s.close()

@@ -119,6 +119,11 @@ typedef struct pism_gpu_ssa_config {
   double mixed_inner_rtol;                         /* inner FP32 solve tolerance     */
   double mg_omega;                                 /* multigrid smoother damping     */
   double mg_correction;                            /* coarse-correction scaling      */
+  /* inexact Picard: KSP rtol of iteration k = clamp(ksp_rtol_factor * (last relative nu*H
+     change), ksp_rtol, ksp_rtol_max); the accepted last iteration is always solved to ksp_rtol */
+  int    ksp_rtol_adaptive;                        /* 0: every solve to ksp_rtol     */
+  double ksp_rtol_max;
+  double ksp_rtol_factor;
   int    verbosity;                                /* 0 silent .. 3 per-iteration    */
 } pism_gpu_ssa_config;
 

@@ -89,6 +89,9 @@ class SSAConfig:
     mixed_inner_rtol: float = 1.0e-3
     mg_omega: float = 0.9
     mg_correction: float = 1.2
+    ksp_rtol_adaptive: bool = False
+    ksp_rtol_max: float = 1.0e-2
+    ksp_rtol_factor: float = 1.0e-2
     verbosity: int = 0
     # geometry helpers (not part of the C struct)
     mask_icefree_thickness_standard: float = 0.01
@@ -143,7 +146,8 @@ class CConfig(C.Structure):
         ("fracture_density_softening_lower_limit", _D), ("brutal_sliding", _I),
         ("brutal_sliding_scale", _D), ("ksp_type", _I), ("pc_type", _I), ("ksp_rtol", _D),
         ("ksp_max_it", _I), ("gmres_restart", _I), ("precision", _I), ("mixed_inner_rtol", _D),
-        ("mg_omega", _D), ("mg_correction", _D), ("verbosity", _I),
+        ("mg_omega", _D), ("mg_correction", _D), ("ksp_rtol_adaptive", _I), ("ksp_rtol_max", _D),
+        ("ksp_rtol_factor", _D), ("verbosity", _I),
     ]
 
 

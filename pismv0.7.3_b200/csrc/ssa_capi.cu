@@ -150,6 +150,8 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "mixed_inner_rtol must be in (0, 1)");
   if (c->pc_type != PISM_PC_BLOCK_JACOBI && c->pc_type != PISM_PC_MULTIGRID)
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
+  if (c->ksp_rtol_adaptive && !(c->ksp_rtol_max >= c->ksp_rtol && c->ksp_rtol_max < 1.0 && c->ksp_rtol_factor > 0.0))
+    return fail(h, PISM_GPU_SSA_EINVAL, "adaptive KSP tolerance needs ksp_rtol <= ksp_rtol_max < 1, ksp_rtol_factor > 0");
   if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
     return fail(h, PISM_GPU_SSA_EINVAL, "ksp_rtol, ksp_max_it and max_iterations_ssafd must be positive");
   if (!(c->ssa_Glen_exponent > 0.0) || !(c->min_thickness_strength_extension_ssa > 0.0))
@@ -158,11 +160,11 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
 }
 
 // ---- one linear solve: BiCGStab on the device, host reads the state per chunk ----
-int linear_solve(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
+int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
   const GridDev &g = h->g;
   Fields f = fields_of(h);
   KState init{};
-  init.rtol = h->cfg.ksp_rtol;
+  init.rtol = rtol;
   init.maxit = h->use_fallback ? 4 * h->cfg.ksp_max_it : h->cfg.ksp_max_it;
   *h->st_host = init;
   CK(h, cudaMemcpyAsync(h->K.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
@@ -189,7 +191,7 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
 
 // Mixed precision: FP64 iterative refinement around FP32 BiCGStab + FP32 multigrid.  The
 // convergence test ||b - A x|| <= ksp_rtol ||b|| is evaluated in FP64 each refinement step.
-int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_out) {
+int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
   const GridDev &g = h->g;
   Fields f = fields_of(h);
   const MGHierarchy *mg = active_mg(h);
@@ -202,10 +204,12 @@ int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, int *its_out, int *status_ou
     const double rn = sqrt(h->res_host[0]), bn = sqrt(h->res_host[1]);
     h->stats.final_linear_residual = bn > 0 ? rn / bn : rn;
     if (!std::isfinite(rn)) { status = KSP_NAN; break; }
-    if (rn <= h->cfg.ksp_rtol * bn || bn == 0.0) break;
+    if (rn <= rtol * bn || bn == 0.0) break;
     if (refine >= max_refine) { status = KSP_MAXIT; break; }
+    // the inner solve reduces its residual by what this step still needs (with a margin),
+    // but never asks FP32 for more than mixed_inner_rtol
     KState init{};
-    init.rtol = h->cfg.mixed_inner_rtol;
+    init.rtol = std::min(0.5, std::max(h->cfg.mixed_inner_rtol, 0.7 * rtol * bn / rn));
     init.maxit = h->cfg.ksp_max_it;
     *h->st_host = init;
     CK(h, cudaMemcpyAsync(h->K32.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
@@ -236,13 +240,19 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
   const pism_gpu_ssa_config &c = h->cfg;
   Fields f = fields_of(h);
   launch_nuH(h->L, h->g, c, f, reg, 1.0, false, h->norm_dev);
+  double last_change = 1.0;   // relative nu*H change of the previous iteration
   for (int k = 0; k < c.max_iterations_ssafd; ++k) {
     RET(pc_setup(h));
+    // inexact Picard: the linear solve of an iterate that is still far from the fixed point
+    // only needs to be as accurate as the nonlinear iteration it feeds
+    double rtol = c.ksp_rtol;
+    if (c.ksp_rtol_adaptive && last_change >= 2.0 * c.ssafd_relative_convergence)
+      rtol = std::min(c.ksp_rtol_max, std::max(c.ksp_rtol, c.ksp_rtol_factor * last_change));
     int its = 0, status = 0;
     if (h->cfg.precision == PISM_PRECISION_MIXED && active_mg(h))
-      RET(linear_solve_mixed(h, h->vel, &its, &status));
+      RET(linear_solve_mixed(h, h->vel, rtol, &its, &status));
     else
-      RET(linear_solve(h, h->vel, &its, &status));
+      RET(linear_solve(h, h->vel, rtol, &its, &status));
     CK(h, cudaMemcpyAsync(h->zd_host, h->zd_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     h->stats.ksp_iterations += its;
@@ -263,11 +273,12 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
     h->stats.nuH_norm = norm;
     h->stats.nuH_norm_change = change;
     if (c.verbosity > 2)
-      fprintf(stderr, "  %2d: S:%d,%d: |nu|_2, |Delta nu|_2/|nu|_2 = %10.3e %10.3e\n", k, its, status, norm,
-              change / norm);
+      fprintf(stderr, "  %2d: S:%d,%d (rtol %.1e): |nu|_2, |Delta nu|_2/|nu|_2 = %10.3e %10.3e\n", k, its, status,
+              rtol, norm, change / norm);
     if (!std::isfinite(norm) || !std::isfinite(change))
       return fail(h, PISM_GPU_SSA_ENAN, "non-finite nu*H norm at Picard iteration %d", k);
-    if (norm == 0 || change / norm < c.ssafd_relative_convergence) return PISM_GPU_SSA_OK;
+    if (norm == 0 || (change / norm < c.ssafd_relative_convergence && rtol <= c.ksp_rtol)) return PISM_GPU_SSA_OK;
+    last_change = norm > 0 ? change / norm : 0.0;
   }
   return fail(h, PISM_GPU_SSA_EPICARD,
               "SSAFD Picard iterations failed: effective viscosity not converged after %d iterations with "
@@ -402,6 +413,9 @@ int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *c) {
   c->mixed_inner_rtol = 1.0e-3;
   c->mg_omega = 0.9;
   c->mg_correction = 1.2;
+  c->ksp_rtol_adaptive = 0;
+  c->ksp_rtol_max = 1.0e-2;
+  c->ksp_rtol_factor = 1.0e-2;
   c->verbosity = 0;
   return PISM_GPU_SSA_OK;
 }
@@ -690,9 +704,9 @@ int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, d
   RET(pc_setup(h));
   int its = 0, status = 0;
   if (h->cfg.precision == PISM_PRECISION_MIXED && active_mg(h))
-    RET(linear_solve_mixed(h, (double2 *)x_dev, &its, &status));
+    RET(linear_solve_mixed(h, (double2 *)x_dev, h->cfg.ksp_rtol, &its, &status));
   else
-    RET(linear_solve(h, (double2 *)x_dev, &its, &status));
+    RET(linear_solve(h, (double2 *)x_dev, h->cfg.ksp_rtol, &its, &status));
   if (iterations) *iterations = its;
   if (rel_residual) *rel_residual = h->stats.final_linear_residual;
   if (status != KSP_OK)

@@ -264,3 +264,29 @@ def test_synthetic_solve_matches_oracle(M, pc, precision):
     assert st["converged"] == 1 and st["strategy"] == o.stats.strategy
     assert abs(st["picard_iterations"] - o.stats.picard_iterations) <= 1
     assert rel(vel, ref) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_inexact_picard_meets_the_same_tolerance(precision):
+    """ksp_rtol_adaptive: early Picard iterations solve to 0.1 x the last relative nu*H
+    change (at most 1e-2), the accepted iteration to ksp_rtol.  The result agrees with
+    the oracle's exact-solve Picard to well inside the 1e-5 velocity bar, in the same
+    number of Picard iterations, with fewer Krylov iterations than exact solves take."""
+    g, c, f, _ = S.build_synthetic(45, 4000e3 / 44, seed=2)
+    c.do_pseudo_plastic_till = True
+    c.ssafd_relative_convergence = 1e-7
+    c.ksp_rtol = 1e-10
+    c.pc_type = "mg"
+    c.precision = precision
+    c.ksp_rtol_adaptive = True
+    c.ksp_rtol_factor = 0.1
+    c.ksp_rtol_max = 1e-2
+    vel, st = _solve_case(g, c, f)
+    o = O.SSAFDOracle(*O.from_case(g, c, f))
+    ref = o.solve()
+    assert st["converged"] == 1
+    assert st["final_linear_residual"] <= 1e-10
+    assert abs(st["picard_iterations"] - o.stats.picard_iterations) <= 1
+    assert rel(vel, ref) < 1e-7
+    exact_ksp = _solve_case(g, c.copy(ksp_rtol_adaptive=False), f)[1]["ksp_iterations"]
+    assert st["ksp_iterations"] < 0.8 * exact_ksp
