@@ -27,6 +27,12 @@ EXPORTS = [
     "pism_gpu_ssa_assemble_rhs", "pism_gpu_ssa_compute_hardness", "pism_gpu_ssa_compute_nuH",
     "pism_gpu_ssa_apply", "pism_gpu_ssa_linear_solve", "pism_gpu_ssa_nuH_noalloc",
 ]
+# every symbol include/pism_unet_gpu.h declares
+UNET_EXPORTS = [
+    "pism_gpu_unet_param_count", "pism_gpu_unet_create", "pism_gpu_unet_destroy", "pism_gpu_unet_last_error",
+    "pism_gpu_unet_set_stream", "pism_gpu_unet_set_params", "pism_gpu_unet_get_params", "pism_gpu_unet_forward",
+    "pism_gpu_unet_backward", "pism_gpu_unet_adam", "pism_gpu_ssa_learned_features", "pism_gpu_ssa_learned_guess",
+]
 
 _lib = None
 
@@ -57,6 +63,18 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_apply": (I, [V, V, V]),
         "pism_gpu_ssa_linear_solve": (I, [V, V, P(I), P(D)]),
         "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
+        "pism_gpu_unet_param_count": (C.c_longlong, []),
+        "pism_gpu_unet_create": (I, [I, I, I, I, P(V)]),
+        "pism_gpu_unet_destroy": (I, [V]),
+        "pism_gpu_unet_last_error": (C.c_char_p, [V]),
+        "pism_gpu_unet_set_stream": (I, [V, V]),
+        "pism_gpu_unet_set_params": (I, [V, V, I]),
+        "pism_gpu_unet_get_params": (I, [V, V, I]),
+        "pism_gpu_unet_forward": (I, [V, V, I, I, I, V]),
+        "pism_gpu_unet_backward": (I, [V, V, V, P(C.c_float), V]),
+        "pism_gpu_unet_adam": (I, [V, C.c_float, C.c_float, C.c_float, C.c_float]),
+        "pism_gpu_ssa_learned_features": (I, [V, I, V, I, I]),
+        "pism_gpu_ssa_learned_guess": (I, [V, V, I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

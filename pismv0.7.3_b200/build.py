@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "lib")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
-CU_SOURCES = ["ssa_kernels.cu", "ssa_mg.cu", "ssa_mixed.cu", "ssa_capi.cu", "ssa_noalloc.cu"]
+CU_SOURCES = ["ssa_kernels.cu", "ssa_mg.cu", "ssa_mixed.cu", "ssa_capi.cu", "ssa_noalloc.cu", "unet.cu"]
 
 
 def _newer(target, sources):
@@ -32,9 +32,10 @@ def _newer(target, sources):
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     so = os.path.join(LIB, "libpism_ssa_gpu.so")
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(REPO, "include", "pism_ssa_gpu.h")]
+    inc = os.path.join(REPO, "include")
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(inc, f) for f in os.listdir(inc)]
     if force or _newer(so, deps):
-        cmd = ["nvcc", *NVCC_FLAGS, "-shared", "-o", so, *[os.path.join(CSRC, f) for f in CU_SOURCES]]
+        cmd = ["nvcc", *NVCC_FLAGS, "-I", inc, "-shared", "-o", so, *[os.path.join(CSRC, f) for f in CU_SOURCES]]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

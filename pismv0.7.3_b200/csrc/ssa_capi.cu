@@ -12,7 +12,9 @@
 #include <string>
 #include <vector>
 
+#include "pism_unet_gpu.h"
 #include "ssa_internal.h"
+#include "unet_internal.h"
 
 using namespace pism_gpu;
 
@@ -54,6 +56,9 @@ struct pism_gpu_ssa {
   int default_pc_failure_count = 0;   // SSAFD.cc:252-253 (m_default_pc_failure_*)
   int use_fallback = 0;
   int last_ksp_its = 0;
+  // the learned initial guess: feature image and network output
+  float *lfeat = nullptr, *lout = nullptr;
+  size_t lcap = 0;   // pixels allocated
   std::string err;
   pism_gpu_ssa_stats stats{};
 };
@@ -508,7 +513,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->vel_old, h->beta, h->bfrict, h->flags, h->K.r, h->K.rhat, h->K.p, h->K.v, h->K.s, h->K.t,
                  h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev,
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.s, h->K32.t, h->K32.phat,
-                 h->K32.shat, h->K32.d, h->K32.st, h->res_dev};
+                 h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -711,6 +716,67 @@ int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, d
   if (rel_residual) *rel_residual = h->stats.final_linear_residual;
   if (status != KSP_OK)
     return fail(h, PISM_GPU_SSA_EKSP, "SSAFD KSP (linear solver) failed: reason %d after %d iterations", status, its);
+  return PISM_GPU_SSA_OK;
+}
+
+// ---- the learned initial guess (include/pism_unet_gpu.h) ----
+namespace {
+
+int learned_image(pism_gpu_ssa *h, int stride, int *height, int *width) {
+  if (stride < 1 || stride > 2) return fail(h, PISM_GPU_SSA_EINVAL, "stride must be 1 or 2");
+  *height = ((h->g.Mx + stride - 1) / stride + 7) / 8 * 8;
+  *width = ((h->g.My + stride - 1) / stride + 7) / 8 * 8;
+  if (!h->prepared) RET(prepare(h));
+  return PISM_GPU_SSA_OK;
+}
+
+}  // namespace
+
+int pism_gpu_ssa_learned_features(pism_gpu_ssa *h, int stride, float *features_dev, int height, int width) {
+  if (!h || !features_dev) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  int hh = 0, ww = 0;
+  RET(learned_image(h, stride, &hh, &ww));
+  if (height < (h->g.Mx + stride - 1) / stride || width < (h->g.My + stride - 1) / stride)
+    return fail(h, PISM_GPU_SSA_EINVAL, "feature image %d x %d is smaller than the grid at stride %d", height, width,
+                stride);
+  pism_unet::launch_features(h->stream, h->g.Mx, h->g.My, stride, h->H, h->bed, h->tauc, h->hardness, h->mask,
+                             h->taud, features_dev, height, width);
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_learned_guess(pism_gpu_ssa *h, pism_gpu_unet *net, int stride) {
+  if (!h || !net) return PISM_GPU_SSA_EINVAL;
+  if (pism_unet::device_of(net) != h->device)
+    return fail(h, PISM_GPU_SSA_EINVAL, "network and solver on different devices");
+  DeviceGuard dg(h->device);
+  int hh = 0, ww = 0;
+  RET(learned_image(h, stride, &hh, &ww));
+  const size_t pix = (size_t)hh * ww;
+  if (pix > h->lcap) {
+    if (h->lfeat) cudaFree(h->lfeat);
+    if (h->lout) cudaFree(h->lout);
+    h->lfeat = h->lout = nullptr;
+    h->lcap = 0;
+    CK(h, cudaMalloc((void **)&h->lfeat, pix * 8 * sizeof(float)));
+    CK(h, cudaMalloc((void **)&h->lout, pix * 2 * sizeof(float)));
+    h->lcap = pix;
+  }
+  pism_unet::launch_features(h->stream, h->g.Mx, h->g.My, stride, h->H, h->bed, h->tauc, h->hardness, h->mask,
+                             h->taud, h->lfeat, hh, ww);
+  CK(h, cudaGetLastError());
+  // the network runs on the solver's stream for this call
+  cudaStream_t ns = pism_unet::stream_of(net);
+  pism_gpu_unet_set_stream(net, h->stream);
+  const int rc = pism_gpu_unet_forward(net, h->lfeat, 1, hh, ww, h->lout);
+  pism_gpu_unet_set_stream(net, ns);
+  if (rc != PISM_GPU_SSA_OK)
+    return fail(h, rc, "learned guess: network forward failed: %s", pism_gpu_unet_last_error(net));
+  pism_unet::launch_velocity(h->stream, h->lout, hh, ww, stride, h->g.Mx, h->g.My, 31556925.9747, h->vel);
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
   return PISM_GPU_SSA_OK;
 }
 

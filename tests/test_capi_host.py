@@ -37,6 +37,26 @@ def test_library_exports_every_declared_symbol(lib):
         assert hasattr(lib, d)
 
 
+def test_unet_library_exports_every_declared_symbol(lib):
+    txt = open(os.path.join(REPO, "include", "pism_unet_gpu.h")).read()
+    decl = sorted(set(re.findall(r"^(?:int|const char \*|long long)\s*(pism_gpu_\w+)\s*\(", txt, flags=re.M)))
+    assert sorted(_capi.UNET_EXPORTS) == decl
+    out = subprocess.run(["nm", "-D", "--defined-only", _capi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (pism_gpu_\w+)", out))
+    assert not [d for d in decl if d not in exported]
+
+
+def test_unet_param_count_matches_the_oracle(lib):
+    from oracle import unet_oracle as U
+    assert lib.pism_gpu_unet_param_count() == U.param_count()
+
+
+def test_unet_rejects_bad_shapes_without_touching_cuda(lib):
+    h = C.c_void_p()
+    for args in ((0, 0, 16, 16), (0, 1, 12, 16), (0, 1, 16, 4), (0, 1, 0, 16)):
+        assert lib.pism_gpu_unet_create(*args, C.byref(h)) == _capi.EINVAL
+
+
 def _c_layout():
     """sizeof / offsetof of the C structs, compiled from the header with gcc."""
     src = r'''
