@@ -57,7 +57,7 @@ struct Launch {
 
 // ---- aggregation multigrid (ssa_mg.cu) ----
 constexpr int MG_MAX_LEVELS = 16;
-constexpr int MG_COARSE_DIM = 8;                 // the coarsest level has <= 8 x 8 cells
+constexpr int MG_COARSE_DIM = 4;                 // the coarsest level has <= 4 x 4 cells
 constexpr int MG_MAX_COARSE_CELLS = MG_COARSE_DIM * MG_COARSE_DIM;
 constexpr int MG_CTA_CELLS = 4096;               // levels this small are cycled by one CTA
 

@@ -5,12 +5,12 @@
 //
 // Hierarchy: level 0 is the fine SSAFD operator, applied matrix-free from an FP32 copy of
 // nu*H and beta (refreshed once per Picard iteration) and the flag word.  Level l+1
-// aggregates 2 x 2 cells of level l (1 in a direction that is already <= 8 cells) and
+// aggregates 2 x 2 cells of level l (1 in a direction that is already <= 4 cells) and
 // carries the Galerkin operator R A P with piecewise-constant P (R = P^T): the sum, over
 // the aggregate, of the fine 2 x 2 blocks grouped by the neighbouring aggregate they
 // couple to.  With a 3 x 3 fine stencil this is again a 3 x 3 stencil of 2 x 2 blocks,
 // stored as 9 float4 arrays (one per block) so that a warp reads 512 contiguous bytes per
-// block.  The coarsest level (<= 8 x 8 cells) is inverted densely in FP64.
+// block.  The coarsest level (<= 4 x 4 cells) is inverted densely in FP64.
 //
 // Cycle (a V(1,1) cycle used as a fixed preconditioner z = M^-1 b):
 //   x_l = omega D_l^-1 b_l                       (computed on the fly, never stored)
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc,
 }
 
 // Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial
-// pivoting, in place in shared memory (n <= 2 * 64), one CTA; written transposed so
+// pivoting, in place in shared memory (n <= 2 * 16), one CTA; written transposed so
 // that the per-cycle product reads it coalesced.  Rows are spread over 8-lane groups.
 __global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
   extern __shared__ double a[];   // n * n, row-major
@@ -478,7 +478,7 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   // the small levels' operators are evicted from L2 by the fine-level passes between
   // cycles; pull all of them back in at once instead of one dependent round per step
   for (int l = S.first; l <= S.last; ++l) {
-    const LevelView &L = S.lev[l];
+    const LevelView L = S.lev[l];
     const char *A = reinterpret_cast<const char *>(L.A), *D = reinterpret_cast<const char *>(L.dinv);
     const int lines_A = (9 * L.N * (int)sizeof(float4) + 127) / 128, lines_D = (L.N * (int)sizeof(float4) + 127) / 128;
     for (int q = rank; q < lines_A + lines_D; q += nthr) {
@@ -488,34 +488,44 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   }
   __shared__ float2 xs[MG_CTA_CELLS];
   __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
+  // Each step below costs one dependent round trip to L2: the staging loops are unrolled so
+  // a thread's loads issue together, and the restriction gives every fine cell of an
+  // aggregate its own thread (four per coarse cell, summed by shuffles).
   // down
   for (int l = S.first; l < S.last; ++l) {
-    const LevelView &L = S.lev[l], &C = S.lev[l + 1];
+    const LevelView L = S.lev[l], C = S.lev[l + 1];
+#pragma unroll 4
     for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
       const float2 v = fmul4(L.dinv[q], L.b[q]);
       xs[q] = make_float2(omega * v.x, omega * v.y);
     }
     __syncthreads();
     auto xa = [&](int ii, int jj) { return xs[ii * L.My + jj]; };
-    for (int kc = rank; kc < C.N; kc += nthr) {
-      const int I = kc / C.My, J = kc - I * C.My;
+    const int span = (4 * C.N + 31) & ~31;   // whole warps take part in the shuffles
+    for (int base = rank; base < span; base += nthr) {
+      const int kc = base >> 2, pi = (base >> 1) & 1, pj = base & 1;
       float ru = 0.0f, rv = 0.0f;
-      for (int pi = 0; pi < L.ax; ++pi)
-        for (int pj = 0; pj < L.ay; ++pj) {
-          const int i = I * L.ax + pi, j = J * L.ay + pj;
-          if (i >= L.Mx || j >= L.My) continue;
+      if (kc < C.N && pi < L.ax && pj < L.ay) {
+        const int I = kc / C.My, J = kc - I * C.My;
+        const int i = I * L.ax + pi, j = J * L.ay + pj;
+        if (i < L.Mx && j < L.My) {
           const float2 y = coarse_apply(L, i, j, xa);
           const float2 bk = L.b[i * L.My + j];
-          ru += bk.x - y.x;
-          rv += bk.y - y.y;
+          ru = bk.x - y.x;
+          rv = bk.y - y.y;
         }
-      C.b[kc] = make_float2(ru, rv);
+      }
+      ru += __shfl_xor_sync(0xffffffffu, ru, 1);
+      rv += __shfl_xor_sync(0xffffffffu, rv, 1);
+      ru += __shfl_xor_sync(0xffffffffu, ru, 2);
+      rv += __shfl_xor_sync(0xffffffffu, rv, 2);
+      if (kc < C.N && (base & 3) == 0) C.b[kc] = make_float2(ru, rv);
     }
     cluster.sync();
   }
   // coarsest: x = A^-1 b
   {
-    const LevelView &C = S.lev[S.last];
+    const LevelView C = S.lev[S.last];
     for (int q = threadIdx.x; q < C.N; q += CTA_THREADS) {
       const float2 v = C.b[q];
       bsh[2 * q] = v.x;
@@ -536,7 +546,8 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   }
   // up
   for (int l = S.last - 1; l >= S.first; --l) {
-    const LevelView &L = S.lev[l], &C = S.lev[l + 1];
+    const LevelView L = S.lev[l], C = S.lev[l + 1];
+#pragma unroll 4
     for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
       const int i = q / L.My, j = q - i * L.My;
       const float2 v = fmul4(L.dinv[q], L.b[q]);
