@@ -41,9 +41,9 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(REPO, "pismv0.7.3_b200")
 METRIC = "SSA solve ms at 801² to rel resid 1e-6: learned+FP32 vs plain FP64, 1 B200"
-# Picard iterations of the GPU FP64 solve of the 801^2 seed-0 case (used to scale the
-# CPU sample to a whole solve when the GPU arm has not run in this process)
-DEFAULT_PICARD_801 = None
+# Picard iterations of the plain FP64 GPU solve of the 801^2 seed-0 sheet (measured; the
+# reference arm scales its CPU sample to a whole solve with it)
+DEFAULT_PICARD_801 = 184
 
 
 def _package():
@@ -127,6 +127,33 @@ def fast_config(c, precision="mixed"):
                   ksp_rtol_max=1e-2)
 
 
+def mg_levels(M):
+    """cells of the multigrid levels below the fine grid (2 x 2 aggregation down to <= 4 x 4)"""
+    out, mx, my = [], M, M
+    while mx > 4 or my > 4:
+        mx, my = (mx + 1) // 2 if mx > 4 else mx, (my + 1) // 2 if my > 4 else my
+        out.append(mx * my)
+    return out
+
+
+def iteration_bytes(M, precision):
+    """Algorithmic HBM bytes of one inner BiCGStab iteration with two V(1,1) cycles: every
+    array a kernel reads or writes, once per kernel (halo neighbours counted once).
+    FP32 Krylov (mixed): v, t 40 B/cell (x 8, nu*H 8, beta 4, flags 4, dot operand 8, out 8),
+    x 64, p 32, s 24.  FP64 Krylov: v, t 76, x 128, p 64, s 48.  Per V-cycle, fine level:
+    restrict b + D^-1 + nu*H + beta + flags (40 / 48 B), post the same + z (50 / 64 B), plus
+    the first coarse vector written and read (16 B per coarse cell); coarse levels: the
+    nine 2 x 2 blocks, D^-1 and b read by both passes and x written (344 B per cell)."""
+    N0 = M * M
+    lev = mg_levels(M)
+    if precision == "mixed":
+        krylov, fine = 200, 90
+    else:
+        krylov, fine = 392, 112
+    vcycle = fine * N0 + 16 * lev[0] + 344 * sum(lev)
+    return krylov * N0 + 2 * vcycle
+
+
 def cpu_reference_sample(M, picard_sample, picard_full, nthreads):
     """The oracle port on the host cores: `picard_sample` Picard iterations of the
     reference algorithm (PETSc-style GMRES(30) + block Jacobi ILU(0), one block
@@ -153,7 +180,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     nthreads = os.cpu_count() or 1
-    picard_full = args.picard_full or 160
+    picard_full = args.picard_full or DEFAULT_PICARD_801
     vals = []
     sample = None
     for k in range(args.warmup + args.steps):
@@ -366,12 +393,30 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = float(te.item()) / world
 
-    # roofline of the dominant kernel: the matrix-free SSAFD apply at the final nu*H
+    # Roofline of the hot loop: one inner BiCGStab + multigrid iteration (the kernels that
+    # repeat ~850 times per fast solve), timed live on a tight linear solve at the final nu*H
+    peak, peak_kind = _peaks()
+    s.set_config(c.copy(ksp_rtol=1e-10, ksp_rtol_adaptive=False))
+    xk = torch.zeros((M, M, 2), dtype=torch.float64, device=dev)
+    s.linear_solve(xk)                     # warm-up
+    xk.zero_()
+    flush.fill_(1.0)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    lin_its, lin_res = s.linear_solve(xk)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    lin_ms = ev[0].elapsed_time(ev[1])
+    it_ms = lin_ms / max(1, lin_its)
+    it_bytes = iteration_bytes(M, c.precision)
+    achieved = it_bytes / (it_ms * 1e-3) / 1e9
+    s.set_config(c)
+
+    # the FP64 matrix-free apply alone (the plain set-up's stencil)
     x = torch.randn((M, M, 2), dtype=torch.float64, device=dev) * 1e-5
     y = torch.empty_like(x)
     for _ in range(5):
         s.apply(x, y)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     flush.fill_(1.0)
     ev[0].record(stream)
     for _ in range(args.apply_launches):
@@ -379,10 +424,7 @@ def main():
     ev[1].record(stream)
     torch.cuda.synchronize()
     apply_ms = ev[0].elapsed_time(ev[1]) / args.apply_launches
-    # algorithmic bytes per cell: x 16, nu*H 16, beta 8, flags 4, y 16 (neighbours counted once)
-    apply_bytes = 60 * N
-    achieved = apply_bytes / (apply_ms * 1e-3) / 1e9
-    peak, peak_kind = _peaks()
+    apply_bytes = 60 * N   # x 16, nu*H 16, beta 8, flags 4, y 16 per cell (neighbours counted once)
 
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -406,9 +448,17 @@ def main():
                                            (other_ms / ms_per_step) if args.mode == "fast" else (ms_per_step / other_ms)),
                        "fast_velocity_error_vs_plain_fp64": vel_error,
                        "accuracy": accuracy},
-        "roofline": {"bound": "hbm", "kernel": "k_apply (SSAFD stencil, matrix-free)", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "peak_kind": peak_kind, "bytes_per_launch": apply_bytes, "launch_ms": apply_ms},
+        "roofline": {"bound": "hbm",
+                     "kernel": ("one inner BiCGStab + V(1,1) multigrid iteration: k32_p/v/s/t/x + 2 x (k_mg0_restrict, "
+                                "k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, k_mg0_post)"
+                                if c.precision == "mixed" else
+                                "one BiCGStab + V(1,1) multigrid iteration (FP64 Krylov vectors)"),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": it_bytes,
+                     "launch_ms": it_ms, "timed": f"linear solve to rtol 1e-10: {lin_its} iterations in {lin_ms:.2f} ms",
+                     "fp64_apply": {"achieved": apply_bytes / (apply_ms * 1e-3) / 1e9, "bytes_per_launch": apply_bytes,
+                                    "launch_ms": apply_ms,
+                                    "frac": apply_bytes / (apply_ms * 1e-3) / 1e9 / peak}},
         "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clocks,

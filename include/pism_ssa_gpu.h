@@ -236,9 +236,8 @@ int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations,
 /* ---- allocation-free entry point ------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * hosts that route every device allocation through their own pool or arena,
- * code that runs while the caller captures a CUDA graph or works under a memory
- * budget that forbids new allocations, and bindings without access to the CUDA
- * allocator.  It computes what pism_gpu_ssa_compute_nuH computes for the plain
+ * code that works under a memory budget that forbids new allocations, and
+ * bindings without access to the CUDA allocator.  It computes what pism_gpu_ssa_compute_nuH computes for the plain
  * (non-CFBC) stencil — nu*H on the staggered grid, under-relaxed against the
  * values in `nuH` when underrelax != 1 (SSAFD.cc:1061-1064), and the basal drag
  * coefficient of the next assembly — and writes the two L1 norms of the Picard

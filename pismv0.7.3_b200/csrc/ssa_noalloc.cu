@@ -2,10 +2,9 @@
 // two L1 norms of the Picard convergence test, computed without allocating any memory.
 //
 // Why: some callers cannot call cudaMalloc at all — a host that hands every
-// allocation to its own pool or arena, code running where a device allocation may
-// not happen (inside a region the caller is capturing into a CUDA graph, or under
-// a memory budget that forbids new allocations), or a language binding with no
-// access to the CUDA allocator.  The handle API allocates its scratch in
+// allocation to its own pool or arena, code running under a memory budget that
+// forbids new device allocations, or a language binding with no access to the
+// CUDA allocator.  The handle API allocates its scratch in
 // pism_gpu_ssa_create; this entry point instead keeps its scratch in the fixed
 // file-scope device array below, so the caller passes only inputs and outputs.
 //

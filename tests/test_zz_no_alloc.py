@@ -1,8 +1,8 @@
 """The allocation-free entry point pism_gpu_ssa_nuH_noalloc, through the C-ABI.
 
 It serves callers that cannot call cudaMalloc (hosts with their own device
-memory pools, code running under graph capture or a fixed memory budget, and
-bindings without access to the CUDA allocator): its scratch is a fixed device
+memory pools, code running under a fixed memory budget, and bindings without
+access to the CUDA allocator): its scratch is a fixed device
 array inside the library, so it takes only inputs and outputs.  This test
 checks it against the handle API's compute_nuH path (pism_gpu_ssa_compute_nuH
 + pism_gpu_ssa_get_field) on two calls in a row — the second call starts from the
