@@ -39,6 +39,7 @@ struct pism_gpu_ssa {
   uint32_t *flags = nullptr;
   Krylov K{};
   Krylov32 K32{};
+  Gmres G{};   // allocated by the first GMRES solve
   double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
   double *res_host = nullptr;
   MGHierarchy mg{};
@@ -153,6 +154,10 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown precision %d", c->precision);
   if (c->precision == PISM_PRECISION_MIXED && !(c->mixed_inner_rtol > 0.0 && c->mixed_inner_rtol < 1.0))
     return fail(h, PISM_GPU_SSA_EINVAL, "mixed_inner_rtol must be in (0, 1)");
+  if (c->ksp_type == PISM_KSP_GMRES && (c->gmres_restart < 1 || c->gmres_restart > GM_MAXM))
+    return fail(h, PISM_GPU_SSA_EINVAL, "gmres_restart must be in [1, %d]", GM_MAXM);
+  if (c->ksp_type == PISM_KSP_GMRES && c->precision == PISM_PRECISION_MIXED)
+    return fail(h, PISM_GPU_SSA_EINVAL, "the mixed-precision inner solve is BiCGStab; use ksp_type GMRES with fp64");
   if (c->pc_type != PISM_PC_BLOCK_JACOBI && c->pc_type != PISM_PC_MULTIGRID)
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
   if (c->ksp_rtol_adaptive && !(c->ksp_rtol_max >= c->ksp_rtol && c->ksp_rtol_max < 1.0 && c->ksp_rtol_factor > 0.0))
@@ -186,6 +191,61 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *st
     if (h->st_host->done) break;
     chunk = std::max(4, std::min(64, launched / 8));
   }
+  h->last_ksp_its = h->st_host->iter;
+  *its_out = h->st_host->iter;
+  *status_out = h->st_host->status;
+  h->stats.final_linear_residual =
+      h->st_host->bnorm2 > 0 ? sqrt(h->st_host->rnorm2 / h->st_host->bnorm2) : sqrt(h->st_host->rnorm2);
+  return PISM_GPU_SSA_OK;
+}
+
+// ---- one linear solve: restarted flexible GMRES(m) on the device (PETSc's default KSP
+// type, restart gmres_restart), right-preconditioned by the active preconditioner ----
+int linear_solve_gmres(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
+  const GridDev &g = h->g;
+  const int m = h->cfg.gmres_restart;
+  if (h->G.m != m) {
+    for (void *p : {(void *)h->G.V, (void *)h->G.Z, (void *)h->G.partials, (void *)h->G.gs, (void *)h->G.st})
+      if (p) cudaFree(p);
+    h->G = Gmres{};
+    RET(dalloc(h, &h->G.V, (size_t)(m + 1) * h->N));
+    RET(dalloc(h, &h->G.Z, (size_t)m * h->N));
+    RET(dalloc(h, &h->G.partials, (size_t)h->L.max_blocks * (GM_MAXM + 2)));
+    RET(dalloc(h, &h->G.gs, 1));
+    RET(dalloc(h, &h->G.st, 1));
+    h->G.m = m;
+  }
+  Fields f = fields_of(h);
+  KState init{};
+  init.rtol = rtol;
+  init.maxit = h->use_fallback ? 4 * h->cfg.ksp_max_it : h->cfg.ksp_max_it;
+  *h->st_host = init;
+  CK(h, cudaMemcpyAsync(h->G.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
+  launch_gmres_residual(h->L, g, f, h->G, h->rhs, x, 1);
+  int j = 0, launched = 0;
+  int chunk = std::max(8, (int)(0.8 * h->last_ksp_its));
+  while (true) {
+    const MGHierarchy *mg = active_mg(h);
+    for (int q = 0; q < chunk; ++q) {
+      launch_gmres_step(h->L, g, f, h->G, h->K.dinv, mg, j);
+      if (j == m - 1) {   // end of a cycle: x += Z y, then a restart unless converged
+        launch_gmres_update(h->L, g, h->G, x);
+        launch_gmres_residual(h->L, g, f, h->G, h->rhs, x, 0);
+        j = 0;
+      } else {
+        ++j;
+      }
+    }
+    launched += chunk;
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(h->st_host, h->G.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (h->st_host->done) break;
+    chunk = std::max(4, std::min(64, launched / 8));
+  }
+  launch_gmres_update(h->L, g, h->G, x);   // a cycle that converged part-way
+  CK(h, cudaGetLastError());
+  CK(h, cudaStreamSynchronize(h->stream));
   h->last_ksp_its = h->st_host->iter;
   *its_out = h->st_host->iter;
   *status_out = h->st_host->status;
@@ -256,6 +316,8 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
     int its = 0, status = 0;
     if (h->cfg.precision == PISM_PRECISION_MIXED && active_mg(h))
       RET(linear_solve_mixed(h, h->vel, rtol, &its, &status));
+    else if (h->cfg.ksp_type == PISM_KSP_GMRES)
+      RET(linear_solve_gmres(h, h->vel, rtol, &its, &status));
     else
       RET(linear_solve(h, h->vel, rtol, &its, &status));
     CK(h, cudaMemcpyAsync(h->zd_host, h->zd_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -513,7 +575,8 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->vel_old, h->beta, h->bfrict, h->flags, h->K.r, h->K.rhat, h->K.p, h->K.v, h->K.s, h->K.t,
                  h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev,
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.s, h->K32.t, h->K32.phat,
-                 h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout};
+                 h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
+                 h->G.partials, h->G.gs, h->G.st};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -711,7 +774,10 @@ int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, d
   if (h->cfg.precision == PISM_PRECISION_MIXED && active_mg(h))
     RET(linear_solve_mixed(h, (double2 *)x_dev, h->cfg.ksp_rtol, &its, &status));
   else
-    RET(linear_solve(h, (double2 *)x_dev, h->cfg.ksp_rtol, &its, &status));
+    if (h->cfg.ksp_type == PISM_KSP_GMRES)
+      RET(linear_solve_gmres(h, (double2 *)x_dev, h->cfg.ksp_rtol, &its, &status));
+    else
+      RET(linear_solve(h, (double2 *)x_dev, h->cfg.ksp_rtol, &its, &status));
   if (iterations) *iterations = its;
   if (rel_residual) *rel_residual = h->stats.final_linear_residual;
   if (status != KSP_OK)

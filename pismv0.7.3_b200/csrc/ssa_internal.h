@@ -38,6 +38,25 @@ struct Krylov {
   KState *st;
 };
 
+// Restarted flexible GMRES(m) (right preconditioning): Arnoldi basis V[0..m], the
+// preconditioned directions Z[0..m-1] and the small dense state on the device
+constexpr int GM_MAXM = 30;   // largest restart length (PETSc's default is 30)
+struct GState {
+  double H[GM_MAXM + 1][GM_MAXM];   // Hessenberg matrix, rotated into R in place
+  double cs[GM_MAXM], sn[GM_MAXM];  // Givens rotations
+  double g[GM_MAXM + 1];            // rotated right-hand side: |g[j+1]| = residual norm
+  double y[GM_MAXM];
+  double bnorm, hnext, scale0;
+  int m, cols, cols_upd, need_update, restart;
+};
+struct Gmres {
+  double2 *V, *Z;   // (m + 1) x N and m x N
+  double *partials; // blocks x 32
+  GState *gs;
+  KState *st;       // done / status / iter / maxit / rtol shared with the multigrid early exit
+  int m;
+};
+
 // FP32 work vectors of the inner solve of the mixed-precision path
 struct Krylov32 {
   float2 *rhs, *r, *rhat, *p, *v, *s, *t, *phat, *shat, *d;
@@ -102,6 +121,12 @@ void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const 
                       const double2 *x);
 void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x,
                            const MGHierarchy *mg);
+// FGMRES: r0 = b - A x into V0 (init) / after a restart; one Arnoldi step j; the end of a cycle
+void launch_gmres_residual(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double2 *b,
+                           const double2 *x, int init);
+void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
+                       const MGHierarchy *mg, int j);
+void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, double2 *x);
 void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b,
                double2 *z, const KState *st);

@@ -869,4 +869,268 @@ void launch_scale(const Launch &L, int n, double a, double *x) {
   k_scale<<<grid_for(L, n), NT, 0, L.stream>>>(n, a, x);
 }
 
+
+// ---------------------------------------------------------------------------
+// Restarted flexible GMRES(m) with right preconditioning (PETSc's KSPFGMRES; with a fixed
+// preconditioner it is GMRES right-preconditioned, the reference's fallback set-up with
+// the unpreconditioned residual norm, SSAFD.cc:164-219).  The Arnoldi basis is
+// orthogonalised by classical Gram-Schmidt in one pass (PETSc's default, no refinement).
+// The Givens rotations, the residual estimate |g[j+1]| and the tests run in the last
+// block of the orthogonalisation kernel.  Stop: ||b - A x||_2 <= rtol ||b||_2.
+// ---------------------------------------------------------------------------
+
+// r = b - A x into V0.  init: the start of a solve (also ||b||); otherwise only after a
+// cycle that ended without convergence (a restart).
+__global__ void __launch_bounds__(NT, 4) k_gm_residual(GridDev g, TileMap tm, StencilConst s,
+                                                    const uint32_t *__restrict__ flags,
+                                                    const double2 *__restrict__ nuH, const double *__restrict__ beta,
+                                                    const double2 *__restrict__ b, const double2 *__restrict__ x,
+                                                    double2 *__restrict__ v0, double *partials, unsigned *ticket,
+                                                    KState *st, GState *gs, int init) {
+  if (!init && (!gs->restart || st->done)) return;
+  double acc[2] = {0.0, 0.0};
+  __shared__ HaloTile<double2> xT, nT;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, j, k;
+    uint32_t f;
+    double bta;
+    double2 bk;
+    if (!stage_tile(g, tm, t, x, nuH, flags, beta, b, xT, nT, i, j, k, f, bta, bk)) continue;
+    const double2 ax = apply_cell_tile(g, s, i, j, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
+    const double2 rk = make_double2(bk.x - ax.x, bk.y - ax.y);
+    v0[k] = rk;
+    acc[0] += dot2(rk, rk);
+    acc[1] += dot2(bk, bk);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) {
+    const double rn = sqrt(tot[0]);
+    if (init) {
+      gs->bnorm = sqrt(tot[1]);
+      st->bnorm2 = tot[1];
+      st->rnorm0 = rn;
+      st->iter = 0;
+      st->status = KSP_OK;
+      st->done = 0;
+    }
+    st->rnorm2 = tot[0];
+    gs->restart = 0;
+    gs->need_update = 0;
+    gs->cols = 0;
+    for (int q = 0; q <= GM_MAXM; ++q) gs->g[q] = 0.0;
+    gs->g[0] = rn;
+    gs->scale0 = rn > 0.0 ? 1.0 / rn : 0.0;
+    if (!isfinite(rn)) {
+      st->done = 1;
+      st->status = KSP_NAN;
+      gs->scale0 = 0.0;
+    } else if (rn <= st->rtol * gs->bnorm || gs->bnorm == 0.0) {
+      st->done = 1;
+      gs->scale0 = 0.0;
+    }
+  }
+}
+
+// V0 *= 1 / ||r0|| after a (re)start (scale0 is cleared by the next orthogonalisation)
+__global__ void __launch_bounds__(NT) k_gm_scale0(int N, double2 *__restrict__ v0, const GState *gs) {
+  const double sc = gs->scale0;
+  if (sc == 0.0) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 v = v0[k];
+    v0[k] = make_double2(v.x * sc, v.y * sc);
+  }
+}
+
+// z = D^-1 v (point-block Jacobi)
+__global__ void __launch_bounds__(NT) k_gm_jacobi(int N, const double2 *__restrict__ v,
+                                                  const double4 *__restrict__ dinv, double2 *__restrict__ z,
+                                                  const KState *st) {
+  if (st->done) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) z[k] = dmul(dinv[k], v[k]);
+}
+
+// w = A z_j into V[j+1];  H[i][j] = <w, v_i> for i <= j
+__global__ void __launch_bounds__(NT, 2) k_gm_apply_dots(GridDev g, TileMap tm, StencilConst s,
+                                                      const uint32_t *__restrict__ flags,
+                                                      const double2 *__restrict__ nuH,
+                                                      const double *__restrict__ beta, const double2 *__restrict__ z,
+                                                      const double2 *__restrict__ V, double2 *__restrict__ w, int j,
+                                                      double *partials, unsigned *ticket, const KState *st,
+                                                      GState *gs) {
+  if (st->done) return;
+  const size_t N = (size_t)g.Mx * g.My;
+  double acc[GM_MAXM + 2];
+#pragma unroll
+  for (int q = 0; q < GM_MAXM + 2; ++q) acc[q] = 0.0;
+  __shared__ HaloTile<double2> xT, nT;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    int i, jj, k;
+    uint32_t f;
+    double bta;
+    double2 ex;
+    if (!stage_tile(g, tm, t, z, nuH, flags, beta, nullptr, xT, nT, i, jj, k, f, bta, ex)) continue;
+    const double2 wk = apply_cell_tile(g, s, i, jj, f, xT, nT, bta, threadIdx.x >> 5, threadIdx.x & 31);
+    w[k] = wk;
+#pragma unroll
+    for (int q = 0; q <= GM_MAXM; ++q)
+      if (q <= j) acc[q] += dot2(V[q * N + k], wk);
+  }
+  double tot[GM_MAXM + 2];
+  if (grid_reduce<GM_MAXM + 2>(acc, partials, ticket, tot))
+    for (int q = 0; q <= j; ++q) gs->H[q][j] = tot[q];
+}
+
+// w -= sum_{i <= j} H[i][j] v_i;  h = ||w||;  rotations, residual estimate and tests
+__global__ void __launch_bounds__(NT) k_gm_orth(int N, const double2 *__restrict__ V, double2 *__restrict__ w, int j,
+                                                int m, double *partials, unsigned *ticket, KState *st, GState *gs) {
+  if (st->done) return;
+  __shared__ double hcol[GM_MAXM + 1];
+  if (threadIdx.x <= j) hcol[threadIdx.x] = gs->H[threadIdx.x][j];
+  __syncthreads();
+  double acc[1] = {0.0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    double2 wk = w[k];
+#pragma unroll
+    for (int q = 0; q <= GM_MAXM; ++q)
+      if (q <= j) {
+        const double2 v = V[(size_t)q * N + k];
+        wk.x -= hcol[q] * v.x;
+        wk.y -= hcol[q] * v.y;
+      }
+    w[k] = wk;
+    acc[0] += dot2(wk, wk);
+  }
+  double tot[1];
+  if (!grid_reduce<1>(acc, partials, ticket, tot)) return;
+  const double hn = sqrt(tot[0]);
+  gs->hnext = hn;
+  gs->scale0 = 0.0;
+  for (int i = 0; i < j; ++i) {
+    const double a = gs->H[i][j], b = gs->H[i + 1][j];
+    gs->H[i][j] = gs->cs[i] * a + gs->sn[i] * b;
+    gs->H[i + 1][j] = -gs->sn[i] * a + gs->cs[i] * b;
+  }
+  const double a = gs->H[j][j], r = hypot(a, hn);
+  st->iter += 1;
+  if (!isfinite(hn) || !isfinite(r)) {
+    st->done = 1;
+    st->status = KSP_NAN;
+    gs->need_update = 0;
+    return;
+  }
+  if (r == 0.0) {   // the new direction and its projection both vanish: nothing to add
+    st->done = 1;
+    st->status = KSP_BREAKDOWN;
+    gs->cols = j;
+    gs->need_update = j > 0;
+    return;
+  }
+  const double c = a / r, sg = hn / r;
+  gs->cs[j] = c;
+  gs->sn[j] = sg;
+  gs->H[j][j] = r;
+  gs->H[j + 1][j] = 0.0;
+  const double gj = gs->g[j];
+  gs->g[j] = c * gj;
+  gs->g[j + 1] = -sg * gj;
+  const double res = fabs(gs->g[j + 1]);
+  st->rnorm2 = res * res;
+  gs->cols = j + 1;
+  if (res <= st->rtol * gs->bnorm || hn == 0.0) {
+    st->done = 1;
+    st->status = KSP_OK;
+    gs->need_update = 1;
+  } else if (st->iter >= st->maxit) {
+    st->done = 1;
+    st->status = KSP_MAXIT;
+    gs->need_update = 1;
+  } else if (j + 1 == m) {
+    gs->restart = 1;
+    gs->need_update = 1;
+  }
+}
+
+// V[j+1] *= 1 / h_{j+1,j} while the cycle goes on
+__global__ void __launch_bounds__(NT) k_gm_scale_next(int N, double2 *__restrict__ w, const KState *st,
+                                                      const GState *gs) {
+  if (st->done || gs->restart) return;
+  const double sc = 1.0 / gs->hnext;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 v = w[k];
+    w[k] = make_double2(v.x * sc, v.y * sc);
+  }
+}
+
+// R y = g over the finished columns (one thread; at most 30 x 30)
+__global__ void k_gm_solve(GState *gs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (!gs->need_update) {
+    gs->cols_upd = 0;
+    return;
+  }
+  const int n = gs->cols;
+  for (int i = n - 1; i >= 0; --i) {
+    double a = gs->g[i];
+    for (int q = i + 1; q < n; ++q) a -= gs->H[i][q] * gs->y[q];
+    gs->y[i] = a / gs->H[i][i];
+  }
+  gs->cols_upd = n;
+  gs->need_update = 0;
+}
+
+// x += sum_{i < cols} y_i z_i
+__global__ void __launch_bounds__(NT) k_gm_update(int N, const double2 *__restrict__ Z, double2 *__restrict__ x,
+                                                  const GState *gs) {
+  const int n = gs->cols_upd;
+  if (n == 0) return;
+  __shared__ double ys[GM_MAXM];
+  if (threadIdx.x < n) ys[threadIdx.x] = gs->y[threadIdx.x];
+  __syncthreads();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    double2 xk = x[k];
+#pragma unroll
+    for (int q = 0; q < GM_MAXM; ++q)
+      if (q < n) {
+        const double2 zv = Z[(size_t)q * N + k];
+        xk.x += ys[q] * zv.x;
+        xk.y += ys[q] * zv.y;
+      }
+    x[k] = xk;
+  }
+}
+
+void launch_gmres_residual(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double2 *b,
+                           const double2 *x, int init) {
+  L.tick(2);
+  TileMap tm = make_tiles(g);
+  const int N = g.Mx * g.My;
+  k_gm_residual<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta,
+                                                                  b, x, G.V, G.partials, L.ticket, G.st, G.gs, init);
+  k_gm_scale0<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.V, G.gs);
+}
+
+void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
+                       const MGHierarchy *mg, int j) {
+  L.tick(mg ? 3 : 4);
+  TileMap tm = make_tiles(g);
+  const int N = g.Mx * g.My;
+  const double2 *vj = G.V + (size_t)j * N;
+  double2 *zj = G.Z + (size_t)j * N, *w = G.V + (size_t)(j + 1) * N;
+  if (mg)
+    mg_vcycle(L, g, f, *mg, vj, zj, G.st);
+  else
+    k_gm_jacobi<<<grid_for(L, N), NT, 0, L.stream>>>(N, vj, dinv, zj, G.st);
+  k_gm_apply_dots<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta,
+                                                                    zj, G.V, w, j, G.partials, L.ticket, G.st, G.gs);
+  k_gm_orth<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.V, w, j, G.m, G.partials, L.ticket, G.st, G.gs);
+  k_gm_scale_next<<<grid_for(L, N), NT, 0, L.stream>>>(N, w, G.st, G.gs);
+}
+
+void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, double2 *x) {
+  L.tick(2);
+  const int N = g.Mx * g.My;
+  k_gm_solve<<<1, 32, 0, L.stream>>>(G.gs);
+  k_gm_update<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.Z, x, G.gs);
+}
+
 }  // namespace pism_gpu

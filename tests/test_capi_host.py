@@ -123,6 +123,16 @@ def test_create_rejects_bad_grids_without_touching_cuda(lib):
     assert lib.pism_gpu_ssa_create(None, C.byref(cfg), 0, C.byref(h)) == _capi.EINVAL
 
 
+def test_gmres_settings_are_checked_before_device_work(lib):
+    """ksp_type GMRES: restart in [1, 30]; the mixed-precision inner solve stays BiCGStab."""
+    g, _z = GridDesc(16, 16, 1e5, 1e5).to_c()
+    h = C.c_void_p()
+    for kw in ({"ksp_type": "gmres", "gmres_restart": 0}, {"ksp_type": "gmres", "gmres_restart": 31},
+               {"ksp_type": "gmres", "precision": "mixed", "pc_type": "mg"}):
+        cfg = SSAConfig(**kw).to_c()
+        assert lib.pism_gpu_ssa_create(C.byref(g), C.byref(cfg), 0, C.byref(h)) == _capi.EINVAL, kw
+
+
 def test_noalloc_rejects_before_any_device_work(lib):
     """Size and argument checks of the allocation-free entry point happen on the host."""
     cfg = SSAConfig().to_c()

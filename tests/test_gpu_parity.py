@@ -122,14 +122,18 @@ def test_hardness_from_enthalpy(law):
     s.close()
 
 
-@pytest.mark.parametrize("pc,precision", [("bjacobi", "fp64"), ("mg", "fp64"), ("mg", "mixed")])
-def test_linear_solve_matches_direct(pc, precision):
+@pytest.mark.parametrize("pc,precision,ksp", [("bjacobi", "fp64", "bicgstab"), ("mg", "fp64", "bicgstab"),
+                                               ("mg", "mixed", "bicgstab"), ("bjacobi", "fp64", "gmres"),
+                                               ("mg", "fp64", "gmres")])
+def test_linear_solve_matches_direct(pc, precision, ksp):
     """One KSPSolve at the first Picard step (zero velocity: plastic drag 1e14, the worst
-    conditioning of the solve).  Both answers must have tiny true residuals and agree."""
+    conditioning of the solve).  Both answers must have tiny true residuals and agree.
+    GMRES (restart 30, classical Gram-Schmidt) runs with restarts on this system."""
     g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=3)
     c.ksp_rtol = 1e-14
     c.pc_type = pc
     c.precision = precision
+    c.ksp_type = ksp
     G, Cc, I = O.from_case(g, c, f)
     s = make_solver(g, c, f)
     s.assemble_rhs()
@@ -184,12 +188,14 @@ def _solve_case(g, c, f):
     return vel, st
 
 
-@pytest.mark.parametrize("pc,precision", [("bjacobi", "fp64"), ("mg", "fp64"), ("mg", "mixed")])
+@pytest.mark.parametrize("pc,precision,ksp", [("bjacobi", "fp64", "bicgstab"), ("mg", "fp64", "bicgstab"),
+                                               ("mg", "mixed", "bicgstab"), ("mg", "fp64", "gmres")])
 @pytest.mark.parametrize("My", [61, 121])
-def test_verification_i(goldens, My, pc, precision):
+def test_verification_i(goldens, My, pc, precision, ksp):
     g, c, f = V.build_test_i(My=My)
     c.pc_type = pc
     c.precision = precision
+    c.ksp_type = ksp
     c.ssafd_relative_convergence = 5e-7
     c.ksp_rtol = 1e-12
     vel, st = _solve_case(g, c, f)
@@ -217,13 +223,15 @@ def test_verification_v_cfbc(goldens, Mx, pc):
     assert rel(vel, ref) < 1e-8
 
 
-@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
+@pytest.mark.parametrize("pc,ksp", [("bjacobi", "bicgstab"), ("mg", "bicgstab"), ("bjacobi", "gmres"),
+                                    ("mg", "gmres")])
 @pytest.mark.parametrize("M", [61, 121])
-def test_verification_j(M, pc):
+def test_verification_j(M, pc, ksp):
     """Test J with a tight KSP equals the oracle's direct solve (the golden itself
     records PETSc's rtol-1e-5 iterate; the CPU suite pins that)."""
     g, c, f = V.build_test_j(M, M)
     c.pc_type = pc
+    c.ksp_type = ksp
     c.ksp_rtol = 1e-13
     vel, st = _solve_case(g, c, f)
     ref = O.SSAFDOracle(*O.from_case(g, c, f)).solve()
@@ -245,9 +253,10 @@ def test_zero_diagonal_is_reported():
     s.close()
 
 
-@pytest.mark.parametrize("pc,precision", [("bjacobi", "fp64"), ("mg", "fp64"), ("mg", "mixed")])
+@pytest.mark.parametrize("pc,precision,ksp", [("bjacobi", "fp64", "bicgstab"), ("mg", "fp64", "bicgstab"),
+                                               ("mg", "mixed", "bicgstab"), ("mg", "fp64", "gmres")])
 @pytest.mark.parametrize("M", [45, 64])
-def test_synthetic_solve_matches_oracle(M, pc, precision):
+def test_synthetic_solve_matches_oracle(M, pc, precision, ksp):
     """A whole SSAFD::solve of the synthetic sheet against the oracle, odd and even grid sizes
     (the multigrid aggregates wrap differently).  Pseudo-plastic till: its Picard iteration
     contracts ~25 % per step, so both solvers stop at the same iteration; with plastic till
@@ -258,6 +267,7 @@ def test_synthetic_solve_matches_oracle(M, pc, precision):
     c.ksp_rtol = 1e-12
     c.pc_type = pc
     c.precision = precision
+    c.ksp_type = ksp
     vel, st = _solve_case(g, c, f)
     o = O.SSAFDOracle(*O.from_case(g, c, f))
     ref = o.solve()
