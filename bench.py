@@ -127,6 +127,24 @@ def fast_config(c, precision="mixed"):
                   ksp_rtol_max=1e-2)
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """The largest value of x over the ranks of the process group (x itself without one).
+    Replicas are timed separately; the job takes as long as its slowest rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_time_per_solve(step_ms_max: float, world: int) -> float:
+    """value of the replica run: every rank solves its own sheet in step_ms_max (the
+    slowest rank), so the job delivers world solves in that time"""
+    return step_ms_max / world
+
+
 def mg_levels(M):
     """cells of the multigrid levels below the fine grid (2 x 2 aggregation down to <= 4 x 4)"""
     out, mx, my = [], M, M
@@ -319,11 +337,8 @@ def main():
     clocks = sampler.stop()
     vel_mode = out.clone()
 
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_per_step = float(t.item()) / args.steps
-    value = ms_per_step / world
+    ms_per_step = max_over_ranks(total_ms, dev) / args.steps
+    value = job_time_per_solve(ms_per_step, world)
 
     other_ms, st_other, vel_error, accuracy = None, {"picard_iterations": None, "ksp_iterations": None}, None, None
     if not args.no_compare:
@@ -388,10 +403,7 @@ def main():
         torch.cuda.synchronize()
         e2e_ms += (time.perf_counter() - t0) * 1e3
     e2e_ms /= max(1, min(args.steps, 2))
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = float(te.item()) / world
+    e2e_value = job_time_per_solve(max_over_ranks(e2e_ms, dev), world)
 
     # Roofline of the hot loop: one inner BiCGStab + multigrid iteration (the kernels that
     # repeat ~850 times per fast solve), timed live on a tight linear solve at the final nu*H
