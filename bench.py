@@ -222,6 +222,114 @@ def run_reference(args):
     return 0
 
 
+def ensemble_member(q, M=401):
+    """member q of the ensemble: a seeded 401^2 sheet (10 km) with its own ice temperature
+    ~ U[-20, -2] C and tau_c median ~ U[20, 200] kPa (seeds disjoint from the training set)"""
+    _package()
+    from pism_b200 import synthetic as S
+    rng = np.random.Generator(np.random.PCG64(77_000 + q))
+    T, med = rng.uniform(-20.0, -2.0), rng.uniform(20e3, 200e3)
+    g, c, f, meta = S.build_synthetic(M, 4000e3 / (M - 1), seed=700_000 + q, temperature_c=T, tauc_median=med)
+    return g, c, f, {"T": T, "tauc_median": med}
+
+
+def run_ensemble(args):
+    """--workload ensemble: pism_gpu_ssa_solve_batch over the members of this rank (the
+    fast set-up with the learned guess), members/s of the whole job; each member's
+    velocity error against the plain FP64 solve of the same member."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    _package()
+    from pism_b200 import learned as Lrn
+    from pism_b200.ssa import SSAFD
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    M = 401
+    mine = list(range(rank * args.members, (rank + 1) * args.members))   # weak scaling: members per GPU fixed
+    names = ("thickness", "surface", "bed", "mask", "tauc", "melange")
+    cases = [ensemble_member(q, M) for q in mine]
+    g, c0 = cases[0][0], cases[0][1]
+    c_fast = fast_config(c0)
+    mem = [{**{k: torch.tensor(f[k], dtype=torch.float64, device=dev) for k in names},
+            "ice_softness": c.ice_softness, "velocity": torch.zeros((M, M, 2), dtype=torch.float64, device=dev)}
+           for _, c, f, _ in cases]
+    hh, ww = Lrn.image_shape(M, M, 1)
+    net = Lrn.UNet(1, hh, ww, device=local, params=np.load(Lrn.DEFAULT_WEIGHTS)["params"])
+    net.set_stream(stream.cuda_stream)
+    s = SSAFD(g, c_fast, device=local)
+    s.set_stream(stream.cuda_stream)
+    s.solve_batch(mem[:2], net=net, stride=1)        # warm-up
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        vels, stats = s.solve_batch(mem, net=net, stride=1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    step_ms = max_over_ranks(float(np.mean(times)), dev)
+    value = len(mine) * world / (step_ms * 1e-3)
+    # end to end: host inputs and outputs through the same call
+    hmem = [{**{k: f[k] for k in names}, "ice_softness": c.ice_softness, "velocity": np.zeros((M, M, 2))}
+            for _, c, f, _ in cases]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.solve_batch(hmem, net=net, stride=1)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dev)
+    # accuracy: the plain FP64 solve of every member
+    errs = []
+    plain = SSAFD(g, c0, device=local)
+    plain.set_stream(stream.cuda_stream)
+    for q, (_, c, f, meta) in enumerate(cases):
+        plain.set_config(c)
+        plain.set_inputs(**{k: mem[q][k] for k in names})
+        plain.set_initial_guess(torch.zeros((M, M, 2), dtype=torch.float64, device=dev))
+        ref = plain.solve(out=torch.empty((M, M, 2), dtype=torch.float64, device=dev))
+        errs.append(float((vels[q] - ref).norm() / ref.norm()))
+    plain.close()
+    s.close()
+    net.close()
+    line = {
+        "metric": f"ensemble members solved/s ({args.members} x {M}^2 per GPU, learned+FP32)", "value": value,
+        "unit": "members/s", "n_gpus": world, "steps": args.steps, "warmup": 1, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": f"ensemble of {args.members} seeded {M}x{M} sheets at 10 km per GPU, temperature "
+                               "U[-20,-2] C and tau_c median U[20,200] kPa per member, solved by "
+                               "pism_gpu_ssa_solve_batch (fast set-up, learned guess)",
+                   "members_per_gpu": args.members, "l2": "flushed (256 MB write) between steps",
+                   "parallelism": f"members sharded over {world} GPU(s)"},
+        "members": {"picard_iterations": [st["picard_iterations"] for st in stats],
+                    "converged": sum(st["converged"] for st in stats),
+                    "rel_l2_error_vs_plain_fp64": {"max": max(errs), "median": float(np.median(errs))}},
+        "e2e": {"value": len(mine) * world / (e2e_ms * 1e-3), "unit": "members/s",
+                "h2d_bytes_per_step": len(mine) * len(names) * M * M * 8,
+                "d2h_bytes_per_step": len(mine) * M * M * 16},
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -244,9 +352,14 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="fast set-up from a zero initial guess")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the converged FP64 reference solve")
     ap.add_argument("--no-compare", action="store_true", help="skip the other set-up (and the accuracy reference)")
+    ap.add_argument("--workload", default="solve", choices=["solve", "ensemble"],
+                    help="ensemble: members solved/s of a 64-member 401^2 ensemble (its own JSON line)")
+    ap.add_argument("--members", type=int, default=64)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ensemble":
+        return run_ensemble(args)
 
     import torch
     import torch.distributed as dist

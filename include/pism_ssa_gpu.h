@@ -162,6 +162,16 @@ typedef struct pism_gpu_ssa_stats {
   long long kernel_launches;       /* kernels launched by the solve                   */
 } pism_gpu_ssa_stats;
 
+/* ---- one member of an ensemble (pism_gpu_ssa_solve_batch) ---- */
+typedef struct pism_gpu_ssa_member {
+  pism_gpu_ssa_inputs inputs;     /* the member's fields on the handle's grid         */
+  double ice_softness;            /* > 0: this member's isothermal Glen softness
+                                     (Pa^-3 s^-1); <= 0: the configuration's          */
+  double *velocity;               /* 2*Mx*My, in inputs.where memory: the initial guess
+                                     on entry (unless a network gives it), the
+                                     solution on return                               */
+} pism_gpu_ssa_member;
+
 typedef struct pism_gpu_ssa pism_gpu_ssa;   /* opaque handle: owns device scratch */
 
 /* Fill *cfg with the pism_config.cdl defaults.  Replaces Config::get_* reads. */
@@ -201,6 +211,17 @@ int pism_gpu_ssa_set_initial_guess(pism_gpu_ssa *h, const double *velocity, int 
  * and fills *stats (may be NULL).  Blocks until the solve is done. */
 int pism_gpu_ssa_solve(pism_gpu_ssa *h, double *velocity_out, int where,
                        pism_gpu_ssa_stats *stats);
+
+/* An ensemble of independent sheets on the handle's grid (no reference counterpart; PISM
+ * runs ensemble members as separate model runs).  Member q: its inputs, its softness, the
+ * learned initial guess when net != NULL (features at `stride`, see pism_unet_gpu.h) or
+ * its velocity otherwise, then pism_gpu_ssa_solve; stats[q] (may be NULL) gets its
+ * statistics.  Members run one after another on the handle's stream.  A member whose
+ * solve fails (KSP, Picard, NaN, zero diagonal) is recorded in stats[q].status and the
+ * batch goes on; the first such status is returned.  Argument and CUDA errors stop the
+ * batch.  The configuration's softness is restored on return. */
+int pism_gpu_ssa_solve_batch(pism_gpu_ssa *h, struct pism_gpu_unet *net, int stride, int n,
+                             pism_gpu_ssa_member *members, pism_gpu_ssa_stats *stats);
 
 /* Field getters (host or device destination per `where`). */
 enum {

@@ -7,7 +7,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from .config import CConfig, CGrid, CInputs, CStats
+from .config import CConfig, CGrid, CInputs, CMember, CStats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libpism_ssa_gpu.so")
@@ -25,7 +25,7 @@ EXPORTS = [
     "pism_gpu_ssa_set_stream", "pism_gpu_ssa_set_config", "pism_gpu_ssa_set_inputs",
     "pism_gpu_ssa_set_initial_guess", "pism_gpu_ssa_solve", "pism_gpu_ssa_get_field",
     "pism_gpu_ssa_assemble_rhs", "pism_gpu_ssa_compute_hardness", "pism_gpu_ssa_compute_nuH",
-    "pism_gpu_ssa_apply", "pism_gpu_ssa_linear_solve", "pism_gpu_ssa_nuH_noalloc",
+    "pism_gpu_ssa_apply", "pism_gpu_ssa_linear_solve", "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch",
 ]
 # every symbol include/pism_unet_gpu.h declares
 UNET_EXPORTS = [
@@ -63,6 +63,7 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_apply": (I, [V, V, V]),
         "pism_gpu_ssa_linear_solve": (I, [V, V, P(I), P(D)]),
         "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
+        "pism_gpu_ssa_solve_batch": (I, [V, V, I, I, P(CMember), P(CStats)]),
         "pism_gpu_unet_param_count": (C.c_longlong, []),
         "pism_gpu_unet_create": (I, [I, I, I, I, P(V)]),
         "pism_gpu_unet_destroy": (I, [V]),

@@ -162,6 +162,10 @@ class CInputs(C.Structure):
         "gl_mask", "enthalpy", "hardness_stag", "fracture_density")]
 
 
+class CMember(C.Structure):
+    _fields_ = [("inputs", CInputs), ("ice_softness", _D), ("velocity", C.POINTER(_D))]
+
+
 class CStats(C.Structure):
     _fields_ = [("status", _I), ("converged", _I), ("strategy", _I), ("picard_iterations", _I),
                 ("ksp_iterations", _I), ("ksp_failures", _I), ("refinement_steps", _I),

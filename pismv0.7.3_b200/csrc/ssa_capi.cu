@@ -846,4 +846,37 @@ int pism_gpu_ssa_learned_guess(pism_gpu_ssa *h, pism_gpu_unet *net, int stride) 
   return PISM_GPU_SSA_OK;
 }
 
+int pism_gpu_ssa_solve_batch(pism_gpu_ssa *h, pism_gpu_unet *net, int stride, int n, pism_gpu_ssa_member *members,
+                             pism_gpu_ssa_stats *stats) {
+  if (!h || n < 0 || (n > 0 && !members)) return PISM_GPU_SSA_EINVAL;
+  const double A0 = h->cfg.ice_softness;
+  int first = PISM_GPU_SSA_OK;
+  for (int q = 0; q < n; ++q) {
+    pism_gpu_ssa_member &m = members[q];
+    if (!m.velocity) {
+      h->cfg.ice_softness = A0;
+      return fail(h, PISM_GPU_SSA_EINVAL, "member %d: velocity is NULL", q);
+    }
+    h->cfg.ice_softness = m.ice_softness > 0.0 ? m.ice_softness : A0;
+    int rc = pism_gpu_ssa_set_inputs(h, &m.inputs);
+    if (rc == PISM_GPU_SSA_OK)
+      rc = net ? pism_gpu_ssa_learned_guess(h, net, stride)
+               : pism_gpu_ssa_set_initial_guess(h, m.velocity, m.inputs.where);
+    if (rc == PISM_GPU_SSA_OK) rc = pism_gpu_ssa_solve(h, m.velocity, m.inputs.where, stats ? &stats[q] : nullptr);
+    else if (stats) {
+      stats[q] = pism_gpu_ssa_stats{};
+      stats[q].status = rc;
+    }
+    if (rc == PISM_GPU_SSA_EINVAL || rc == PISM_GPU_SSA_ECUDA || rc == PISM_GPU_SSA_ENOMEM ||
+        rc == PISM_GPU_SSA_ESTATE || rc == PISM_GPU_SSA_ETOOLARGE) {
+      h->cfg.ice_softness = A0;
+      return rc;
+    }
+    if (rc != PISM_GPU_SSA_OK && first == PISM_GPU_SSA_OK) first = rc;
+  }
+  h->cfg.ice_softness = A0;
+  h->prepared = false;
+  return first;
+}
+
 }  // extern "C"

@@ -20,7 +20,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from .config import CInputs, CStats, GridDesc, SSAConfig
+from .config import CInputs, CMember, CStats, GridDesc, SSAConfig
 
 _D = C.POINTER(C.c_double)
 
@@ -136,15 +136,16 @@ class SSAFD:
             self._bc = (bc_mask, bc_values)
         self._upload()
 
-    def _upload(self):
-        f = self._fields
+    def _inputs(self, f, bc):
+        """the C inputs struct of the fields f (and bc = (bc_mask, bc_values)) plus the
+        buffers that keep them alive"""
         Mx, My = self.shape
         Mz = 0 if self.grid.z is None else len(self.grid.z)
         s2, s3 = (Mx, My), (Mx, My, 2)
         bufs = {
             "thickness": _Buf(f["thickness"], s2), "surface": _Buf(f["surface"], s2),
             "bed": _Buf(f["bed"], s2), "mask": _Buf(f["mask"], s2), "tauc": _Buf(f["tauc"], s2),
-            "bc_mask": _Buf(self._bc[0], s2), "bc_values": _Buf(self._bc[1], s3),
+            "bc_mask": _Buf(bc[0], s2), "bc_values": _Buf(bc[1], s3),
             "melange": _Buf(f.get("melange"), s2), "gl_mask": _Buf(f.get("gl_mask"), s2),
             "enthalpy": _Buf(f.get("enthalpy"), (Mx, My, Mz)), "hardness_stag": _Buf(f.get("hardness"), s3),
             "fracture_density": _Buf(f.get("fracture_density"), s2),
@@ -156,7 +157,45 @@ class SSAFD:
         ci.where = _capi.MEM_DEVICE if kinds == {True} else _capi.MEM_HOST
         for name, b in bufs.items():
             setattr(ci, name, b.ptr)
+        return ci, bufs
+
+    def _upload(self):
+        ci, _keep = self._inputs(self._fields, self._bc)
         self._check(self.lib.pism_gpu_ssa_set_inputs(self._h, C.byref(ci)), "set_inputs")
+
+    def solve_batch(self, members, net=None, stride: int = 1):
+        """pism_gpu_ssa_solve_batch: members is a list of dicts with the set_inputs fields
+        and optionally "ice_softness" and "velocity" (initial guess; output array or CUDA
+        tensor).  Returns (velocities, stats) per member; a member whose solve failed has
+        stats["status"] != 0."""
+        n = len(members)
+        arr = (CMember * max(n, 1))()
+        stats = (CStats * max(n, 1))()
+        keep, outs = [], []
+        for q, m in enumerate(members):
+            f = {k: m.get(k) for k in ("thickness", "surface", "bed", "mask", "tauc", "melange", "gl_mask",
+                                       "enthalpy", "hardness", "fracture_density")}
+            ci, bufs = self._inputs(f, (m.get("bc_mask"), m.get("bc_values")))
+            device = ci.where == _capi.MEM_DEVICE
+            vel = m.get("velocity")
+            if vel is None:
+                if device:
+                    import torch
+                    vel = torch.zeros((*self.shape, 2), dtype=torch.float64, device=f["thickness"].device)
+                else:
+                    vel = np.zeros((*self.shape, 2))
+            vb = _Buf(vel, (*self.shape, 2))
+            if vb.device != device:
+                raise ValueError("a member's velocity must live where its inputs live")
+            arr[q].inputs = ci
+            arr[q].ice_softness = float(m.get("ice_softness", 0.0))
+            arr[q].velocity = vb.ptr
+            keep += [bufs, vb]
+            outs.append(vb.keep)
+        rc = self.lib.pism_gpu_ssa_solve_batch(self._h, net._h if net is not None else None, stride, n, arr, stats)
+        if rc not in (_capi.OK, _capi.EKSP, _capi.EPICARD, _capi.ENAN, _capi.EZERODIAG):
+            self._check(rc, "solve_batch")
+        return outs, [stats[q].as_dict() for q in range(n)]
 
     def set_initial_guess(self, guess):
         """SSA::set_initial_guess (SSA.cc:361-363)."""

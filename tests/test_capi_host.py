@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from pism_b200 import _capi, build as B
-from pism_b200.config import CConfig, CGrid, CInputs, CStats, SSAConfig, GridDesc
+from pism_b200.config import CConfig, CGrid, CInputs, CMember, CStats, SSAConfig, GridDesc
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(REPO, "include", "pism_ssa_gpu.h")
@@ -69,6 +69,8 @@ int main(void) {
   printf("pism_gpu_grid size %zu\n", sizeof(pism_gpu_grid));
   printf("pism_gpu_ssa_inputs size %zu\n", sizeof(pism_gpu_ssa_inputs));
   printf("pism_gpu_ssa_stats size %zu\n", sizeof(pism_gpu_ssa_stats));
+  printf("pism_gpu_ssa_member size %zu\n", sizeof(pism_gpu_ssa_member));
+  F(pism_gpu_ssa_member, ice_softness) F(pism_gpu_ssa_member, velocity)
   F(pism_gpu_ssa_config, ksp_rtol) F(pism_gpu_ssa_config, verbosity) F(pism_gpu_ssa_config, mg_omega)
   F(pism_gpu_ssa_config, flow_law) F(pism_gpu_ssa_config, brutal_sliding_scale)
   F(pism_gpu_grid, z) F(pism_gpu_ssa_inputs, fracture_density) F(pism_gpu_ssa_stats, kernel_launches)
@@ -90,11 +92,12 @@ def test_ctypes_structs_match_the_header():
     assert lay[("pism_gpu_grid", "size")] == C.sizeof(CGrid)
     assert lay[("pism_gpu_ssa_inputs", "size")] == C.sizeof(CInputs)
     assert lay[("pism_gpu_ssa_stats", "size")] == C.sizeof(CStats)
+    assert lay[("pism_gpu_ssa_member", "size")] == C.sizeof(CMember)
     for (struct, member), off in lay.items():
         if member == "size":
             continue
         cls = {"pism_gpu_ssa_config": CConfig, "pism_gpu_grid": CGrid, "pism_gpu_ssa_inputs": CInputs,
-               "pism_gpu_ssa_stats": CStats}[struct]
+               "pism_gpu_ssa_stats": CStats, "pism_gpu_ssa_member": CMember}[struct]
         assert getattr(cls, member).offset == off, (struct, member)
 
 
