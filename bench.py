@@ -346,6 +346,8 @@ def main():
     ap.add_argument("--mg-correction", type=float, default=None)
     ap.add_argument("--verbosity", type=int, default=0)
     ap.add_argument("--mode", default="fast", choices=["fast", "plain"])
+    ap.add_argument("--ksp", default=None, choices=["bicgstab", "gmres"], help="override the Krylov method")
+    ap.add_argument("--gmres-restart", type=int, default=None)
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="override the mode's precision (fast: mixed, plain: fp64)")
     ap.add_argument("--inner-rtol", type=float, default=None)
@@ -385,6 +387,12 @@ def main():
     c, c_other = (c_fast, c_plain) if args.mode == "fast" else (c_plain, c_fast)
     if args.precision is not None:
         c.precision = args.precision
+    if args.ksp is not None:
+        c.ksp_type = args.ksp
+        if args.ksp == "gmres":
+            c.precision = "fp64"
+    if args.gmres_restart is not None:
+        c.gmres_restart = args.gmres_restart
     M = args.size
     N = M * M
     dev = torch.device("cuda", local)
@@ -558,7 +566,8 @@ def main():
         "config": {"workload": f"SSAFD solve, synthetic ice sheet {M}x{M} at {4000 / (M - 1):.0f} km, plastic till, "
                                f"Picard 1e-4; {args.mode} set-up",
                    "mode": args.mode, "grid": [M, M], "seed": 0, "precision": c.precision,
-                   "ksp": f"BiCGStab + {'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'}",
+                   "ksp": f"{'FGMRES(%d)' % c.gmres_restart if c.ksp_type == 'gmres' else 'BiCGStab'} + "
+                          f"{'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'}",
                    "ksp_rtol": c.ksp_rtol, "ksp_rtol_adaptive": bool(c.ksp_rtol_adaptive),
                    "warm_start": (f"learned (U-Net, features at stride {stride})" if net is not None else "zero"),
                    "l2": "flushed (256 MB write) between steps",

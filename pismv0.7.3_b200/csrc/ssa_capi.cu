@@ -535,7 +535,7 @@ int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cf
   AL(h->K32.rhs, N); AL(h->K32.r, N); AL(h->K32.rhat, N); AL(h->K32.p, N); AL(h->K32.v, N);
   AL(h->K32.s, N); AL(h->K32.t, N); AL(h->K32.phat, N); AL(h->K32.shat, N); AL(h->K32.d, N); AL(h->K32.st, 1);
   AL(h->res_dev, 2);
-  h->L.max_blocks = sms * 8;
+  h->L.max_blocks = sms * 4;   // persistent grids: one wave at the tile kernels' 4 blocks per SM
   if (mg_plan(grid->Mx, grid->My, h->mg) > 0) {
     if (mg_allocate(h->mg, h->N) != 0) return bail(PISM_GPU_SSA_ENOMEM);
     if (cudaMemsetAsync(h->mg.singular, 0, sizeof(int), h->stream) != cudaSuccess) return bail(PISM_GPU_SSA_ECUDA);
