@@ -40,6 +40,13 @@ struct pism_gpu_ssa {
   Krylov K{};
   Krylov32 K32{};
   Gmres G{};   // allocated by the first GMRES solve
+  // captured Krylov iterations (GRAPH_ITERS per graph), one per kind of iteration
+  struct IterGraph {
+    cudaGraphExec_t exec = nullptr;
+    const void *x = nullptr;   // the solution vector the iterations update
+    long long kernels = 0;
+    bool failed = false;
+  } graphs[3];
   double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
   double *res_host = nullptr;
   MGHierarchy mg{};
@@ -169,6 +176,50 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
   return PISM_GPU_SSA_OK;
 }
 
+// Launch `count` Krylov iterations.  Every iteration is the same fixed sequence of kernels
+// whose scalars live on the device, so GRAPH_ITERS of them are captured once into a CUDA
+// graph and replayed (fewer launches, shorter gaps between dependent kernels); a stream
+// that cannot be captured (the legacy default stream) keeps the direct launches.
+constexpr int GRAPH_ITERS = 4;
+enum { GRAPH_BICG_MG = 0, GRAPH_BICG_JACOBI = 1, GRAPH_MIXED = 2 };
+
+template <class ONE>
+int run_iterations(pism_gpu_ssa *h, int kind, const void *x, int count, const ONE &one) {
+  auto &G = h->graphs[kind];
+  if (G.exec && G.x != x) {
+    cudaGraphExecDestroy(G.exec);
+    G = {};
+  }
+  if (!G.exec && !G.failed) {
+    const long long before = h->stats.kernel_launches;
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      for (int q = 0; q < GRAPH_ITERS; ++q) one();
+      ok = cudaStreamEndCapture(h->stream, &graph) == cudaSuccess && graph != nullptr;
+    }
+    if (ok) ok = cudaGraphInstantiate(&G.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (ok) {
+      G.x = x;
+      G.kernels = h->stats.kernel_launches - before;
+    } else {
+      G.exec = nullptr;
+      G.failed = true;
+      cudaGetLastError();   // clear the capture's error; the direct launches follow
+    }
+    h->stats.kernel_launches = before;   // nothing ran during the capture
+  }
+  int q = 0;
+  if (G.exec)
+    for (; q + GRAPH_ITERS <= count; q += GRAPH_ITERS) {
+      CK(h, cudaGraphLaunch(G.exec, h->stream));
+      h->stats.kernel_launches += G.kernels;
+    }
+  for (; q < count; ++q) one();
+  return PISM_GPU_SSA_OK;
+}
+
 // ---- one linear solve: BiCGStab on the device, host reads the state per chunk ----
 int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
   const GridDev &g = h->g;
@@ -183,7 +234,8 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *st
   int chunk = std::max(8, (int)(0.8 * h->last_ksp_its));
   while (true) {
     const MGHierarchy *mg = active_mg(h);
-    for (int q = 0; q < chunk; ++q) launch_bicg_iteration(h->L, g, f, h->K, x, mg);
+    RET(run_iterations(h, mg ? GRAPH_BICG_MG : GRAPH_BICG_JACOBI, x, chunk,
+                       [&] { launch_bicg_iteration(h->L, g, f, h->K, x, mg); }));
     launched += chunk;
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(h->st_host, h->K.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
@@ -281,7 +333,8 @@ int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, i
     launch_mixed_init(h->L, g.Mx * g.My, h->K32);
     int launched = 0, chunk = 8;
     while (true) {
-      for (int q = 0; q < chunk; ++q) launch_mixed_iteration(h->L, g, f, *mg, h->K32);
+      RET(run_iterations(h, GRAPH_MIXED, nullptr, chunk,
+                         [&] { launch_mixed_iteration(h->L, g, f, *mg, h->K32); }));
       launched += chunk;
       CK(h, cudaGetLastError());
       CK(h, cudaMemcpyAsync(h->st_host, h->K32.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
@@ -585,6 +638,8 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
   if (h->res_host) cudaFreeHost(h->res_host);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (auto &gr : h->graphs)
+    if (gr.exec) cudaGraphExecDestroy(gr.exec);
   mg_free(h->mg);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -603,6 +658,10 @@ int pism_gpu_ssa_set_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *cfg) {
   RET(check_config(h, cfg));
   h->cfg = *cfg;
   h->prepared = false;
+  for (auto &gr : h->graphs) {   // the multigrid damping is captured by value
+    if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    gr = {};
+  }
   return PISM_GPU_SSA_OK;
 }
 
