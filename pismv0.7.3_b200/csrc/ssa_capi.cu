@@ -47,6 +47,14 @@ struct pism_gpu_ssa {
     long long kernels = 0;
     bool failed = false;
   } graphs[3];
+  // graph-resident Krylov loops (a conditional WHILE node around one iteration)
+  struct LoopGraph {
+    cudaGraphExec_t exec = nullptr;
+    const void *x = nullptr;
+    long long per_iteration = 0;   // kernels of one iteration
+    int body_iters = 1;            // iterations per pass of the loop body
+    bool failed = false;
+  } loops[3];
   double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
   double *res_host = nullptr;
   MGHierarchy mg{};
@@ -220,6 +228,110 @@ int run_iterations(pism_gpu_ssa *h, int kind, const void *x, int count, const ON
   return PISM_GPU_SSA_OK;
 }
 
+// A Krylov solve as one graph: a kernel sets a conditional handle from st->done, and a
+// WHILE node runs the loop body (one or a few iterations) plus that kernel again until the
+// solve is done, so the whole solve is one graph launch and one read-back.  Iterations of a
+// pass that start after convergence return at once.  Built once per handle and kind.
+template <class ONE>
+bool build_loop(pism_gpu_ssa *h, pism_gpu_ssa::LoopGraph &G, const KState *st, const ONE &one) {
+  const cudaStream_t s = h->stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  bool ok = true;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  cudaGraphConditionalHandle cond{};
+  ok = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd) == cudaSuccess && cs == cudaStreamCaptureStatusActive;
+  if (ok) ok = cudaGraphConditionalHandleCreate(&cond, cg, 0, 0) == cudaSuccess;
+  if (ok) {
+    launch_loop_condition(h->L, cond, st);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  if (ok) ok = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd) == cudaSuccess;
+  cudaGraphNode_t node{};
+  cudaGraphNodeParams p{};
+  if (ok) {
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = cond;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    ok = cudaGraphAddNode(&node, cg, deps, nd, &p) == cudaSuccess;
+  }
+  cudaStream_t bs = nullptr;
+  if (ok) ok = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) == cudaSuccess;
+  if (ok) ok = cudaStreamBeginCaptureToGraph(bs, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    h->L.stream = bs;
+    one();
+    launch_loop_condition(h->L, cond, st);
+    h->L.stream = s;
+    const bool launched = cudaGetLastError() == cudaSuccess;
+    ok = cudaStreamEndCapture(bs, nullptr) == cudaSuccess && launched;
+  }
+  if (ok) ok = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+  cudaGraph_t out = nullptr;
+  const bool ended = cudaStreamEndCapture(s, &out) == cudaSuccess;
+  ok = ok && ended && out != nullptr;
+  if (ok) ok = cudaGraphInstantiate(&G.exec, out, 0) == cudaSuccess;
+  if (out) cudaGraphDestroy(out);
+  if (bs) cudaStreamDestroy(bs);
+  if (!ok) {
+    G.exec = nullptr;
+    cudaGetLastError();
+  }
+  return ok;
+}
+
+// Run Krylov iterations until st->done: the graph-resident loop, or (where the loop graph
+// cannot be built) chunks of iterations with a read-back before each chunk.  Leaves the
+// final state in h->st_host.
+template <class ONE>
+int run_until_done(pism_gpu_ssa *h, int kind, const void *x, KState *st, int chunk0, int body_iters,
+                   const ONE &one) {
+  auto &G = h->loops[kind];
+  if (G.exec && G.x != x) {
+    cudaGraphExecDestroy(G.exec);
+    G = {};
+  }
+  if (!G.exec && !G.failed) {
+    const long long before = h->stats.kernel_launches;
+    long long per = 0;
+    G.failed = !build_loop(h, G, st, [&] {
+      const long long b0 = h->stats.kernel_launches;
+      for (int q = 0; q < body_iters; ++q) one();
+      per = (h->stats.kernel_launches - b0) / body_iters;
+    });
+    G.x = x;
+    G.per_iteration = per;
+    G.body_iters = body_iters;
+    h->stats.kernel_launches = before;   // nothing ran during the capture
+  }
+  if (G.exec) {
+    CK(h, cudaGraphLaunch(G.exec, h->stream));
+    CK(h, cudaMemcpyAsync(h->st_host, st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const long long passes = (h->st_host->iter + G.body_iters - 1) / G.body_iters;
+    h->stats.kernel_launches += 1 + passes * (G.body_iters * G.per_iteration + 1);
+    return PISM_GPU_SSA_OK;
+  }
+  int launched = 0, chunk = chunk0;
+  while (true) {
+    CK(h, cudaMemcpyAsync(h->st_host, st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (h->st_host->done) break;
+    RET(run_iterations(h, kind, x, chunk, one));
+    CK(h, cudaGetLastError());
+    launched += chunk;
+    chunk = std::max(4, std::min(64, launched / 8));
+  }
+  return PISM_GPU_SSA_OK;
+}
+
 // ---- one linear solve: BiCGStab on the device, host reads the state per chunk ----
 int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
   const GridDev &g = h->g;
@@ -230,19 +342,10 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *st
   *h->st_host = init;
   CK(h, cudaMemcpyAsync(h->K.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
   launch_bicg_init(h->L, g, f, h->K, h->rhs, x);
-  int launched = 0;
-  int chunk = std::max(8, (int)(0.8 * h->last_ksp_its));
-  while (true) {
-    const MGHierarchy *mg = active_mg(h);
-    RET(run_iterations(h, mg ? GRAPH_BICG_MG : GRAPH_BICG_JACOBI, x, chunk,
-                       [&] { launch_bicg_iteration(h->L, g, f, h->K, x, mg); }));
-    launched += chunk;
-    CK(h, cudaGetLastError());
-    CK(h, cudaMemcpyAsync(h->st_host, h->K.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
-    if (h->st_host->done) break;
-    chunk = std::max(4, std::min(64, launched / 8));
-  }
+  const MGHierarchy *mg = active_mg(h);
+  // long FP64 solves: four iterations per pass of the loop body
+  RET(run_until_done(h, mg ? GRAPH_BICG_MG : GRAPH_BICG_JACOBI, x, h->K.st, std::max(8, (int)(0.8 * h->last_ksp_its)),
+                     4, [&] { launch_bicg_iteration(h->L, g, f, h->K, x, mg); }));
   h->last_ksp_its = h->st_host->iter;
   *its_out = h->st_host->iter;
   *status_out = h->st_host->status;
@@ -314,39 +417,25 @@ int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, i
   const MGHierarchy *mg = active_mg(h);
   const int max_refine = 60;
   int inner_total = 0, status = KSP_OK;
+  // One host read-back per chunk of inner iterations: the outer test (FP64 residual of the
+  // step) and the inner tolerance are taken on the device by the inner solve's start.
+  launch_residual32(h->L, g, f, h->rhs, x, h->K32.rhs, h->res_dev);
   for (int refine = 0;; ++refine) {
-    launch_residual32(h->L, g, f, h->rhs, x, h->K32.rhs, h->res_dev);
-    CK(h, cudaMemcpyAsync(h->res_host, h->res_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
-    const double rn = sqrt(h->res_host[0]), bn = sqrt(h->res_host[1]);
+    launch_mixed_init(h->L, g.Mx * g.My, h->K32, h->res_dev, rtol, h->cfg.mixed_inner_rtol, h->cfg.ksp_max_it);
+    // short inner solves (a few iterations each): one iteration per pass
+    RET(run_until_done(h, GRAPH_MIXED, nullptr, h->K32.st, 8, 1,
+                       [&] { launch_mixed_iteration(h->L, g, f, *mg, h->K32); }));
+    const double rn = sqrt(h->st_host->outer_r2), bn = sqrt(h->st_host->outer_b2);
     h->stats.final_linear_residual = bn > 0 ? rn / bn : rn;
     if (!std::isfinite(rn)) { status = KSP_NAN; break; }
-    if (rn <= rtol * bn || bn == 0.0) break;
+    if (h->st_host->status == KSP_OUTER_DONE) break;
     if (refine >= max_refine) { status = KSP_MAXIT; break; }
-    // the inner solve reduces its residual by what this step still needs (with a margin),
-    // but never asks FP32 for more than mixed_inner_rtol
-    KState init{};
-    init.rtol = std::min(0.5, std::max(h->cfg.mixed_inner_rtol, 0.7 * rtol * bn / rn));
-    init.maxit = h->cfg.ksp_max_it;
-    *h->st_host = init;
-    CK(h, cudaMemcpyAsync(h->K32.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
-    launch_mixed_init(h->L, g.Mx * g.My, h->K32);
-    int launched = 0, chunk = 8;
-    while (true) {
-      RET(run_iterations(h, GRAPH_MIXED, nullptr, chunk,
-                         [&] { launch_mixed_iteration(h->L, g, f, *mg, h->K32); }));
-      launched += chunk;
-      CK(h, cudaGetLastError());
-      CK(h, cudaMemcpyAsync(h->st_host, h->K32.st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
-      CK(h, cudaStreamSynchronize(h->stream));
-      if (h->st_host->done) break;
-      chunk = std::max(4, std::min(32, launched / 4));
-    }
     inner_total += h->st_host->iter;
     h->stats.refinement_steps += 1;
     if (h->st_host->status == KSP_NAN) { status = KSP_NAN; break; }
     if (h->st_host->iter == 0) { status = KSP_BREAKDOWN; break; }   // no progress possible
     launch_axpy32(h->L, g.Mx * g.My, h->K32.d, x);
+    launch_residual32(h->L, g, f, h->rhs, x, h->K32.rhs, h->res_dev);
   }
   *its_out = inner_total;
   *status_out = status;
@@ -640,6 +729,8 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
   if (h->ev1) cudaEventDestroy(h->ev1);
   for (auto &gr : h->graphs)
     if (gr.exec) cudaGraphExecDestroy(gr.exec);
+  for (auto &lp : h->loops)
+    if (lp.exec) cudaGraphExecDestroy(lp.exec);
   mg_free(h->mg);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -661,6 +752,10 @@ int pism_gpu_ssa_set_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *cfg) {
   for (auto &gr : h->graphs) {   // the multigrid damping is captured by value
     if (gr.exec) cudaGraphExecDestroy(gr.exec);
     gr = {};
+  }
+  for (auto &lp : h->loops) {
+    if (lp.exec) cudaGraphExecDestroy(lp.exec);
+    lp = {};
   }
   return PISM_GPU_SSA_OK;
 }

@@ -11,11 +11,13 @@ namespace pism_gpu {
 
 // Krylov status codes written by the device (KSPConvergedReason analogues)
 enum : int { KSP_OK = 0, KSP_MAXIT = -3, KSP_BREAKDOWN = -5, KSP_NAN = -7 };
+constexpr int KSP_OUTER_DONE = 1;   // mixed precision: the outer residual already meets the tolerance
 
 // scalars of one Krylov solve, owned by the device
 struct KState {
   double rho, alpha, omega, beta;
   double rnorm2, bnorm2, rnorm0, rtol;
+  double outer_r2, outer_b2;   // the FP64 outer residual of a mixed-precision refinement step
   int iter, maxit, done, status;
 };
 
@@ -132,7 +134,13 @@ void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHiera
                double2 *z, const KState *st);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
                const KState *st);
-void launch_mixed_init(const Launch &L, int N, const Krylov32 &K);
+// the loop condition of a graph-resident Krylov loop: continue while st->done is 0
+void launch_loop_condition(const Launch &L, cudaGraphConditionalHandle cond, const KState *st);
+
+// the start of an inner FP32 solve; the outer test and the inner tolerance are taken on the
+// device from res2 = {||b - A x||^2, ||b||^2} (launch_residual32)
+void launch_mixed_init(const Launch &L, int N, const Krylov32 &K, const double *res2, double outer_rtol,
+                       double inner_min, int maxit);
 void launch_mixed_iteration(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H,
                             const Krylov32 &K);
 // r32 = (float) (b - A x) with FP64 arithmetic; out2 = {||b - A x||^2, ||b||^2}

@@ -1133,4 +1133,14 @@ void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, doub
   k_gm_update<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.Z, x, G.gs);
 }
 
+// sets the WHILE condition of a graph-resident Krylov loop from the device state
+__global__ void k_loop_condition(cudaGraphConditionalHandle cond, const KState *st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+}
+
+void launch_loop_condition(const Launch &L, cudaGraphConditionalHandle cond, const KState *st) {
+  L.tick();
+  k_loop_condition<<<1, 32, 0, L.stream>>>(cond, st);
+}
+
 }  // namespace pism_gpu

@@ -191,18 +191,18 @@ __global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc,
 }
 
 // Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial
-// pivoting, in place in shared memory (n <= 2 * 16), one CTA; written transposed so
-// that the per-cycle product reads it coalesced.  Rows are spread over 8-lane groups.
-__global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
+// pivoting, in place in shared memory (n <= 2 * 16 = 32), by one warp: lane q owns column
+// q, so every step needs only warp-level synchronisation.  Written transposed so that the
+// per-cycle product reads it coalesced.
+__global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
   extern __shared__ double a[];   // n * n, row-major
   const int n = 2 * L.N;
   __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
-  __shared__ int piv_row;
-  const int t = threadIdx.x, lane8 = t & 7, grp = t >> 3, ngrp = CTA_THREADS >> 3;
-  for (int q = t; q < n * n; q += CTA_THREADS) a[q] = 0.0;
-  __syncthreads();
-  if (t < L.N) {   // each cell's two rows are written by one thread
-    const int k = t, i = k / L.My, j = k % L.My;
+  const int q = threadIdx.x;
+  for (int e = q; e < n * n; e += 32) a[e] = 0.0;
+  __syncwarp();
+  if (q < L.N) {   // each cell's two rows are written by one lane
+    const int k = q, i = k / L.My, j = k % L.My;
     for (int b = 0; b < 9; ++b) {
       const int di = (b % 3) - 1, dj = 1 - (b / 3);
       const int kn = wrap(i + di, L.Mx) * L.My + wrap(j + dj, L.My);
@@ -213,67 +213,62 @@ __global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, d
       a[(2 * k + 1) * n + 2 * kn + 1] += (double)v.w;
     }
   }
-  __syncthreads();
+  __syncwarp();
   for (int col = 0; col < n; ++col) {
-    if (t < 32) {   // pivot search by warp 0
-      double best = -1.0;
-      int bi = col;
-      for (int r = col + t; r < n; r += 32) {
-        const double v = fabs(a[r * n + col]);
-        if (v > best) { best = v; bi = r; }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (t == 0) {
-        piv_row = bi;
-        perm[col] = bi;
-        if (!(best > 0.0)) *singular = 1;
+    // pivot: the largest |a[r][col]|, r >= col (lane r looks at row r), ties to the lower row
+    double best = (q >= col && q < n) ? fabs(a[q * n + col]) : -1.0;
+    int bi = (q >= col && q < n) ? q : col;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
       }
     }
-    __syncthreads();
-    const int p = piv_row;
-    if (p != col)
-      for (int q = t; q < n; q += CTA_THREADS) {
-        const double tmp = a[col * n + q];
-        a[col * n + q] = a[p * n + q];
-        a[p * n + q] = tmp;
-      }
-    __syncthreads();
+    const int p = bi;
+    if (q == 0) {
+      perm[col] = p;
+      if (!(best > 0.0)) *singular = 1;
+    }
+    if (p != col && q < n) {
+      const double tmp = a[col * n + q];
+      a[col * n + q] = a[p * n + q];
+      a[p * n + q] = tmp;
+    }
+    __syncwarp();
     const double pv = a[col * n + col];
     const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    __syncthreads();
+    __syncwarp();
     // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
-    for (int q = t; q < n; q += CTA_THREADS) a[col * n + q] = (q == col ? 1.0 : a[col * n + q]) * pinv;
-    __syncthreads();
-    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
-    for (int r = grp; r < n; r += ngrp) {
-      if (r == col) continue;
-      const double f = a[r * n + col];
-      for (int q = lane8; q < n; q += 8)
-        if (q != col) a[r * n + q] -= f * a[col * n + q];
+    if (q < n) a[col * n + q] = (q == col ? 1.0 : a[col * n + q]) * pinv;
+    __syncwarp();
+    // other rows: a[r][q] -= a[r][col] a[col][q] (q != col), then a[r][col] <- -a[r][col] / pivot
+    if (q < n && q != col) {
+      const double pq = a[col * n + q];
+      for (int r = 0; r < n; ++r)
+        if (r != col) a[r * n + q] -= a[r * n + col] * pq;
     }
-    __syncthreads();
-    for (int r = t; r < n; r += CTA_THREADS)
-      if (r != col) a[r * n + col] = -a[r * n + col] * a[col * n + col];
-    __syncthreads();
+    __syncwarp();
+    if (q == col)
+      for (int r = 0; r < n; ++r)
+        if (r != col) a[r * n + col] = -a[r * n + col] * pinv;
+    __syncwarp();
   }
-  // undo the row interchanges as column interchanges, in reverse order
+  // undo the row interchanges as column interchanges, in reverse order (lane q: row q)
   for (int col = n - 1; col >= 0; --col) {
     const int p = perm[col];
-    if (p != col)
-      for (int r = t; r < n; r += CTA_THREADS) {
-        const double tmp = a[r * n + col];
-        a[r * n + col] = a[r * n + p];
-        a[r * n + p] = tmp;
-      }
-    __syncthreads();
+    if (p != col && q < n) {
+      const double tmp = a[q * n + col];
+      a[q * n + col] = a[q * n + p];
+      a[q * n + p] = tmp;
+    }
+    __syncwarp();
   }
-  for (int q = t; q < n * n; q += CTA_THREADS) {
-    const int r = q / n, c = q - r * n;
-    invT_out[c * n + r] = a[q];
+  for (int e = q; e < n * n; e += 32) {
+    const int r = e / n, c = e - r * n;
+    invT_out[c * n + r] = a[e];
   }
 }
 
@@ -704,7 +699,7 @@ void mg_setup(const Launch &Lc, const GridDev &g, const Fields &f, const double4
   }
   const MGLevel &C = H.lev[H.nlev - 1];
   const int n = 2 * C.N;
-  k_mg_coarse_invert<<<1, CTA_THREADS, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
+  k_mg_coarse_invert<<<1, 32, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
   Lc.tick(H.nlev + 2);
 }
 

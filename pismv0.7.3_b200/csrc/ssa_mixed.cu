@@ -53,23 +53,33 @@ __device__ __forceinline__ double dotf(const float2 &a, const float2 &b) {
   return (double)a.x * (double)b.x + (double)a.y * (double)b.y;
 }
 
-// start of an inner solve with d0 = 0: r = rhat = rhs, p = v = d = 0
+// start of an inner solve with d0 = 0: r = rhat = rhs, p = v = d = 0.  The outer test
+// ||b - A x|| <= outer_rtol ||b|| and the inner tolerance (what this refinement step still
+// needs, with a margin, never below inner_min) come from the FP64 norms in res2.
 __global__ void __launch_bounds__(NT32) k32_init(int N, const float2 *__restrict__ rhs, float2 *__restrict__ r,
                                                  float2 *__restrict__ rhat, float2 *__restrict__ p,
                                                  float2 *__restrict__ v, float2 *__restrict__ d, double *partials,
-                                                 unsigned *ticket, KState *st) {
+                                                 unsigned *ticket, KState *st, const double *res2,
+                                                 double outer_rtol, double inner_min, int maxit) {
+  const double rn = sqrt(res2[0]), bn = sqrt(res2[1]);
+  const bool outer_done = !(rn > outer_rtol * bn) || bn == 0.0;   // NaN counts as done: the host reports it
   double acc[1] = {0.0};
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    const float2 b = rhs[k], z = make_float2(0.0f, 0.0f);
-    r[k] = b;
-    rhat[k] = b;
-    p[k] = z;
-    v[k] = z;
-    d[k] = z;
-    acc[0] += dotf(b, b);
-  }
+  if (!outer_done)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+      const float2 b = rhs[k], z = make_float2(0.0f, 0.0f);
+      r[k] = b;
+      rhat[k] = b;
+      p[k] = z;
+      v[k] = z;
+      d[k] = z;
+      acc[0] += dotf(b, b);
+    }
   double tot[1];
   if (grid_reduce<1>(acc, partials, ticket, tot)) {
+    st->outer_r2 = res2[0];
+    st->outer_b2 = res2[1];
+    st->rtol = fmin(0.5, fmax(inner_min, 0.7 * outer_rtol * bn / rn));
+    st->maxit = maxit;
     st->rnorm2 = tot[0];
     st->bnorm2 = tot[0];
     st->rnorm0 = sqrt(tot[0]);
@@ -80,7 +90,13 @@ __global__ void __launch_bounds__(NT32) k32_init(int N, const float2 *__restrict
     st->iter = 0;
     st->status = 0;
     st->done = (tot[0] == 0.0) ? 1 : 0;
-    if (!isfinite(tot[0])) { st->done = 1; st->status = KSP_NAN; }
+    if (outer_done) {
+      st->done = 1;
+      st->status = KSP_OUTER_DONE;
+    } else if (!isfinite(tot[0])) {
+      st->done = 1;
+      st->status = KSP_NAN;
+    }
   }
 }
 
@@ -190,8 +206,10 @@ int blocks_n(const Launch &L, int n) { return std::min((n + NT32 - 1) / NT32, L.
 
 }  // namespace
 
-void launch_mixed_init(const Launch &L, int N, const Krylov32 &K) {
-  k32_init<<<blocks_n(L, N), NT32, 0, L.stream>>>(N, K.rhs, K.r, K.rhat, K.p, K.v, K.d, L.partials, L.ticket, K.st);
+void launch_mixed_init(const Launch &L, int N, const Krylov32 &K, const double *res2, double outer_rtol,
+                       double inner_min, int maxit) {
+  k32_init<<<blocks_n(L, N), NT32, 0, L.stream>>>(N, K.rhs, K.r, K.rhat, K.p, K.v, K.d, L.partials, L.ticket, K.st,
+                                                  res2, outer_rtol, inner_min, maxit);
   L.tick();
 }
 
