@@ -358,6 +358,8 @@ def main():
     ap.add_argument("--workload", default="solve", choices=["solve", "ensemble"],
                     help="ensemble: members solved/s of a 64-member 401^2 ensemble (its own JSON line)")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2],
+                    help="Krylov launch mode: 2 graph-resident loops, 1 replayed graphs, 0 direct (for profilers)")
     ap.add_argument("--ksp-factor", type=float, default=1.0,
                     help="fast set-up: KSP rtol of a Picard iteration = factor x the last relative nu*H change")
     ap.add_argument("--ksp-max", type=float, default=1e-1, help="fast set-up: loosest KSP rtol of a Picard iteration")
@@ -385,6 +387,7 @@ def main():
     if args.mg_correction is not None:
         c_plain.mg_correction = args.mg_correction
     c_plain.verbosity = args.verbosity
+    c_plain.graphs = args.graphs
     c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max)
     if args.inner_rtol is not None:
         c_fast.mixed_inner_rtol = args.inner_rtol

@@ -124,6 +124,10 @@ typedef struct pism_gpu_ssa_config {
   int    ksp_rtol_adaptive;                        /* 0: every solve to ksp_rtol     */
   double ksp_rtol_max;
   double ksp_rtol_factor;
+  /* launch mode of the Krylov iterations: 2 a graph-resident loop per solve (a CUDA graph
+     with a conditional WHILE node), 1 captured graphs of a few iterations, 0 direct launches
+     (kernel profilers that cannot look into conditional graphs need 0 or 1) */
+  int    graphs;
   int    verbosity;                                /* 0 silent .. 3 per-iteration    */
 } pism_gpu_ssa_config;
 

@@ -177,6 +177,7 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
   if (c->ksp_rtol_adaptive && !(c->ksp_rtol_max >= c->ksp_rtol && c->ksp_rtol_max < 1.0 && c->ksp_rtol_factor > 0.0))
     return fail(h, PISM_GPU_SSA_EINVAL, "adaptive KSP tolerance needs ksp_rtol <= ksp_rtol_max < 1, ksp_rtol_factor > 0");
+  if (c->graphs < 0 || c->graphs > 2) return fail(h, PISM_GPU_SSA_EINVAL, "graphs must be 0, 1 or 2");
   if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
     return fail(h, PISM_GPU_SSA_EINVAL, "ksp_rtol, ksp_max_it and max_iterations_ssafd must be positive");
   if (!(c->ssa_Glen_exponent > 0.0) || !(c->min_thickness_strength_extension_ssa > 0.0))
@@ -198,7 +199,7 @@ int run_iterations(pism_gpu_ssa *h, int kind, const void *x, int count, const ON
     cudaGraphExecDestroy(G.exec);
     G = {};
   }
-  if (!G.exec && !G.failed) {
+  if (h->cfg.graphs >= 1 && !G.exec && !G.failed) {
     const long long before = h->stats.kernel_launches;
     cudaGraph_t graph = nullptr;
     bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
@@ -219,7 +220,7 @@ int run_iterations(pism_gpu_ssa *h, int kind, const void *x, int count, const ON
     h->stats.kernel_launches = before;   // nothing ran during the capture
   }
   int q = 0;
-  if (G.exec)
+  if (G.exec && h->cfg.graphs >= 1)
     for (; q + GRAPH_ITERS <= count; q += GRAPH_ITERS) {
       CK(h, cudaGraphLaunch(G.exec, h->stream));
       h->stats.kernel_launches += G.kernels;
@@ -298,7 +299,7 @@ int run_until_done(pism_gpu_ssa *h, int kind, const void *x, KState *st, int chu
     cudaGraphExecDestroy(G.exec);
     G = {};
   }
-  if (!G.exec && !G.failed) {
+  if (h->cfg.graphs >= 2 && !G.exec && !G.failed) {
     const long long before = h->stats.kernel_launches;
     long long per = 0;
     G.failed = !build_loop(h, G, st, [&] {
@@ -311,7 +312,7 @@ int run_until_done(pism_gpu_ssa *h, int kind, const void *x, KState *st, int chu
     G.body_iters = body_iters;
     h->stats.kernel_launches = before;   // nothing ran during the capture
   }
-  if (G.exec) {
+  if (G.exec && h->cfg.graphs >= 2) {
     CK(h, cudaGraphLaunch(G.exec, h->stream));
     CK(h, cudaMemcpyAsync(h->st_host, st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
@@ -625,6 +626,7 @@ int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *c) {
   c->ksp_rtol_adaptive = 0;
   c->ksp_rtol_max = 1.0e-2;
   c->ksp_rtol_factor = 1.0e-2;
+  c->graphs = 2;
   c->verbosity = 0;
   return PISM_GPU_SSA_OK;
 }

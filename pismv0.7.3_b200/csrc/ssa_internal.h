@@ -80,7 +80,7 @@ struct Launch {
 constexpr int MG_MAX_LEVELS = 16;
 constexpr int MG_COARSE_DIM = 4;                 // the coarsest level has <= 4 x 4 cells
 constexpr int MG_MAX_COARSE_CELLS = MG_COARSE_DIM * MG_COARSE_DIM;
-constexpr int MG_CTA_CELLS = 4096;               // levels this small are cycled by one CTA
+constexpr int MG_CTA_CELLS = 4096;               // levels this small are cycled by one thread-block cluster
 
 struct MGLevel {
   int Mx = 0, My = 0, N = 0;
@@ -94,7 +94,8 @@ struct MGHierarchy {
   int nlev = 0;                                  // coarse levels (level 1 .. nlev)
   int fine_ax = 1, fine_ay = 1;                  // aggregation of the fine grid
   MGLevel lev[MG_MAX_LEVELS];
-  int small_first = 0;                           // first level cycled by one CTA
+  int small_first = 0;                           // first level cycled by the cluster
+  int small_smem = 0;                            // its per-CTA staging buffer (bytes)
   float omega = 0.9f;                            // damping of the block-Jacobi smoother
   float correction = 1.2f;                       // scaling of the coarse-grid correction
   double *cinv = nullptr;                        // dense inverse of the coarsest operator (transposed)

@@ -190,34 +190,39 @@ __global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc,
   }
 }
 
-// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial
-// pivoting, in place in shared memory (n <= 2 * 16 = 32), by one warp: lane q owns column
-// q, so every step needs only warp-level synchronisation.  Written transposed so that the
-// per-cycle product reads it coalesced.
+// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial pivoting,
+// in one warp's registers: lane r holds row r of the matrix padded to 32 x 32 with the
+// identity (n = 2 * cells <= 32), every loop over columns is unrolled so the row lives in
+// registers, and the pivot row reaches the other lanes by shuffles.  Written transposed so
+// that the per-cycle product reads it coalesced.
 __global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
-  extern __shared__ double a[];   // n * n, row-major
-  const int n = 2 * L.N;
-  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
-  const int q = threadIdx.x;
-  for (int e = q; e < n * n; e += 32) a[e] = 0.0;
+  __shared__ double m[32 * 32];
+  const int n = 2 * L.N, lane = threadIdx.x;
+  for (int e = lane; e < 32 * 32; e += 32) m[e] = (e / 32 == e % 32 && e / 32 >= n) ? 1.0 : 0.0;
   __syncwarp();
-  if (q < L.N) {   // each cell's two rows are written by one lane
-    const int k = q, i = k / L.My, j = k % L.My;
+  if (lane < L.N) {   // each cell's two rows are assembled by one lane
+    const int k = lane, i = k / L.My, j = k % L.My;
     for (int b = 0; b < 9; ++b) {
       const int di = (b % 3) - 1, dj = 1 - (b / 3);
       const int kn = wrap(i + di, L.Mx) * L.My + wrap(j + dj, L.My);
       const float4 v = L.A[b * L.N + k];
-      a[(2 * k + 0) * n + 2 * kn + 0] += (double)v.x;
-      a[(2 * k + 0) * n + 2 * kn + 1] += (double)v.y;
-      a[(2 * k + 1) * n + 2 * kn + 0] += (double)v.z;
-      a[(2 * k + 1) * n + 2 * kn + 1] += (double)v.w;
+      m[(2 * k + 0) * 32 + 2 * kn + 0] += (double)v.x;
+      m[(2 * k + 0) * 32 + 2 * kn + 1] += (double)v.y;
+      m[(2 * k + 1) * 32 + 2 * kn + 0] += (double)v.z;
+      m[(2 * k + 1) * 32 + 2 * kn + 1] += (double)v.w;
     }
   }
   __syncwarp();
-  for (int col = 0; col < n; ++col) {
-    // pivot: the largest |a[r][col]|, r >= col (lane r looks at row r), ties to the lower row
-    double best = (q >= col && q < n) ? fabs(a[q * n + col]) : -1.0;
-    int bi = (q >= col && q < n) ? q : col;
+  double a[32];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) a[c] = m[lane * 32 + c];
+  int perm[32];
+  bool sing = false;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    // pivot: the largest |a[r][k]| over rows r >= k, ties to the lower row
+    double best = lane >= k ? fabs(a[k]) : -1.0;
+    int bi = lane >= k ? lane : k;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double ob = __shfl_xor_sync(0xffffffffu, best, o);
@@ -228,48 +233,47 @@ __global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *in
       }
     }
     const int p = bi;
-    if (q == 0) {
-      perm[col] = p;
-      if (!(best > 0.0)) *singular = 1;
+    perm[k] = p;
+    sing |= !(best > 0.0);
+    if (p != k) {   // rows k and p trade places
+      const int src = lane == k ? p : (lane == p ? k : lane);
+#pragma unroll
+      for (int c = 0; c < 32; ++c) a[c] = __shfl_sync(0xffffffffu, a[c], src);
     }
-    if (p != col && q < n) {
-      const double tmp = a[col * n + q];
-      a[col * n + q] = a[p * n + q];
-      a[p * n + q] = tmp;
-    }
-    __syncwarp();
-    const double pv = a[col * n + col];
+    const double pv = __shfl_sync(0xffffffffu, a[k], k);
     const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    __syncwarp();
-    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
-    if (q < n) a[col * n + q] = (q == col ? 1.0 : a[col * n + q]) * pinv;
-    __syncwarp();
-    // other rows: a[r][q] -= a[r][col] a[col][q] (q != col), then a[r][col] <- -a[r][col] / pivot
-    if (q < n && q != col) {
-      const double pq = a[col * n + q];
-      for (int r = 0; r < n; ++r)
-        if (r != col) a[r * n + q] -= a[r * n + col] * pq;
+    if (lane == k) {   // pivot row: a[k][k] <- 1, then scaled, so it holds 1 / pivot
+#pragma unroll
+      for (int c = 0; c < 32; ++c) a[c] = (c == k ? 1.0 : a[c]) * pinv;
     }
-    __syncwarp();
-    if (q == col)
-      for (int r = 0; r < n; ++r)
-        if (r != col) a[r * n + col] = -a[r * n + col] * pinv;
-    __syncwarp();
-  }
-  // undo the row interchanges as column interchanges, in reverse order (lane q: row q)
-  for (int col = n - 1; col >= 0; --col) {
-    const int p = perm[col];
-    if (p != col && q < n) {
-      const double tmp = a[q * n + col];
-      a[q * n + col] = a[q * n + p];
-      a[q * n + p] = tmp;
+    const double f = a[k];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      const double pc = __shfl_sync(0xffffffffu, a[c], k);
+      if (lane != k) a[c] = (c == k) ? -f * pinv : a[c] - f * pc;
     }
-    __syncwarp();
   }
-  for (int e = q; e < n * n; e += 32) {
-    const int r = e / n, c = e - r * n;
-    invT_out[c * n + r] = a[e];
+  // undo the row interchanges as column interchanges, in reverse order
+#pragma unroll
+  for (int k = 31; k >= 0; --k) {
+    const int p = perm[k];
+    if (p != k) {
+      const double ak = a[k];
+      double ap = 0.0;
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        if (c == p) ap = a[c];
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        if (c == p) a[c] = ak;
+      a[k] = ap;
+    }
   }
+  if (sing && lane == 0) *singular = 1;
+  if (lane < n)
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+      if (c < n) invT_out[c * n + lane] = a[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -451,7 +455,7 @@ __global__ void __launch_bounds__(NTm) k_mgc_post(LevelView L, float omega, floa
   }
 }
 
-// The small levels (first .. last, <= MG_CTA_CELLS cells each) in one CTA: restrictions
+// The small levels (first .. last, <= MG_CTA_CELLS cells each) in one launch: restrictions
 // down, the dense solve, post-smoothing up; __syncthreads between the steps.
 struct SmallLevels {
   int first, last;        // level indices into lev[]
@@ -481,7 +485,7 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
       asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }
   }
-  __shared__ float2 xs[MG_CTA_CELLS];
+  extern __shared__ float2 xs[];   // the largest small level (H.small_smem bytes)
   __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
   // Each step below costs one dependent round trip to L2: the staging loops are unrolled so
   // a thread's loads issue together, and the restriction gives every fine cell of an
@@ -593,9 +597,10 @@ int mg_plan(int Mx, int My, MGHierarchy &H) {
     return 0;
   }
   C.ax = C.ay = 1;
-  // the levels cycled by one CTA: the trailing run of levels with <= MG_CTA_CELLS cells
+  // the levels cycled by the cluster kernel: the trailing run of levels with <= MG_CTA_CELLS cells
   H.small_first = H.nlev - 1;
   while (H.small_first > 0 && H.lev[H.small_first - 1].N <= MG_CTA_CELLS) --H.small_first;
+  H.small_smem = (int)sizeof(float2) * H.lev[H.small_first].N;   // every CTA stages a whole level
   return H.nlev;
 }
 
@@ -621,8 +626,7 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
     if (cudaMalloc(&H.views, sizeof(LevelView) * MG_MAX_LEVELS) != cudaSuccess) return 1;
     if (cudaMemcpy(H.views, v, sizeof(LevelView) * H.nlev, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
   }
-  if (cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(sizeof(double) * n * n)) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_mg_small_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, H.small_smem) != cudaSuccess)
     return 1;
   if (cudaFuncSetAttribute(k_mg_build1, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(double) * 36 * NTm)) != cudaSuccess)
@@ -698,8 +702,7 @@ void mg_setup(const Launch &Lc, const GridDev &g, const Fields &f, const double4
     k_mg_build<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(view(F), C.Mx, C.My, tm, C.A, C.dinv);
   }
   const MGLevel &C = H.lev[H.nlev - 1];
-  const int n = 2 * C.N;
-  k_mg_coarse_invert<<<1, 32, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
+  k_mg_coarse_invert<<<1, 32, 0, Lc.stream>>>(view(C), H.cinv, H.singular);
   Lc.tick(H.nlev + 2);
 }
 
@@ -746,7 +749,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     S.lev = reinterpret_cast<const LevelView *>(H.views);
     S.invT = H.cinv;
     S.n = 2 * H.lev[H.nlev - 1].N;
-    k_mg_small_cycle<<<SMALL_CLUSTER, CTA_THREADS, 0, Lc.stream>>>(S, omega, corr, st);
+    k_mg_small_cycle<<<SMALL_CLUSTER, CTA_THREADS, H.small_smem, Lc.stream>>>(S, omega, corr, st);
     ++launches;
   }
   // up through the large coarse levels
