@@ -128,6 +128,10 @@ def fast_config(c, precision="mixed", factor=1.0, rtol_max=1e-1):
                   ksp_rtol_max=rtol_max)
 
 
+def ms_per_step_local(total_ms, steps):
+    return total_ms / max(1, steps)
+
+
 def max_over_ranks(x: float, device=None) -> float:
     """The largest value of x over the ranks of the process group (x itself without one).
     Replicas are timed separately; the job takes as long as its slowest rank."""
@@ -358,6 +362,8 @@ def main():
     ap.add_argument("--workload", default="solve", choices=["solve", "ensemble"],
                     help="ensemble: members solved/s of a 64-member 401^2 ensemble (its own JSON line)")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--profile", action="store_true",
+                    help="time the solve only (no end-to-end, roofline, comparison or CPU runs): for kernel profilers")
     ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2],
                     help="Krylov launch mode: 2 graph-resident loops, 1 replayed graphs, 0 direct (for profilers)")
     ap.add_argument("--ksp-factor", type=float, default=1.0,
@@ -464,6 +470,12 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     vel_mode = out.clone()
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": ms_per_step_local(total_ms, args.steps), "unit": "ms",
+                              "profile": True, "solver": {"picard_iterations": picard, "ksp_iterations": ksp}}))
+        s.close()
+        return 0
 
     ms_per_step = max_over_ranks(total_ms, dev) / args.steps
     value = job_time_per_solve(ms_per_step, world)

@@ -320,7 +320,9 @@ int run_until_done(pism_gpu_ssa *h, int kind, const void *x, KState *st, int chu
     h->stats.kernel_launches += 1 + passes * (G.body_iters * G.per_iteration + 1);
     return PISM_GPU_SSA_OK;
   }
-  int launched = 0, chunk = chunk0;
+  // graphs == 0 (kernel profiling): one read-back per iteration, so that no iteration is
+  // launched after convergence; otherwise growing chunks
+  int launched = 0, chunk = h->cfg.graphs == 0 ? 1 : chunk0;
   while (true) {
     CK(h, cudaMemcpyAsync(h->st_host, st, sizeof(KState), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
@@ -328,7 +330,7 @@ int run_until_done(pism_gpu_ssa *h, int kind, const void *x, KState *st, int chu
     RET(run_iterations(h, kind, x, chunk, one));
     CK(h, cudaGetLastError());
     launched += chunk;
-    chunk = std::max(4, std::min(64, launched / 8));
+    if (h->cfg.graphs != 0) chunk = std::max(4, std::min(64, launched / 8));
   }
   return PISM_GPU_SSA_OK;
 }

@@ -190,90 +190,91 @@ __global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc,
   }
 }
 
-// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial pivoting,
-// in one warp's registers: lane r holds row r of the matrix padded to 32 x 32 with the
-// identity (n = 2 * cells <= 32), every loop over columns is unrolled so the row lives in
-// registers, and the pivot row reaches the other lanes by shuffles.  Written transposed so
-// that the per-cycle product reads it coalesced.
-__global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
-  __shared__ double m[32 * 32];
-  const int n = 2 * L.N, lane = threadIdx.x;
-  for (int e = lane; e < 32 * 32; e += 32) m[e] = (e / 32 == e % 32 && e / 32 >= n) ? 1.0 : 0.0;
-  __syncwarp();
-  if (lane < L.N) {   // each cell's two rows are assembled by one lane
-    const int k = lane, i = k / L.My, j = k % L.My;
+// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial
+// pivoting, in place in shared memory (n <= 2 * 16), one CTA; written transposed so
+// that the per-cycle product reads it coalesced.  Rows are spread over 8-lane groups.
+__global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
+  extern __shared__ double a[];   // n * n, row-major
+  const int n = 2 * L.N;
+  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
+  __shared__ int piv_row;
+  const int t = threadIdx.x, lane8 = t & 7, grp = t >> 3, ngrp = CTA_THREADS >> 3;
+  for (int q = t; q < n * n; q += CTA_THREADS) a[q] = 0.0;
+  __syncthreads();
+  if (t < L.N) {   // each cell's two rows are written by one thread
+    const int k = t, i = k / L.My, j = k % L.My;
     for (int b = 0; b < 9; ++b) {
       const int di = (b % 3) - 1, dj = 1 - (b / 3);
       const int kn = wrap(i + di, L.Mx) * L.My + wrap(j + dj, L.My);
       const float4 v = L.A[b * L.N + k];
-      m[(2 * k + 0) * 32 + 2 * kn + 0] += (double)v.x;
-      m[(2 * k + 0) * 32 + 2 * kn + 1] += (double)v.y;
-      m[(2 * k + 1) * 32 + 2 * kn + 0] += (double)v.z;
-      m[(2 * k + 1) * 32 + 2 * kn + 1] += (double)v.w;
+      a[(2 * k + 0) * n + 2 * kn + 0] += (double)v.x;
+      a[(2 * k + 0) * n + 2 * kn + 1] += (double)v.y;
+      a[(2 * k + 1) * n + 2 * kn + 0] += (double)v.z;
+      a[(2 * k + 1) * n + 2 * kn + 1] += (double)v.w;
     }
   }
-  __syncwarp();
-  double a[32];
-#pragma unroll
-  for (int c = 0; c < 32; ++c) a[c] = m[lane * 32 + c];
-  int perm[32];
-  bool sing = false;
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    // pivot: the largest |a[r][k]| over rows r >= k, ties to the lower row
-    double best = lane >= k ? fabs(a[k]) : -1.0;
-    int bi = lane >= k ? lane : k;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
+  __syncthreads();
+  for (int col = 0; col < n; ++col) {
+    if (t < 32) {   // pivot search by warp 0
+      double best = -1.0;
+      int bi = col;
+      for (int r = col + t; r < n; r += 32) {
+        const double v = fabs(a[r * n + col]);
+        if (v > best) { best = v; bi = r; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (t == 0) {
+        piv_row = bi;
+        perm[col] = bi;
+        if (!(best > 0.0)) *singular = 1;
       }
     }
-    const int p = bi;
-    perm[k] = p;
-    sing |= !(best > 0.0);
-    if (p != k) {   // rows k and p trade places
-      const int src = lane == k ? p : (lane == p ? k : lane);
-#pragma unroll
-      for (int c = 0; c < 32; ++c) a[c] = __shfl_sync(0xffffffffu, a[c], src);
-    }
-    const double pv = __shfl_sync(0xffffffffu, a[k], k);
+    __syncthreads();
+    const int p = piv_row;
+    if (p != col)
+      for (int q = t; q < n; q += CTA_THREADS) {
+        const double tmp = a[col * n + q];
+        a[col * n + q] = a[p * n + q];
+        a[p * n + q] = tmp;
+      }
+    __syncthreads();
+    const double pv = a[col * n + col];
     const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    if (lane == k) {   // pivot row: a[k][k] <- 1, then scaled, so it holds 1 / pivot
-#pragma unroll
-      for (int c = 0; c < 32; ++c) a[c] = (c == k ? 1.0 : a[c]) * pinv;
+    __syncthreads();
+    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
+    for (int q = t; q < n; q += CTA_THREADS) a[col * n + q] = (q == col ? 1.0 : a[col * n + q]) * pinv;
+    __syncthreads();
+    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
+    for (int r = grp; r < n; r += ngrp) {
+      if (r == col) continue;
+      const double f = a[r * n + col];
+      for (int q = lane8; q < n; q += 8)
+        if (q != col) a[r * n + q] -= f * a[col * n + q];
     }
-    const double f = a[k];
-#pragma unroll
-    for (int c = 0; c < 32; ++c) {
-      const double pc = __shfl_sync(0xffffffffu, a[c], k);
-      if (lane != k) a[c] = (c == k) ? -f * pinv : a[c] - f * pc;
-    }
+    __syncthreads();
+    for (int r = t; r < n; r += CTA_THREADS)
+      if (r != col) a[r * n + col] = -a[r * n + col] * a[col * n + col];
+    __syncthreads();
   }
   // undo the row interchanges as column interchanges, in reverse order
-#pragma unroll
-  for (int k = 31; k >= 0; --k) {
-    const int p = perm[k];
-    if (p != k) {
-      const double ak = a[k];
-      double ap = 0.0;
-#pragma unroll
-      for (int c = 0; c < 32; ++c)
-        if (c == p) ap = a[c];
-#pragma unroll
-      for (int c = 0; c < 32; ++c)
-        if (c == p) a[c] = ak;
-      a[k] = ap;
-    }
+  for (int col = n - 1; col >= 0; --col) {
+    const int p = perm[col];
+    if (p != col)
+      for (int r = t; r < n; r += CTA_THREADS) {
+        const double tmp = a[r * n + col];
+        a[r * n + col] = a[r * n + p];
+        a[r * n + p] = tmp;
+      }
+    __syncthreads();
   }
-  if (sing && lane == 0) *singular = 1;
-  if (lane < n)
-#pragma unroll
-    for (int c = 0; c < 32; ++c)
-      if (c < n) invT_out[c * n + lane] = a[c];
+  for (int q = t; q < n * n; q += CTA_THREADS) {
+    const int r = q / n, c = q - r * n;
+    invT_out[c * n + r] = a[q];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -628,6 +629,9 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
   }
   if (cudaFuncSetAttribute(k_mg_small_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, H.small_smem) != cudaSuccess)
     return 1;
+  if (cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(double) * n * n)) != cudaSuccess)
+    return 1;
   if (cudaFuncSetAttribute(k_mg_build1, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(double) * 36 * NTm)) != cudaSuccess)
     return 1;
@@ -702,7 +706,8 @@ void mg_setup(const Launch &Lc, const GridDev &g, const Fields &f, const double4
     k_mg_build<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(view(F), C.Mx, C.My, tm, C.A, C.dinv);
   }
   const MGLevel &C = H.lev[H.nlev - 1];
-  k_mg_coarse_invert<<<1, 32, 0, Lc.stream>>>(view(C), H.cinv, H.singular);
+  const int n = 2 * C.N;
+  k_mg_coarse_invert<<<1, CTA_THREADS, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
   Lc.tick(H.nlev + 2);
 }
 
