@@ -192,10 +192,12 @@ def solve_config(c: SSAConfig) -> SSAConfig:
                   ksp_rtol_max=1e-2, ssafd_relative_convergence=1e-4)
 
 
-def generate(seeds, M: int = 401, device: int = 0, workers: int = 4, log=None):
-    """Solve the training cases (``workers`` solver handles on their own CUDA streams, one
-    host thread each) and return [(features [H8, W8, 8], target [H8, W8, 2], weight [H8, W8])]
-    on the device plus per-case stats."""
+def generate(seeds, M: int = 401, device: int = 0, workers: int = 1, log=None):
+    """Solve the training cases and return [(features [H8, W8, 8], target [H8, W8, 2],
+    weight [H8, W8])] on the device plus per-case stats.  workers > 1 drives that many solver
+    handles from host threads on their own CUDA streams; one such run ended in an illegal
+    memory access whose cause was not found, so the default (and the committed weights) use
+    a single worker."""
     import torch
     from .ssa import SSAFD
     dev = torch.device("cuda", device)
