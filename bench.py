@@ -362,6 +362,8 @@ def main():
     ap.add_argument("--workload", default="solve", choices=["solve", "ensemble"],
                     help="ensemble: members solved/s of a 64-member 401^2 ensemble (its own JSON line)")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--picard-rtol", type=float, default=None,
+                    help="Picard nu*H tolerance of both set-ups (default: the configuration's 1e-4)")
     ap.add_argument("--profile", action="store_true",
                     help="time the solve only (no end-to-end, roofline, comparison or CPU runs): for kernel profilers")
     ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2],
@@ -393,6 +395,9 @@ def main():
     if args.mg_correction is not None:
         c_plain.mg_correction = args.mg_correction
     c_plain.verbosity = args.verbosity
+    if args.picard_rtol is not None:
+        c_plain.ssafd_relative_convergence = args.picard_rtol
+        c_plain.max_iterations_ssafd = 5000
     c_plain.graphs = args.graphs
     c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max)
     if args.inner_rtol is not None:
@@ -510,7 +515,8 @@ def main():
         # against an FP64 solve continued from the plain answer to a nu*H change of 1e-8.
         accuracy = None
         if not args.no_accuracy:
-            c_conv = c_plain.copy(ssafd_relative_convergence=1e-8, ksp_rtol=1e-10, ksp_rtol_adaptive=True,
+            c_conv = c_plain.copy(ssafd_relative_convergence=min(1e-8, 0.01 * c_plain.ssafd_relative_convergence),
+                              ksp_rtol=1e-10, ksp_rtol_adaptive=True,
                                   ksp_rtol_factor=0.1, ksp_rtol_max=1e-2, max_iterations_ssafd=5000, precision="fp64")
             s_ref = SSAFD(g, c_conv, device=local)
             s_ref.set_stream(stream.cuda_stream)
@@ -520,11 +526,40 @@ def main():
             s_ref.solve(out=vel_conv)
             st_ref = s_ref.stats()
             s_ref.close()
-            accuracy = {"reference": "FP64 Picard continued from the plain answer to nu*H change 1e-8, KSP rtol 1e-10",
+            accuracy = {"reference": f"FP64 Picard continued from the plain answer to nu*H change "
+                                     f"{c_conv.ssafd_relative_convergence:g}, KSP rtol 1e-10",
                         "reference_picard_iterations": st_ref["picard_iterations"],
                         "reference_converged": st_ref["converged"],
                         "plain_vs_reference": errors(vel_plain, vel_conv),
                         "fast_vs_reference": errors(vel_fast, vel_conv)}
+            # both set-ups again at Picard tolerance 1e-6, against the same converged solve
+            if args.picard_rtol is None:
+                def timed(cfg, learned):
+                    h = SSAFD(g, cfg.copy(ssafd_relative_convergence=1e-6, max_iterations_ssafd=5000), device=local)
+                    h.set_stream(stream.cuda_stream)
+                    h.set_inputs(**dfields)
+                    o = torch.empty_like(out)
+                    for _ in range(2):
+                        flush.fill_(1.0)
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        if learned:
+                            Lrn.learned_guess(h, net, stride)
+                        else:
+                            h.set_initial_guess(zero)
+                        h.solve(out=o)
+                        e1.record(stream)
+                        torch.cuda.synchronize()
+                    stt = h.stats()
+                    h.close()
+                    return o, e0.elapsed_time(e1), stt
+                uf, tf, sf = timed(c_fast, net is not None)
+                up, tp, sp = timed(c_plain, False)
+                accuracy["picard_rtol_1e-6"] = {
+                    "fast_ms": tf, "fast_picard_iterations": sf["picard_iterations"],
+                    "plain_ms": tp, "plain_picard_iterations": sp["picard_iterations"],
+                    "plain_over_fast": tp / tf, "fast_vs_reference": errors(uf, vel_conv),
+                    "plain_vs_reference": errors(up, vel_conv)}
 
     # end to end through the C-ABI with pinned host buffers: H2D inputs, solve, D2H velocity
     hfields = {k: torch.tensor(f[k], dtype=torch.float64).pin_memory() for k in names}
@@ -583,7 +618,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if c.precision == "fp64" else "f64+f32", "data": "synthetic",
         "config": {"workload": f"SSAFD solve, synthetic ice sheet {M}x{M} at {4000 / (M - 1):.0f} km, plastic till, "
-                               f"Picard 1e-4; {args.mode} set-up",
+                               f"Picard {c.ssafd_relative_convergence:g}; {args.mode} set-up",
                    "mode": args.mode, "grid": [M, M], "seed": 0, "precision": c.precision,
                    "ksp": f"{'FGMRES(%d)' % c.gmres_restart if c.ksp_type == 'gmres' else 'BiCGStab'} + "
                           f"{'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'}",
