@@ -300,3 +300,23 @@ def test_inexact_picard_meets_the_same_tolerance(precision):
     assert rel(vel, ref) < 1e-7
     exact_ksp = _solve_case(g, c.copy(ksp_rtol_adaptive=False), f)[1]["ksp_iterations"]
     assert st["ksp_iterations"] < 0.8 * exact_ksp
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_launch_modes_agree_bitwise(precision):
+    """graphs = 2 (graph-resident loops), 1 (replayed iteration graphs) and 0 (direct
+    launches) run the same kernels in the same order: identical velocities and counts."""
+    g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=8)
+    c.pc_type = "mg"
+    c.precision = precision
+    c.ksp_rtol = 1e-8
+    c.ksp_rtol_adaptive = True
+    c.ksp_rtol_factor = 1.0
+    c.ksp_rtol_max = 1e-1
+    out = {}
+    for mode in (2, 1, 0):
+        vel, st = _solve_case(g, c.copy(graphs=mode), f)
+        out[mode] = (vel, st["picard_iterations"], st["ksp_iterations"], st["refinement_steps"])
+    for mode in (1, 0):
+        np.testing.assert_array_equal(out[mode][0], out[2][0])
+        assert out[mode][1:] == out[2][1:]
