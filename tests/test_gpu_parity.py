@@ -320,3 +320,26 @@ def test_launch_modes_agree_bitwise(precision):
     for mode in (1, 0):
         np.testing.assert_array_equal(out[mode][0], out[2][0])
         assert out[mode][1:] == out[2][1:]
+
+
+def test_ksp_failure_falls_back_and_is_reported():
+    """A Krylov budget too small to converge (FP64 path): the failure switches
+    preconditioner (multigrid -> block Jacobi, as the reference switches to ASM,
+    SSAFD.cc:929-958), the retry fails too and SSAFD::solve reports KSPFailure; the handle
+    stays usable and a solve with a normal budget afterwards succeeds.  (With precision
+    mixed, ksp_max_it bounds each inner FP32 solve and the FP64 refinement goes on.)"""
+    from pism_b200.ssa import KSPFailure
+    g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=9)
+    c.pc_type = "mg"
+    c.precision = "fp64"
+    c.ksp_rtol = 1e-10
+    c.ksp_max_it = 2
+    s = make_solver(g, c, f)
+    with pytest.raises(KSPFailure):
+        s.solve()
+    s.set_config(c.copy(ksp_max_it=10000))
+    s.set_initial_guess(np.zeros((g.Mx, g.My, 2)))
+    vel = s.solve()
+    st = s.stats()
+    assert st["converged"] == 1 and np.all(np.isfinite(vel))
+    s.close()
