@@ -4,7 +4,7 @@
  * No reference counterpart: PISM v0.7.3 starts SSAFD::solve from the previous velocity
  * (SSA.cc:178, SSA::set_initial_guess SSA.cc:361-363).  This network predicts that initial
  * velocity from the solve's inputs; the Picard / Krylov path then iterates from it and is
- * the judge of every accepted answer (the same stopping tests as from any other guess).
+ * what decides every accepted answer (the same stopping tests as from any other guess).
  *
  * Network (input 8 channels, output 2, images H x W with H, W multiples of 8):
  *   e1 = conv(conv(x, 16->32), 32->32)          full resolution  (x padded 8 -> 16 channels)

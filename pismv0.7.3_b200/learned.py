@@ -8,7 +8,7 @@
   ice sheets) and the training loop (random crops, flips and transposes, weighted MSE on
   asinh(u / 10 m/yr)).
 
-The solver stays the judge: a learned guess only replaces the zero / previous-step initial
+The solver decides what is accepted: a learned guess only replaces the zero / previous-step initial
 velocity of SSA::set_initial_guess (src/base/stressbalance/ssa/SSA.cc:361-363); the Picard
 and Krylov stopping tests are unchanged.  There is no CPU fallback: without the compiled
 library every call raises.

@@ -2,7 +2,7 @@
 
 Tolerances: FP64 stage values agree to 1e-12 relative (the GPU multiplies by
 reciprocals of dx^2, dy^2, 2 dx dy, 4 dx dy and contracts to FMA where the oracle
-divides); converged velocities agree to the north-star bar of 1e-8 relative L2
+divides); converged velocities agree to the parity bar of 1e-8 relative L2
 with tight Picard / KSP tolerances.
 """
 import numpy as np
