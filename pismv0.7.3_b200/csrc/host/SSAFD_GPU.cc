@@ -69,7 +69,10 @@ void SSAFD_GPU::solve() {
   in.enthalpy = m_vars.enthalpy ? m_vars.enthalpy->data() : nullptr;
   in.fracture_density = m_vars.fracture_density ? m_vars.fracture_density->a.data() : nullptr;
   check(pism_gpu_ssa_set_inputs(m_gpu, &in), "set_inputs");
-  check(pism_gpu_ssa_set_initial_guess(m_gpu, m_velocity.a.data(), PISM_MEM_HOST), "set_initial_guess");
+  if (m_net)
+    check(pism_gpu_ssa_learned_guess(m_gpu, m_net, m_stride), "learned initial guess");
+  else
+    check(pism_gpu_ssa_set_initial_guess(m_gpu, m_velocity.a.data(), PISM_MEM_HOST), "set_initial_guess");
   check(pism_gpu_ssa_solve(m_gpu, m_velocity.a.data(), PISM_MEM_HOST, &m_stats), "SSAFD solve");
   check(pism_gpu_ssa_get_field(m_gpu, PISM_FIELD_BFRICT, m_bfrict.a.data(), PISM_MEM_HOST), "bfrict");
   char buf[128];

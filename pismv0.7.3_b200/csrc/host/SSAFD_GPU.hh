@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "pism_ssa_gpu.h"
+#include "pism_unet_gpu.h"
 
 namespace pism_b200 {
 
@@ -123,6 +123,12 @@ class SSAFD_GPU : public SSA {
   const pism_gpu_ssa_stats &stats() const { return m_stats; }
   // the SSAFD_nuH diagnostic (SSAFD.cc:1790-1823): staggered nu*H, interleaved
   std::vector<double> nuH() const;
+  // Start the solves from the learned initial guess (include/pism_unet_gpu.h) instead of the
+  // previous velocity; nullptr restores the reference's start.  The network is borrowed.
+  void set_warm_start(pism_gpu_unet *net, int stride = 1) {
+    m_net = net;
+    m_stride = stride;
+  }
 
  protected:
   void init_impl() override;
@@ -132,6 +138,8 @@ class SSAFD_GPU : public SSA {
   void check(int rc, const char *what) const;
   pism_gpu_ssa *m_gpu = nullptr;
   pism_gpu_ssa_stats m_stats{};
+  pism_gpu_unet *m_net = nullptr;
+  int m_stride = 1;
 };
 
 typedef SSA *(*SSAFactory)(const Grid &, const pism_gpu_ssa_config &);

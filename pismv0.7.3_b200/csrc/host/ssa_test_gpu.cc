@@ -3,6 +3,7 @@
 // (src/base/stressbalance/ssa/tests/, SSATestCase.cc) on top of SSAFD_GPU.
 //
 //   ssa_test_gpu -test I|J|V [-Mx N] [-My N] [-ssa_rtol R] [-ssafd_ksp_rtol R] [-pc mg|bjacobi]
+//                [-learned params.f32]   (start from the learned guess; raw FP32 parameters)
 //
 // It prints the error table of SSATestCase::report (SSATestCase.cc:231-244) in the same
 // format, so its output can be compared with test/regression/ssa/*.sh line by line.
@@ -200,7 +201,7 @@ void report(const Field2V &vel, const Field2V &exact) {
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string test = "I", pc = "mg";
+  std::string test = "I", pc = "mg", learned;
   int Mx = -1, My = -1;
   double ssa_rtol = -1, ksp_rtol = -1;
   for (int a = 1; a + 1 < argc; a += 2) {
@@ -211,6 +212,7 @@ int main(int argc, char **argv) {
     else if (k == "-ssa_rtol") ssa_rtol = atof(argv[a + 1]);
     else if (k == "-ssafd_ksp_rtol") ksp_rtol = atof(argv[a + 1]);
     else if (k == "-pc") pc = argv[a + 1];
+    else if (k == "-learned") learned = argv[a + 1];
     else {
       fprintf(stderr, "unknown option %s\n", k.c_str());
       return 2;
@@ -228,8 +230,22 @@ int main(int argc, char **argv) {
   if (ssa_rtol > 0) c.cfg.ssafd_relative_convergence = ssa_rtol;
   if (ksp_rtol > 0) c.cfg.ksp_rtol = ksp_rtol;
   c.cfg.pc_type = pc == "bjacobi" ? PISM_PC_BLOCK_JACOBI : PISM_PC_MULTIGRID;
+  pism_gpu_unet *net = nullptr;
+  if (!learned.empty()) {   // the warm-start network, parameters as raw FP32
+    std::vector<float> params((size_t)pism_gpu_unet_param_count());
+    FILE *fp = fopen(learned.c_str(), "rb");
+    const size_t got = fp ? fread(params.data(), sizeof(float), params.size(), fp) : 0;
+    if (fp) fclose(fp);
+    const int hh = (c.grid.Mx + 7) / 8 * 8, ww = (c.grid.My + 7) / 8 * 8;
+    if (got != params.size() || pism_gpu_unet_create(0, 1, hh, ww, &net) != PISM_GPU_SSA_OK ||
+        pism_gpu_unet_set_params(net, params.data(), PISM_MEM_HOST) != PISM_GPU_SSA_OK) {
+      fprintf(stderr, "cannot load the network parameters from %s\n", learned.c_str());
+      return 2;
+    }
+  }
   try {
     SSA *ssa = SSAFD_GPUFactory(c.grid, c.cfg);   // testcase.init(Mx, My, ssafactory)
+    if (net) static_cast<SSAFD_GPU *>(ssa)->set_warm_start(net, 1);
     Vars v;
     v.mask = &c.mask;
     v.thickness = &c.thickness;
@@ -245,7 +261,9 @@ int main(int argc, char **argv) {
     delete ssa;
   } catch (const std::exception &e) {
     fprintf(stderr, "PISM ERROR: %s\n", e.what());
+    pism_gpu_unet_destroy(net);
     return 1;
   }
+  pism_gpu_unet_destroy(net);
   return 0;
 }

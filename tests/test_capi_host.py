@@ -156,6 +156,17 @@ def test_host_driver_is_built(lib):
     assert r.returncode == 2 and "unknown test" in r.stderr
 
 
+def test_host_driver_rejects_short_parameter_files(lib, tmp_path):
+    """-learned reads pism_gpu_unet_param_count() floats; a short or missing file is an
+    error before any device work."""
+    exe = os.path.join(REPO, "pismv0.7.3_b200", "lib", "ssa_test_gpu")
+    short = tmp_path / "short.f32"
+    np.zeros(100, np.float32).tofile(short)
+    for path in (str(short), str(tmp_path / "missing.f32")):
+        r = subprocess.run([exe, "-test", "I", "-My", "61", "-learned", path], capture_output=True, text=True)
+        assert r.returncode == 2 and "cannot load the network parameters" in r.stderr
+
+
 def test_grid_coordinates_match_icegrid():
     """GridDesc follows IceGrid::compute_horizontal_coordinates (IceGrid.cc:550-610)."""
     g = GridDesc(5, 7, 60e3, 120e3, periodicity=2)

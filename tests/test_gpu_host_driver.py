@@ -5,6 +5,8 @@ output recorded in test/regression/ssa/ssa_testi_fd.sh and ssa_test_cfbc.sh."""
 import os
 import subprocess
 
+import numpy as np
+
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -44,3 +46,13 @@ def test_driver_test_v(goldens, k):
     case = goldens["test_v_cfbc"]["cases"][k]
     got = run("-test", "V", "-Mx", str(case["Mx"]), "-My", "3", "-ssafd_ksp_rtol", "1e-13")
     assert got == table_line(case)
+
+
+def test_driver_learned_warm_start(tmp_path):
+    """SSAFD_GPU::set_warm_start: starting test I from the learned guess ends at the same
+    answer once the Picard tolerance is tight (the table agrees to its printed digits)."""
+    params = np.load(os.path.join(REPO, "pismv0.7.3_b200", "weights", "unet_ssa_10km.npz"))["params"]
+    f32 = tmp_path / "unet.f32"
+    params.astype(np.float32).tofile(f32)
+    args = ("-test", "I", "-My", "61", "-ssa_rtol", "1e-9", "-ssafd_ksp_rtol", "1e-12")
+    assert run(*args, "-learned", str(f32)) == run(*args)
