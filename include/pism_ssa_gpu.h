@@ -57,8 +57,13 @@ enum { PISM_NOT_PERIODIC = 0, PISM_X_PERIODIC = 1, PISM_Y_PERIODIC = 2, PISM_XY_
 /* Krylov method (replaces PETSc KSPSolve, SSAFD.cc:1018) */
 enum { PISM_KSP_BICGSTAB = 0, PISM_KSP_GMRES = 1 };
 
-/* preconditioner (replaces PCBJACOBI/ILU(0) and PCASM/LU, SSAFD.cc:136-219) */
-enum { PISM_PC_BLOCK_JACOBI = 0, PISM_PC_MULTIGRID = 1 };
+/* preconditioner (replaces PCBJACOBI/ILU(0) and PCASM/LU, SSAFD.cc:136-219):
+ *   BLOCK_JACOBI  the inverse 2 x 2 diagonal block of each cell
+ *   MULTIGRID     an FP32 aggregation-multigrid V(1,1) cycle
+ *   LINE          line block Jacobi: the 2 x 2-block tridiagonal couplings of each grid line
+ *                 of constant i (j - 1, j, j + 1; none across the line's ends) solved exactly
+ * A KSP failure retries with MULTIGRID (BLOCK_JACOBI after a MULTIGRID failure). */
+enum { PISM_PC_BLOCK_JACOBI = 0, PISM_PC_MULTIGRID = 1, PISM_PC_LINE = 2 };
 
 /* arithmetic of the inner Krylov iterations */
 enum { PISM_PRECISION_FP64 = 0, PISM_PRECISION_MIXED = 1 };
@@ -251,6 +256,10 @@ int pism_gpu_ssa_assemble_rhs(pism_gpu_ssa *h);
 int pism_gpu_ssa_compute_hardness(pism_gpu_ssa *h);
 int pism_gpu_ssa_compute_nuH(pism_gpu_ssa *h, double reg);
 int pism_gpu_ssa_apply(pism_gpu_ssa *h, const double *x_dev, double *y_dev);
+
+/* z = M^-1 r with the active preconditioner, set up at the current nu*H / beta (PETSc's
+ * PCSetUp + PCApply inside KSPSolve, SSAFD.cc:1018).  Device pointers, 2N each, not the same. */
+int pism_gpu_ssa_apply_preconditioner(pism_gpu_ssa *h, const double *r_dev, double *z_dev);
 
 /* One linear solve A x = b at the current nu*H / beta with the configured
  * Krylov method (the body of KSPSolve, SSAFD.cc:1018).  x (device, 2N) holds the

@@ -828,6 +828,55 @@ def apply_stencil(grid: Grid, cfg: Config, inp: Inputs, nuH, beta, x: np.ndarray
     return y
 
 
+def line_block_part(grid: Grid, A):
+    """The line block-Jacobi preconditioner's matrix M: the entries of A (unknown index
+    2 * (i * My + j) + c) that couple a cell to itself and to its neighbours j - 1 and
+    j + 1 on the same grid line of constant i; the couplings across the line's two ends
+    (the periodic wrap) and between lines are dropped.  No reference counterpart: it
+    stands in for the ILU(0) of PETSc's default block Jacobi (SSAFD.cc:136-161)."""
+    A = A.tocoo()
+    My = grid.My
+    rc, cc = A.row // 2, A.col // 2
+    keep = (rc // My == cc // My) & (np.abs(rc % My - cc % My) <= 1)
+    return sp.csr_matrix((A.data[keep], (A.row[keep], A.col[keep])), shape=A.shape)
+
+
+def line_block_solve(grid: Grid, A, r: np.ndarray) -> np.ndarray:
+    """z = M^-1 r for M = line_block_part(grid, A), by a sparse direct solve."""
+    M = line_block_part(grid, A).tocsc()
+    return spla.spsolve(M, r.ravel()).reshape(r.shape)
+
+
+def line_block_lu_solve(grid: Grid, A, r: np.ndarray) -> np.ndarray:
+    """The same z by the per-line block LU recurrences (pure Python, small grids):
+    P_j = (D_j - L_j G_{j-1})^-1, F_j = -P_j L_j, G_j = P_j U_j;
+    y_j = P_j r_j + F_j y_{j-1};  z_j = y_j - G_j z_{j+1}."""
+    Mx, My = grid.Mx, grid.My
+    A = A.tocsr()
+
+    def block(k, kk):
+        return A[2 * k:2 * k + 2, 2 * kk:2 * kk + 2].toarray()
+
+    z = np.zeros((Mx, My, 2))
+    for i in range(Mx):
+        G, y = [], []
+        Gp, yp = np.zeros((2, 2)), np.zeros(2)
+        for j in range(My):
+            k = i * My + j
+            Lb = block(k, k - 1) if j > 0 else np.zeros((2, 2))
+            U = block(k, k + 1) if j < My - 1 else np.zeros((2, 2))
+            Pj = np.linalg.inv(block(k, k) - Lb @ Gp)
+            Gp = Pj @ U
+            yp = Pj @ r[i, j] - Pj @ Lb @ yp
+            G.append(Gp)
+            y.append(yp)
+        x = np.zeros(2)
+        for j in range(My - 1, -1, -1):
+            x = y[j] - G[j] @ x
+            z[i, j] = x
+    return z
+
+
 # ---------------------------------------------------------------------------
 # Picard loop and recovery strategies
 # ---------------------------------------------------------------------------

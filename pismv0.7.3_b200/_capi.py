@@ -25,7 +25,8 @@ EXPORTS = [
     "pism_gpu_ssa_set_stream", "pism_gpu_ssa_set_config", "pism_gpu_ssa_set_inputs",
     "pism_gpu_ssa_set_initial_guess", "pism_gpu_ssa_solve", "pism_gpu_ssa_get_field",
     "pism_gpu_ssa_assemble_rhs", "pism_gpu_ssa_compute_hardness", "pism_gpu_ssa_compute_nuH",
-    "pism_gpu_ssa_apply", "pism_gpu_ssa_linear_solve", "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch",
+    "pism_gpu_ssa_apply", "pism_gpu_ssa_apply_preconditioner", "pism_gpu_ssa_linear_solve",
+    "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch",
 ]
 # every symbol include/pism_unet_gpu.h declares
 UNET_EXPORTS = [
@@ -61,6 +62,7 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_compute_hardness": (I, [V]),
         "pism_gpu_ssa_compute_nuH": (I, [V, D]),
         "pism_gpu_ssa_apply": (I, [V, V, V]),
+        "pism_gpu_ssa_apply_preconditioner": (I, [V, V, V]),
         "pism_gpu_ssa_linear_solve": (I, [V, V, P(I), P(D)]),
         "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
         "pism_gpu_ssa_solve_batch": (I, [V, V, I, I, P(CMember), P(CStats)]),

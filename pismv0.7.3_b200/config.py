@@ -21,7 +21,7 @@ XY_PERIODIC = 3
 
 FLOW_LAWS = {"isothermal_glen": 0, "pb": 1, "gpbld": 2, "arr": 3, "arrwarm": 4, "hooke": 5}
 KSP_TYPES = {"bicgstab": 0, "gmres": 1}
-PC_TYPES = {"bjacobi": 0, "mg": 1}
+PC_TYPES = {"bjacobi": 0, "mg": 1, "line": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
 

@@ -2,7 +2,7 @@
 // reference's ssa_testi / ssa_testj / ssa_test_cfbc executables
 // (src/base/stressbalance/ssa/tests/, SSATestCase.cc) on top of SSAFD_GPU.
 //
-//   ssa_test_gpu -test I|J|V [-Mx N] [-My N] [-ssa_rtol R] [-ssafd_ksp_rtol R] [-pc mg|bjacobi]
+//   ssa_test_gpu -test I|J|V [-Mx N] [-My N] [-ssa_rtol R] [-ssafd_ksp_rtol R] [-pc mg|bjacobi|line]
 //                [-learned params.f32]   (start from the learned guess; raw FP32 parameters)
 //
 // It prints the error table of SSATestCase::report (SSATestCase.cc:231-244) in the same
@@ -229,7 +229,7 @@ int main(int argc, char **argv) {
   }
   if (ssa_rtol > 0) c.cfg.ssafd_relative_convergence = ssa_rtol;
   if (ksp_rtol > 0) c.cfg.ksp_rtol = ksp_rtol;
-  c.cfg.pc_type = pc == "bjacobi" ? PISM_PC_BLOCK_JACOBI : PISM_PC_MULTIGRID;
+  c.cfg.pc_type = pc == "bjacobi" ? PISM_PC_BLOCK_JACOBI : pc == "line" ? PISM_PC_LINE : PISM_PC_MULTIGRID;
   pism_gpu_unet *net = nullptr;
   if (!learned.empty()) {   // the warm-start network, parameters as raw FP32
     std::vector<float> params((size_t)pism_gpu_unet_param_count());

@@ -40,13 +40,14 @@ struct pism_gpu_ssa {
   Krylov K{};
   Krylov32 K32{};
   Gmres G{};   // allocated by the first GMRES solve
+  LinePC line{};   // allocated by the first set-up of the line preconditioner
   // captured Krylov iterations (GRAPH_ITERS per graph), one per kind of iteration
   struct IterGraph {
     cudaGraphExec_t exec = nullptr;
     const void *x = nullptr;   // the solution vector the iterations update
     long long kernels = 0;
     bool failed = false;
-  } graphs[3];
+  } graphs[4];
   // graph-resident Krylov loops (a conditional WHILE node around one iteration)
   struct LoopGraph {
     cudaGraphExec_t exec = nullptr;
@@ -54,7 +55,7 @@ struct pism_gpu_ssa {
     long long per_iteration = 0;   // kernels of one iteration
     int body_iters = 1;            // iterations per pass of the loop body
     bool failed = false;
-  } loops[3];
+  } loops[4];
   double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
   double *res_host = nullptr;
   MGHierarchy mg{};
@@ -138,13 +139,17 @@ Fields fields_of(pism_gpu_ssa *h) {
   return f;
 }
 
-// the multigrid hierarchy when it is the active preconditioner; a KSP failure switches
-// between multigrid and block Jacobi (the reference switches BJacobi -> ASM, SSAFD.cc:929-958)
-const MGHierarchy *active_mg(pism_gpu_ssa *h) {
-  bool want = h->cfg.pc_type == PISM_PC_MULTIGRID;
-  if (h->use_fallback) want = !want;
-  return (want && h->mg.nlev > 0) ? &h->mg : nullptr;
+// The preconditioner in use.  A KSP failure switches multigrid to block Jacobi and block
+// Jacobi or the line solve to multigrid (the reference switches BJacobi -> ASM,
+// SSAFD.cc:929-958); grids too small for a coarse level use block Jacobi.
+int active_pc(pism_gpu_ssa *h) {
+  int pc = h->cfg.pc_type;
+  if (h->use_fallback) pc = pc == PISM_PC_MULTIGRID ? PISM_PC_BLOCK_JACOBI : PISM_PC_MULTIGRID;
+  if (pc == PISM_PC_MULTIGRID && h->mg.nlev == 0) pc = PISM_PC_BLOCK_JACOBI;
+  return pc;
 }
+const MGHierarchy *active_mg(pism_gpu_ssa *h) { return active_pc(h) == PISM_PC_MULTIGRID ? &h->mg : nullptr; }
+const LinePC *active_line(pism_gpu_ssa *h) { return active_pc(h) == PISM_PC_LINE ? &h->line : nullptr; }
 
 // preconditioner set-up after nu*H / beta changed (replaces PCSetUp)
 int pc_setup(pism_gpu_ssa *h) {
@@ -155,6 +160,14 @@ int pc_setup(pism_gpu_ssa *h) {
   h->mg.omega = (float)h->cfg.mg_omega;
   h->mg.correction = (float)h->cfg.mg_correction;
   if (active_mg(h)) mg_setup(h->L, h->g, f, h->K.dinv, h->mg);
+  if (active_line(h)) {
+    if (!h->line.P) {
+      RET(dalloc(h, &h->line.P, h->N));
+      RET(dalloc(h, &h->line.F, h->N));
+      RET(dalloc(h, &h->line.G, h->N));
+    }
+    line_setup(h->L, h->g, f, h->K.dinv, h->line);
+  }
   CK(h, cudaGetLastError());
   return PISM_GPU_SSA_OK;
 }
@@ -173,7 +186,7 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "gmres_restart must be in [1, %d]", GM_MAXM);
   if (c->ksp_type == PISM_KSP_GMRES && c->precision == PISM_PRECISION_MIXED)
     return fail(h, PISM_GPU_SSA_EINVAL, "the mixed-precision inner solve is BiCGStab; use ksp_type GMRES with fp64");
-  if (c->pc_type != PISM_PC_BLOCK_JACOBI && c->pc_type != PISM_PC_MULTIGRID)
+  if (c->pc_type != PISM_PC_BLOCK_JACOBI && c->pc_type != PISM_PC_MULTIGRID && c->pc_type != PISM_PC_LINE)
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
   if (c->ksp_rtol_adaptive && !(c->ksp_rtol_max >= c->ksp_rtol && c->ksp_rtol_max < 1.0 && c->ksp_rtol_factor > 0.0))
     return fail(h, PISM_GPU_SSA_EINVAL, "adaptive KSP tolerance needs ksp_rtol <= ksp_rtol_max < 1, ksp_rtol_factor > 0");
@@ -190,7 +203,7 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
 // graph and replayed (fewer launches, shorter gaps between dependent kernels); a stream
 // that cannot be captured (the legacy default stream) keeps the direct launches.
 constexpr int GRAPH_ITERS = 4;
-enum { GRAPH_BICG_MG = 0, GRAPH_BICG_JACOBI = 1, GRAPH_MIXED = 2 };
+enum { GRAPH_BICG_MG = 0, GRAPH_BICG_JACOBI = 1, GRAPH_MIXED = 2, GRAPH_BICG_LINE = 3 };
 
 template <class ONE>
 int run_iterations(pism_gpu_ssa *h, int kind, const void *x, int count, const ONE &one) {
@@ -346,9 +359,11 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *st
   CK(h, cudaMemcpyAsync(h->K.st, h->st_host, sizeof(KState), cudaMemcpyHostToDevice, h->stream));
   launch_bicg_init(h->L, g, f, h->K, h->rhs, x);
   const MGHierarchy *mg = active_mg(h);
+  const LinePC *line = active_line(h);
+  const int kind = mg ? GRAPH_BICG_MG : line ? GRAPH_BICG_LINE : GRAPH_BICG_JACOBI;
   // long FP64 solves: four iterations per pass of the loop body
-  RET(run_until_done(h, mg ? GRAPH_BICG_MG : GRAPH_BICG_JACOBI, x, h->K.st, std::max(8, (int)(0.8 * h->last_ksp_its)),
-                     4, [&] { launch_bicg_iteration(h->L, g, f, h->K, x, mg); }));
+  RET(run_until_done(h, kind, x, h->K.st, std::max(8, (int)(0.8 * h->last_ksp_its)), 4,
+                     [&] { launch_bicg_iteration(h->L, g, f, h->K, x, mg, line); }));
   h->last_ksp_its = h->st_host->iter;
   *its_out = h->st_host->iter;
   *status_out = h->st_host->status;
@@ -384,8 +399,9 @@ int linear_solve_gmres(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, i
   int chunk = std::max(8, (int)(0.8 * h->last_ksp_its));
   while (true) {
     const MGHierarchy *mg = active_mg(h);
+    const LinePC *line = active_line(h);
     for (int q = 0; q < chunk; ++q) {
-      launch_gmres_step(h->L, g, f, h->G, h->K.dinv, mg, j);
+      launch_gmres_step(h->L, g, f, h->G, h->K.dinv, mg, line, j);
       if (j == m - 1) {   // end of a cycle: x += Z y, then a restart unless converged
         launch_gmres_update(h->L, g, h->G, x);
         launch_gmres_residual(h->L, g, f, h->G, h->rhs, x, 0);
@@ -722,7 +738,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev,
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.s, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
-                 h->G.partials, h->G.gs, h->G.st};
+                 h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -920,6 +936,17 @@ int pism_gpu_ssa_apply(pism_gpu_ssa *h, const double *x_dev, double *y_dev) {
   if (!h || !x_dev || !y_dev) return PISM_GPU_SSA_EINVAL;
   DeviceGuard dg(h->device);
   launch_apply(h->L, h->g, fields_of(h), (const double2 *)x_dev, (double2 *)y_dev);
+  CK(h, cudaGetLastError());
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_apply_preconditioner(pism_gpu_ssa *h, const double *r_dev, double *z_dev) {
+  if (!h || !r_dev || !z_dev) return PISM_GPU_SSA_EINVAL;
+  if (r_dev == z_dev) return fail(h, PISM_GPU_SSA_EINVAL, "apply_preconditioner: r and z must be different vectors");
+  DeviceGuard dg(h->device);
+  RET(pc_setup(h));
+  launch_pc_apply(h->L, h->g, fields_of(h), h->K.dinv, active_mg(h), active_line(h), (const double2 *)r_dev,
+                  (double2 *)z_dev);
   CK(h, cudaGetLastError());
   return PISM_GPU_SSA_OK;
 }

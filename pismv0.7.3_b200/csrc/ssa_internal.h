@@ -110,6 +110,13 @@ int mg_plan(int Mx, int My, MGHierarchy &H);
 int mg_allocate(MGHierarchy &H, int fine_cells);
 void mg_free(MGHierarchy &H);
 
+// Line block-Jacobi preconditioner.  Per cell, after line_setup: P = the inverse pivot
+// block, F = -P L (forward multiplier), G = P U (backward multiplier) of the block LU
+// factorisation of each grid line's 2 x 2-block tridiagonal part.
+struct LinePC {
+  double4 *P = nullptr, *F = nullptr, *G = nullptr;
+};
+
 void launch_convert_masks(const Launch &L, int N, const double *mask, const double *bc_mask, int8_t *mask_i,
                           uint8_t *bc_i);
 void launch_prepare(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int periodicity,
@@ -123,18 +130,25 @@ void launch_diag_setup(const Launch &L, const GridDev &g, const Fields &f, doubl
 void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, const double2 *b,
                       const double2 *x);
 void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x,
-                           const MGHierarchy *mg);
+                           const MGHierarchy *mg, const LinePC *line);
 // FGMRES: r0 = b - A x into V0 (init) / after a restart; one Arnoldi step j; the end of a cycle
 void launch_gmres_residual(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double2 *b,
                            const double2 *x, int init);
 void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
-                       const MGHierarchy *mg, int j);
+                       const MGHierarchy *mg, const LinePC *line, int j);
 void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, double2 *x);
 void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b,
                double2 *z, const KState *st);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
                const KState *st);
+// ---- line block-Jacobi preconditioner (ssa_line.cu) ----
+void line_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const LinePC &lp);
+void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const double2 *b, double2 *z, const KState *st);
+// z = M^-1 r with block Jacobi (dinv), the multigrid cycle (mg) or the line solve (line)
+void launch_pc_apply(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const MGHierarchy *mg,
+                     const LinePC *line, const double2 *r, double2 *z);
+
 // the loop condition of a graph-resident Krylov loop: continue while st->done is 0
 void launch_loop_condition(const Launch &L, cudaGraphConditionalHandle cond, const KState *st);
 

@@ -822,7 +822,7 @@ void launch_bicg_init(const Launch &L, const GridDev &g, const Fields &f, const 
 }
 
 void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, const Krylov &K, double2 *x,
-                           const MGHierarchy *mg) {
+                           const MGHierarchy *mg, const LinePC *line) {
   L.tick(5);
   TileMap tm = make_tiles(g);
   const int N = g.Mx * g.My;
@@ -831,6 +831,9 @@ void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, c
   if (mg) {
     k_bicg_p<false><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
     mg_vcycle(L, g, f, *mg, K.p, K.phat, K.st);
+  } else if (line) {
+    k_bicg_p<false><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
+    line_apply(L, g, *line, K.p, K.phat, K.st);
   } else {
     k_bicg_p<true><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.p, K.phat, K.st);
   }
@@ -839,6 +842,9 @@ void launch_bicg_iteration(const Launch &L, const GridDev &g, const Fields &f, c
   if (mg) {
     k_bicg_s<false><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
     mg_vcycle(L, g, f, *mg, K.s, K.shat, K.st);
+  } else if (line) {
+    k_bicg_s<false><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
+    line_apply(L, g, *line, K.s, K.shat, K.st);
   } else {
     k_bicg_s<true><<<bv, NT, 0, L.stream>>>(N, K.r, K.v, K.dinv, K.s, K.shat, K.st);
   }
@@ -945,7 +951,7 @@ __global__ void __launch_bounds__(NT) k_gm_scale0(int N, double2 *__restrict__ v
 __global__ void __launch_bounds__(NT) k_gm_jacobi(int N, const double2 *__restrict__ v,
                                                   const double4 *__restrict__ dinv, double2 *__restrict__ z,
                                                   const KState *st) {
-  if (st->done) return;
+  if (st && st->done) return;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) z[k] = dmul(dinv[k], v[k]);
 }
 
@@ -1110,20 +1116,35 @@ void launch_gmres_residual(const Launch &L, const GridDev &g, const Fields &f, c
 }
 
 void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
-                       const MGHierarchy *mg, int j) {
-  L.tick(mg ? 3 : 4);
+                       const MGHierarchy *mg, const LinePC *line, int j) {
+  L.tick(mg || line ? 3 : 4);
   TileMap tm = make_tiles(g);
   const int N = g.Mx * g.My;
   const double2 *vj = G.V + (size_t)j * N;
   double2 *zj = G.Z + (size_t)j * N, *w = G.V + (size_t)(j + 1) * N;
   if (mg)
     mg_vcycle(L, g, f, *mg, vj, zj, G.st);
+  else if (line)
+    line_apply(L, g, *line, vj, zj, G.st);
   else
     k_gm_jacobi<<<grid_for(L, N), NT, 0, L.stream>>>(N, vj, dinv, zj, G.st);
   k_gm_apply_dots<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta,
                                                                     zj, G.V, w, j, G.partials, L.ticket, G.st, G.gs);
   k_gm_orth<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.V, w, j, G.m, G.partials, L.ticket, G.st, G.gs);
   k_gm_scale_next<<<grid_for(L, N), NT, 0, L.stream>>>(N, w, G.st, G.gs);
+}
+
+void launch_pc_apply(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const MGHierarchy *mg,
+                     const LinePC *line, const double2 *r, double2 *z) {
+  const int N = g.Mx * g.My;
+  if (mg) {
+    mg_vcycle(L, g, f, *mg, r, z, nullptr);
+  } else if (line) {
+    line_apply(L, g, *line, r, z, nullptr);
+  } else {
+    L.tick();
+    k_gm_jacobi<<<grid_for(L, N), NT, 0, L.stream>>>(N, r, dinv, z, nullptr);
+  }
 }
 
 void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, double2 *x) {

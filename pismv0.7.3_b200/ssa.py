@@ -276,6 +276,12 @@ class SSAFD:
         self._check(self.lib.pism_gpu_ssa_apply(self._h, C.c_void_p(x_dev.data_ptr()),
                                                 C.c_void_p(y_dev.data_ptr())), "apply")
 
+    def apply_preconditioner(self, r_dev, z_dev):
+        """z = M^-1 r with the active preconditioner at the current nu*H / beta (PCApply);
+        device tensors [Mx, My, 2] float64, not the same tensor."""
+        self._check(self.lib.pism_gpu_ssa_apply_preconditioner(self._h, C.c_void_p(r_dev.data_ptr()),
+                                                               C.c_void_p(z_dev.data_ptr())), "PCApply")
+
     def linear_solve(self, x_dev):
         its = C.c_int(0)
         res = C.c_double(0)

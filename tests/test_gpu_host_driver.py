@@ -33,7 +33,7 @@ def run(*args):
     return lines[2]
 
 
-@pytest.mark.parametrize("pc", ["mg", "bjacobi"])
+@pytest.mark.parametrize("pc", ["mg", "bjacobi", "line"])
 @pytest.mark.parametrize("k", [0, 1])
 def test_driver_test_i(goldens, k, pc):
     case = goldens["test_i_fd"]["cases"][k]

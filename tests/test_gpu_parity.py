@@ -112,6 +112,46 @@ def test_stage_parity(name):
     s.close()
 
 
+@pytest.mark.parametrize("pc,shape,periodicity", [("bjacobi", (23, 19), 0), ("line", (23, 19), 0),
+                                                  ("line", (23, 19), Y_PERIODIC), ("line", (5, 601), 0),
+                                                  ("line", (7, 512), X_PERIODIC)])
+def test_preconditioner_apply_matches_oracle(pc, shape, periodicity):
+    """z = M^-1 r (PCApply) against the oracle: block Jacobi inverts each cell's 2 x 2
+    diagonal block; the line preconditioner solves the 2 x 2-block tridiagonal part of every
+    grid line of constant i (no wrap across its ends), in chunks of 256 cells (601 = two
+    full chunks and a partial one, 512 = exactly two).  Every mask case, Dirichlet rows
+    included."""
+    g, c, f = random_case(11 + shape[1], Mx=shape[0], My=shape[1], periodicity=periodicity)
+    c.pc_type = pc
+    G, Cc, I = O.from_case(g, c, f)
+    s = make_solver(g, c, f)
+    s.assemble_rhs()
+    s.compute_hardav_staggered()
+    rng = np.random.default_rng(2)
+    s.set_initial_guess(rng.normal(0, 3e-6, (g.Mx, g.My, 2)))
+    s.compute_nuH_staggered(1e13)
+    A = O.assemble_matrix(G, Cc, I, s.nuH(), s.beta(), check_diagonal=False)
+    if pc == "line":
+        M = O.line_block_part(G, A)
+    else:
+        A = A.tocoo()
+        keep = A.row // 2 == A.col // 2
+        M = O.sp.csr_matrix((A.data[keep], (A.row[keep], A.col[keep])), shape=A.shape)
+    r = rng.standard_normal((g.Mx, g.My, 2))
+    rd = torch.tensor(r, device="cuda")
+    zd = torch.empty_like(rd)
+    s.apply_preconditioner(rd, zd)
+    torch.cuda.synchronize()
+    z = zd.cpu().numpy()
+    # backward error of the device solve, row by row: |r - M z| <= 1e-12 sum_m |M_m z_m|
+    scale = (abs(M) @ np.abs(z).ravel()).reshape(r.shape)
+    back = np.abs(r - (M @ z.ravel()).reshape(r.shape))
+    assert np.all(back <= 1e-12 * scale + 1e-300), np.max(back / (scale + 1e-300))
+    z_ref = O.spla.spsolve(M.tocsc(), r.ravel()).reshape(r.shape)
+    assert rel(z, z_ref) < 1e-8
+    s.close()
+
+
 @pytest.mark.parametrize("law", ["gpbld", "pb", "arr", "arrwarm", "hooke"])
 def test_hardness_from_enthalpy(law):
     g, c, f = random_case(7, flow_law=law)
@@ -124,7 +164,8 @@ def test_hardness_from_enthalpy(law):
 
 @pytest.mark.parametrize("pc,precision,ksp", [("bjacobi", "fp64", "bicgstab"), ("mg", "fp64", "bicgstab"),
                                                ("mg", "mixed", "bicgstab"), ("bjacobi", "fp64", "gmres"),
-                                               ("mg", "fp64", "gmres")])
+                                               ("mg", "fp64", "gmres"), ("line", "fp64", "bicgstab"),
+                                               ("line", "fp64", "gmres")])
 def test_linear_solve_matches_direct(pc, precision, ksp):
     """One KSPSolve at the first Picard step (zero velocity: plastic drag 1e14, the worst
     conditioning of the solve).  Both answers must have tiny true residuals and agree.
@@ -189,7 +230,8 @@ def _solve_case(g, c, f):
 
 
 @pytest.mark.parametrize("pc,precision,ksp", [("bjacobi", "fp64", "bicgstab"), ("mg", "fp64", "bicgstab"),
-                                               ("mg", "mixed", "bicgstab"), ("mg", "fp64", "gmres")])
+                                               ("mg", "mixed", "bicgstab"), ("mg", "fp64", "gmres"),
+                                               ("line", "fp64", "bicgstab")])
 @pytest.mark.parametrize("My", [61, 121])
 def test_verification_i(goldens, My, pc, precision, ksp):
     g, c, f = V.build_test_i(My=My)
@@ -208,7 +250,7 @@ def test_verification_i(goldens, My, pc, precision, ksp):
     assert rel(vel, ref) < 1e-8
 
 
-@pytest.mark.parametrize("pc", ["bjacobi", "mg"])
+@pytest.mark.parametrize("pc", ["bjacobi", "mg", "line"])
 @pytest.mark.parametrize("Mx", [201, 401])
 def test_verification_v_cfbc(goldens, Mx, pc):
     g, c, f = V.build_test_v(Mx)
@@ -224,7 +266,7 @@ def test_verification_v_cfbc(goldens, Mx, pc):
 
 
 @pytest.mark.parametrize("pc,ksp", [("bjacobi", "bicgstab"), ("mg", "bicgstab"), ("bjacobi", "gmres"),
-                                    ("mg", "gmres")])
+                                    ("mg", "gmres"), ("line", "bicgstab")])
 @pytest.mark.parametrize("M", [61, 121])
 def test_verification_j(M, pc, ksp):
     """Test J with a tight KSP equals the oracle's direct solve (the golden itself
@@ -254,7 +296,8 @@ def test_zero_diagonal_is_reported():
 
 
 @pytest.mark.parametrize("pc,precision,ksp", [("bjacobi", "fp64", "bicgstab"), ("mg", "fp64", "bicgstab"),
-                                               ("mg", "mixed", "bicgstab"), ("mg", "fp64", "gmres")])
+                                               ("mg", "mixed", "bicgstab"), ("mg", "fp64", "gmres"),
+                                               ("line", "fp64", "bicgstab")])
 @pytest.mark.parametrize("M", [45, 64])
 def test_synthetic_solve_matches_oracle(M, pc, precision, ksp):
     """A whole SSAFD::solve of the synthetic sheet against the oracle, odd and even grid sizes

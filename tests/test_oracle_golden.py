@@ -121,3 +121,25 @@ def test_apply_stencil_equals_assembled_matrix():
     x = rng.standard_normal((G.Mx, G.My, 2))
     y = O.apply_stencil(G, Cc, I, nuH, beta, x)
     np.testing.assert_allclose(y.ravel(), A @ x.ravel(), rtol=1e-12, atol=1e-9 * np.abs(y).max())
+
+
+def test_line_block_recurrences_equal_the_direct_solve():
+    """The line preconditioner's block LU recurrences (the device algorithm) solve exactly
+    the line-tridiagonal part of A, periodic wrap across the line ends dropped."""
+    rng = np.random.default_rng(1)
+    g, c, f = V.build_test_v(13, 7)
+    G, Cc, I = O.from_case(g, c, f)
+    nuH = rng.uniform(1e14, 1e17, (G.Mx, G.My, 2))
+    beta = rng.uniform(0, 1e10, (G.Mx, G.My))
+    A = O.assemble_matrix(G, Cc, I, nuH, beta)
+    M = O.line_block_part(G, A)
+    assert M.nnz < A.nnz
+    r = rng.standard_normal((G.Mx, G.My, 2))
+    z = O.line_block_solve(G, A, r)
+    np.testing.assert_allclose((M @ z.ravel()).reshape(r.shape), r, rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(O.line_block_lu_solve(G, A, r), z, rtol=1e-9, atol=1e-12 * np.abs(z).max())
+    # no coupling between lines: a right-hand side on one line stays on it
+    r1 = np.zeros_like(r)
+    r1[3] = r[3]
+    z1 = O.line_block_solve(G, A, r1)
+    assert np.all(z1[:3] == 0) and np.all(z1[4:] == 0)
