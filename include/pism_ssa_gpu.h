@@ -131,7 +131,10 @@ typedef struct pism_gpu_ssa_config {
   double ksp_rtol_factor;
   /* launch mode of the Krylov iterations: 2 a graph-resident loop per solve (a CUDA graph
      with a conditional WHILE node), 1 captured graphs of a few iterations, 0 direct launches
-     (kernel profilers that cannot look into conditional graphs need 0 or 1) */
+     (kernel profilers that cannot look into conditional graphs need 0 or 1).
+     3 (BiCGStab only, otherwise as 2): the whole Picard loop of a solve is one CUDA graph
+     with nested conditional nodes, its decisions taken on the device, one launch and one
+     read-back per solve; not yet run on a GPU, off by default */
   int    graphs;
   int    verbosity;                                /* 0 silent .. 3 per-iteration    */
 } pism_gpu_ssa_config;

@@ -56,6 +56,18 @@ struct pism_gpu_ssa {
     int body_iters = 1;            // iterations per pass of the loop body
     bool failed = false;
   } loops[4];
+  // the whole Picard loop as one graph (graphs = 3), with the kernels per pass of each of its
+  // loops (for the launch count)
+  struct SolveGraph {
+    cudaGraphExec_t exec = nullptr;
+    double reg = 0.0, underrelax = 0.0;
+    Fields key{};
+    bool mixed = false;
+    long long pre = 0, per_picard = 0, per_refine = 0, per_inner = 0, per_go = 0, per_test = 0;
+    bool failed = false;
+  } sgraph;
+  PState *pstate = nullptr;
+  PState *pstate_host = nullptr;
   double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
   double *res_host = nullptr;
   MGHierarchy mg{};
@@ -190,7 +202,7 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "unknown pc_type %d", c->pc_type);
   if (c->ksp_rtol_adaptive && !(c->ksp_rtol_max >= c->ksp_rtol && c->ksp_rtol_max < 1.0 && c->ksp_rtol_factor > 0.0))
     return fail(h, PISM_GPU_SSA_EINVAL, "adaptive KSP tolerance needs ksp_rtol <= ksp_rtol_max < 1, ksp_rtol_factor > 0");
-  if (c->graphs < 0 || c->graphs > 2) return fail(h, PISM_GPU_SSA_EINVAL, "graphs must be 0, 1 or 2");
+  if (c->graphs < 0 || c->graphs > 3) return fail(h, PISM_GPU_SSA_EINVAL, "graphs must be 0, 1, 2 or 3");
   if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
     return fail(h, PISM_GPU_SSA_EINVAL, "ksp_rtol, ksp_max_it and max_iterations_ssafd must be positive");
   if (!(c->ssa_Glen_exponent > 0.0) || !(c->min_thickness_strength_extension_ssa > 0.0))
@@ -348,6 +360,233 @@ int run_until_done(pism_gpu_ssa *h, int kind, const void *x, KState *st, int chu
   return PISM_GPU_SSA_OK;
 }
 
+// Inside an active capture on h->L.stream: add a conditional node (WHILE or IF) after the
+// capture's current dependencies.  `set(cond)` launches the kernel that gives the node its
+// value, once before the node and, for a WHILE node, again at the end of each pass of the
+// body; `body()` launches the body on h->L.stream (itself capturing into the node's body
+// graph, so bodies nest).  *body_kernels gets the kernels of one pass, nested bodies
+// included.  The capture continues after the node.
+template <class SET, class BODY>
+bool add_conditional(pism_gpu_ssa *h, cudaGraphConditionalNodeType type, const SET &set, const BODY &body,
+                     long long *body_kernels) {
+  const cudaStream_t s = h->L.stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd) != cudaSuccess || cs != cudaStreamCaptureStatusActive)
+    return false;
+  cudaGraphConditionalHandle cond{};
+  if (cudaGraphConditionalHandleCreate(&cond, cg, 0, 0) != cudaSuccess) return false;
+  set(cond);
+  if (cudaGetLastError() != cudaSuccess) return false;
+  if (cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd) != cudaSuccess) return false;
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = cond;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node{};
+  if (cudaGraphAddNode(&node, cg, deps, nd, &p) != cudaSuccess) return false;
+  cudaStream_t bs = nullptr;
+  if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess) return false;
+  bool ok = cudaStreamBeginCaptureToGraph(bs, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    const long long b0 = h->stats.kernel_launches;
+    h->L.stream = bs;
+    ok = body();
+    if (type == cudaGraphCondTypeWhile) set(cond);
+    h->L.stream = s;
+    *body_kernels = h->stats.kernel_launches - b0;
+    ok = cudaGetLastError() == cudaSuccess && ok;
+    ok = cudaStreamEndCapture(bs, nullptr) == cudaSuccess && ok;
+  }
+  cudaStreamDestroy(bs);
+  return ok && cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+}
+
+// ---- the whole Picard loop as one CUDA graph (graphs = 3) ----
+// SSAFD::picard_manager with its linear solves, nu*H updates and stopping test in one graph
+// launch and one read-back: a WHILE node over Picard iterations (its decisions taken on the
+// device by ssa_control.cu), inside it the linear solve — FP64 BiCGStab as a WHILE node of
+// four iterations per pass, or the mixed-precision refinement as a WHILE node over
+// refinement steps around the inner FP32 BiCGStab's WHILE node and an IF node for the
+// correction — and an IF node for the nu*H update and Picard test after a successful solve.
+// Used for BiCGStab without a fallback preconditioner and verbosity <= 2; everything else
+// (and a stream that cannot be captured) takes the host loop.
+bool solve_graph_eligible(const pism_gpu_ssa *h) {
+  return h->cfg.graphs >= 3 && !h->use_fallback && h->cfg.verbosity <= 2 && h->cfg.ksp_type == PISM_KSP_BICGSTAB;
+}
+
+int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *built) {
+  auto &S = h->sgraph;
+  *built = false;
+  if (S.exec) cudaGraphExecDestroy(S.exec);
+  S = {};
+  const pism_gpu_ssa_config &c = h->cfg;
+  const GridDev &g = h->g;
+  const Fields f = fields_of(h);
+  const MGHierarchy *mg = active_mg(h);
+  const LinePC *line = active_line(h);
+  const bool mixed = c.precision == PISM_PRECISION_MIXED && mg;
+  const int N = g.Mx * g.My;
+  if (!h->pstate) RET(dalloc(h, &h->pstate, 1));
+  if (!h->pstate_host) CK(h, cudaMallocHost((void **)&h->pstate_host, sizeof(PState)));
+  if (line && !h->line.P) {
+    RET(dalloc(h, &h->line.P, h->N));
+    RET(dalloc(h, &h->line.F, h->N));
+    RET(dalloc(h, &h->line.G, h->N));
+  }
+  h->mg.omega = (float)c.mg_omega;   // captured by value, as pc_setup sets them
+  h->mg.correction = (float)c.mg_correction;
+  PicardConst pc{c.ksp_rtol, c.ksp_rtol_max, c.ksp_rtol_factor, c.ssafd_relative_convergence,
+                 c.ksp_rtol_adaptive ? 1 : 0, c.max_iterations_ssafd};
+  PState *P = h->pstate;
+  const long long t0 = h->stats.kernel_launches;
+  long long inc_picard = 0, inc_refine = 0, inc_inner = 0, inc_go = 0, inc_test = 0, pre = 0;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    S.failed = true;
+    return PISM_GPU_SSA_OK;
+  }
+  launch_nuH(h->L, g, c, f, reg, 1.0, false, h->norm_dev);
+  launch_picard_start(h->L, P);
+  auto not_done = [&](const int *flag) {
+    return [&h, flag](cudaGraphConditionalHandle cond) { launch_flag_condition(h->L, cond, flag, true); };
+  };
+  const long long before_loop = h->stats.kernel_launches;
+  bool ok = add_conditional(h, cudaGraphCondTypeWhile, not_done(&P->done), [&] {
+    bool inner_ok = true;
+    launch_picard_begin(h->L, P, pc, h->zd_dev);
+    launch_diag_setup(h->L, g, f, h->K.dinv, h->zd_dev);
+    if (mg) mg_setup(h->L, g, f, h->K.dinv, h->mg);
+    if (line) line_setup(h->L, g, f, h->K.dinv, h->line);
+    if (mixed) {
+      launch_residual32(h->L, g, f, h->rhs, h->vel, h->K32.rhs, h->res_dev);
+      inner_ok = add_conditional(h, cudaGraphCondTypeWhile, not_done(&P->refine_done), [&] {
+        launch_mixed_init_dev(h->L, N, h->K32, h->res_dev, &P->rtol, c.mixed_inner_rtol, c.ksp_max_it);
+        bool ok2 = add_conditional(
+            h, cudaGraphCondTypeWhile,
+            [&](cudaGraphConditionalHandle cond) { launch_loop_condition(h->L, cond, h->K32.st); },
+            [&] {
+              launch_mixed_iteration(h->L, g, f, *mg, h->K32);
+              return true;
+            },
+            &inc_inner);
+        launch_refine_end(h->L, P, h->K32.st, 60);
+        ok2 = ok2 && add_conditional(
+                         h, cudaGraphCondTypeIf,
+                         [&](cudaGraphConditionalHandle cond) { launch_flag_condition(h->L, cond, &P->go, false); },
+                         [&] {
+                           launch_axpy32(h->L, N, h->K32.d, h->vel);
+                           launch_residual32(h->L, g, f, h->rhs, h->vel, h->K32.rhs, h->res_dev);
+                           return true;
+                         },
+                         &inc_go);
+        return ok2;
+      }, &inc_refine);
+    } else {
+      launch_ksp_begin(h->L, h->K.st, P, c.ksp_max_it);
+      launch_bicg_init(h->L, g, f, h->K, h->rhs, h->vel);
+      inner_ok = add_conditional(
+          h, cudaGraphCondTypeWhile,
+          [&](cudaGraphConditionalHandle cond) { launch_loop_condition(h->L, cond, h->K.st); },
+          [&] {
+            for (int q = 0; q < 4; ++q) launch_bicg_iteration(h->L, g, f, h->K, h->vel, mg, line);
+            return true;
+          },
+          &inc_inner);
+      launch_ksp_end(h->L, P, h->K.st, 4);
+    }
+    launch_picard_after_solve(h->L, P, h->zd_dev);
+    inner_ok = inner_ok && add_conditional(h, cudaGraphCondTypeIf, not_done(&P->done), [&] {
+      launch_nuH(h->L, g, c, f, reg, underrelax, true, h->norm_dev);
+      launch_picard_test(h->L, P, h->norm_dev, pc);
+      return true;
+    }, &inc_test);
+    return inner_ok;
+  }, &inc_picard);
+  pre = before_loop - t0 + 1;   // + the WHILE node's first condition kernel
+  cudaGraph_t out = nullptr;
+  const bool ended = cudaStreamEndCapture(h->stream, &out) == cudaSuccess;
+  ok = ok && ended && out != nullptr;
+  if (ok) ok = cudaGraphInstantiate(&S.exec, out, 0) == cudaSuccess;
+  if (out) cudaGraphDestroy(out);
+  h->stats.kernel_launches = t0;   // nothing ran during the capture
+  if (!ok) {
+    S.exec = nullptr;
+    S.failed = true;
+    cudaGetLastError();
+    return PISM_GPU_SSA_OK;
+  }
+  S.reg = reg;
+  S.underrelax = underrelax;
+  S.key = f;
+  S.mixed = mixed;
+  S.pre = pre;
+  S.per_inner = inc_inner;
+  S.per_go = inc_go;
+  S.per_test = inc_test;
+  S.per_refine = mixed ? inc_refine - inc_inner - inc_go : 0;
+  S.per_picard = inc_picard - (mixed ? inc_refine : inc_inner) - inc_test;
+  *built = true;
+  return PISM_GPU_SSA_OK;
+}
+
+// The Picard loop through the whole-solve graph when it applies (*used), with the host
+// loop's return codes, messages and statistics.
+int picard_manager_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *used) {
+  *used = false;
+  if (!solve_graph_eligible(h)) return PISM_GPU_SSA_OK;
+  auto &S = h->sgraph;
+  const Fields f = fields_of(h);
+  if (!S.exec || S.reg != reg || S.underrelax != underrelax || memcmp(&S.key, &f, sizeof(Fields)) != 0) {
+    if (S.failed && S.reg == reg && S.underrelax == underrelax) return PISM_GPU_SSA_OK;
+    bool built = false;
+    RET(build_solve_graph(h, reg, underrelax, &built));
+    if (!built) {
+      S.reg = reg;
+      S.underrelax = underrelax;
+      return PISM_GPU_SSA_OK;
+    }
+  }
+  CK(h, cudaGraphLaunch(S.exec, h->stream));
+  CK(h, cudaMemcpyAsync(h->pstate_host, h->pstate, sizeof(PState), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  *used = true;
+  const PState &P = *h->pstate_host;
+  h->stats.kernel_launches += S.pre + P.passes * S.per_picard + P.refine_passes * S.per_refine +
+                              P.inner_passes * S.per_inner + P.go_count * S.per_go + P.k * S.per_test;
+  h->stats.ksp_iterations += P.ksp_total;
+  h->stats.refinement_steps += P.refine_steps;
+  h->stats.final_linear_residual = P.final_res;
+  h->last_ksp_its = P.ksp_its;
+  if (P.k > 0) {
+    h->stats.picard_iterations = P.k;
+    h->stats.nuH_norm = P.norm;
+    h->stats.nuH_norm_change = P.change;
+  }
+  switch (P.status) {
+    case PISM_GPU_SSA_OK:
+      return PISM_GPU_SSA_OK;
+    case PISM_GPU_SSA_EZERODIAG:
+      return fail(h, PISM_GPU_SSA_EZERODIAG,
+                  "SSAFD system: zero diagonal entry at a regular (not Dirichlet B.C.) location: i = %d, j = %d",
+                  P.zd_cell / h->g.My, P.zd_cell % h->g.My);
+    case PISM_GPU_SSA_EKSP:
+      return fail(h, PISM_GPU_SSA_EKSP, "SSAFD KSP (linear solver) failed: reason %d after %d iterations",
+                  P.ksp_status, P.ksp_its);
+    case PISM_GPU_SSA_ENAN:
+      return fail(h, PISM_GPU_SSA_ENAN, "non-finite nu*H norm at Picard iteration %d", P.k - 1);
+    default:
+      return fail(h, PISM_GPU_SSA_EPICARD,
+                  "SSAFD Picard iterations failed: effective viscosity not converged after %d iterations with "
+                  "nuH_regularization=%8.2e.",
+                  h->cfg.max_iterations_ssafd, reg);
+  }
+}
+
 // ---- one linear solve: BiCGStab on the device, host reads the state per chunk ----
 int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
   const GridDev &g = h->g;
@@ -463,6 +702,9 @@ int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, i
 
 // SSAFD::picard_manager, SSAFD.cc:962-1119
 int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
+  bool used = false;
+  const int rc = picard_manager_graph(h, reg, underrelax, &used);
+  if (used || rc != PISM_GPU_SSA_OK) return rc;
   const pism_gpu_ssa_config &c = h->cfg;
   Fields f = fields_of(h);
   launch_nuH(h->L, h->g, c, f, reg, 1.0, false, h->norm_dev);
@@ -751,6 +993,9 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
     if (gr.exec) cudaGraphExecDestroy(gr.exec);
   for (auto &lp : h->loops)
     if (lp.exec) cudaGraphExecDestroy(lp.exec);
+  if (h->sgraph.exec) cudaGraphExecDestroy(h->sgraph.exec);
+  if (h->pstate) cudaFree(h->pstate);
+  if (h->pstate_host) cudaFreeHost(h->pstate_host);
   mg_free(h->mg);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -777,6 +1022,8 @@ int pism_gpu_ssa_set_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *cfg) {
     if (lp.exec) cudaGraphExecDestroy(lp.exec);
     lp = {};
   }
+  if (h->sgraph.exec) cudaGraphExecDestroy(h->sgraph.exec);
+  h->sgraph = {};
   return PISM_GPU_SSA_OK;
 }
 

@@ -149,6 +149,43 @@ void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const doubl
 void launch_pc_apply(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const MGHierarchy *mg,
                      const LinePC *line, const double2 *r, double2 *z);
 
+// ---- device-side control of the Picard loop (ssa_control.cu) ----
+// The state a whole-solve graph keeps on the device: the decisions of the host loop
+// (SSAFD::picard_manager, SSAFD.cc:962-1119, and the refinement loop of the mixed-precision
+// solve) taken by single-thread kernels, and the counts the host reads back once.
+struct PState {
+  double rtol;          // KSP tolerance of the current Picard iteration
+  double last_change;   // relative nu*H change of the previous iteration
+  double norm, change;  // the last Picard test's norms
+  double final_res;     // relative residual of the last linear solve
+  int k;                // Picard tests taken (= Picard iterations)
+  int passes;           // Picard loop passes
+  int done, status;     // status: a PISM_GPU_SSA_* code once done
+  int zd_cell;          // the zero-diagonal cell, when status is EZERODIAG
+  int ksp_its, ksp_status, ksp_total;
+  int refine, refine_done, go, go_count, refine_steps, refine_passes;
+  long long inner_passes;   // passes of the innermost Krylov loop body
+};
+struct PicardConst {
+  double ksp_rtol, ksp_rtol_max, ksp_rtol_factor, picard_rtol;
+  int adaptive, max_iterations;
+};
+void launch_picard_start(const Launch &L, PState *P);
+// a Picard pass begins: zero-diagonal marker reset, the pass's KSP tolerance
+void launch_picard_begin(const Launch &L, PState *P, const PicardConst &c, int *zero_diag_cell);
+// FP64 BiCGStab inside the graph: its state from the pass's tolerance; its outcome
+void launch_ksp_begin(const Launch &L, KState *st, const PState *P, int maxit);
+void launch_ksp_end(const Launch &L, PState *P, const KState *st, int body_iters);
+// the end of one refinement step of the mixed-precision solve (go = apply its correction)
+void launch_refine_end(const Launch &L, PState *P, const KState *st, int max_refine);
+void launch_picard_after_solve(const Launch &L, PState *P, const int *zero_diag_cell);
+void launch_picard_test(const Launch &L, PState *P, const double *norm2, const PicardConst &c);
+// a conditional node's value from a flag: flag != 0 (or == 0 when negate)
+void launch_flag_condition(const Launch &L, cudaGraphConditionalHandle cond, const int *flag, bool negate);
+// launch_mixed_init with the outer tolerance read from the device
+void launch_mixed_init_dev(const Launch &L, int N, const Krylov32 &K, const double *res2, const double *outer_rtol,
+                           double inner_min, int maxit);
+
 // the loop condition of a graph-resident Krylov loop: continue while st->done is 0
 void launch_loop_condition(const Launch &L, cudaGraphConditionalHandle cond, const KState *st);
 

@@ -56,11 +56,16 @@ __device__ __forceinline__ double dotf(const float2 &a, const float2 &b) {
 // start of an inner solve with d0 = 0: r = rhat = rhs, p = v = d = 0.  The outer test
 // ||b - A x|| <= outer_rtol ||b|| and the inner tolerance (what this refinement step still
 // needs, with a margin, never below inner_min) come from the FP64 norms in res2.
+// DEV_RTOL: the outer tolerance is read from outer_rtol_dev (a whole-solve graph, whose
+// tolerance changes from one Picard iteration to the next) instead of outer_rtol.
+template <bool DEV_RTOL>
 __global__ void __launch_bounds__(NT32) k32_init(int N, const float2 *__restrict__ rhs, float2 *__restrict__ r,
                                                  float2 *__restrict__ rhat, float2 *__restrict__ p,
                                                  float2 *__restrict__ v, float2 *__restrict__ d, double *partials,
                                                  unsigned *ticket, KState *st, const double *res2,
-                                                 double outer_rtol, double inner_min, int maxit) {
+                                                 double outer_rtol, const double *outer_rtol_dev, double inner_min,
+                                                 int maxit) {
+  if constexpr (DEV_RTOL) outer_rtol = *outer_rtol_dev;
   const double rn = sqrt(res2[0]), bn = sqrt(res2[1]);
   const bool outer_done = !(rn > outer_rtol * bn) || bn == 0.0;   // NaN counts as done: the host reports it
   double acc[1] = {0.0};
@@ -208,8 +213,15 @@ int blocks_n(const Launch &L, int n) { return std::min((n + NT32 - 1) / NT32, L.
 
 void launch_mixed_init(const Launch &L, int N, const Krylov32 &K, const double *res2, double outer_rtol,
                        double inner_min, int maxit) {
-  k32_init<<<blocks_n(L, N), NT32, 0, L.stream>>>(N, K.rhs, K.r, K.rhat, K.p, K.v, K.d, L.partials, L.ticket, K.st,
-                                                  res2, outer_rtol, inner_min, maxit);
+  k32_init<false><<<blocks_n(L, N), NT32, 0, L.stream>>>(N, K.rhs, K.r, K.rhat, K.p, K.v, K.d, L.partials, L.ticket,
+                                                         K.st, res2, outer_rtol, nullptr, inner_min, maxit);
+  L.tick();
+}
+
+void launch_mixed_init_dev(const Launch &L, int N, const Krylov32 &K, const double *res2, const double *outer_rtol,
+                           double inner_min, int maxit) {
+  k32_init<true><<<blocks_n(L, N), NT32, 0, L.stream>>>(N, K.rhs, K.r, K.rhat, K.p, K.v, K.d, L.partials, L.ticket,
+                                                        K.st, res2, 0.0, outer_rtol, inner_min, maxit);
   L.tick();
 }
 
