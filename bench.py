@@ -366,8 +366,9 @@ def main():
                     help="Picard nu*H tolerance of both set-ups (default: the configuration's 1e-4)")
     ap.add_argument("--profile", action="store_true",
                     help="time the solve only (no end-to-end, roofline, comparison or CPU runs): for kernel profilers")
-    ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2],
-                    help="Krylov launch mode: 2 graph-resident loops, 1 replayed graphs, 0 direct (for profilers)")
+    ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2, 3],
+                    help="Krylov launch mode: 2 graph-resident loops, 1 replayed graphs, 0 direct (for profilers), "
+                         "3 the whole Picard loop as one graph")
     ap.add_argument("--ksp-factor", type=float, default=1.0,
                     help="fast set-up: KSP rtol of a Picard iteration = factor x the last relative nu*H change")
     ap.add_argument("--ksp-max", type=float, default=1e-1, help="fast set-up: loosest KSP rtol of a Picard iteration")
