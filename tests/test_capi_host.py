@@ -175,3 +175,24 @@ def test_grid_coordinates_match_icegrid():
     dy = 240e3 / 7
     assert g.dy == pytest.approx(dy)
     assert y[0] == pytest.approx(-120e3 + 0.5 * dy) and y[-1] == pytest.approx(120e3 - 0.5 * dy)
+
+
+def _header_enum(prefix):
+    text = open(os.path.join(REPO, "include", "pism_ssa_gpu.h")).read()
+    return {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(" + prefix + r"\w+)\s*=\s*(\d+)", text)}
+
+
+def test_option_tables_match_the_header():
+    """The Python option names map to the header's enum values."""
+    from pism_b200 import config as Cfg
+    pc = _header_enum("PISM_PC_")
+    assert Cfg.PC_TYPES == {"bjacobi": pc["PISM_PC_BLOCK_JACOBI"], "mg": pc["PISM_PC_MULTIGRID"],
+                            "line": pc["PISM_PC_LINE"]}
+    ksp = _header_enum("PISM_KSP_")
+    assert Cfg.KSP_TYPES == {"bicgstab": ksp["PISM_KSP_BICGSTAB"], "gmres": ksp["PISM_KSP_GMRES"]}
+    prec = _header_enum("PISM_PRECISION_")
+    assert Cfg.PRECISIONS == {"fp64": prec["PISM_PRECISION_FP64"], "mixed": prec["PISM_PRECISION_MIXED"]}
+    law = _header_enum("PISM_FLOW_LAW_")
+    assert Cfg.FLOW_LAWS == {"isothermal_glen": law["PISM_FLOW_LAW_ISOTHERMAL_GLEN"], "pb": law["PISM_FLOW_LAW_PB"],
+                             "gpbld": law["PISM_FLOW_LAW_GPBLD"], "arr": law["PISM_FLOW_LAW_ARR"],
+                             "arrwarm": law["PISM_FLOW_LAW_ARRWARM"], "hooke": law["PISM_FLOW_LAW_HOOKE"]}
