@@ -235,6 +235,18 @@ int pism_gpu_ssa_solve(pism_gpu_ssa *h, double *velocity_out, int where,
 int pism_gpu_ssa_solve_batch(pism_gpu_ssa *h, struct pism_gpu_unet *net, int stride, int n,
                              pism_gpu_ssa_member *members, pism_gpu_ssa_stats *stats);
 
+/* The same ensemble with `streams` members in flight at once (no reference counterpart).
+ * The handle keeps `streams` extra solver states on its grid (created on first use, each
+ * with its own memory and CUDA stream, freed with the handle); each member's whole Picard
+ * loop is one graph launch (graphs = 3), so members on different streams overlap from the
+ * calling thread alone.  Per member the same arithmetic and results as
+ * pism_gpu_ssa_solve_batch; a member whose first Picard attempt fails is solved again
+ * through the strategy ladder.  Device inputs are read after the work already queued on
+ * the handle's stream; every output is complete on return.  Built, not yet run on a GPU. */
+#define PISM_GPU_SSA_MAX_STREAMS 16
+int pism_gpu_ssa_solve_batch_concurrent(pism_gpu_ssa *h, struct pism_gpu_unet *net, int stride, int n,
+                                        pism_gpu_ssa_member *members, pism_gpu_ssa_stats *stats, int streams);
+
 /* Field getters (host or device destination per `where`). */
 enum {
   PISM_FIELD_VELOCITY = 0,        /* 2N  m_velocity                                   */

@@ -163,11 +163,12 @@ class SSAFD:
         ci, _keep = self._inputs(self._fields, self._bc)
         self._check(self.lib.pism_gpu_ssa_set_inputs(self._h, C.byref(ci)), "set_inputs")
 
-    def solve_batch(self, members, net=None, stride: int = 1):
+    def solve_batch(self, members, net=None, stride: int = 1, streams: int = 1):
         """pism_gpu_ssa_solve_batch: members is a list of dicts with the set_inputs fields
         and optionally "ice_softness" and "velocity" (initial guess; output array or CUDA
         tensor).  Returns (velocities, stats) per member; a member whose solve failed has
-        stats["status"] != 0."""
+        stats["status"] != 0.  streams > 1: pism_gpu_ssa_solve_batch_concurrent with that
+        many members in flight."""
         n = len(members)
         arr = (CMember * max(n, 1))()
         stats = (CStats * max(n, 1))()
@@ -192,7 +193,11 @@ class SSAFD:
             arr[q].velocity = vb.ptr
             keep += [bufs, vb]
             outs.append(vb.keep)
-        rc = self.lib.pism_gpu_ssa_solve_batch(self._h, net._h if net is not None else None, stride, n, arr, stats)
+        nh = net._h if net is not None else None
+        if streams > 1:
+            rc = self.lib.pism_gpu_ssa_solve_batch_concurrent(self._h, nh, stride, n, arr, stats, streams)
+        else:
+            rc = self.lib.pism_gpu_ssa_solve_batch(self._h, nh, stride, n, arr, stats)
         if rc not in (_capi.OK, _capi.EKSP, _capi.EPICARD, _capi.ENAN, _capi.EZERODIAG):
             self._check(rc, "solve_batch")
         return outs, [stats[q].as_dict() for q in range(n)]
