@@ -1,0 +1,97 @@
+"""The autotuner's choice, timing protocol and cache (CPU, with an injected timer)."""
+import json
+
+import pytest
+
+from pism_b200.autotune import Autotuner, tune_ensemble_streams
+
+
+class FakeClock:
+    """Timer whose reading is the cost the candidate run declared."""
+
+    def __init__(self):
+        self.cost = 0.0
+        self.calls = 0
+
+    def __call__(self, run):
+        run()
+        self.calls += 1
+        return self.cost
+
+
+def make(tmp_path, repeats=3, warmup=1):
+    clock = FakeClock()
+    tuner = Autotuner(str(tmp_path / "tune.json"), repeats=repeats, warmup=warmup, timer=clock,
+                      device=lambda: "B200-fake")
+    return tuner, clock
+
+
+def test_picks_the_fastest_and_counts_runs(tmp_path):
+    tuner, clock = make(tmp_path)
+    costs = {1: 5.0, 2: 3.0, 4: 2.0, 8: 2.5}
+    runs = []
+
+    def run(c):
+        runs.append(c["streams"])
+        clock.cost = costs[c["streams"]]
+
+    best = tuner.choose({"w": 1}, [{"streams": s} for s in (1, 2, 4, 8)], run)
+    assert best == {"streams": 4}
+    assert len(runs) == 4 * (1 + 3) and clock.calls == 4 * 3   # warm-up untimed, repeats timed
+    assert tuner.last_times[json.dumps({"streams": 4})] == 2.0
+
+
+def test_median_of_repeats_and_ties_go_to_the_first(tmp_path):
+    tuner, clock = make(tmp_path, repeats=3, warmup=0)
+    seq = iter([10.0, 1.0, 10.0,   # a: median 10 despite one fast sample
+                4.0, 4.0, 4.0,     # b: 4
+                4.0, 4.0, 4.0])    # c: 4, tie with b
+    def run(c):
+        clock.cost = next(seq)
+    assert tuner.choose({"w": 2}, [{"x": "a"}, {"x": "b"}, {"x": "c"}], run) == {"x": "b"}
+
+
+def test_cache_is_reused_and_keyed_by_device_and_workload(tmp_path):
+    tuner, clock = make(tmp_path)
+    clock.cost = 1.0
+    cands = [{"streams": 1}, {"streams": 2}]
+    tuner.choose({"grid": [401, 401]}, cands, lambda c: None)
+    n = clock.calls
+    again = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "B200-fake")
+    assert again.choose({"grid": [401, 401]}, cands, lambda c: pytest.fail("ran despite the cache")) == {"streams": 1}
+    assert clock.calls == n
+    other_dev = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "other")
+    other_dev.choose({"grid": [401, 401]}, cands, lambda c: None)
+    assert clock.calls > n
+    # a cached choice that is no longer a candidate is tuned again
+    m = clock.calls
+    again.choose({"grid": [401, 401]}, [{"streams": 4}], lambda c: None)
+    assert clock.calls > m
+
+
+def test_rejects_bad_arguments(tmp_path):
+    with pytest.raises(ValueError):
+        Autotuner(repeats=0)
+    tuner, _ = make(tmp_path)
+    with pytest.raises(ValueError):
+        tuner.choose({"w": 3}, [], lambda c: None)
+
+
+def test_ensemble_streams_through_the_solver_interface(tmp_path):
+    """tune_ensemble_streams drives solve_batch(streams=...) and returns the fastest count."""
+    tuner, clock = make(tmp_path, repeats=1, warmup=0)
+
+    class Solver:
+        shape = (41, 41)
+
+        def __init__(self):
+            self.seen = []
+
+        def solve_batch(self, members, net=None, stride=1, streams=1):
+            self.seen.append(streams)
+            clock.cost = {1: 8.0, 2: 5.0, 4: 3.0, 8: 4.0}[streams]
+            return [], []
+
+    s = Solver()
+    assert tune_ensemble_streams(s, [{}] * 8, tuner=tuner) == 4
+    assert s.seen == [1, 2, 4, 8]
