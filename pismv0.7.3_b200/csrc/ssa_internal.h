@@ -6,20 +6,9 @@
 #include <cuda_runtime.h>
 
 #include "ssa_device.cuh"
+#include "ssa_state.h"
 
 namespace pism_gpu {
-
-// Krylov status codes written by the device (KSPConvergedReason analogues)
-enum : int { KSP_OK = 0, KSP_MAXIT = -3, KSP_BREAKDOWN = -5, KSP_NAN = -7 };
-constexpr int KSP_OUTER_DONE = 1;   // mixed precision: the outer residual already meets the tolerance
-
-// scalars of one Krylov solve, owned by the device
-struct KState {
-  double rho, alpha, omega, beta;
-  double rnorm2, bnorm2, rnorm0, rtol;
-  double outer_r2, outer_b2;   // the FP64 outer residual of a mixed-precision refinement step
-  int iter, maxit, done, status;
-};
 
 // device fields of one grid (non-owning view)
 struct Fields {
@@ -149,27 +138,8 @@ void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const doubl
 void launch_pc_apply(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const MGHierarchy *mg,
                      const LinePC *line, const double2 *r, double2 *z);
 
-// ---- device-side control of the Picard loop (ssa_control.cu) ----
-// The state a whole-solve graph keeps on the device: the decisions of the host loop
-// (SSAFD::picard_manager, SSAFD.cc:962-1119, and the refinement loop of the mixed-precision
-// solve) taken by single-thread kernels, and the counts the host reads back once.
-struct PState {
-  double rtol;          // KSP tolerance of the current Picard iteration
-  double last_change;   // relative nu*H change of the previous iteration
-  double norm, change;  // the last Picard test's norms
-  double final_res;     // relative residual of the last linear solve
-  int k;                // Picard tests taken (= Picard iterations)
-  int passes;           // Picard loop passes
-  int done, status;     // status: a PISM_GPU_SSA_* code once done
-  int zd_cell;          // the zero-diagonal cell, when status is EZERODIAG
-  int ksp_its, ksp_status, ksp_total;
-  int refine, refine_done, go, go_count, refine_steps, refine_passes;
-  long long inner_passes;   // passes of the innermost Krylov loop body
-};
-struct PicardConst {
-  double ksp_rtol, ksp_rtol_max, ksp_rtol_factor, picard_rtol;
-  int adaptive, max_iterations;
-};
+// ---- device-side control of the Picard loop (ssa_control.cu; state and decisions in
+// ssa_state.h) ----
 void launch_picard_start(const Launch &L, PState *P);
 // a Picard pass begins: zero-diagonal marker reset, the pass's KSP tolerance
 void launch_picard_begin(const Launch &L, PState *P, const PicardConst &c, int *zero_diag_cell);
