@@ -134,7 +134,7 @@ typedef struct pism_gpu_ssa_config {
      (kernel profilers that cannot look into conditional graphs need 0 or 1).
      3 (BiCGStab only, otherwise as 2): the whole Picard loop of a solve is one CUDA graph
      with nested conditional nodes, its decisions taken on the device, one launch and one
-     read-back per solve; not yet run on a GPU, off by default */
+     read-back per solve; the same results as 2, bit for bit */
   int    graphs;
   int    verbosity;                                /* 0 silent .. 3 per-iteration    */
 } pism_gpu_ssa_config;
