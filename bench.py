@@ -666,6 +666,34 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    # the same solve with the whole Picard loop as one CUDA graph (graphs = 3), after all of
+    # the above: timed like a step (L2 flushed, mean of two after one untimed solve) and
+    # checked bit for bit against the timed answer; an error is reported, not raised
+    if not args.no_compare and args.graphs == 2 and c.ksp_type == "bicgstab":
+        try:
+            s.set_config(c.copy(graphs=3))
+            step()
+            t3 = []
+            for _ in range(2):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                t3.append(e0.elapsed_time(e1))
+            st3 = s.stats()
+            line["comparison"]["whole_solve_graph"] = {
+                "ms": float(np.mean(t3)), "graph_resident_loops_ms": ms_per_step_local(total_ms, args.steps),
+                "bitwise_equal": bool(torch.equal(out, vel_mode)), "picard_iterations": st3["picard_iterations"],
+                "kernel_launches": st3["kernel_launches"]}
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["comparison"]["whole_solve_graph"] = {"error": str(e)[:200]}
+        finally:
+            try:
+                s.set_config(c)
+            except Exception:   # noqa: BLE001
+                pass
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
         picard_plain = (st_other["picard_iterations"] or 184) if args.mode == "fast" else picard[-1]
