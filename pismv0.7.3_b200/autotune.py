@@ -103,3 +103,24 @@ def tune_ensemble_streams(solver, members, net=None, stride: int = 1, candidates
                         lambda cand: solver.solve_batch([dict(m) for m in members], net=net, stride=stride,
                                                         streams=cand["streams"]))
     return best["streams"]
+
+
+def tune_launch_mode(solver, config, prime, candidates=(2, 3), tuner: Optional[Autotuner] = None,
+                     workload: Optional[dict] = None) -> int:
+    """The `graphs` launch mode for repeated solves of this workload: graph-resident Krylov
+    loops (2) or the whole Picard loop as one graph (3), both giving the same answers.
+    prime() sets the initial guess of one solve (the solver's inputs are already set)."""
+    tuner = tuner or Autotuner()
+    wl = {"workload": "ssa solve", "grid": list(solver.shape), "precision": config.precision,
+          "pc": config.pc_type, **(workload or {})}
+
+    def run(cand):
+        solver.set_config(config.copy(graphs=cand["graphs"]))
+        prime()
+        solver.solve()
+
+    try:
+        best = tuner.choose(wl, [{"graphs": int(g)} for g in candidates], run)
+    finally:
+        solver.set_config(config)
+    return best["graphs"]

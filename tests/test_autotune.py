@@ -95,3 +95,29 @@ def test_ensemble_streams_through_the_solver_interface(tmp_path):
     s = Solver()
     assert tune_ensemble_streams(s, [{}] * 8, tuner=tuner) == 4
     assert s.seen == [1, 2, 4, 8]
+
+
+def test_launch_mode_through_the_solver_interface(tmp_path):
+    """tune_launch_mode times solves under each `graphs` value and restores the config."""
+    from pism_b200.autotune import tune_launch_mode
+    from pism_b200.config import SSAConfig
+    tuner, clock = make(tmp_path, repeats=1, warmup=0)
+
+    class Solver:
+        shape = (801, 801)
+
+        def __init__(self):
+            self.cfg = None
+            self.log = []
+
+        def set_config(self, c):
+            self.cfg = c
+
+        def solve(self):
+            self.log.append(self.cfg.graphs)
+            clock.cost = {2: 130.0, 3: 120.0}[self.cfg.graphs]
+
+    s = Solver()
+    base = SSAConfig(pc_type="mg", precision="mixed")
+    assert tune_launch_mode(s, base, prime=lambda: None, tuner=tuner) == 3
+    assert s.log == [2, 3] and s.cfg is base
