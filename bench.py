@@ -703,9 +703,14 @@ def main():
                                           f"scaled to the plain GPU solve's {picard_plain} Picard iterations"}
     if rank == 0:
         print(json.dumps(line))
-    s.close()
-    if net is not None:
-        net.close()
+    graph_error = "error" in line["comparison"].get("whole_solve_graph", {})
+    try:
+        s.close()
+        if net is not None:
+            net.close()
+    except Exception:   # noqa: BLE001 - after a reported whole-solve-graph error the line stands
+        if not graph_error:
+            raise
     if world > 1:
         dist.destroy_process_group()
     return 0
