@@ -380,6 +380,8 @@ def main():
                     help="Picard nu*H tolerance of both set-ups (default: the configuration's 1e-4)")
     ap.add_argument("--profile", action="store_true",
                     help="time the solve only (no end-to-end, roofline, comparison or CPU runs): for kernel profilers")
+    ap.add_argument("--mg-post-blocks", type=int, default=None, choices=[1, 2, 3, 4],
+                    help="resident blocks per SM the coarse-level post-smoothing grid is sized for (default 4)")
     ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2, 3],
                     help="Krylov launch mode: 2 graph-resident loops, 1 replayed graphs, 0 direct (for profilers), "
                          "3 the whole Picard loop as one graph")
@@ -414,6 +416,8 @@ def main():
         c_plain.ssafd_relative_convergence = args.picard_rtol
         c_plain.max_iterations_ssafd = 5000
     c_plain.graphs = args.graphs
+    if args.mg_post_blocks is not None:
+        c_plain.mg_post_blocks_per_sm = args.mg_post_blocks
     c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max)
     if args.inner_rtol is not None:
         c_fast.mixed_inner_rtol = args.inner_rtol

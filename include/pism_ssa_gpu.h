@@ -137,6 +137,9 @@ typedef struct pism_gpu_ssa_config {
      read-back per solve; the same results as 2, bit for bit */
   int    graphs;
   int    verbosity;                                /* 0 silent .. 3 per-iteration    */
+  /* resident blocks per SM that the coarse-level multigrid post-smoothing grid is sized for
+     (1..4; 0 = 4, the other tile kernels' size): a launch-shape knob for the autotuner */
+  int    mg_post_blocks_per_sm;
 } pism_gpu_ssa_config;
 
 /* ---- input fields (SSA::init_impl, SSA.cc:134-184; SSAFD::update) -------- */

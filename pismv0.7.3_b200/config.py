@@ -94,6 +94,7 @@ class SSAConfig:
     ksp_rtol_factor: float = 1.0e-2
     graphs: int = 2
     verbosity: int = 0
+    mg_post_blocks_per_sm: int = 0
     # geometry helpers (not part of the C struct)
     mask_icefree_thickness_standard: float = 0.01
     mask_is_floating_thickness_standard: float = 1.0
@@ -148,7 +149,7 @@ class CConfig(C.Structure):
         ("brutal_sliding_scale", _D), ("ksp_type", _I), ("pc_type", _I), ("ksp_rtol", _D),
         ("ksp_max_it", _I), ("gmres_restart", _I), ("precision", _I), ("mixed_inner_rtol", _D),
         ("mg_omega", _D), ("mg_correction", _D), ("ksp_rtol_adaptive", _I), ("ksp_rtol_max", _D),
-        ("ksp_rtol_factor", _D), ("graphs", _I), ("verbosity", _I),
+        ("ksp_rtol_factor", _D), ("graphs", _I), ("verbosity", _I), ("mg_post_blocks_per_sm", _I),
     ]
 
 

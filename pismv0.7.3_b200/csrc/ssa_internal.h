@@ -87,6 +87,7 @@ struct MGHierarchy {
   int small_smem = 0;                            // its per-CTA staging buffer (bytes)
   float omega = 0.9f;                            // damping of the block-Jacobi smoother
   float correction = 1.2f;                       // scaling of the coarse-grid correction
+  int post_blocks = 0;                           // grid cap of the coarse post-smoothing (0: none)
   double *cinv = nullptr;                        // dense inverse of the coarsest operator (transposed)
   int *singular = nullptr;
   float2 *nuHf = nullptr;                        // FP32 copies of the fine nu*H, beta, D^-1

@@ -762,7 +762,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     const MGLevel &L = H.lev[l], &C = H.lev[l + 1];
     const LevelView V = view(L);
     const TileM tm = tiles_of(L.Mx, L.My);
-    const int nb = blocks_for(Lc, tm.tiles);
+    const int nb = H.post_blocks > 0 ? std::min(blocks_for(Lc, tm.tiles), H.post_blocks) : blocks_for(Lc, tm.tiles);
 #define MGCP(AX, AY) [&] { k_mgc_post<AX, AY><<<nb, NTm, 0, Lc.stream>>>(V, omega, corr, C.My, C.x, tm, st); }
     dispatch_ax(L.ax, L.ay, MGCP(2, 2), MGCP(2, 1), MGCP(1, 2), MGCP(1, 1));
 #undef MGCP

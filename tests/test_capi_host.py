@@ -131,7 +131,7 @@ def test_gmres_settings_are_checked_before_device_work(lib):
     g, _z = GridDesc(16, 16, 1e5, 1e5).to_c()
     h = C.c_void_p()
     for kw in ({"ksp_type": "gmres", "gmres_restart": 0}, {"ksp_type": "gmres", "gmres_restart": 31},
-               {"ksp_type": "gmres", "precision": "mixed", "pc_type": "mg"}, {"graphs": 4}, {"graphs": -1}):
+               {"ksp_type": "gmres", "precision": "mixed", "pc_type": "mg"}, {"graphs": 4}, {"graphs": -1}, {"mg_post_blocks_per_sm": 5}):
         cfg = SSAConfig(**kw).to_c()
         assert lib.pism_gpu_ssa_create(C.byref(g), C.byref(cfg), 0, C.byref(h)) == _capi.EINVAL, kw
 
