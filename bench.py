@@ -271,15 +271,7 @@ def run_ensemble(args):
     net.set_stream(stream.cuda_stream)
     s = SSAFD(g, c_fast, device=local)
     s.set_stream(stream.cuda_stream)
-    tuned = None
-    if args.streams == "auto":
-        from pism_b200.autotune import Autotuner, tune_ensemble_streams
-        tuner = Autotuner(repeats=2, warmup=1)
-        streams = tune_ensemble_streams(s, mem[:8], net=net, stride=1, tuner=tuner)
-        tuned = {"candidates": [1, 2, 4, 8], "times_ms": tuner.last_times, "choice": streams}
-    else:
-        streams = int(args.streams)
-    s.solve_batch(mem[:max(2, streams)], net=net, stride=1, streams=streams)   # warm-up
+    s.solve_batch(mem[:2], net=net, stride=1)   # warm-up
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
     sampler = ClockSampler(local)
     sampler.start()
@@ -291,7 +283,7 @@ def run_ensemble(args):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        vels, stats = s.solve_batch(mem, net=net, stride=1, streams=streams)
+        vels, stats = s.solve_batch(mem, net=net, stride=1)
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -303,7 +295,7 @@ def run_ensemble(args):
             for _, c, f, _ in cases]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s.solve_batch(hmem, net=net, stride=1, streams=streams)
+    s.solve_batch(hmem, net=net, stride=1)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dev)
     # accuracy: the plain FP64 solve of every member
@@ -325,11 +317,8 @@ def run_ensemble(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": f"ensemble of {args.members} seeded {M}x{M} sheets at 10 km per GPU, temperature "
                                "U[-20,-2] C and tau_c median U[20,200] kPa per member, solved by "
-                               + ("pism_gpu_ssa_solve_batch" if streams == 1 else
-                                  f"pism_gpu_ssa_solve_batch_concurrent ({streams} streams)")
-                               + " (fast set-up, learned guess)",
+                               "pism_gpu_ssa_solve_batch (fast set-up, learned guess)",
                    "members_per_gpu": args.members, "l2": "flushed (256 MB write) between steps",
-                   "streams": streams, "autotune": tuned,
                    "parallelism": f"members sharded over {world} GPU(s)"},
         "members": {"picard_iterations": [st["picard_iterations"] for st in stats],
                     "converged": sum(st["converged"] for st in stats),
@@ -373,9 +362,6 @@ def main():
     ap.add_argument("--workload", default="solve", choices=["solve", "ensemble"],
                     help="ensemble: members solved/s of a 64-member 401^2 ensemble (its own JSON line)")
     ap.add_argument("--members", type=int, default=64)
-    ap.add_argument("--streams", default="1",
-                    help="ensemble members in flight at once (pism_gpu_ssa_solve_batch_concurrent when > 1); "
-                         "'auto': chosen by the autotuner on the first 8 members")
     ap.add_argument("--picard-rtol", type=float, default=None,
                     help="Picard nu*H tolerance of both set-ups (default: the configuration's 1e-4)")
     ap.add_argument("--profile", action="store_true",

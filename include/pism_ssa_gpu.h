@@ -238,18 +238,6 @@ int pism_gpu_ssa_solve(pism_gpu_ssa *h, double *velocity_out, int where,
 int pism_gpu_ssa_solve_batch(pism_gpu_ssa *h, struct pism_gpu_unet *net, int stride, int n,
                              pism_gpu_ssa_member *members, pism_gpu_ssa_stats *stats);
 
-/* The same ensemble with `streams` members in flight at once (no reference counterpart).
- * The handle keeps `streams` extra solver states on its grid (created on first use, each
- * with its own memory and CUDA stream, freed with the handle); each member's whole Picard
- * loop is one graph launch (graphs = 3), so members on different streams overlap from the
- * calling thread alone.  Per member the same arithmetic and results as
- * pism_gpu_ssa_solve_batch; a member whose first Picard attempt fails is solved again
- * through the strategy ladder.  Device inputs are read after the work already queued on
- * the handle's stream; every output is complete on return.  Built, not yet run on a GPU. */
-#define PISM_GPU_SSA_MAX_STREAMS 16
-int pism_gpu_ssa_solve_batch_concurrent(pism_gpu_ssa *h, struct pism_gpu_unet *net, int stride, int n,
-                                        pism_gpu_ssa_member *members, pism_gpu_ssa_stats *stats, int streams);
-
 /* Field getters (host or device destination per `where`). */
 enum {
   PISM_FIELD_VELOCITY = 0,        /* 2N  m_velocity                                   */
@@ -304,11 +292,13 @@ int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations,
  *
  * It allocates nothing: its scratch is a fixed 512 KiB device array inside the
  * library, which every GPU that loads the library holds until the process exits.
- * So the grid may have at most PISM_GPU_SSA_NOALLOC_MAX_CELLS cells (larger grids
- * return PISM_GPU_SSA_ETOOLARGE), and because every call shares that array, calls
- * whose work overlaps on the GPU (other streams, other host threads) race: order
- * them on one stream.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture.
+ * So the grid may have at most PISM_GPU_SSA_NOALLOC_MAX_CELLS cells, in any shape
+ * (larger grids return PISM_GPU_SSA_ETOOLARGE), and because every call shares that
+ * array, calls whose work overlaps on the GPU (other streams, other host threads)
+ * race: order them on one stream.  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  The return value
+ * is this call's own status: an error that earlier work left pending in the CUDA
+ * runtime (cudaGetLastError) is neither read nor cleared.
  * CFBC configurations return PISM_GPU_SSA_EINVAL (use the handle API). */
 #define PISM_GPU_SSA_NOALLOC_MAX_CELLS (2048 * 2048)
 int pism_gpu_ssa_nuH_noalloc(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cfg,

@@ -26,7 +26,7 @@ EXPORTS = [
     "pism_gpu_ssa_set_initial_guess", "pism_gpu_ssa_solve", "pism_gpu_ssa_get_field",
     "pism_gpu_ssa_assemble_rhs", "pism_gpu_ssa_compute_hardness", "pism_gpu_ssa_compute_nuH",
     "pism_gpu_ssa_apply", "pism_gpu_ssa_apply_preconditioner", "pism_gpu_ssa_linear_solve",
-    "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch", "pism_gpu_ssa_solve_batch_concurrent",
+    "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch",
 ]
 # every symbol include/pism_unet_gpu.h declares
 UNET_EXPORTS = [
@@ -66,7 +66,6 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_linear_solve": (I, [V, V, P(I), P(D)]),
         "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
         "pism_gpu_ssa_solve_batch": (I, [V, V, I, I, P(CMember), P(CStats)]),
-        "pism_gpu_ssa_solve_batch_concurrent": (I, [V, V, I, I, P(CMember), P(CStats), I]),
         "pism_gpu_unet_param_count": (C.c_longlong, []),
         "pism_gpu_unet_create": (I, [I, I, I, I, P(V)]),
         "pism_gpu_unet_destroy": (I, [V]),

@@ -6,7 +6,7 @@
 //   SSAFactory            SSA.hh:77
 // It stands alone (no PETSc): fields are plain arrays in the reference's DMDA layout,
 // [i][j] with j contiguous, vectors interleaved (u, v).  Inside pismr the same class
-// derives from pism::stressbalance::SSA and reads IceModelVec arrays (INTEGRATION.md).
+// derives from pism::stressbalance::SSA and reads IceModelVec arrays.
 #pragma once
 
 #include <stdexcept>

@@ -68,10 +68,6 @@ struct pism_gpu_ssa {
   } sgraph;
   PState *pstate = nullptr;
   PState *pstate_host = nullptr;
-  // concurrent ensemble members: solver states on their own streams, kept with the handle
-  std::vector<pism_gpu_ssa *> subs;
-  cudaEvent_t batch_ev = nullptr;
-  std::chrono::steady_clock::time_point t_start{};
   double *res_dev = nullptr;   // {||r||^2, ||b||^2} of the refinement
   double *res_host = nullptr;
   MGHierarchy mg{};
@@ -1018,9 +1014,6 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
     if (gr.exec) cudaGraphExecDestroy(gr.exec);
   for (auto &lp : h->loops)
     if (lp.exec) cudaGraphExecDestroy(lp.exec);
-  for (pism_gpu_ssa *sub : h->subs) pism_gpu_ssa_destroy(sub);
-  h->subs.clear();
-  if (h->batch_ev) cudaEventDestroy(h->batch_ev);
   if (h->sgraph.exec) cudaGraphExecDestroy(h->sgraph.exec);
   if (h->pstate) cudaFree(h->pstate);
   if (h->pstate_host) cudaFreeHost(h->pstate_host);
@@ -1337,145 +1330,6 @@ int pism_gpu_ssa_solve_batch(pism_gpu_ssa *h, pism_gpu_unet *net, int stride, in
   h->cfg.ice_softness = A0;
   h->prepared = false;
   return first;
-}
-
-}  // extern "C"
-
-// ---- ensemble members solved concurrently ----
-namespace {
-
-bool hard_error(int rc) {
-  return rc == PISM_GPU_SSA_EINVAL || rc == PISM_GPU_SSA_ECUDA || rc == PISM_GPU_SSA_ENOMEM ||
-         rc == PISM_GPU_SSA_ESTATE || rc == PISM_GPU_SSA_ETOOLARGE;
-}
-
-// pism_gpu_ssa_solve up to its first Picard attempt, which is launched as the whole-solve
-// graph without waiting (*launched); not launched, nothing but the preparation has run.
-int member_start(pism_gpu_ssa *h, bool *launched) {
-  *launched = false;
-  h->t_start = std::chrono::steady_clock::now();
-  h->stats = pism_gpu_ssa_stats{};
-  h->err.clear();
-  h->L.count = &h->stats.kernel_launches;
-  if (h->default_pc_failure_count >= 5) return PISM_GPU_SSA_OK;   // picard_iteration's fallback-only branch
-  CK(h, cudaEventRecord(h->ev0, h->stream));
-  CK(h, cudaMemcpyAsync(h->vel_old, h->vel, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
-  RET(prepare(h));
-  h->use_fallback = 0;
-  h->stats.strategy = 0;
-  return solve_graph_launch(h, h->cfg.epsilon_ssa, 1.0, launched);
-}
-
-// The rest of pism_gpu_ssa_solve for a launched member: on success its epilogue and the
-// copy-out; after a failed first attempt the whole solve again through the host's strategy
-// ladder, from the member's initial guess (kept in vel_old), as pism_gpu_ssa_solve does it.
-int member_finish(pism_gpu_ssa *h, pism_gpu_ssa_member &m, pism_gpu_ssa_stats *stats) {
-  const int rc = solve_graph_collect(h, h->cfg.epsilon_ssa);
-  if (rc != PISM_GPU_SSA_OK) {
-    if (hard_error(rc)) return rc;
-    CK(h, cudaMemcpyAsync(h->vel, h->vel_old, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
-    return pism_gpu_ssa_solve(h, m.velocity, m.inputs.where, stats);
-  }
-  h->stats.converged = 1;
-  if (h->cfg.brutal_sliding) launch_scale(h->L, 2 * h->N, h->cfg.brutal_sliding_scale, (double *)h->vel);
-  launch_bfrict(h->L, h->N, h->cfg, fields_of(h), h->bfrict);
-  CK(h, cudaGetLastError());
-  CK(h, cudaEventRecord(h->ev1, h->stream));
-  CK(h, cudaStreamSynchronize(h->stream));
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-  h->stats.kernel_ms = ms;
-  h->stats.status = PISM_GPU_SSA_OK;
-  h->stats.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h->t_start).count();
-  if (stats) *stats = h->stats;
-  return copy_out(h, m.velocity, h->vel, sizeof(double2) * h->N, m.inputs.where);
-}
-
-}  // namespace
-
-extern "C" {
-
-int pism_gpu_ssa_solve_batch_concurrent(pism_gpu_ssa *h, pism_gpu_unet *net, int stride, int n,
-                                        pism_gpu_ssa_member *members, pism_gpu_ssa_stats *stats, int streams) {
-  if (!h || n < 0 || (n > 0 && !members)) return PISM_GPU_SSA_EINVAL;
-  if (streams < 1 || streams > PISM_GPU_SSA_MAX_STREAMS)
-    return fail(h, PISM_GPU_SSA_EINVAL, "streams must be in [1, %d]", PISM_GPU_SSA_MAX_STREAMS);
-  for (int q = 0; q < n; ++q)
-    if (!members[q].velocity) return fail(h, PISM_GPU_SSA_EINVAL, "member %d: velocity is NULL", q);
-  DeviceGuard dg(h->device);
-  pism_gpu_ssa_config cfg = h->cfg;
-  cfg.graphs = 3;
-  // the solver states, created on first use with the handle's grid and device
-  while ((int)h->subs.size() < streams) {
-    pism_gpu_grid gd = h->grid;
-    gd.z = h->z_host.empty() ? nullptr : h->z_host.data();
-    pism_gpu_ssa *sub = nullptr;
-    const int rc = pism_gpu_ssa_create(&gd, &cfg, h->device, &sub);
-    if (rc != PISM_GPU_SSA_OK) return fail(h, rc, "creating the solver state of stream %d failed", (int)h->subs.size());
-    h->subs.push_back(sub);
-  }
-  // members' device inputs may come from work queued on the handle's stream
-  if (!h->batch_ev) CK(h, cudaEventCreateWithFlags(&h->batch_ev, cudaEventDisableTiming));
-  CK(h, cudaEventRecord(h->batch_ev, h->stream));
-  for (int s = 0; s < streams; ++s) {
-    pism_gpu_ssa *sub = h->subs[s];
-    pism_gpu_ssa_config want = cfg;
-    want.ice_softness = sub->cfg.ice_softness;
-    if (memcmp(&want, &sub->cfg, sizeof(want)) != 0) RET(pism_gpu_ssa_set_config(sub, &cfg));
-    CK(h, cudaStreamWaitEvent(sub->stream, h->batch_ev, 0));
-  }
-  std::vector<int> pending(streams, -1);
-  int first = PISM_GPU_SSA_OK;
-  auto finish = [&](int s) -> int {
-    const int q = pending[s];
-    pending[s] = -1;
-    pism_gpu_ssa *sub = h->subs[s];
-    const int rc = member_finish(sub, members[q], stats ? &stats[q] : nullptr);
-    if (stats) stats[q].status = rc;
-    if (rc != PISM_GPU_SSA_OK && first == PISM_GPU_SSA_OK) first = rc;
-    if (rc != PISM_GPU_SSA_OK) h->err = sub->err;
-    return rc;
-  };
-  int hard = PISM_GPU_SSA_OK;
-  for (int q = 0; q < n && hard == PISM_GPU_SSA_OK; ++q) {
-    const int s = q % streams;
-    pism_gpu_ssa *sub = h->subs[s];
-    if (pending[s] >= 0 && hard_error(finish(s))) {
-      hard = first;
-      break;
-    }
-    pism_gpu_ssa_member &m = members[q];
-    sub->cfg.ice_softness = m.ice_softness > 0.0 ? m.ice_softness : cfg.ice_softness;
-    int rc = pism_gpu_ssa_set_inputs(sub, &m.inputs);
-    if (rc == PISM_GPU_SSA_OK)
-      rc = net ? pism_gpu_ssa_learned_guess(sub, net, stride)
-               : pism_gpu_ssa_set_initial_guess(sub, m.velocity, m.inputs.where);
-    bool launched = false;
-    if (rc == PISM_GPU_SSA_OK) rc = member_start(sub, &launched);
-    if (rc == PISM_GPU_SSA_OK && launched) {
-      pending[s] = q;
-      continue;
-    }
-    if (rc == PISM_GPU_SSA_OK)   // the graph does not apply here: the ordinary solve
-      rc = pism_gpu_ssa_solve(sub, m.velocity, m.inputs.where, stats ? &stats[q] : nullptr);
-    else if (stats) {
-      stats[q] = pism_gpu_ssa_stats{};
-      stats[q].status = rc;
-    }
-    if (rc != PISM_GPU_SSA_OK) {
-      h->err = sub->err;
-      if (first == PISM_GPU_SSA_OK) first = rc;
-      if (hard_error(rc)) hard = rc;
-    }
-  }
-  for (int k = 0; k < streams; ++k) {   // the members still in flight, oldest first
-    int best = -1;
-    for (int s = 0; s < streams; ++s)
-      if (pending[s] >= 0 && (best < 0 || pending[s] < pending[best])) best = s;
-    if (best < 0) break;
-    finish(best);
-  }
-  return hard != PISM_GPU_SSA_OK ? hard : first;
 }
 
 }  // extern "C"

@@ -25,6 +25,9 @@
 // (0.85, 1.5); omega >= 1 makes the damped block-Jacobi smoother unstable (> 1e5).
 #include <algorithm>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include <cooperative_groups.h>
 
@@ -605,6 +608,24 @@ int mg_plan(int Mx, int My, MGHierarchy &H) {
   return H.nlev;
 }
 
+// The dynamic shared-memory limit of a kernel is an attribute of the function on the current
+// device, shared by every handle of the process: a handle on a smaller grid must not lower the
+// limit that a live handle on a larger grid launches with.  So the attribute is only ever
+// raised, to the largest size any handle has asked for on that device (under a lock: handles
+// may be created from several host threads).
+static int raise_dynamic_smem(const void *func, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, int> granted;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  std::lock_guard<std::mutex> lock(mu);
+  int &have = granted[{dev, func}];
+  if (bytes <= have) return 0;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) return 1;
+  have = bytes;
+  return 0;
+}
+
 int mg_allocate(MGHierarchy &H, int fine_cells) {
   for (int l = 0; l < H.nlev; ++l) {
     MGLevel &L = H.lev[l];
@@ -627,17 +648,10 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
     if (cudaMalloc(&H.views, sizeof(LevelView) * MG_MAX_LEVELS) != cudaSuccess) return 1;
     if (cudaMemcpy(H.views, v, sizeof(LevelView) * H.nlev, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
   }
-  if (cudaFuncSetAttribute(k_mg_small_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, H.small_smem) != cudaSuccess)
-    return 1;
-  if (cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(sizeof(double) * n * n)) != cudaSuccess)
-    return 1;
-  if (cudaFuncSetAttribute(k_mg_build1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(sizeof(double) * 36 * NTm)) != cudaSuccess)
-    return 1;
-  if (cudaFuncSetAttribute(k_mg_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(sizeof(double) * 36 * NTm)) != cudaSuccess)
-    return 1;
+  if (raise_dynamic_smem((const void *)k_mg_small_cycle, H.small_smem) != 0) return 1;
+  if (raise_dynamic_smem((const void *)k_mg_coarse_invert, (int)(sizeof(double) * n * n)) != 0) return 1;
+  if (raise_dynamic_smem((const void *)k_mg_build1, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
+  if (raise_dynamic_smem((const void *)k_mg_build, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
   return 0;
 }
 

@@ -8,10 +8,11 @@
 // pism_gpu_ssa_create; this entry point instead keeps its scratch in the fixed
 // file-scope device array below, so the caller passes only inputs and outputs.
 //
-// The scratch (per-block partial sums + the last-block ticket) holds at most
-// NOALLOC_MAX_BLOCKS blocks of 32 x 8 cells, i.e. grids of up to
-// PISM_GPU_SSA_NOALLOC_MAX_CELLS cells; larger grids are rejected.  Every GPU that
-// loads this library holds the array (512 KiB) until the process exits.
+// The scratch holds the partial sums of at most NOALLOC_MAX_BLOCKS blocks and the last-block
+// ticket.  The kernel's blocks walk the grid's 32 x 8-cell tiles with a stride of the block
+// count, so every grid shape of up to PISM_GPU_SSA_NOALLOC_MAX_CELLS cells fits, however
+// thin; larger grids are rejected.  Every GPU that loads this library holds the array
+// (512 KiB) until the process exits.
 #include <mutex>
 
 #include "ssa_device.cuh"
@@ -39,72 +40,76 @@ struct Params {
 };
 
 // compute_nuH_staggered (SSAFD.cc:1359-1421) + under-relaxation (SSAFD.cc:1061-1064) +
-// compute_nuH_norm (SSAFD.cc:1170-1189) + the drag of SSAFD.cc:744-759; one block per tile
-__global__ void __launch_bounds__(NTn) k_nuH_noalloc(GridDev g, int tiles_j, pism_gpu_ssa_config c, Params p,
-                                                     const double2 *__restrict__ vel, const double *__restrict__ H,
+// compute_nuH_norm (SSAFD.cc:1170-1189) + the drag of SSAFD.cc:744-759; each block takes the
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+__global__ void __launch_bounds__(NTn) k_nuH_noalloc(GridDev g, int tiles_j, int tiles, pism_gpu_ssa_config c,
+                                                     Params p, const double2 *__restrict__ vel,
+                                                     const double *__restrict__ H,
                                                      const double2 *__restrict__ hardness,
                                                      const double *__restrict__ mask, const double *__restrict__ tauc,
                                                      const double *__restrict__ gl_mask, double2 *__restrict__ nuH,
                                                      double *__restrict__ beta, double *scratch, double *norms) {
-  const int ti = blockIdx.x / tiles_j, tj = blockIdx.x - ti * tiles_j;
-  const int j = tj * TJn + (threadIdx.x & (TJn - 1)), i = ti * TIn + (threadIdx.x >> 5);
   double acc[NV] = {0.0, 0.0, 0.0, 0.0};
-  if (i < g.Mx && j < g.My) {
-    const double dx = g.dx, dy = g.dy;
-    const int k = cell(g, i, j);
-    const double2 uc = vel[k], ue = vel[nbr(g, i, j, 1, 0)], un = vel[nbr(g, i, j, 0, 1)],
-                  us = vel[nbr(g, i, j, 0, -1)], uw = vel[nbr(g, i, j, -1, 0)], une = vel[nbr(g, i, j, 1, 1)],
-                  use = vel[nbr(g, i, j, 1, -1)], unw = vel[nbr(g, i, j, -1, 1)];
-    const double Hc = H[k];
-    const double2 B = hardness[k];
-    double r[2];
-    for (int o = 0; o < 2; ++o) {
-      const double Hf = 0.5 * (Hc + H[nbr(g, i, j, 1 - o, o)]);
-      if (Hf < p.Hmin) {
-        r[o] = p.notional;
-        continue;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int ti = tile / tiles_j, tj = tile - ti * tiles_j;
+    const int j = tj * TJn + (threadIdx.x & (TJn - 1)), i = ti * TIn + (threadIdx.x >> 5);
+    if (i < g.Mx && j < g.My) {
+      const double dx = g.dx, dy = g.dy;
+      const int k = cell(g, i, j);
+      const double2 uc = vel[k], ue = vel[nbr(g, i, j, 1, 0)], un = vel[nbr(g, i, j, 0, 1)],
+                    us = vel[nbr(g, i, j, 0, -1)], uw = vel[nbr(g, i, j, -1, 0)], une = vel[nbr(g, i, j, 1, 1)],
+                    use = vel[nbr(g, i, j, 1, -1)], unw = vel[nbr(g, i, j, -1, 1)];
+      const double Hc = H[k];
+      const double2 B = hardness[k];
+      double r[2];
+      for (int o = 0; o < 2; ++o) {
+        const double Hf = 0.5 * (Hc + H[nbr(g, i, j, 1 - o, o)]);
+        if (Hf < p.Hmin) {
+          r[o] = p.notional;
+          continue;
+        }
+        double u_x, u_y, v_x, v_y;
+        if (o == 0) {
+          u_x = (ue.x - uc.x) / dx;
+          u_y = (un.x + une.x - us.x - use.x) / (4 * dy);
+          v_x = (ue.y - uc.y) / dx;
+          v_y = (un.y + une.y - us.y - use.y) / (4 * dy);
+        } else {
+          u_x = (ue.x + une.x - uw.x - unw.x) / (4 * dx);
+          u_y = (un.x - uc.x) / dy;
+          v_x = (ue.y + une.y - uw.y - unw.y) / (4 * dx);
+          v_y = (un.y - uc.y) / dy;
+        }
+        const double Bo = o == 0 ? B.x : B.y;
+        const double nu = 0.5 * Bo * pow(p.schoof_reg + second_invariant_2d(u_x, u_y, v_x, v_y), p.visc_power);
+        r[o] = nu * Hf;
+        r[o] *= p.enh_scaling;
+        r[o] += p.reg;
       }
-      double u_x, u_y, v_x, v_y;
-      if (o == 0) {
-        u_x = (ue.x - uc.x) / dx;
-        u_y = (un.x + une.x - us.x - use.x) / (4 * dy);
-        v_x = (ue.y - uc.y) / dx;
-        v_y = (un.y + une.y - us.y - use.y) / (4 * dy);
-      } else {
-        u_x = (ue.x + une.x - uw.x - unw.x) / (4 * dx);
-        u_y = (un.x - uc.x) / dy;
-        v_x = (ue.y + une.y - uw.y - unw.y) / (4 * dx);
-        v_y = (un.y - uc.y) / dy;
+      const double2 old = nuH[k];
+      if (p.underrelax != 1.0) {
+        r[0] *= p.underrelax;
+        r[0] += (1.0 - p.underrelax) * old.x;
+        r[1] *= p.underrelax;
+        r[1] += (1.0 - p.underrelax) * old.y;
       }
-      const double Bo = o == 0 ? B.x : B.y;
-      const double nu = 0.5 * Bo * pow(p.schoof_reg + second_invariant_2d(u_x, u_y, v_x, v_y), p.visc_power);
-      r[o] = nu * Hf;
-      r[o] *= p.enh_scaling;
-      r[o] += p.reg;
+      nuH[k] = make_double2(r[0], r[1]);
+      // L1 over the ghosted local vector: periodic ghost copies of the edge cells count again
+      const double w = ((i == 0 ? 1.0 : 0.0) + (i == g.Mx - 1 ? 1.0 : 0.0) + 1.0) *
+                       ((j == 0 ? 1.0 : 0.0) + (j == g.My - 1 ? 1.0 : 0.0) + 1.0);
+      acc[0] += fabs(r[0]) * w;
+      acc[1] += fabs(r[1]) * w;
+      acc[2] += fabs(old.x - r[0]) * w;
+      acc[3] += fabs(old.y - r[1]) * w;
+      const int M = as_int(mask[k]);
+      double bta = 0.0;
+      if (m_grounded_ice(M))
+        bta = basal_drag(c, tauc[k], uc.x, uc.y);
+      else if (m_ice_free_land(M))
+        bta = c.beta_ice_free_bedrock;
+      if (c.sub_groundingline && m_icy(M)) bta = gl_mask[k] * basal_drag(c, tauc[k], uc.x, uc.y);
+      beta[k] = bta;
     }
-    const double2 old = nuH[k];
-    if (p.underrelax != 1.0) {
-      r[0] *= p.underrelax;
-      r[0] += (1.0 - p.underrelax) * old.x;
-      r[1] *= p.underrelax;
-      r[1] += (1.0 - p.underrelax) * old.y;
-    }
-    nuH[k] = make_double2(r[0], r[1]);
-    // L1 over the ghosted local vector: periodic ghost copies of the edge cells count again
-    const double w = ((i == 0 ? 1.0 : 0.0) + (i == g.Mx - 1 ? 1.0 : 0.0) + 1.0) *
-                     ((j == 0 ? 1.0 : 0.0) + (j == g.My - 1 ? 1.0 : 0.0) + 1.0);
-    acc[0] = fabs(r[0]) * w;
-    acc[1] = fabs(r[1]) * w;
-    acc[2] = fabs(old.x - r[0]) * w;
-    acc[3] = fabs(old.y - r[1]) * w;
-    const int M = as_int(mask[k]);
-    double bta = 0.0;
-    if (m_grounded_ice(M))
-      bta = basal_drag(c, tauc[k], uc.x, uc.y);
-    else if (m_ice_free_land(M))
-      bta = c.beta_ice_free_bedrock;
-    if (c.sub_groundingline && m_icy(M)) bta = gl_mask[k] * basal_drag(c, tauc[k], uc.x, uc.y);
-    beta[k] = bta;
   }
   // block sums -> scratch; the last block adds them in block order
   __shared__ double sh[NV][NTn / 32];
@@ -167,10 +172,10 @@ extern "C" int pism_gpu_ssa_nuH_noalloc(const pism_gpu_grid *grid, const pism_gp
   if (grid->Mx < 3 || grid->My < 3 || !(grid->dx > 0) || !(grid->dy > 0)) return PISM_GPU_SSA_EINVAL;
   if (cfg->calving_front_stress_boundary_condition) return PISM_GPU_SSA_EINVAL;   // plain stencil only
   if (cfg->sub_groundingline && !gl_mask) return PISM_GPU_SSA_EINVAL;
+  if ((long long)grid->Mx * grid->My > PISM_GPU_SSA_NOALLOC_MAX_CELLS) return PISM_GPU_SSA_ETOOLARGE;
   const int tiles_j = (grid->My + TJn - 1) / TJn;
-  const long long tiles = (long long)tiles_j * ((grid->Mx + TIn - 1) / TIn);
-  if ((long long)grid->Mx * grid->My > PISM_GPU_SSA_NOALLOC_MAX_CELLS || tiles > NOALLOC_MAX_BLOCKS)
-    return PISM_GPU_SSA_ETOOLARGE;
+  const int tiles = tiles_j * ((grid->Mx + TIn - 1) / TIn);   // < 2^31: Mx, My >= 3, cells <= 2^22
+  const int blocks = tiles < NOALLOC_MAX_BLOCKS ? tiles : NOALLOC_MAX_BLOCKS;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return PISM_GPU_SSA_ECUDA;
   double *scratch;
@@ -199,8 +204,13 @@ extern "C" int pism_gpu_ssa_nuH_noalloc(const pism_gpu_grid *grid, const pism_gp
            (1.0 - n) / (2.0 * n),
            1.0 / pow(cfg->ssa_enhancement_factor, 1.0 / n),
            grid->dx * grid->dy};
-  k_nuH_noalloc<<<(unsigned)tiles, NTn, 0, stream>>>(g, tiles_j, *cfg, p, (const double2 *)velocity, thickness,
-                                                      (const double2 *)hardness_stag, mask, tauc, gl_mask,
-                                                      (double2 *)nuH, beta, scratch, norms);
-  return cudaGetLastError() == cudaSuccess ? PISM_GPU_SSA_OK : PISM_GPU_SSA_ECUDA;
+  // launched through cudaLaunchKernel, whose return value is this launch's own status: an
+  // error that earlier work of the caller left pending is neither read nor cleared here
+  const double2 *vel2 = (const double2 *)velocity, *hard2 = (const double2 *)hardness_stag;
+  double2 *nuH2 = (double2 *)nuH;
+  void *args[] = {&g, (void *)&tiles_j, (void *)&tiles, (void *)cfg, &p, &vel2, (void *)&thickness, &hard2,
+                  (void *)&mask, (void *)&tauc, (void *)&gl_mask, &nuH2, &beta, &scratch, &norms};
+  const cudaError_t e = cudaLaunchKernel((const void *)k_nuH_noalloc, dim3((unsigned)blocks), dim3(NTn), args, 0,
+                                         stream);
+  return e == cudaSuccess ? PISM_GPU_SSA_OK : PISM_GPU_SSA_ECUDA;
 }

@@ -18,7 +18,6 @@ from __future__ import annotations
 import ctypes as C
 import math
 import os
-import threading
 import time
 
 import numpy as np
@@ -192,64 +191,47 @@ def solve_config(c: SSAConfig) -> SSAConfig:
                   ksp_rtol_max=1e-2, ssafd_relative_convergence=1e-4)
 
 
-def generate(seeds, M: int = 401, device: int = 0, workers: int = 1, log=None):
-    """Solve the training cases and return [(features [H8, W8, 8], target [H8, W8, 2],
-    weight [H8, W8])] on the device plus per-case stats.  workers > 1 drives that many solver
-    handles from host threads on their own CUDA streams; one such run ended in an illegal
-    memory access whose cause was not found, so the default (and the committed weights) use
-    a single worker."""
+def generate(seeds, M: int = 401, device: int = 0, log=None):
+    """Solve the training cases one after another on one solver handle and return
+    [(features [H8, W8, 8], target [H8, W8, 2], weight [H8, W8])] on the device plus per-case
+    stats.  The handle's work runs on a stream of its own; every output is complete on
+    return."""
     import torch
     from .ssa import SSAFD
     dev = torch.device("cuda", device)
     out = [None] * len(seeds)
     stats = [None] * len(seeds)
-    lock = threading.Lock()
-    nxt = [0]
-    err = []
-
-    def work():
-        stream = torch.cuda.Stream(device=dev)
-        while True:
-            with lock:
-                if nxt[0] >= len(seeds) or err:
-                    return
-                q = nxt[0]
-                nxt[0] += 1
-            try:
-                g, c, f, meta = training_case(seeds[q], M)
-                with torch.cuda.stream(stream):
+    stream = torch.cuda.Stream(device=dev)
+    s = None
+    try:
+        with torch.cuda.stream(stream):
+            for q, seed in enumerate(seeds):
+                g, c, f, meta = training_case(seed, M)
+                if s is None:
                     s = SSAFD(g, solve_config(c), device=device)
                     s.set_stream(stream.cuda_stream)
-                    s.set_inputs(**{k: f[k] for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
-                    vel = torch.empty((M, M, 2), dtype=torch.float64, device=dev)
-                    s.set_initial_guess(torch.zeros_like(vel))
-                    s.solve(out=vel)
-                    st = s.stats()
-                    x = features(s, 1)
-                    hh, ww = x.shape[:2]
-                    t = target_image(vel, hh, ww)
-                    m = torch.zeros((hh, ww), dtype=torch.float32, device=dev)
-                    mask = torch.tensor(f["mask"], device=dev)
-                    m[:M, :M] = torch.where((mask == 2) | (mask == 3), 1.0, 0.2).float()
-                    stream.synchronize()
-                    s.close()
+                else:
+                    s.set_config(solve_config(c))
+                s.set_inputs(**{k: f[k] for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
+                vel = torch.empty((M, M, 2), dtype=torch.float64, device=dev)
+                s.set_initial_guess(torch.zeros_like(vel))
+                s.solve(out=vel)
+                st = s.stats()
+                x = features(s, 1)
+                hh, ww = x.shape[:2]
+                t = target_image(vel, hh, ww)
+                m = torch.zeros((hh, ww), dtype=torch.float32, device=dev)
+                mask = torch.tensor(f["mask"], device=dev)
+                m[:M, :M] = torch.where((mask == 2) | (mask == 3), 1.0, 0.2).float()
                 out[q] = (x, t, m)
-                stats[q] = {"seed": seeds[q], "picard": st["picard_iterations"], "ksp": st["ksp_iterations"],
+                stats[q] = {"seed": seed, "picard": st["picard_iterations"], "ksp": st["ksp_iterations"],
                             "converged": st["converged"], "ms": st["kernel_ms"]}
                 if log:
-                    log(f"case {q} seed {seeds[q]}: {st['picard_iterations']} Picard, {st['kernel_ms']:.0f} ms")
-            except Exception as e:   # noqa: BLE001 - re-raised after the join
-                with lock:
-                    err.append(e)
-                return
-
-    threads = [threading.Thread(target=work) for _ in range(workers)]
-    for t in threads:
-        t.start()
-    for t in threads:
-        t.join()
-    if err:
-        raise err[0]
+                    log(f"case {q} seed {seed}: {st['picard_iterations']} Picard, {st['kernel_ms']:.0f} ms")
+        stream.synchronize()
+    finally:
+        if s is not None:
+            s.close()
     return out, stats
 
 

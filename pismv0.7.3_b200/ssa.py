@@ -60,6 +60,10 @@ class _Buf:
             t = a.to(torch.float64).contiguous()
             if tuple(t.shape) != tuple(shape):
                 t = t.reshape(shape)
+            if t.data_ptr() != a.data_ptr():
+                # the converted copy was written on torch's current stream; the library reads
+                # it on the handle's stream, which does not wait for that one
+                torch.cuda.current_stream(t.device).synchronize()
             self.keep, self.device = t, True
             self.ptr = C.cast(C.c_void_p(t.data_ptr()), _D)
         else:
@@ -163,12 +167,11 @@ class SSAFD:
         ci, _keep = self._inputs(self._fields, self._bc)
         self._check(self.lib.pism_gpu_ssa_set_inputs(self._h, C.byref(ci)), "set_inputs")
 
-    def solve_batch(self, members, net=None, stride: int = 1, streams: int = 1):
+    def solve_batch(self, members, net=None, stride: int = 1):
         """pism_gpu_ssa_solve_batch: members is a list of dicts with the set_inputs fields
         and optionally "ice_softness" and "velocity" (initial guess; output array or CUDA
         tensor).  Returns (velocities, stats) per member; a member whose solve failed has
-        stats["status"] != 0.  streams > 1: pism_gpu_ssa_solve_batch_concurrent with that
-        many members in flight."""
+        stats["status"] != 0."""
         n = len(members)
         arr = (CMember * max(n, 1))()
         stats = (CStats * max(n, 1))()
@@ -194,10 +197,7 @@ class SSAFD:
             keep += [bufs, vb]
             outs.append(vb.keep)
         nh = net._h if net is not None else None
-        if streams > 1:
-            rc = self.lib.pism_gpu_ssa_solve_batch_concurrent(self._h, nh, stride, n, arr, stats, streams)
-        else:
-            rc = self.lib.pism_gpu_ssa_solve_batch(self._h, nh, stride, n, arr, stats)
+        rc = self.lib.pism_gpu_ssa_solve_batch(self._h, nh, stride, n, arr, stats)
         if rc not in (_capi.OK, _capi.EKSP, _capi.EPICARD, _capi.ENAN, _capi.EZERODIAG):
             self._check(rc, "solve_batch")
         return outs, [stats[q].as_dict() for q in range(n)]

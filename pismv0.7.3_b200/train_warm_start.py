@@ -5,7 +5,7 @@
 1. Training data: ``--cases`` seeded synthetic ice sheets at 401 x 401 (10 km over the
    4000 km domain of the 801 x 801 benchmark, so the 801^2 inputs subsampled by 2 are drawn
    from the same distribution), each solved by the FP64 Picard / BiCGStab + multigrid path
-   (``learned.solve_config``), one solver handle at a time (``--workers``, see learned.generate).
+   (``learned.solve_config``) on one solver handle.
    ``--gen-seconds`` caps the generation time; the cases solved by then are used.
 2. Training: Adam on random ``--crop``^2 crops (flips / transposes), weighted MSE on
    asinh(u / 10 m/yr) (weight 1 on ice, 0.2 off ice), with the network's own CUDA kernels.
@@ -40,7 +40,6 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--cases", type=int, default=2000)
     ap.add_argument("--val-cases", type=int, default=16)
-    ap.add_argument("--workers", type=int, default=1)
     ap.add_argument("--gen-seconds", type=float, default=600.0)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=16)
@@ -70,16 +69,16 @@ def main(argv=None):
     t0 = time.perf_counter()
     seeds = list(range(args.cases))
     data, stats = [], []
-    chunk = max(args.workers * 8, 32)
+    chunk = 32
     for start in range(0, len(seeds), chunk):
         if time.perf_counter() - t0 > args.gen_seconds:
             break
-        d, s = L.generate(seeds[start:start + chunk], workers=args.workers)
+        d, s = L.generate(seeds[start:start + chunk])
         data += d
         stats += s
         log(f"generated {len(data)} cases in {time.perf_counter() - t0:.0f} s")
     gen_s = time.perf_counter() - t0
-    val, _ = L.generate(list(range(1_000_000, 1_000_000 + args.val_cases)), workers=args.workers)
+    val, _ = L.generate(list(range(1_000_000, 1_000_000 + args.val_cases)))
     report["generation"] = {"cases": len(data), "seconds": gen_s,
                             "mean_picard": float(np.mean([s["picard"] for s in stats])),
                             "unconverged": int(sum(1 for s in stats if not s["converged"]))}

@@ -1,8 +1,9 @@
 """Generate tests/golden/reference_goldens.json from the reference tree.
 
-Run in a container that has the reference checkout (default /root/reference):
+Run where the reference checkout is present, naming its root (or setting
+PISM_REFERENCE_ROOT):
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 What it records (nothing here is run at test time; the JSON is committed):
 
@@ -126,4 +127,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PISM_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set PISM_REFERENCE_ROOT)")
+    main(root)

@@ -3,7 +3,7 @@ import json
 
 import pytest
 
-from pism_b200.autotune import Autotuner, tune_ensemble_streams
+from pism_b200.autotune import Autotuner
 
 
 class FakeClock:
@@ -22,7 +22,7 @@ class FakeClock:
 def make(tmp_path, repeats=3, warmup=1):
     clock = FakeClock()
     tuner = Autotuner(str(tmp_path / "tune.json"), repeats=repeats, warmup=warmup, timer=clock,
-                      device=lambda: "B200-fake")
+                      device=lambda: "B200-fake", library=lambda: "lib-a")
     return tuner, clock
 
 
@@ -57,10 +57,10 @@ def test_cache_is_reused_and_keyed_by_device_and_workload(tmp_path):
     cands = [{"streams": 1}, {"streams": 2}]
     tuner.choose({"grid": [401, 401]}, cands, lambda c: None)
     n = clock.calls
-    again = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "B200-fake")
+    again = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "B200-fake", library=lambda: "lib-a")
     assert again.choose({"grid": [401, 401]}, cands, lambda c: pytest.fail("ran despite the cache")) == {"streams": 1}
     assert clock.calls == n
-    other_dev = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "other")
+    other_dev = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "other", library=lambda: "lib-a")
     other_dev.choose({"grid": [401, 401]}, cands, lambda c: None)
     assert clock.calls > n
     # a cached choice that is no longer a candidate is tuned again
@@ -77,24 +77,65 @@ def test_rejects_bad_arguments(tmp_path):
         tuner.choose({"w": 3}, [], lambda c: None)
 
 
-def test_ensemble_streams_through_the_solver_interface(tmp_path):
-    """tune_ensemble_streams drives solve_batch(streams=...) and returns the fastest count."""
+def test_another_library_build_is_tuned_again(tmp_path):
+    """the cache key holds the library's fingerprint: a choice made with other kernels is not reused"""
+    tuner, clock = make(tmp_path)
+    clock.cost = 1.0
+    cands = [{"streams": 1}, {"streams": 2}]
+    tuner.choose({"grid": [401, 401]}, cands, lambda c: None)
+    n = clock.calls
+    rebuilt = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "B200-fake", library=lambda: "lib-b")
+    rebuilt.choose({"grid": [401, 401]}, cands, lambda c: None)
+    assert clock.calls > n
+
+
+def test_a_candidate_with_another_answer_is_never_chosen(tmp_path):
+    """verify(candidate, answer, reference answer): the first candidate's answer is the
+    reference; a faster candidate whose answer differs is rejected and recorded"""
+    tuner, clock = make(tmp_path, repeats=1, warmup=0)
+    costs = {"a": 5.0, "b": 1.0, "c": 3.0}
+    answers = {"a": 42, "b": 41, "c": 42}
+
+    def run(c):
+        clock.cost = costs[c["x"]]
+        return answers[c["x"]]
+
+    best = tuner.choose({"w": 9}, [{"x": "a"}, {"x": "b"}, {"x": "c"}], run,
+                        verify=lambda cand, out, ref: out == ref)
+    assert best == {"x": "c"}
+    assert tuner.last_rejected == [{"x": "b"}]
+    # the cached entry keeps the rejection
+    again = Autotuner(str(tmp_path / "tune.json"), timer=clock, device=lambda: "B200-fake", library=lambda: "lib-a")
+    assert again.choose({"w": 9}, [{"x": "a"}, {"x": "b"}, {"x": "c"}], lambda c: pytest.fail("ran")) == {"x": "c"}
+    assert again.last_rejected == [{"x": "b"}]
+
+
+def test_mg_post_blocks_through_the_solver_interface(tmp_path):
+    """tune_mg_post_blocks: the launch shape changes the time, never the answer; a candidate
+    whose velocities differ from the default's is rejected"""
+    import numpy as np
+    from pism_b200.autotune import tune_mg_post_blocks
+    from pism_b200.config import SSAConfig
     tuner, clock = make(tmp_path, repeats=1, warmup=0)
 
     class Solver:
-        shape = (41, 41)
+        shape = (801, 801)
 
         def __init__(self):
-            self.seen = []
+            self.cfg = None
 
-        def solve_batch(self, members, net=None, stride=1, streams=1):
-            self.seen.append(streams)
-            clock.cost = {1: 8.0, 2: 5.0, 4: 3.0, 8: 4.0}[streams]
-            return [], []
+        def set_config(self, c):
+            self.cfg = c
+
+        def solve(self):
+            b = self.cfg.mg_post_blocks_per_sm
+            clock.cost = {0: 130.0, 3: 120.0, 2: 110.0}[b]
+            return np.ones(4) * (2.0 if b == 2 else 1.0)   # the 2-block run "differs"
 
     s = Solver()
-    assert tune_ensemble_streams(s, [{}] * 8, tuner=tuner) == 4
-    assert s.seen == [1, 2, 4, 8]
+    base = SSAConfig(pc_type="mg", precision="mixed")
+    assert tune_mg_post_blocks(s, base, prime=lambda: None, tuner=tuner) == 3
+    assert s.cfg is base
 
 
 def test_launch_mode_through_the_solver_interface(tmp_path):
@@ -116,6 +157,7 @@ def test_launch_mode_through_the_solver_interface(tmp_path):
         def solve(self):
             self.log.append(self.cfg.graphs)
             clock.cost = {2: 130.0, 3: 120.0}[self.cfg.graphs]
+            return [1.0, 2.0]
 
     s = Solver()
     base = SSAConfig(pc_type="mg", precision="mixed")
