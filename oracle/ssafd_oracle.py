@@ -1133,3 +1133,68 @@ def petsc_gmres_bjacobi(A, b, x0, Mx, My, nranks=1, rtol=1e-5, maxit=10000, rest
     x = np.empty_like(xp)
     x[perm] = xp
     return x, its.value, reason
+
+
+def picard_native(grid: Grid, cfg: Config, inp: Inputs, hardness, b, vel0, reg, underrelax=1.0, nranks=1,
+                  nthreads=0, ksp_rtol=1e-8, max_iterations=None, picard_rtol=None, ksp_maxit=10000, restart=30):
+    """SSAFD::picard_manager on the host cores in native code (ssafd_cpu.cc): the same
+    arithmetic as SSAFDOracle.picard_manager with linear="petsc" (nu*H, drag, the 18-column
+    assembly in PETSc's rank-major order, GMRES(30) + block Jacobi / ILU(0) with one block
+    per rank, under-relaxation, norms, stopping test).  No calving-front boundary condition,
+    nu_bedrock or sub-grid grounding line (the benchmark sheet uses none of them).
+
+    Returns (velocity, info) with info = {"status": 0 converged / 1 Picard limit / < 0 KSP
+    reason, "picard_iterations", "nuH_norm", "nuH_norm_change", "ksp_iterations" [per
+    iteration], "t_nuH", "t_assemble", "t_ksp" [seconds per iteration]}."""
+    import ctypes
+    if cfg.calving_front_stress_boundary_condition or cfg.nu_bedrock_set or cfg.sub_groundingline:
+        raise ValueError("picard_native: CFBC, nu_bedrock and sub_groundingline are not restated natively")
+    lib = _ksp_lib()
+    if not hasattr(lib, "_picard_bound"):
+        P = ctypes.POINTER
+        D, I = ctypes.c_double, ctypes.c_int
+        lib.ssafd_cpu_picard.restype = I
+        lib.ssafd_cpu_picard.argtypes = [I, I, P(D), P(D), P(I), P(D), P(D), P(I), P(D), P(D), P(I), I, P(I), I, I,
+                                         D, D, I, I, D, D, P(I), P(D), P(D), P(I), P(D), P(D), P(D)]
+        lib._picard_bound = True
+    Mx, My = grid.Mx, grid.My
+    n_it = max_iterations if max_iterations is not None else cfg.max_iterations_ssafd
+    rtol = picard_rtol if picard_rtol is not None else cfg.ssafd_relative_convergence
+    par = np.array([grid.dx, grid.dy, cfg.ssa_Glen_exponent, cfg.ssa_enhancement_factor, schoof_reg(cfg),
+                    cfg.min_thickness_strength_extension_ssa, cfg.constant_nu_strength_extension_ssa,
+                    cfg.plastic_regularization, 1.0 if cfg.do_pseudo_plastic_till else 0.0, cfg.pseudo_plastic_q,
+                    cfg.pseudo_plastic_uthreshold, cfg.sliding_scale_factor_reduces_tauc,
+                    cfg.beta_ice_free_bedrock, cfg.scaling], dtype=np.float64)
+    perm, starts = petsc_order(Mx, My, nranks)
+    H = np.ascontiguousarray(inp.thickness, dtype=np.float64)
+    mask = np.ascontiguousarray(as_int(inp.mask), dtype=np.int32)
+    tauc = np.ascontiguousarray(inp.tauc, dtype=np.float64)
+    hard = np.ascontiguousarray(hardness, dtype=np.float64)
+    bc = None
+    if inp.bc_mask is not None and inp.bc_values is not None:
+        bc = np.ascontiguousarray(as_int(inp.bc_mask) == 1, dtype=np.int32)
+    bb = np.ascontiguousarray(b, dtype=np.float64).ravel()
+    vel = np.ascontiguousarray(np.array(vel0, dtype=np.float64).reshape(Mx, My, 2))
+    perm = np.ascontiguousarray(perm, dtype=np.int32)
+    starts = np.ascontiguousarray(starts, dtype=np.int32)
+    its = np.zeros(n_it, dtype=np.int32)
+    t_nuH, t_asm, t_ksp = np.zeros(n_it), np.zeros(n_it), np.zeros(n_it)
+    npic = ctypes.c_int(0)
+    norm, change = ctypes.c_double(0), ctypes.c_double(0)
+    P = ctypes.POINTER
+
+    def dp(a):
+        return a.ctypes.data_as(P(ctypes.c_double))
+
+    def ip(a):
+        return a.ctypes.data_as(P(ctypes.c_int)) if a is not None else None
+
+    st = lib.ssafd_cpu_picard(Mx, My, dp(par), dp(H), ip(mask), dp(tauc), dp(hard), ip(bc), dp(bb), dp(vel),
+                              ip(perm), len(starts) - 1, ip(starts), nthreads, n_it, rtol, ksp_rtol, ksp_maxit,
+                              restart, reg, underrelax, ctypes.byref(npic), ctypes.byref(norm),
+                              ctypes.byref(change), ip(its), dp(t_nuH), dp(t_asm), dp(t_ksp))
+    k = npic.value
+    m = k if st >= 0 else k + 1
+    return vel, {"status": st, "picard_iterations": k, "nuH_norm": norm.value, "nuH_norm_change": change.value,
+                 "ksp_iterations": its[:m].tolist(), "t_nuH": t_nuH[:k].tolist(), "t_assemble": t_asm[:k].tolist(),
+                 "t_ksp": t_ksp[:k].tolist()}
