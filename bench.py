@@ -3,8 +3,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size M]
 
 A step is one complete SSA solve (SSAFD::solve: driving stress, hardness, the
-Picard loop with its linear solves) of the seeded synthetic sheet (plastic till,
-Picard nu*H tolerance 1e-4).  Two solver set-ups run on the same inputs:
+Picard loop with its linear solves) of the seeded synthetic sheet (plastic till).
+Two solver set-ups run on the same inputs and the same Picard tolerance:
 
 * ``plain``: FP64 throughout, every Picard linear solve to KSP rtol 1e-8
   (BiCGStab + aggregation multigrid), from a zero initial guess;
@@ -13,17 +13,20 @@ Picard nu*H tolerance 1e-4).  Two solver set-ups run on the same inputs:
   inner BiCGStab + FP32 multigrid inside FP64 iterative refinement, and the learned
   warm start when trained weights are present.
 
-The metric is milliseconds per solve (lower is better) of ``--mode`` (default
-fast); the other set-up is timed once beside it and the fast result's velocity
-error against the plain FP64 result is reported.  With N GPUs every rank solves
-its own replica (no data-path collective: the solve does not shard) and
-``value`` is the job's time per solve = max-over-ranks step time / N.
+The Picard tolerance defaults to a relative nu*H change of 1e-6, where the fast
+answer is within 1e-5 of the converged FP64 solve (``velocity_error_vs_fp64_oracle``
+in the line); the configuration text's 1e-4 is timed beside it
+(``comparison.accuracy.picard_rtol_1e-4``).  The metric is milliseconds per solve
+(lower is better) of ``--mode`` (default fast); the other set-up is timed beside it.
+With N GPUs every rank solves its own replica (no data-path collective: the solve
+does not shard) and ``value`` is the job's time per solve = max-over-ranks step
+time / N.
 
-``--impl reference`` times the CPU restatement of the reference's own path
-(numpy assembly of the SSAFD matrix + PETSc-style GMRES(30) / block-Jacobi
-ILU(0) with one block per host thread, oracle/) on a bounded sample of the same
-solve: the first few Picard iterations, scaled to a full solve by the GPU run's
-Picard count for the same input.
+``--impl reference`` times the native CPU restatement of the reference's path
+(oracle/ssafd_cpu.cc + oracle/ksp_cpu.cc: nu*H, drag and the 18-column assembly, then
+PETSc's default GMRES(30) / block-Jacobi ILU(0) with one block per host thread) on a
+bounded sample of the same solve, the first Picard iterations, scaled to the whole
+solve by one complete run of the same restatement on this sheet.
 """
 from __future__ import annotations
 
@@ -41,9 +44,19 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(REPO, "pismv0.7.3_b200")
 METRIC = "SSA solve ms at 801² to rel resid 1e-6: learned+FP32 vs plain FP64, 1 B200"
-# Picard iterations of the plain FP64 GPU solve of the 801^2 seed-0 sheet (measured; the
-# reference arm scales its CPU sample to a whole solve with it)
-DEFAULT_PICARD_801 = 184
+# The headline Picard tolerance: at nu*H change 1e-6 the fast set-up's answer is within 1e-5
+# (relative L2 and Linf) of the converged FP64 solve, the accuracy the metric is stated at;
+# the configuration text's 1e-4 leaves both set-ups ~1e-3 from it and is reported beside.
+HEADLINE_PICARD_RTOL = 1e-6
+# fast set-up: lagged multigrid coarse levels (rebuilt once the summed relative nu*H change
+# since the last build reaches this)
+FAST_MG_LAG = 0.0
+# launch mode of the timed solves (2: graph-resident Krylov loops, 3: the whole Picard loop as
+# one graph); the other one is timed beside it
+DEFAULT_GRAPHS = 2
+# In-solve DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control
+# none) of one inner iteration's kernels on the 801^2 sheet, per (grid, precision)
+INNER_ITERATION_TRAFFIC: dict = {}
 
 
 def _package():
@@ -120,12 +133,13 @@ def build_case(M, pc="mg"):
     return g, c, f, meta
 
 
-def fast_config(c, precision="mixed", factor=1.0, rtol_max=1e-1):
+def fast_config(c, precision="mixed", factor=1.0, rtol_max=1e-1, mg_lag=0.0):
     """The fast set-up: inexact Picard with FP32 inner solves (the linear solve of a Picard
-    iteration only as accurate as the last relative nu*H change, at most 1e-1); the accepted
-    linear solve reaches relative residual 1e-6 in FP64."""
+    iteration only as accurate as the last relative nu*H change, at most 1e-1), multigrid
+    coarse levels rebuilt once the summed relative nu*H change reaches mg_lag (0: every
+    Picard iteration); the accepted linear solve reaches relative residual 1e-6 in FP64."""
     return c.copy(precision=precision, ksp_rtol=1e-6, ksp_rtol_adaptive=True, ksp_rtol_factor=factor,
-                  ksp_rtol_max=rtol_max)
+                  ksp_rtol_max=rtol_max, mg_rebuild_rtol=mg_lag)
 
 
 def ms_per_step_local(total_ms, steps):
@@ -177,25 +191,114 @@ def iteration_bytes(M, precision):
     return krylov * N0 + 2 * vcycle
 
 
-def cpu_reference_sample(M, picard_sample, picard_full, nthreads):
-    """The oracle port on the host cores: `picard_sample` Picard iterations of the
-    reference algorithm (PETSc-style GMRES(30) + block Jacobi ILU(0), one block
-    per thread), scaled to `picard_full` iterations."""
+def iteration_roofline(s, c, M, stream, flush, dev):
+    """one inner Krylov iteration of the solver `s` (inputs set, nu*H at the last solve's):
+    a tight linear solve from zero after one untimed one, L2 flushed before it; its
+    algorithmic bytes per iteration over the time per iteration"""
+    import torch
+    s.set_config(c.copy(ksp_rtol=1e-10, ksp_rtol_adaptive=False))
+    xk = torch.zeros((M, M, 2), dtype=torch.float64, device=dev)
+    s.linear_solve(xk)                     # warm-up
+    xk.zero_()
+    flush.fill_(1.0)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    lin_its, lin_res = s.linear_solve(xk)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    lin_ms = ev[0].elapsed_time(ev[1])
+    it_ms = lin_ms / max(1, lin_its)
+    it_bytes = iteration_bytes(M, c.precision)
+    return {"achieved": it_bytes / (it_ms * 1e-3) / 1e9, "unit": "GB/s", "bytes_per_launch": it_bytes,
+            "launch_ms": it_ms, "timed": f"linear solve to rtol 1e-10: {lin_its} iterations in {lin_ms:.2f} ms"}
+
+
+def working_set_bytes(M, precision):
+    """bytes the inner iteration touches (every array once): the fine level's Krylov vectors,
+    nu*H, beta, flags, D^-1 and the multigrid hierarchy"""
+    N0, lev = M * M, mg_levels(M)
+    krylov = (9 if precision == "mixed" else 9 * 2) * 8 * N0   # r, rhat, p, v, s, t, phat, shat, x
+    fine = (8 + 4 + 4 + 16 + 8) * N0                           # FP32 nu*H, beta, flags, D^-1, rhs
+    return krylov + fine + (9 * 16 + 16 + 8 + 8) * sum(lev)
+
+
+def large_roofline(c, stream, flush, dev, peak, M=1601):
+    """the inner iteration on a 1601^2 sheet of the same construction (2.5 km): its working
+    set is several times the 126 MB L2, so the iteration reads HBM"""
+    import torch
+    from pism_b200.ssa import SSAFD
+    g, cl, f, _ = build_case(M)
+    cfg = c.copy(ssafd_relative_convergence=cl.ssafd_relative_convergence)
+    s = SSAFD(g, cfg.copy(ssafd_relative_convergence=1e-2, max_iterations_ssafd=300), device=dev.index)
+    try:
+        s.set_stream(stream.cuda_stream)
+        s.set_inputs(**{k: torch.tensor(f[k], dtype=torch.float64, device=dev)
+                        for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
+        s.set_initial_guess(torch.zeros((M, M, 2), dtype=torch.float64, device=dev))
+        s.solve(out=torch.empty((M, M, 2), dtype=torch.float64, device=dev))   # nu*H of a partly converged state
+        r = iteration_roofline(s, cfg, M, stream, flush, dev)
+    finally:
+        s.close()
+    r.update(grid=[M, M], frac=r["achieved"] / peak, working_set_bytes=working_set_bytes(M, c.precision),
+             l2_bytes=torch.cuda.get_device_properties(dev).L2_cache_size)
+    return r
+
+
+# One complete run of the native CPU restatement (oracle/ssafd_cpu.cc: nu*H, drag, 18-column
+# assembly, PETSc-style GMRES(30) + block Jacobi / ILU(0), norms) on the 801^2 seed-0 sheet at
+# KSP rtol 1e-8 from a zero guess, to Picard tolerance 1e-6 (the tolerance-1e-4 solve is its
+# prefix), on 8 host threads: seconds after each of the first iterations and for the whole
+# solve.  The timed CPU baseline runs the first CPU_SAMPLE_PICARD iterations on the host
+# and scales them by whole / first from this run (profiles/cpu_baseline_801_native.md).
+CPU_FULL_RUN_801 = None
+CPU_SAMPLE_PICARD = 3
+
+
+def cpu_estimate(sample_s, k, picard_rtol, full=None):
+    """(estimated ms of the whole CPU solve, how) from the first k iterations' seconds"""
+    full = full if full is not None else CPU_FULL_RUN_801
+    if full is None or k > len(full["cumulative_s"]):
+        return None, "no complete CPU run on record"
+    key = f"{picard_rtol:g}"
+    if key not in full["total_s"]:
+        return None, f"no complete CPU run at Picard tolerance {key}"
+    ratio = full["total_s"][key] / full["cumulative_s"][k - 1]
+    how = (f"first {k} Picard iterations timed on the host cores ({sample_s:.1f} s), x {ratio:.2f} = whole / "
+           f"first-{k} time of one complete run of the same restatement on this sheet at Picard tolerance {key} "
+           f"({full['picard_iterations'][key]} iterations, {full['total_s'][key]:.0f} s on {full['threads']} "
+           f"threads)")
+    return sample_s * ratio * 1e3, how
+
+
+def cpu_reference_sample(M, picard_sample, nthreads, picard_rtol):
+    """The native CPU restatement of the reference's Picard loop (oracle/ssafd_cpu.cc) on the
+    host cores: driving stress / right-hand side / hardness (oracle.prepare), then
+    `picard_sample` Picard iterations from a zero guess (nu*H, drag, assembly, PETSc-style
+    GMRES(30) + block Jacobi ILU(0) with one block per thread, norms).  Returns (seconds,
+    Picard iterations done)."""
     sys.path.insert(0, REPO)
     from oracle import ssafd_oracle as O
     g, c, f, _ = build_case(M)
+    c.ssafd_relative_convergence = picard_rtol
     G, Cc, I = O.from_case(g, c, f)
-    o = O.SSAFDOracle(G, Cc, I, linear="petsc", ksp_rtol=c.ksp_rtol, nranks=nthreads, nthreads=nthreads)
-    Cc.max_iterations_ssafd = picard_sample
     t0 = time.perf_counter()
-    try:
-        o.prepare()
-        o.picard_manager(Cc.epsilon_ssa, 1.0)
-    except O.PicardFailure:
-        pass
-    dt = time.perf_counter() - t0
-    done = max(1, o.stats.picard_iterations)
-    return dt * 1e3 / done * picard_full, done, dt
+    o = O.SSAFDOracle(G, Cc, I)
+    o.prepare()
+    _, info = O.picard_native(G, Cc, I, o.hardness, o.b, np.zeros((M, M, 2)), Cc.epsilon_ssa, nranks=nthreads,
+                              nthreads=nthreads, ksp_rtol=c.ksp_rtol, max_iterations=picard_sample,
+                              picard_rtol=picard_rtol)
+    return time.perf_counter() - t0, info["picard_iterations"]
+
+
+def cpu_baseline(M, picard_rtol, nthreads, picard_gpu=None):
+    """the cpu_baseline object: the host-core sample and its whole-solve estimate"""
+    dt, done = cpu_reference_sample(M, CPU_SAMPLE_PICARD, nthreads, picard_rtol)
+    est, how = (cpu_estimate(dt, done, picard_rtol) if M == 801 else (None, "no complete CPU run at this size"))
+    if est is None and picard_gpu:
+        est = dt * 1e3 / max(1, done) * picard_gpu
+        how = (f"first {done} Picard iterations timed on the host cores ({dt:.1f} s), scaled by the iteration count "
+               f"of the plain GPU solve ({picard_gpu}; {how})")
+    return {"value": est, "unit": "ms", "cores": nthreads, "kind": "port", "sample": how}
 
 
 def run_reference(args):
@@ -203,28 +306,35 @@ def run_reference(args):
     if rank != 0:
         return 0
     nthreads = os.cpu_count() or 1
-    picard_full = args.picard_full or DEFAULT_PICARD_801
-    vals = []
-    sample = None
+    vals, sample = [], None
     for k in range(args.warmup + args.steps):
-        ms, done, dt = cpu_reference_sample(args.size, args.cpu_picard, picard_full, nthreads)
+        cb = cpu_baseline(args.size, args.picard_rtol, nthreads, picard_gpu=args.picard_full or None)
         if k >= args.warmup:
-            vals.append(ms)
-            sample = f"first {done} Picard iterations of the {args.size}^2 seed-0 solve ({dt:.1f} s), " \
-                     f"scaled to {picard_full} Picard iterations"
-    v = float(np.mean(vals))
+            vals.append(cb["value"])
+            sample = cb["sample"]
+    v = float(np.mean(vals)) if all(x is not None for x in vals) else None
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"SSAFD solve, synthetic ice sheet {args.size}x{args.size} at "
-                               f"{4000 / (args.size - 1):.0f} km, plastic till, Picard 1e-4, KSP 1e-8",
-                   "grid": [args.size, args.size], "seed": 0},
+                               f"{4000 / (args.size - 1):.0f} km, plastic till, Picard {args.picard_rtol:g}, KSP 1e-8",
+                   "grid": [args.size, args.size], "seed": 0,
+                   "implementation": "native restatement of SSAFD's Picard loop with PETSc's default KSP "
+                                     "(oracle/ssafd_cpu.cc, oracle/ksp_cpu.cc), one block-Jacobi block per thread"},
         "cpu_baseline": {"value": v, "unit": "ms", "cores": nthreads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def members_of_rank(rank: int, world: int, per_gpu: int) -> list:
+    """the ensemble members rank `rank` of `world` solves: a contiguous block of `per_gpu`
+    member indices, disjoint between ranks, the whole job covering 0 .. world * per_gpu - 1"""
+    if not (0 <= rank < world) or per_gpu < 0:
+        raise ValueError("0 <= rank < world and per_gpu >= 0")
+    return list(range(rank * per_gpu, (rank + 1) * per_gpu))
 
 
 def ensemble_member(q, M=401):
@@ -258,7 +368,7 @@ def run_ensemble(args):
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     M = 401
-    mine = list(range(rank * args.members, (rank + 1) * args.members))   # weak scaling: members per GPU fixed
+    mine = members_of_rank(rank, world, args.members)   # weak scaling: members per GPU fixed
     names = ("thickness", "surface", "bed", "mask", "tauc", "melange")
     cases = [ensemble_member(q, M) for q in mine]
     g, c0 = cases[0][0], cases[0][1]
@@ -342,8 +452,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--size", type=int, default=801)
-    ap.add_argument("--cpu-picard", type=int, default=2, help="Picard iterations in the CPU sample")
-    ap.add_argument("--picard-full", type=int, default=0)
+    ap.add_argument("--picard-full", type=int, default=0,
+                    help="reference arm away from 801^2: Picard iterations to scale the CPU sample by")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--apply-launches", type=int, default=50)
     ap.add_argument("--pc", default="mg", choices=["mg", "bjacobi"])
@@ -359,21 +469,26 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="fast set-up from a zero initial guess")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the converged FP64 reference solve")
     ap.add_argument("--no-compare", action="store_true", help="skip the other set-up (and the accuracy reference)")
+    ap.add_argument("--no-large", action="store_true", help="skip the larger-than-L2 roofline point")
     ap.add_argument("--workload", default="solve", choices=["solve", "ensemble"],
                     help="ensemble: members solved/s of a 64-member 401^2 ensemble (its own JSON line)")
     ap.add_argument("--members", type=int, default=64)
-    ap.add_argument("--picard-rtol", type=float, default=None,
-                    help="Picard nu*H tolerance of both set-ups (default: the configuration's 1e-4)")
+    ap.add_argument("--picard-rtol", type=float, default=HEADLINE_PICARD_RTOL,
+                    help="Picard nu*H tolerance of both set-ups (default 1e-6: the tolerance at which the fast "
+                         "answer is within 1e-5 of the converged FP64 solve)")
     ap.add_argument("--profile", action="store_true",
                     help="time the solve only (no end-to-end, roofline, comparison or CPU runs): for kernel profilers")
     ap.add_argument("--mg-post-blocks", type=int, default=None, choices=[1, 2, 3, 4],
                     help="resident blocks per SM the coarse-level post-smoothing grid is sized for (default 4)")
-    ap.add_argument("--graphs", type=int, default=2, choices=[0, 1, 2, 3],
+    ap.add_argument("--graphs", type=int, default=DEFAULT_GRAPHS, choices=[0, 1, 2, 3],
                     help="Krylov launch mode: 2 graph-resident loops, 1 replayed graphs, 0 direct (for profilers), "
                          "3 the whole Picard loop as one graph")
     ap.add_argument("--ksp-factor", type=float, default=1.0,
                     help="fast set-up: KSP rtol of a Picard iteration = factor x the last relative nu*H change")
     ap.add_argument("--ksp-max", type=float, default=1e-1, help="fast set-up: loosest KSP rtol of a Picard iteration")
+    ap.add_argument("--mg-lag", type=float, default=FAST_MG_LAG,
+                    help="fast set-up: rebuild the multigrid coarse levels once the summed relative nu*H change "
+                         "reaches this (0: every Picard iteration)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -398,13 +513,12 @@ def main():
     if args.mg_correction is not None:
         c_plain.mg_correction = args.mg_correction
     c_plain.verbosity = args.verbosity
-    if args.picard_rtol is not None:
-        c_plain.ssafd_relative_convergence = args.picard_rtol
-        c_plain.max_iterations_ssafd = 5000
+    c_plain.ssafd_relative_convergence = args.picard_rtol
+    c_plain.max_iterations_ssafd = 5000
     c_plain.graphs = args.graphs
     if args.mg_post_blocks is not None:
         c_plain.mg_post_blocks_per_sm = args.mg_post_blocks
-    c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max)
+    c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max, mg_lag=args.mg_lag)
     if args.inner_rtol is not None:
         c_fast.mixed_inner_rtol = args.inner_rtol
     c, c_other = (c_fast, c_plain) if args.mode == "fast" else (c_plain, c_fast)
@@ -414,6 +528,7 @@ def main():
         c.ksp_type = args.ksp
         if args.ksp == "gmres":
             c.precision = "fp64"
+            c.graphs = min(c.graphs, 2)
     if args.gmres_restart is not None:
         c.gmres_restart = args.gmres_restart
     M = args.size
@@ -439,16 +554,32 @@ def main():
         net = Lrn.UNet(1, hh, ww, device=local, params=np.load(Lrn.DEFAULT_WEIGHTS)["params"])
         net.set_stream(stream.cuda_stream)
 
-    def prime(host_zero=None):
+    def prime(solver, learned, host_zero=None):
         """the initial guess of one solve: the network's prediction, or zero"""
-        if net is not None:
-            Lrn.learned_guess(s, net, stride)
+        if learned:
+            Lrn.learned_guess(solver, net, stride)
         else:
-            s.set_initial_guess(zero if host_zero is None else host_zero)
+            solver.set_initial_guess(zero if host_zero is None else host_zero)
 
     def step():
-        prime()
+        prime(s, net is not None)
         s.solve(out=out)
+
+    def timed(solver, learned, result, reps=2):
+        """mean device time of `reps` solves after one untimed one, L2 flushed before each"""
+        prime(solver, learned)
+        solver.solve(out=result)
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prime(solver, learned)
+            solver.solve(out=result)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.mean(ts)), solver.stats()
 
     for _ in range(args.warmup):
         step()
@@ -460,9 +591,7 @@ def main():
     torch.cuda.synchronize()
     total_ms = 0.0
     launches = 0
-    picard = []
-    ksp = []
-    refine = []
+    picard, ksp, refine, rebuilds = [], [], [], []
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -477,6 +606,9 @@ def main():
         picard.append(st["picard_iterations"])
         ksp.append(st["ksp_iterations"])
         refine.append(st["refinement_steps"])
+        rebuilds.append(st["mg_rebuilds"])
+    if world > 1:
+        dist.barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     vel_mode = out.clone()
@@ -490,39 +622,29 @@ def main():
     ms_per_step = max_over_ranks(total_ms, dev) / args.steps
     value = job_time_per_solve(ms_per_step, world)
 
-    other_ms, st_other, vel_error, accuracy = None, {"picard_iterations": None, "ksp_iterations": None}, None, None
+    def errors(a, ref):
+        d = a - ref
+        return {"l2_rel": float(d.norm() / ref.norm()), "linf_rel": float(d.abs().max() / ref.abs().max())}
+
+    other_ms, st_other, vel_error, accuracy, headline_error = None, {"picard_iterations": None,
+                                                                     "ksp_iterations": None}, None, None, None
     if not args.no_compare:
-        # the other set-up on the same inputs, timed once (after one untimed solve)
+        # the other set-up on the same inputs and tolerance, timed like a step
         s_other = SSAFD(g, c_other, device=local)
         s_other.set_stream(stream.cuda_stream)
         s_other.set_inputs(**dfields)
         out_other = torch.empty_like(out)
-        for rep in range(2):
-            flush.fill_(1.0)
-            s_other.set_initial_guess(zero)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            s_other.solve(out=out_other)
-            e1.record(stream)
-            torch.cuda.synchronize()
-        other_ms = e0.elapsed_time(e1)
-        st_other = s_other.stats()
+        other_ms, st_other = timed(s_other, args.mode == "plain" and net is not None, out_other)
         s_other.close()
         vel_fast, vel_plain = (vel_mode, out_other) if args.mode == "fast" else (out_other, vel_mode)
-
-        def errors(a, ref):
-            d = a - ref
-            return {"l2_rel": float(d.norm() / ref.norm()), "linf_rel": float(d.abs().max() / ref.abs().max())}
-
         vel_error = errors(vel_fast, vel_plain)
-        # Both set-ups stop Picard at a relative nu*H change of 1e-4, which leaves each of them
-        # ~1e-3 away from the fixed point along its own trajectory; their accuracy is measured
-        # against an FP64 solve continued from the plain answer to a nu*H change of 1e-8.
-        accuracy = None
         if not args.no_accuracy:
-            c_conv = c_plain.copy(ssafd_relative_convergence=min(1e-8, 0.01 * c_plain.ssafd_relative_convergence),
-                              ksp_rtol=1e-10, ksp_rtol_adaptive=True,
-                                  ksp_rtol_factor=0.1, ksp_rtol_max=1e-2, max_iterations_ssafd=5000, precision="fp64")
+            # the FP64 oracle answer: an FP64 Picard iteration continued from the plain answer to
+            # a nu*H change 100 x below the set-ups' tolerance (the GPU FP64 path equals the CPU
+            # oracle to 1e-8 relative, tests/test_gpu_parity*.py)
+            c_conv = c_plain.copy(ssafd_relative_convergence=min(1e-8, 0.01 * args.picard_rtol), ksp_rtol=1e-10,
+                                  ksp_rtol_adaptive=True, ksp_rtol_factor=0.1, ksp_rtol_max=1e-2,
+                                  max_iterations_ssafd=20000, precision="fp64", graphs=2)
             s_ref = SSAFD(g, c_conv, device=local)
             s_ref.set_stream(stream.cuda_stream)
             s_ref.set_inputs(**dfields)
@@ -537,86 +659,76 @@ def main():
                         "reference_converged": st_ref["converged"],
                         "plain_vs_reference": errors(vel_plain, vel_conv),
                         "fast_vs_reference": errors(vel_fast, vel_conv)}
-            # both set-ups again at Picard tolerance 1e-6, against the same converged solve
-            if args.picard_rtol is None:
-                def timed(cfg, learned):
-                    h = SSAFD(g, cfg.copy(ssafd_relative_convergence=1e-6, max_iterations_ssafd=5000), device=local)
+            headline_error = accuracy["fast_vs_reference" if args.mode == "fast" else "plain_vs_reference"]
+            # both set-ups at the configuration text's Picard tolerance 1e-4, against the same answer
+            if args.picard_rtol != 1e-4:
+                o4 = torch.empty_like(out)
+                pair = {}
+                for nm, cfg, learned in (("fast", c_fast, net is not None), ("plain", c_plain, False)):
+                    h = SSAFD(g, cfg.copy(ssafd_relative_convergence=1e-4, max_iterations_ssafd=300), device=local)
                     h.set_stream(stream.cuda_stream)
                     h.set_inputs(**dfields)
-                    o = torch.empty_like(out)
-                    for _ in range(2):
-                        flush.fill_(1.0)
-                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                        e0.record(stream)
-                        if learned:
-                            Lrn.learned_guess(h, net, stride)
-                        else:
-                            h.set_initial_guess(zero)
-                        h.solve(out=o)
-                        e1.record(stream)
-                        torch.cuda.synchronize()
-                    stt = h.stats()
+                    t, sh = timed(h, learned, o4)
                     h.close()
-                    return o, e0.elapsed_time(e1), stt
-                uf, tf, sf = timed(c_fast, net is not None)
-                up, tp, sp = timed(c_plain, False)
-                accuracy["picard_rtol_1e-6"] = {
-                    "fast_ms": tf, "fast_picard_iterations": sf["picard_iterations"],
-                    "plain_ms": tp, "plain_picard_iterations": sp["picard_iterations"],
-                    "plain_over_fast": tp / tf, "fast_vs_reference": errors(uf, vel_conv),
-                    "plain_vs_reference": errors(up, vel_conv)}
+                    pair[nm + "_ms"] = t
+                    pair[nm + "_picard_iterations"] = sh["picard_iterations"]
+                    pair[nm + "_vs_reference"] = errors(o4, vel_conv)
+                pair["plain_over_fast"] = pair["plain_ms"] / pair["fast_ms"]
+                accuracy["picard_rtol_1e-4"] = pair
 
-    # end to end through the C-ABI with pinned host buffers: H2D inputs, solve, D2H velocity
+    # end to end through the C-ABI with pinned host buffers, every step: H2D inputs, the
+    # initial guess, the solve, D2H velocity
     hfields = {k: torch.tensor(f[k], dtype=torch.float64).pin_memory() for k in names}
     hzero = torch.zeros((M, M, 2), dtype=torch.float64).pin_memory()
     hout = torch.empty((M, M, 2), dtype=torch.float64).pin_memory()
     h2d = sum(v.numel() * 8 for v in hfields.values()) + (0 if net is not None else hzero.numel() * 8)
     d2h = hout.numel() * 8
     e2e_ms = 0.0
-    for _ in range(max(1, min(args.steps, 2))):
+    for _ in range(max(1, args.steps)):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s.set_inputs(**{k: v.numpy() for k, v in hfields.items()})
-        prime(hzero.numpy())
+        prime(s, net is not None, hzero.numpy())
         s.solve(out=hout.numpy())
         torch.cuda.synchronize()
         e2e_ms += (time.perf_counter() - t0) * 1e3
-    e2e_ms /= max(1, min(args.steps, 2))
+    e2e_ms /= max(1, args.steps)
     e2e_value = job_time_per_solve(max_over_ranks(e2e_ms, dev), world)
+    e2e_same = bool(torch.equal(hout, vel_mode.cpu()))
 
     # Roofline of the hot loop: one inner BiCGStab + multigrid iteration (the kernels that
-    # repeat ~850 times per fast solve), timed live on a tight linear solve at the final nu*H
+    # repeat ~1000 times per fast solve), timed live on a tight linear solve at the final nu*H
     peak, peak_kind = _peaks()
-    s.set_config(c.copy(ksp_rtol=1e-10, ksp_rtol_adaptive=False))
-    xk = torch.zeros((M, M, 2), dtype=torch.float64, device=dev)
-    s.linear_solve(xk)                     # warm-up
-    xk.zero_()
-    flush.fill_(1.0)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    ev[0].record(stream)
-    lin_its, lin_res = s.linear_solve(xk)
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    lin_ms = ev[0].elapsed_time(ev[1])
-    it_ms = lin_ms / max(1, lin_its)
-    it_bytes = iteration_bytes(M, c.precision)
-    achieved = it_bytes / (it_ms * 1e-3) / 1e9
+    roof = iteration_roofline(s, c, M, stream, flush, dev)
     s.set_config(c)
-
-    # the FP64 matrix-free apply alone (the plain set-up's stencil)
+    roof.update(peak=peak, frac=roof["achieved"] / peak, peak_kind=peak_kind, bound="hbm",
+                traffic=INNER_ITERATION_TRAFFIC.get((M, c.precision)))
+    roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the iteration's 23 kernels, "
+                              "in-solve (--cache-control none), profiles/inner_iteration_traffic_801.md"
+                              if roof["traffic"] is not None else None)
+    roof["kernel"] = ("one inner BiCGStab + V(1,1) multigrid iteration: k32_p/v/s/t/x + 2 x (k_mg0_restrict, "
+                      "k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, k_mg0_post)"
+                      if c.precision == "mixed" else "one BiCGStab + V(1,1) multigrid iteration (FP64 Krylov vectors)")
+    # the FP64 matrix-free apply alone, each launch timed with L2 flushed before it (HBM-bound)
     x = torch.randn((M, M, 2), dtype=torch.float64, device=dev) * 1e-5
     y = torch.empty_like(x)
     for _ in range(5):
         s.apply(x, y)
-    flush.fill_(1.0)
-    ev[0].record(stream)
+    apply_ms = []
     for _ in range(args.apply_launches):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         s.apply(x, y)
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    apply_ms = ev[0].elapsed_time(ev[1]) / args.apply_launches
+        e1.record(stream)
+        torch.cuda.synchronize()
+        apply_ms.append(e0.elapsed_time(e1))
+    apply_ms = float(np.median(apply_ms))
     apply_bytes = 60 * N   # x 16, nu*H 16, beta 8, flags 4, y 16 per cell (neighbours counted once)
+    roof["fp64_apply"] = {"achieved": apply_bytes / (apply_ms * 1e-3) / 1e9, "bytes_per_launch": apply_bytes,
+                          "launch_ms": apply_ms, "frac": apply_bytes / (apply_ms * 1e-3) / 1e9 / peak,
+                          "cache": "cold: L2 flushed (256 MB write) before each launch, median of launches"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -628,11 +740,14 @@ def main():
                    "ksp": f"{'FGMRES(%d)' % c.gmres_restart if c.ksp_type == 'gmres' else 'BiCGStab'} + "
                           f"{'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'}",
                    "ksp_rtol": c.ksp_rtol, "ksp_rtol_adaptive": bool(c.ksp_rtol_adaptive),
+                   "picard_rtol": c.ssafd_relative_convergence, "graphs": c.graphs,
+                   "mg_rebuild_rtol": c.mg_rebuild_rtol,
                    "warm_start": (f"learned (U-Net, features at stride {stride})" if net is not None else "zero"),
                    "l2": "flushed (256 MB write) between steps",
                    "parallelism": f"replicas x{world}"},
+        "velocity_error_vs_fp64_oracle": headline_error,
         "solver": {"picard_iterations": picard, "ksp_iterations": ksp, "converged": st["converged"],
-                   "refinement_steps": refine,
+                   "refinement_steps": refine, "mg_rebuilds": rebuilds,
                    "strategy": st["strategy"], "final_linear_residual": st["final_linear_residual"]},
         "comparison": {"other_mode": "plain" if args.mode == "fast" else "fast", "other_ms": other_ms,
                        "other_picard_iterations": st_other["picard_iterations"],
@@ -641,65 +756,52 @@ def main():
                                            (other_ms / ms_per_step) if args.mode == "fast" else (ms_per_step / other_ms)),
                        "fast_velocity_error_vs_plain_fp64": vel_error,
                        "accuracy": accuracy},
-        "roofline": {"bound": "hbm",
-                     "kernel": ("one inner BiCGStab + V(1,1) multigrid iteration: k32_p/v/s/t/x + 2 x (k_mg0_restrict, "
-                                "k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, k_mg0_post)"
-                                if c.precision == "mixed" else
-                                "one BiCGStab + V(1,1) multigrid iteration (FP64 Krylov vectors)"),
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": it_bytes,
-                     "launch_ms": it_ms, "timed": f"linear solve to rtol 1e-10: {lin_its} iterations in {lin_ms:.2f} ms",
-                     "fp64_apply": {"achieved": apply_bytes / (apply_ms * 1e-3) / 1e9, "bytes_per_launch": apply_bytes,
-                                    "launch_ms": apply_ms,
-                                    "frac": apply_bytes / (apply_ms * 1e-3) / 1e9 / peak}},
-        "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roof,
+        "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": max(1, args.steps), "same_velocity_as_timed": e2e_same},
         "gpu_launches": launches,
         "clocks": clocks,
     }
-    # the same solve with the whole Picard loop as one CUDA graph (graphs = 3), after all of
-    # the above: timed like a step (L2 flushed, mean of two after one untimed solve) and
-    # checked bit for bit against the timed answer; an error is reported, not raised
-    if not args.no_compare and args.graphs == 2 and c.ksp_type == "bicgstab":
+    # the same solve in the other launch mode (graph-resident loops <-> the whole Picard loop
+    # as one CUDA graph), after all of the above: timed like a step and checked bit for bit
+    # against the timed answer; an error is reported, not raised
+    if not args.no_compare and c.graphs in (2, 3) and c.ksp_type == "bicgstab":
+        other_graphs = 5 - c.graphs
         try:
-            s.set_config(c.copy(graphs=3))
-            step()
-            t3 = []
-            for _ in range(2):
-                flush.fill_(1.0)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                step()
-                e1.record(stream)
-                torch.cuda.synchronize()
-                t3.append(e0.elapsed_time(e1))
-            st3 = s.stats()
-            line["comparison"]["whole_solve_graph"] = {
-                "ms": float(np.mean(t3)), "graph_resident_loops_ms": ms_per_step_local(total_ms, args.steps),
-                "bitwise_equal": bool(torch.equal(out, vel_mode)), "picard_iterations": st3["picard_iterations"],
+            s.set_config(c.copy(graphs=other_graphs))
+            o3 = torch.empty_like(out)
+            t3, st3 = timed(s, net is not None, o3)
+            line["comparison"]["launch_mode"] = {
+                "graphs": other_graphs, "ms": t3, "timed_mode_ms": ms_per_step_local(total_ms, args.steps),
+                "bitwise_equal": bool(torch.equal(o3, vel_mode)), "picard_iterations": st3["picard_iterations"],
                 "kernel_launches": st3["kernel_launches"]}
         except Exception as e:   # noqa: BLE001 - reported in the line
-            line["comparison"]["whole_solve_graph"] = {"error": str(e)[:200]}
+            line["comparison"]["launch_mode"] = {"graphs": other_graphs, "error": str(e)[:200]}
         finally:
             try:
                 s.set_config(c)
             except Exception:   # noqa: BLE001
                 pass
+    # the larger-than-L2 roofline point: the same iteration on a 1601^2 sheet (working set
+    # ~4x the 801^2 one, well above the 126 MB L2)
+    if not args.no_large and M == 801:
+        try:
+            line["roofline"]["large"] = large_roofline(c, stream, flush, dev, peak)
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["roofline"]["large"] = {"error": str(e)[:200]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        picard_plain = (st_other["picard_iterations"] or 184) if args.mode == "fast" else picard[-1]
-        cms, done, dt = cpu_reference_sample(M, args.cpu_picard, picard_plain, nthreads)
-        line["cpu_baseline"] = {"value": cms, "unit": "ms", "cores": nthreads, "kind": "port",
-                                "sample": f"first {done} Picard iterations of the same solve ({dt:.1f} s), "
-                                          f"scaled to the plain GPU solve's {picard_plain} Picard iterations"}
+        plain_picard = st_other["picard_iterations"] if args.mode == "fast" else picard[-1]
+        line["cpu_baseline"] = cpu_baseline(M, c.ssafd_relative_convergence, nthreads, picard_gpu=plain_picard)
     if rank == 0:
         print(json.dumps(line))
-    graph_error = "error" in line["comparison"].get("whole_solve_graph", {})
+    mode_error = "error" in line["comparison"].get("launch_mode", {})
     try:
         s.close()
         if net is not None:
             net.close()
-    except Exception:   # noqa: BLE001 - after a reported whole-solve-graph error the line stands
-        if not graph_error:
+    except Exception:   # noqa: BLE001 - after a reported launch-mode error the line stands
+        if not mode_error:
             raise
     if world > 1:
         dist.destroy_process_group()

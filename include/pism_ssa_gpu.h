@@ -140,6 +140,13 @@ typedef struct pism_gpu_ssa_config {
   /* resident blocks per SM that the coarse-level multigrid post-smoothing grid is sized for
      (1..4; 0 = 4, the other tile kernels' size): a launch-shape knob for the autotuner */
   int    mg_post_blocks_per_sm;
+  /* lagged multigrid coarse levels (0 = rebuilt every Picard iteration, as PETSc sets its
+     preconditioner up on every KSPSolve): the coarse Galerkin operators and the coarsest
+     inverse are rebuilt on the first Picard iteration of a solve and then once the relative
+     nu*H changes summed since the last build reach this value.  The fine level and the
+     Krylov operator always use the current nu*H, so a lagged coarse level changes the
+     iteration counts, not the tolerance the solve meets */
+  double mg_rebuild_rtol;
 } pism_gpu_ssa_config;
 
 /* ---- input fields (SSA::init_impl, SSA.cc:134-184; SSAFD::update) -------- */
@@ -175,6 +182,7 @@ typedef struct pism_gpu_ssa_stats {
   double solve_ms;                 /* wall time of pism_gpu_ssa_solve                 */
   double kernel_ms;                /* device time (CUDA events) of the solve          */
   long long kernel_launches;       /* kernels launched by the solve                   */
+  int    mg_rebuilds;              /* multigrid coarse-level builds (mg_rebuild_rtol)   */
 } pism_gpu_ssa_stats;
 
 /* ---- one member of an ensemble (pism_gpu_ssa_solve_batch) ---- */

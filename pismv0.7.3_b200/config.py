@@ -95,6 +95,7 @@ class SSAConfig:
     graphs: int = 2
     verbosity: int = 0
     mg_post_blocks_per_sm: int = 0
+    mg_rebuild_rtol: float = 0.0
     # geometry helpers (not part of the C struct)
     mask_icefree_thickness_standard: float = 0.01
     mask_is_floating_thickness_standard: float = 1.0
@@ -150,6 +151,7 @@ class CConfig(C.Structure):
         ("ksp_max_it", _I), ("gmres_restart", _I), ("precision", _I), ("mixed_inner_rtol", _D),
         ("mg_omega", _D), ("mg_correction", _D), ("ksp_rtol_adaptive", _I), ("ksp_rtol_max", _D),
         ("ksp_rtol_factor", _D), ("graphs", _I), ("verbosity", _I), ("mg_post_blocks_per_sm", _I),
+        ("mg_rebuild_rtol", _D),
     ]
 
 
@@ -172,7 +174,7 @@ class CStats(C.Structure):
     _fields_ = [("status", _I), ("converged", _I), ("strategy", _I), ("picard_iterations", _I),
                 ("ksp_iterations", _I), ("ksp_failures", _I), ("refinement_steps", _I),
                 ("nuH_norm", _D), ("nuH_norm_change", _D), ("final_linear_residual", _D),
-                ("solve_ms", _D), ("kernel_ms", _D), ("kernel_launches", C.c_longlong)]
+                ("solve_ms", _D), ("kernel_ms", _D), ("kernel_launches", C.c_longlong), ("mg_rebuilds", _I)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

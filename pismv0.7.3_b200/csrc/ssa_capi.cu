@@ -63,7 +63,7 @@ struct pism_gpu_ssa {
     double reg = 0.0, underrelax = 0.0;
     Fields key{};
     bool mixed = false;
-    long long pre = 0, per_picard = 0, per_refine = 0, per_inner = 0, per_go = 0, per_test = 0;
+    long long pre = 0, per_picard = 0, per_refine = 0, per_inner = 0, per_go = 0, per_test = 0, per_rebuild = 0;
     bool failed = false;
   } sgraph;
   PState *pstate = nullptr;
@@ -163,8 +163,9 @@ int active_pc(pism_gpu_ssa *h) {
 const MGHierarchy *active_mg(pism_gpu_ssa *h) { return active_pc(h) == PISM_PC_MULTIGRID ? &h->mg : nullptr; }
 const LinePC *active_line(pism_gpu_ssa *h) { return active_pc(h) == PISM_PC_LINE ? &h->line : nullptr; }
 
-// preconditioner set-up after nu*H / beta changed (replaces PCSetUp)
-int pc_setup(pism_gpu_ssa *h) {
+// preconditioner set-up after nu*H / beta changed (replaces PCSetUp); the multigrid coarse
+// levels only when rebuild_coarse (lagged coarse levels, mg_rebuild_rtol)
+int pc_setup(pism_gpu_ssa *h, bool rebuild_coarse = true) {
   Fields f = fields_of(h);
   *h->zd_host = INT_MAX;
   CK(h, cudaMemcpyAsync(h->zd_dev, h->zd_host, sizeof(int), cudaMemcpyHostToDevice, h->stream));
@@ -172,7 +173,13 @@ int pc_setup(pism_gpu_ssa *h) {
   h->mg.omega = (float)h->cfg.mg_omega;
   h->mg.correction = (float)h->cfg.mg_correction;
   h->mg.post_blocks = h->cfg.mg_post_blocks_per_sm > 0 ? h->L.max_blocks / 4 * h->cfg.mg_post_blocks_per_sm : 0;
-  if (active_mg(h)) mg_setup(h->L, h->g, f, h->K.dinv, h->mg);
+  if (active_mg(h)) {
+    mg_setup_fine(h->L, h->g, f, h->K.dinv, h->mg);
+    if (rebuild_coarse) {
+      mg_setup_coarse(h->L, h->g, f, h->mg);
+      h->stats.mg_rebuilds += 1;
+    }
+  }
   if (active_line(h)) {
     if (!h->line.P) {
       RET(dalloc(h, &h->line.P, h->N));
@@ -445,10 +452,11 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   h->mg.correction = (float)c.mg_correction;
   h->mg.post_blocks = c.mg_post_blocks_per_sm > 0 ? h->L.max_blocks / 4 * c.mg_post_blocks_per_sm : 0;
   PicardConst pc{c.ksp_rtol, c.ksp_rtol_max, c.ksp_rtol_factor, c.ssafd_relative_convergence,
-                 c.ksp_rtol_adaptive ? 1 : 0, c.max_iterations_ssafd};
+                 c.ksp_rtol_adaptive ? 1 : 0, c.max_iterations_ssafd, c.mg_rebuild_rtol};
   PState *P = h->pstate;
   const long long t0 = h->stats.kernel_launches;
-  long long inc_picard = 0, inc_refine = 0, inc_inner = 0, inc_go = 0, inc_test = 0, pre = 0;
+  long long inc_picard = 0, inc_refine = 0, inc_inner = 0, inc_go = 0, inc_test = 0, inc_rebuild = 0, pre = 0;
+  const bool lagged = mg && c.mg_rebuild_rtol > 0.0;
   if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
     S.failed = true;
@@ -461,10 +469,22 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   };
   const long long before_loop = h->stats.kernel_launches;
   bool ok = add_conditional(h, cudaGraphCondTypeWhile, not_done(&P->done), [&] {
-    bool inner_ok = true;
+    bool inner_ok = true, rebuild_ok = true;
     launch_picard_begin(h->L, P, pc, h->zd_dev);
     launch_diag_setup(h->L, g, f, h->K.dinv, h->zd_dev);
-    if (mg) mg_setup(h->L, g, f, h->K.dinv, h->mg);
+    if (lagged) {
+      mg_setup_fine(h->L, g, f, h->K.dinv, h->mg);
+      rebuild_ok = add_conditional(
+          h, cudaGraphCondTypeIf,
+          [&](cudaGraphConditionalHandle cond) { launch_flag_condition(h->L, cond, &P->rebuild, false); },
+          [&] {
+            mg_setup_coarse(h->L, g, f, h->mg);
+            return true;
+          },
+          &inc_rebuild);
+    } else if (mg) {
+      mg_setup(h->L, g, f, h->K.dinv, h->mg);
+    }
     if (line) line_setup(h->L, g, f, h->K.dinv, h->line);
     if (mixed) {
       launch_residual32(h->L, g, f, h->rhs, h->vel, h->K32.rhs, h->res_dev);
@@ -509,7 +529,7 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
       launch_picard_test(h->L, P, h->norm_dev, pc);
       return true;
     }, &inc_test);
-    return inner_ok;
+    return inner_ok && rebuild_ok;
   }, &inc_picard);
   pre = before_loop - t0 + 1;   // + the WHILE node's first condition kernel
   cudaGraph_t out = nullptr;
@@ -532,8 +552,9 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   S.per_inner = inc_inner;
   S.per_go = inc_go;
   S.per_test = inc_test;
+  S.per_rebuild = inc_rebuild;
   S.per_refine = mixed ? inc_refine - inc_inner - inc_go : 0;
-  S.per_picard = inc_picard - (mixed ? inc_refine : inc_inner) - inc_test;
+  S.per_picard = inc_picard - (mixed ? inc_refine : inc_inner) - inc_test - inc_rebuild;
   *built = true;
   return PISM_GPU_SSA_OK;
 }
@@ -568,7 +589,9 @@ int solve_graph_collect(pism_gpu_ssa *h, double reg) {
   const auto &S = h->sgraph;
   const PState &P = *h->pstate_host;
   h->stats.kernel_launches += S.pre + P.passes * S.per_picard + P.refine_passes * S.per_refine +
-                              P.inner_passes * S.per_inner + P.go_count * S.per_go + P.k * S.per_test;
+                              P.inner_passes * S.per_inner + P.go_count * S.per_go + P.k * S.per_test +
+                              P.rebuilds * S.per_rebuild;
+  if (active_mg(h)) h->stats.mg_rebuilds += P.rebuilds;
   h->stats.ksp_iterations += P.ksp_total;
   h->stats.refinement_steps += P.refine_steps;
   h->stats.final_linear_residual = P.final_res;
@@ -730,8 +753,9 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
   Fields f = fields_of(h);
   launch_nuH(h->L, h->g, c, f, reg, 1.0, false, h->norm_dev);
   double last_change = 1.0;   // relative nu*H change of the previous iteration
+  double coarse_change = 0.0;   // relative nu*H changes summed since the coarse levels were built
   for (int k = 0; k < c.max_iterations_ssafd; ++k) {
-    RET(pc_setup(h));
+    RET(pc_setup(h, mg_rebuild_due(coarse_change, k == 0, c.mg_rebuild_rtol)));
     // inexact Picard: the linear solve of an iterate that is still far from the fixed point
     // only needs to be as accurate as the nonlinear iteration it feeds
     double rtol = c.ksp_rtol;
@@ -760,6 +784,7 @@ int picard_manager(pism_gpu_ssa *h, double reg, double underrelax) {
     CK(h, cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     const double norm = h->norm_host[0], change = h->norm_host[1];
+    mg_change_add(coarse_change, norm, change);
     h->stats.picard_iterations = k + 1;
     h->stats.nuH_norm = norm;
     h->stats.nuH_norm_change = change;

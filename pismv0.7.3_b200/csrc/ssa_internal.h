@@ -128,6 +128,8 @@ void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const
                        const MGHierarchy *mg, const LinePC *line, int j);
 void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, double2 *x);
 void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
+void mg_setup_fine(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
+void mg_setup_coarse(const Launch &L, const GridDev &g, const Fields &f, MGHierarchy &H);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b,
                double2 *z, const KState *st);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,

@@ -703,11 +703,23 @@ FineF fine_view(const GridDev &g, const Fields &f, const MGHierarchy &H) {
 }
 
 void mg_setup(const Launch &Lc, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H) {
-  const StencilConst s = stencil_const(g, f);
-  const size_t smem = sizeof(double) * 36 * NTm;
+  mg_setup_fine(Lc, g, f, dinv0, H);
+  mg_setup_coarse(Lc, g, f, H);
+}
+
+// the FP32 fine-level copies of nu*H, beta and D^-1 (the smoother's and the FP32 Krylov
+// operator's): always from the current nu*H
+void mg_setup_fine(const Launch &Lc, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H) {
   const int N = g.Mx * g.My;
   k_mg0_compact<<<std::min((N + NTm - 1) / NTm, Lc.max_blocks), NTm, 0, Lc.stream>>>(N, f.nuH, f.beta, dinv0, H.nuHf,
                                                                                      H.betaf, H.dinvf);
+  Lc.tick();
+}
+
+// the coarse levels: Galerkin operators and D^-1 of every level, the coarsest inverse
+void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHierarchy &H) {
+  const StencilConst s = stencil_const(g, f);
+  const size_t smem = sizeof(double) * 36 * NTm;
   {
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(C.Mx, C.My);
@@ -722,7 +734,7 @@ void mg_setup(const Launch &Lc, const GridDev &g, const Fields &f, const double4
   const MGLevel &C = H.lev[H.nlev - 1];
   const int n = 2 * C.N;
   k_mg_coarse_invert<<<1, CTA_THREADS, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
-  Lc.tick(H.nlev + 2);
+  Lc.tick(H.nlev + 1);
 }
 
 template <class F22, class F21, class F12, class F11>

@@ -43,13 +43,34 @@ struct PState {
   int ksp_its, ksp_status, ksp_total;
   int refine, refine_done, go, go_count, refine_steps, refine_passes;
   long long inner_passes;   // passes of the innermost Krylov loop body
+  double coarse_change;     // relative nu*H changes summed since the coarse levels were built
+  int rebuild;              // this pass rebuilds the multigrid coarse levels
+  int rebuilds;             // coarse-level builds of the solve
 };
 struct PicardConst {
   double ksp_rtol, ksp_rtol_max, ksp_rtol_factor, picard_rtol;
   int adaptive, max_iterations;
+  double mg_rebuild_rtol;   // lagged coarse levels: rebuild once the summed change reaches this (0: always)
 };
 
 // ---- the decisions (the host loop's, in the same double arithmetic) ----
+
+// Whether a Picard pass rebuilds the multigrid coarse levels (their Galerkin operators and
+// the coarsest inverse) from the current nu*H: always on the first pass of a solve and
+// without lagging; with lagging once the relative nu*H changes summed since the last build
+// (a bound on the relative change since then) reach mg_rebuild_rtol.  The fine level and
+// the Krylov operator always use the current nu*H; a lagged coarse level only changes how
+// fast the preconditioned iteration converges, not the tolerance it meets.
+PISM_HD bool mg_rebuild_due(double &coarse_change, bool first, double mg_rebuild_rtol) {
+  const bool due = first || !(mg_rebuild_rtol > 0.0) || coarse_change >= mg_rebuild_rtol;
+  if (due) coarse_change = 0.0;
+  return due;
+}
+
+// after a Picard test: the change since the coarse levels were built grows by this one
+PISM_HD void mg_change_add(double &coarse_change, double norm, double change) {
+  if (norm > 0.0 && std::isfinite(norm) && std::isfinite(change)) coarse_change += change / norm;
+}
 
 PISM_HD void picard_start(PState &P) {
   P = PState{};
@@ -58,6 +79,8 @@ PISM_HD void picard_start(PState &P) {
 
 // a Picard pass begins: the KSP tolerance of inexact Picard (picard_manager's rtol)
 PISM_HD void picard_begin(PState &P, const PicardConst &c) {
+  P.rebuild = mg_rebuild_due(P.coarse_change, P.passes == 0, c.mg_rebuild_rtol) ? 1 : 0;
+  P.rebuilds += P.rebuild;
   double rtol = c.ksp_rtol;
   if (c.adaptive && P.last_change >= 2.0 * c.picard_rtol)
     rtol = fmin(c.ksp_rtol_max, fmax(c.ksp_rtol, c.ksp_rtol_factor * P.last_change));
@@ -138,6 +161,7 @@ PISM_HD void picard_test(PState &P, double norm, double change, const PicardCons
   P.k += 1;
   P.norm = norm;
   P.change = change;
+  mg_change_add(P.coarse_change, norm, change);
   if (!std::isfinite(norm) || !std::isfinite(change)) {
     P.status = PISM_GPU_SSA_ENAN;
     P.done = 1;

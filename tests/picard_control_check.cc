@@ -1,7 +1,7 @@
 // Host driver for the Picard-loop decisions of ssa_state.h (the functions the whole-solve
 // graph's control kernels run on the device).  Reads commands from stdin, one per line,
 // and prints the state after each "print" as one JSON object:
-//   const <adaptive> <ksp_rtol> <ksp_rtol_max> <factor> <picard_rtol> <max_iterations>
+//   const <adaptive> <ksp_rtol> <ksp_rtol_max> <factor> <picard_rtol> <max_iterations> <mg_rebuild_rtol>
 //   start | begin | print
 //   ksp_end <iter> <status> <rnorm2> <bnorm2> <body_iters>
 //   refine_end <iter> <status> <outer_r2> <outer_b2> <max_refine>
@@ -48,6 +48,7 @@ int main() {
       c.ksp_rtol_factor = num(in);
       c.picard_rtol = num(in);
       c.max_iterations = (int)num(in);
+      c.mg_rebuild_rtol = num(in);
     } else if (cmd == "start") {
       picard_start(P);
     } else if (cmd == "begin") {
@@ -80,10 +81,11 @@ int main() {
       printf("{\"rtol\": %s, \"last_change\": %s, \"final_res\": %s, \"k\": %d, \"passes\": %d, "
              "\"done\": %d, \"status\": %d, \"zd_cell\": %d, \"ksp_its\": %d, \"ksp_status\": %d, "
              "\"ksp_total\": %d, \"refine\": %d, \"refine_done\": %d, \"go\": %d, \"go_count\": %d, "
-             "\"refine_steps\": %d, \"refine_passes\": %d, \"inner_passes\": %lld}\n",
+             "\"refine_steps\": %d, \"refine_passes\": %d, \"inner_passes\": %lld, \"rebuild\": %d, "
+             "\"rebuilds\": %d, \"coarse_change\": %s}\n",
              js(P.rtol).c_str(), js(P.last_change).c_str(), js(P.final_res).c_str(), P.k, P.passes, P.done, P.status, P.zd_cell, P.ksp_its,
              P.ksp_status, P.ksp_total, P.refine, P.refine_done, P.go, P.go_count, P.refine_steps,
-             P.refine_passes, P.inner_passes);
+             P.refine_passes, P.inner_passes, P.rebuild, P.rebuilds, js(P.coarse_change).c_str());
     }
   }
   return 0;

@@ -28,18 +28,25 @@ def solve(g, c, f):
     return vel, st
 
 
-@pytest.mark.parametrize("pc,precision,adaptive", [("mg", "mixed", True), ("mg", "fp64", True),
-                                                   ("mg", "fp64", False), ("bjacobi", "fp64", False),
-                                                   ("line", "fp64", False)])
-def test_whole_solve_graph_equals_graph_resident_loops(pc, precision, adaptive):
+@pytest.mark.parametrize("pc,precision,adaptive,lag", [("mg", "mixed", True, 0.0), ("mg", "fp64", True, 0.0),
+                                                       ("mg", "fp64", False, 0.0), ("bjacobi", "fp64", False, 0.0),
+                                                       ("line", "fp64", False, 0.0), ("mg", "mixed", True, 0.05),
+                                                       ("mg", "fp64", False, 0.05)])
+def test_whole_solve_graph_equals_graph_resident_loops(pc, precision, adaptive, lag):
+    """lag > 0: lagged multigrid coarse levels (the graph's IF node around the coarse
+    build against the host loop's decision)"""
     g, c, f, _ = S.build_synthetic(41, 4000e3 / 40, seed=8)
     c = c.copy(pc_type=pc, precision=precision, ksp_rtol=1e-8, ksp_rtol_adaptive=adaptive, ksp_rtol_factor=1.0,
-               ksp_rtol_max=1e-1)
+               ksp_rtol_max=1e-1, mg_rebuild_rtol=lag)
     v2, s2 = solve(g, c.copy(graphs=2), f)
     v3, s3 = solve(g, c.copy(graphs=3), f)
     np.testing.assert_array_equal(v3, v2)
-    for k in ("picard_iterations", "ksp_iterations", "refinement_steps", "converged", "strategy"):
+    for k in ("picard_iterations", "ksp_iterations", "refinement_steps", "converged", "strategy", "mg_rebuilds"):
         assert s3[k] == s2[k], k
+    if lag > 0:
+        assert 1 <= s2["mg_rebuilds"] < s2["picard_iterations"]
+    elif pc == "mg":
+        assert s2["mg_rebuilds"] == s2["picard_iterations"]
     assert s3["final_linear_residual"] == s2["final_linear_residual"]
     assert s3["nuH_norm"] == s2["nuH_norm"] and s3["nuH_norm_change"] == s2["nuH_norm_change"]
     # the graph adds its single-thread control kernels: about six per Picard pass and three

@@ -73,10 +73,17 @@ def host_mixed(records, max_refine):
     return inner, status, steps, final, used
 
 
-def host_picard(c, iters, mixed, max_refine):
-    """picard_manager: returns status, Picard iterations, KSP total, refinement steps, rtols."""
+def host_picard(c, iters, mixed, max_refine, rebuilds=None):
+    """picard_manager: returns status, Picard iterations, KSP total, refinement steps, rtols;
+    `rebuilds` (a list) gets, per Picard pass, whether it rebuilds the coarse levels"""
     last, ksp_total, steps, rtols, k_done = 1.0, 0, 0, [], 0
+    acc = 0.0
+    rebuilds = rebuilds if rebuilds is not None else []
     for k in range(c["max_it"]):
+        due = k == 0 or not (c["lag"] > 0.0) or acc >= c["lag"]
+        if due:
+            acc = 0.0
+        rebuilds.append(1 if due else 0)
         rtol = c["ksp_rtol"]
         if c["adaptive"] and last >= 2.0 * c["tol"]:
             rtol = min(c["max"], max(c["ksp_rtol"], c["factor"] * last))
@@ -94,6 +101,8 @@ def host_picard(c, iters, mixed, max_refine):
         if status != KSP_OK:
             return EKSP, k_done, ksp_total, steps, rtols
         norm, change = rec["norm"], rec["change"]
+        if norm > 0 and math.isfinite(norm) and math.isfinite(change):
+            acc += change / norm
         k_done = k + 1
         if not (math.isfinite(norm) and math.isfinite(change)):
             return ENAN, k_done, ksp_total, steps, rtols
@@ -109,7 +118,8 @@ def scenario(seed, mixed):
     rng = np.random.default_rng(seed)
     c = {"adaptive": int(rng.random() < 0.7), "ksp_rtol": float(10.0 ** rng.uniform(-10, -5)),
          "max": float(10.0 ** rng.uniform(-3, -1)), "factor": float(rng.choice([0.1, 0.5, 1.0, 2.0])),
-         "tol": float(10.0 ** rng.uniform(-6, -3)), "max_it": int(rng.integers(3, 40))}
+         "tol": float(10.0 ** rng.uniform(-6, -3)), "max_it": int(rng.integers(3, 40)),
+         "lag": float(rng.choice([0.0, 0.0, 1e-3, 1e-2, 0.1, 0.5]))}
     c["max"] = max(c["max"], c["ksp_rtol"])
     max_refine = int(rng.integers(2, 8))
     clean = seed % 2 == 0   # even seeds: no injected failures, a contracting Picard iteration
@@ -156,7 +166,8 @@ def scenario(seed, mixed):
 
 def run_device(driver, c, iters, mixed, max_refine):
     """The graph's sequence of control steps, fed the records the host loop consumed."""
-    lines = ["const %d %r %r %r %r %d" % (c["adaptive"], c["ksp_rtol"], c["max"], c["factor"], c["tol"], c["max_it"]),
+    lines = ["const %d %r %r %r %r %d %r" % (c["adaptive"], c["ksp_rtol"], c["max"], c["factor"], c["tol"],
+                                              c["max_it"], c["lag"]),
              "start"]
     marks = []   # what each print checks
     for k, rec in enumerate(iters):
@@ -182,7 +193,8 @@ def run_device(driver, c, iters, mixed, max_refine):
 @pytest.mark.parametrize("seed", range(40))
 def test_device_decisions_equal_the_host_loop(driver, seed, mixed):
     c, max_refine, iters = scenario(seed, mixed)
-    status, k_done, ksp_total, steps, rtols = host_picard(c, iters, mixed, max_refine)
+    rebuilds = []
+    status, k_done, ksp_total, steps, rtols = host_picard(c, iters, mixed, max_refine, rebuilds)
     n_iters = len(rtols)
     states, marks = run_device(driver, c, iters[:n_iters], mixed, max_refine)
     # the graph stops where the host loop stops: not done before the last Picard pass
@@ -192,6 +204,8 @@ def test_device_decisions_equal_the_host_loop(driver, seed, mixed):
         if kind == "begin":
             assert st["rtol"] == rtols[k], (k, st["rtol"], rtols[k])
             assert st["passes"] == k + 1
+            assert st["rebuild"] == rebuilds[k], (k, st["rebuild"], rebuilds[k])
+            assert st["rebuilds"] == sum(rebuilds[:k + 1])
         if kind == "refine":
             q, used = mark[2], mark[3]
             assert st["refine_done"] == (1 if q == used - 1 else 0), (k, q, used)

@@ -36,7 +36,11 @@ def _rank(rank, world, port, q):
     b = _bench()
     local = [120.0, 175.5][rank]
     m = b.max_over_ranks(local)
-    q.put((rank, m, b.job_time_per_solve(m, world)))
+    # the ensemble partition: every rank's members, gathered on every rank
+    mine = b.members_of_rank(rank, world, 3)
+    got = [None] * world
+    dist.all_gather_object(got, mine)
+    q.put((rank, m, b.job_time_per_solve(m, world), got))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -52,13 +56,22 @@ def test_max_over_ranks_and_job_value():
         p.join(timeout=120)
     assert all(p.exitcode == 0 for p in procs)
     got = sorted(q.get(timeout=10) for _ in range(2))
-    assert got == [(0, 175.5, 87.75), (1, 175.5, 87.75)]
+    assert [g[:3] for g in got] == [(0, 175.5, 87.75), (1, 175.5, 87.75)]
+    # members sharded with no overlap, the job covering 0 .. world * per_gpu - 1
+    for g in got:
+        parts = g[3]
+        assert parts == [[0, 1, 2], [3, 4, 5]]
+        flat = [m for p in parts for m in p]
+        assert sorted(flat) == list(range(6)) and len(set(flat)) == len(flat)
 
 
 def test_single_process_needs_no_group():
     b = _bench()
     assert b.max_over_ranks(3.5) == 3.5
     assert b.job_time_per_solve(10.0, 1) == 10.0
+    assert b.members_of_rank(0, 1, 64) == list(range(64))
+    with pytest.raises(ValueError):
+        b.members_of_rank(2, 2, 4)
 
 
 def test_reference_arm_prints_from_rank_zero_only():
