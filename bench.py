@@ -49,14 +49,19 @@ METRIC = "SSA solve ms at 801² to rel resid 1e-6: learned+FP32 vs plain FP64, 1
 # the configuration text's 1e-4 leaves both set-ups ~1e-3 from it and is reported beside.
 HEADLINE_PICARD_RTOL = 1e-6
 # fast set-up: lagged multigrid coarse levels (rebuilt once the summed relative nu*H change
-# since the last build reaches this)
+# since the last build reaches this).  Off: on the B200 the 801^2 fast solve at Picard 1e-6
+# took 655 Krylov iterations / 236 ms rebuilding every iteration, 978 / 265 ms at 0.01 and
+# 2261 / 533 ms at 0.05 (its linear solves are 2-3 iterations long, so a weaker coarse
+# correction costs more than the rebuild it saves)
 FAST_MG_LAG = 0.0
-# launch mode of the timed solves (2: graph-resident Krylov loops, 3: the whole Picard loop as
-# one graph); the other one is timed beside it
-DEFAULT_GRAPHS = 2
+# launch mode of the timed solves (3: the whole Picard loop as one graph, 2: graph-resident
+# Krylov loops, bit for bit the same answers; on the B200 the 801^2 fast solve at Picard
+# tolerance 1e-6 took 224 ms with 3 and 236 ms with 2); the other one is timed beside it
+DEFAULT_GRAPHS = 3
 # In-solve DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control
 # none) of one inner iteration's kernels on the 801^2 sheet, per (grid, precision)
-INNER_ITERATION_TRAFFIC: dict = {}
+# (profiles/inner_iteration_traffic_801.md: the per-launch averages of the 23 kernels)
+INNER_ITERATION_TRAFFIC = {(801, "mixed"): 96.7e6}
 
 
 def _package():
@@ -705,7 +710,8 @@ def main():
     roof.update(peak=peak, frac=roof["achieved"] / peak, peak_kind=peak_kind, bound="hbm",
                 traffic=INNER_ITERATION_TRAFFIC.get((M, c.precision)))
     roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the iteration's 23 kernels, "
-                              "in-solve (--cache-control none), profiles/inner_iteration_traffic_801.md"
+                              "in-solve (--cache-control none), profiles/inner_iteration_traffic_801.md: the working "
+                              "set stays in L2, so DRAM traffic is a quarter of the algorithmic bytes"
                               if roof["traffic"] is not None else None)
     roof["kernel"] = ("one inner BiCGStab + V(1,1) multigrid iteration: k32_p/v/s/t/x + 2 x (k_mg0_restrict, "
                       "k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, k_mg0_post)"

@@ -135,10 +135,10 @@ def test_config1_test_i_reference_default_tolerances(goldens):
     """Configuration 1 as stated: test I on Mx = 5, My = 201 with the reference's default
     Picard and KSP tolerances (ssa_rtol 1e-4, KSP rtol 1e-5), the plain FP64 set-up
     (BiCGStab + block Jacobi).  Both the GPU and the oracle stop the Picard iteration at the
-    same default test; the inexact linear solves make the two answers differ by what a
-    1e-5 residual allows, which the oracle's own two linear solvers bound (PETSc-like GMRES
-    at 1e-5 against a direct solve: 3.5e-3 relative L2).  The error table against the exact
-    solution is reported."""
+    same default test; the GPU's inexact linear solves (relative residual 1e-5 per Picard
+    iteration) against the oracle's direct solves leave the answers 1e-6 apart at most
+    (7.6e-8 measured on a B200; the oracle's own PETSc-like GMRES at 1e-5 is 3.5e-3 from its
+    direct solve).  The error table against the exact solution is reported."""
     g, c, f = V.build_test_i(My=201)
     assert c.ssafd_relative_convergence == 1e-4 and c.ksp_rtol == 1e-5
     s = make_solver(g, c, f)
@@ -149,7 +149,7 @@ def test_config1_test_i_reference_default_tolerances(goldens):
     ref = o.solve()
     assert st["converged"] == 1 and st["strategy"] == 0
     assert abs(st["picard_iterations"] - o.stats.picard_iterations) <= 3
-    assert rel(vel, ref) < 1e-2, rel(vel, ref)
+    assert rel(vel, ref) < 1e-6, rel(vel, ref)
     r = V.report(vel, V.exact_velocity_i(g))
     r_ref = V.report(ref, V.exact_velocity_i(g))
     print(f"test I 5x201 defaults: GPU picard {st['picard_iterations']} maxvector {r['maxvector']:.4f} "
@@ -248,14 +248,19 @@ def test_fused_norms_and_frictional_heating_match_oracle(name):
     over the ghosted arrays) against the oracle's nuH_norm of the GPU's nu*H before and
     after, and compute_basal_frictional_heating (ShallowStressBalance.cc:179-205) against
     the oracle's at the GPU's velocity."""
-    kw = {"plain": dict(), "cfbc": dict(cfbc=True), "pseudo_subgl": dict(pseudo=True, sub_gl=True)}[name]
-    g, c, f = random_case(31 + len(name), bc=False, **kw)
+    if name == "cfbc":
+        # verification test V (a calving front with the CFBC stencil); random -cfbc mask
+        # patterns nearly always leave an isolated icy cell with a zero diagonal, which the
+        # solve reports as the reference does (SSAFD.cc:766-776; the oracle finds the same cell)
+        g, c, f = V.build_test_v(201)
+    else:
+        kw = {"plain": dict(), "pseudo_subgl": dict(pseudo=True, sub_gl=True)}[name]
+        g, c, f = random_case(31 + len(name), bc=False, **kw)
+    vel0 = np.random.default_rng(8).normal(0, 3e-6, (g.Mx, g.My, 2))
     c.max_iterations_ssafd = 1
     c.ssafd_relative_convergence = 1e30
     c.ksp_rtol = 1e-10
     G, Cc, I = O.from_case(g, c, f)
-    rng = np.random.default_rng(8)
-    vel0 = rng.normal(0, 3e-6, (g.Mx, g.My, 2))
     s = make_solver(g, c, f)
     s.compute_hardav_staggered()
     nuH0 = O.compute_nuH(G, Cc, I, O.hardness_staggered(G, Cc, I), vel0, c.epsilon_ssa)
@@ -271,5 +276,5 @@ def test_fused_norms_and_frictional_heating_match_oracle(name):
     assert st["nuH_norm_change"] == pytest.approx(change, rel=1e-10)
     heat = O.basal_frictional_heating(Cc, I, vel)
     np.testing.assert_allclose(s.basal_frictional_heating(), heat, rtol=1e-12, atol=1e-12 * np.abs(heat).max())
-    assert np.abs(heat).max() > 0
+    assert name == "cfbc" or np.abs(heat).max() > 0   # test V's shelf is all afloat: no friction
     s.close()
