@@ -491,6 +491,8 @@ def main():
     ap.add_argument("--ksp-factor", type=float, default=1.0,
                     help="fast set-up: KSP rtol of a Picard iteration = factor x the last relative nu*H change")
     ap.add_argument("--ksp-max", type=float, default=1e-1, help="fast set-up: loosest KSP rtol of a Picard iteration")
+    ap.add_argument("--mg-small-kernel", type=int, default=0, choices=[0, 1],
+                    help="multigrid small levels: 0 held in the cluster's shared memory, 1 staged from L2 per step")
     ap.add_argument("--mg-lag", type=float, default=FAST_MG_LAG,
                     help="fast set-up: rebuild the multigrid coarse levels once the summed relative nu*H change "
                          "reaches this (0: every Picard iteration)")
@@ -523,6 +525,7 @@ def main():
     c_plain.graphs = args.graphs
     if args.mg_post_blocks is not None:
         c_plain.mg_post_blocks_per_sm = args.mg_post_blocks
+    c_plain.mg_small_kernel = args.mg_small_kernel
     c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max, mg_lag=args.mg_lag)
     if args.inner_rtol is not None:
         c_fast.mixed_inner_rtol = args.inner_rtol
@@ -747,7 +750,7 @@ def main():
                           f"{'aggregation multigrid' if args.pc == 'mg' else 'block Jacobi'}",
                    "ksp_rtol": c.ksp_rtol, "ksp_rtol_adaptive": bool(c.ksp_rtol_adaptive),
                    "picard_rtol": c.ssafd_relative_convergence, "graphs": c.graphs,
-                   "mg_rebuild_rtol": c.mg_rebuild_rtol,
+                   "mg_rebuild_rtol": c.mg_rebuild_rtol, "mg_small_kernel": c.mg_small_kernel,
                    "warm_start": (f"learned (U-Net, features at stride {stride})" if net is not None else "zero"),
                    "l2": "flushed (256 MB write) between steps",
                    "parallelism": f"replicas x{world}"},

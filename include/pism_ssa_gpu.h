@@ -147,6 +147,12 @@ typedef struct pism_gpu_ssa_config {
      Krylov operator always use the current nu*H, so a lagged coarse level changes the
      iteration counts, not the tolerance the solve meets */
   double mg_rebuild_rtol;
+  /* the multigrid's small levels (<= 4096 cells each) in one thread-block cluster:
+     0 each CTA holds a block of every small level in its shared memory (operators staged by
+     bulk asynchronous copies, halos read from the neighbouring CTAs' shared memory), where the
+     blocks fit; 1 the levels are staged from L2 at every step.  Both give the same results;
+     a launch-shape knob for the autotuner */
+  int    mg_small_kernel;
 } pism_gpu_ssa_config;
 
 /* ---- input fields (SSA::init_impl, SSA.cc:134-184; SSAFD::update) -------- */

@@ -173,6 +173,7 @@ int pc_setup(pism_gpu_ssa *h, bool rebuild_coarse = true) {
   h->mg.omega = (float)h->cfg.mg_omega;
   h->mg.correction = (float)h->cfg.mg_correction;
   h->mg.post_blocks = h->cfg.mg_post_blocks_per_sm > 0 ? h->L.max_blocks / 4 * h->cfg.mg_post_blocks_per_sm : 0;
+  h->mg.small_kernel = h->cfg.mg_small_kernel;
   if (active_mg(h)) {
     mg_setup_fine(h->L, h->g, f, h->K.dinv, h->mg);
     if (rebuild_coarse) {
@@ -213,6 +214,9 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
   if (c->graphs < 0 || c->graphs > 3) return fail(h, PISM_GPU_SSA_EINVAL, "graphs must be 0, 1, 2 or 3");
   if (c->mg_post_blocks_per_sm < 0 || c->mg_post_blocks_per_sm > 4)
     return fail(h, PISM_GPU_SSA_EINVAL, "mg_post_blocks_per_sm must be in [0, 4]");
+  if (c->mg_small_kernel < 0 || c->mg_small_kernel > 1)
+    return fail(h, PISM_GPU_SSA_EINVAL, "mg_small_kernel must be 0 or 1");
+  if (!(c->mg_rebuild_rtol >= 0.0)) return fail(h, PISM_GPU_SSA_EINVAL, "mg_rebuild_rtol must be >= 0");
   if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
     return fail(h, PISM_GPU_SSA_EINVAL, "ksp_rtol, ksp_max_it and max_iterations_ssafd must be positive");
   if (!(c->ssa_Glen_exponent > 0.0) || !(c->min_thickness_strength_extension_ssa > 0.0))
@@ -451,6 +455,7 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   h->mg.omega = (float)c.mg_omega;   // captured by value, as pc_setup sets them
   h->mg.correction = (float)c.mg_correction;
   h->mg.post_blocks = c.mg_post_blocks_per_sm > 0 ? h->L.max_blocks / 4 * c.mg_post_blocks_per_sm : 0;
+  h->mg.small_kernel = c.mg_small_kernel;
   PicardConst pc{c.ksp_rtol, c.ksp_rtol_max, c.ksp_rtol_factor, c.ssafd_relative_convergence,
                  c.ksp_rtol_adaptive ? 1 : 0, c.max_iterations_ssafd, c.mg_rebuild_rtol};
   PState *P = h->pstate;

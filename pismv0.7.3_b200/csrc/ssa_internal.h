@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "ssa_device.cuh"
+#include "ssa_small_plan.h"
 #include "ssa_state.h"
 
 namespace pism_gpu {
@@ -85,6 +86,11 @@ struct MGHierarchy {
   MGLevel lev[MG_MAX_LEVELS];
   int small_first = 0;                           // first level cycled by the cluster
   int small_smem = 0;                            // its per-CTA staging buffer (bytes)
+  bool small_dsmem = false;                      // the small levels fit the cluster's shared memory
+  int small_kernel = 0;                          // mg_small_kernel of the configuration
+  SmallPlan small_plan{};                        // their split over the cluster's CTAs
+  void *small_plan_dev = nullptr;                // device copy of small_plan
+  int *small_timeout = nullptr;                  // set when that cycle's staging wait gave up
   float omega = 0.9f;                            // damping of the block-Jacobi smoother
   float correction = 1.2f;                       // scaling of the coarse-grid correction
   int post_blocks = 0;                           // grid cap of the coarse post-smoothing (0: none)

@@ -32,6 +32,7 @@
 #include <cooperative_groups.h>
 
 #include "ssa_fine32.cuh"
+#include "ssa_small_plan.h"
 
 namespace pism_gpu {
 
@@ -40,6 +41,9 @@ namespace {
 constexpr int TJm = 32, TIm = 8, NTm = TJm * TIm;
 constexpr int CTA_THREADS = 1024;
 constexpr int SMALL_CLUSTER = 8;   // CTAs (SMs) of the cluster that cycles the small levels
+static_assert(SMALL_CLUSTER == SC_CTAS, "the shared-memory cycle's split assumes the cluster size");
+// dynamic shared memory of the shared-memory cycle (the kernel's static part is < 2 KB)
+constexpr int SMALL_DSMEM_MAX_BYTES = 220 * 1024;
 
 struct TileM {
   int tiles_j, tiles;
@@ -571,6 +575,242 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   }
 }
 
+// ---------------------------------------------------------------------------
+// The small levels in the cluster's shared memory.  Every CTA holds a nested block of every
+// small level (ssa_small_plan.h): the nine 2 x 2 operator blocks and D^-1, staged once per
+// cycle by bulk asynchronous copies (one per block row and array) completing on an
+// mbarrier, and b, x0, x, z.  A step reads its own cells from its shared memory and the
+// neighbours' halo values from the neighbouring CTAs' shared memory (distributed shared
+// memory), so no step waits on L2; the restriction and the prolongation stay inside a CTA
+// because the blocks nest.  The arithmetic of every cell is that of k_mg_small_cycle, in the
+// same order, so the two give the same bits.
+// ---------------------------------------------------------------------------
+struct SmallDs {
+  const SmallPlan *plan;   // device copy of the split
+  const LevelView *lev;    // device level views
+  int first;               // index of the first small level
+  const double *invT;      // dense inverse of the coarsest operator (transposed)
+  int n;                   // unknowns of the coarsest level
+  int *stage_timeout;      // set when the staging wait gave up (the cycle then runs on what arrived)
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// bounded wait for phase `phase` of an mbarrier: false when it did not complete
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// y = A x at the cell with slot s of this CTA's block (level cells (i, j)), the nine blocks
+// from shared memory, x through xf(i', j') (wrapped indices)
+template <class XF>
+__device__ __forceinline__ float2 small_apply(const float4 *__restrict__ A0, int cap, int s, int i, int j, int Mx,
+                                              int My, const XF &xf) {
+  const int ip = wrap(i + 1, Mx), im = wrap(i - 1, Mx), jp = wrap(j + 1, My), jm = wrap(j - 1, My);
+  const int ii[9] = {im, i, ip, im, i, ip, im, i, ip};
+  const int jj[9] = {jp, jp, jp, j, j, j, jm, jm, jm};
+  float y1 = 0.0f, y2 = 0.0f;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const float4 a = A0[b * cap + s];
+    const float2 xv = xf(ii[b], jj[b]);
+    y1 += a.x * xv.x + a.y * xv.y;
+    y2 += a.z * xv.x + a.w * xv.y;
+  }
+  return make_float2(y1, y2);
+}
+
+__global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THREADS)
+    k_mg_small_dsmem(SmallDs S, float omega, float corr, const KState *st) {
+  if (st && st->done) return;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ SmallPlan P;
+  __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
+  __shared__ __align__(8) unsigned long long bar;
+  const unsigned rank = cluster.block_rank();
+  const int tid = threadIdx.x;
+  for (int q = tid; q < (int)(sizeof(SmallPlan) / sizeof(int)); q += CTA_THREADS)
+    reinterpret_cast<int *>(&P)[q] = reinterpret_cast<const int *>(S.plan)[q];
+  __syncthreads();
+  const int pr = (int)rank / P.Pc, pc = (int)rank % P.Pc;
+  const bool active = (int)rank < P.Pr * P.Pc;
+  auto cap = [&](int l) { return P.mi[l] * P.mj[l]; };
+  // arrays of level l: blocks 0..8 of A and D^-1 (float4); b, x0, x, z (float2)
+  auto A4 = [&](int l) { return reinterpret_cast<float4 *>(sm + P.off4[l]); };
+  auto F2 = [&](int l, int a) { return reinterpret_cast<float2 *>(sm + P.off2[l]) + a * cap(l); };
+  auto r0 = [&](int l) { return active ? P.rb[l][pr] : 0; };
+  auto c0 = [&](int l) { return active ? P.cb[l][pc] : 0; };
+  auto ni = [&](int l) { return active ? P.rb[l][pr + 1] - P.rb[l][pr] : 0; };
+  auto nj = [&](int l) { return active ? P.cb[l][pc + 1] - P.cb[l][pc] : 0; };
+  // array `a` of level l at cell (ii, jj), from whichever CTA holds it
+  auto fetch = [&](int l, int a, int ii, int jj) {
+    const int qp = small_owner(P.rb[l], P.Pr, ii), qc = small_owner(P.cb[l], P.Pc, jj);
+    const int s = (ii - P.rb[l][qp]) * P.mj[l] + (jj - P.cb[l][qc]);
+    float2 *base = F2(l, a);
+    const unsigned owner = (unsigned)(qp * P.Pc + qc);
+    return owner == rank ? base[s] : cluster.map_shared_rank(base, owner)[s];
+  };
+
+  // ---- staging: this CTA's block of every level's operator by bulk copies, b of the first ----
+  const unsigned bar_a = smem_addr(&bar);
+  unsigned total = 0;
+  for (int l = 0; l < P.nlev; ++l) total += (unsigned)(ni(l) * nj(l) * 10 * 16);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (total > 0)
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(total) : "memory");
+  }
+  __syncthreads();
+  if (total > 0) {
+    int nrow_total = 0;
+    for (int l = 0; l < P.nlev; ++l) nrow_total += ni(l) * 10;
+    for (int q = tid; q < nrow_total; q += CTA_THREADS) {
+      int l = 0, rem = q;
+      while (rem >= ni(l) * 10) {
+        rem -= ni(l) * 10;
+        ++l;
+      }
+      const int row = rem / 10, blk = rem - row * 10;
+      const LevelView L = S.lev[S.first + l];
+      const int i = r0(l) + row;
+      const float4 *src = (blk < 9 ? L.A + (size_t)blk * L.N : L.dinv) + (size_t)i * L.My + c0(l);
+      float4 *dst = A4(l) + blk * cap(l) + row * P.mj[l];
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(dst)),
+          "l"(src), "r"((unsigned)(nj(l) * 16)), "r"(bar_a)
+          : "memory");
+    }
+  }
+  {
+    const LevelView L = S.lev[S.first];
+    float2 *b = F2(0, 0);
+    for (int q = tid; q < ni(0) * nj(0); q += CTA_THREADS) {
+      const int li = q / nj(0), lj = q - li * nj(0);
+      b[li * P.mj[0] + lj] = L.b[(r0(0) + li) * L.My + c0(0) + lj];
+    }
+  }
+  bool staged = true;
+  if (total > 0) {
+    staged = mbar_wait_bounded(bar_a, 0);
+    if (!staged && tid == 0) *S.stage_timeout = 1;
+  }
+  __syncthreads();
+
+  // ---- down: x0 = omega D^-1 b; b_{l+1} = R (b - A x0) ----
+  for (int l = 0; l + 1 < P.nlev; ++l) {
+    const int Mx = P.Mx[l], My = P.My[l], mj = P.mj[l], cp = cap(l);
+    const float4 *A = A4(l), *D = A4(l) + 9 * cp;
+    const float2 *b = F2(l, 0);
+    float2 *x0 = F2(l, 1);
+    for (int q = tid; q < ni(l) * nj(l); q += CTA_THREADS) {
+      const int li = q / nj(l), s = li * mj + (q - li * nj(l));
+      const float2 v = fmul4(D[s], b[s]);
+      x0[s] = make_float2(omega * v.x, omega * v.y);
+    }
+    cluster.sync();
+    const int ax = P.ax[l], ay = P.ay[l], R0 = r0(l + 1), C0 = c0(l + 1), ncj = nj(l + 1), nc = ni(l + 1) * ncj;
+    float2 *bc = F2(l + 1, 0);
+    const int span = (4 * nc + 31) & ~31;   // whole warps take part in the shuffles
+    for (int base = tid; base < span; base += CTA_THREADS) {
+      const int kc = base >> 2, pi = (base >> 1) & 1, pj = base & 1;
+      float ru = 0.0f, rv = 0.0f;
+      if (kc < nc && pi < ax && pj < ay) {
+        const int I = R0 + kc / ncj, J = C0 + kc % ncj;
+        const int i = I * ax + pi, j = J * ay + pj;
+        if (i < Mx && j < My) {
+          const int s = (i - r0(l)) * mj + (j - c0(l));
+          const float2 y = small_apply(A, cp, s, i, j, Mx, My, [&](int ii, int jj) { return fetch(l, 1, ii, jj); });
+          const float2 bk = b[s];
+          ru = bk.x - y.x;
+          rv = bk.y - y.y;
+        }
+      }
+      ru += __shfl_xor_sync(0xffffffffu, ru, 1);
+      rv += __shfl_xor_sync(0xffffffffu, rv, 1);
+      ru += __shfl_xor_sync(0xffffffffu, ru, 2);
+      rv += __shfl_xor_sync(0xffffffffu, rv, 2);
+      if (kc < nc && (base & 3) == 0) bc[(kc / ncj) * P.mj[l + 1] + kc % ncj] = make_float2(ru, rv);
+    }
+    __syncthreads();
+  }
+
+  // ---- coarsest: x = A^-1 b (every CTA gathers b, each computes the rows of its cells) ----
+  {
+    const int l = P.nlev - 1, Myc = P.My[l], Nc = P.Mx[l] * Myc;
+    cluster.sync();
+    for (int q = tid; q < Nc; q += CTA_THREADS) {
+      const float2 v = fetch(l, 0, q / Myc, q % Myc);
+      bsh[2 * q] = v.x;
+      bsh[2 * q + 1] = v.y;
+    }
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5, nrows = 2 * ni(l) * nj(l);
+    float *z = reinterpret_cast<float *>(F2(l, 3));
+    const LevelView Lc = S.lev[S.first + l];
+    for (int w = warp; w < nrows; w += CTA_THREADS / 32) {
+      const int q = w >> 1, comp = w & 1, li = q / nj(l), lj = q - li * nj(l);
+      const int r = 2 * ((r0(l) + li) * Myc + c0(l) + lj) + comp;
+      double acc = 0.0;
+      for (int c = lane; c < S.n; c += 32) acc += S.invT[c * S.n + r] * (double)bsh[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) {
+        z[2 * (li * P.mj[l] + lj) + comp] = (float)acc;
+        if (P.nlev == 1) reinterpret_cast<float *>(Lc.x)[r] = (float)acc;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- up: x = omega D^-1 b + s P z_{l+1}; z = x + omega D^-1 (b - A x) ----
+  for (int l = P.nlev - 2; l >= 0; --l) {
+    const int Mx = P.Mx[l], My = P.My[l], mj = P.mj[l], cp = cap(l);
+    const float4 *A = A4(l), *D = A4(l) + 9 * cp;
+    const float2 *b = F2(l, 0), *zc = F2(l + 1, 3);
+    float2 *x = F2(l, 2), *z = F2(l, 3);
+    const int ax = P.ax[l], ay = P.ay[l], R0 = r0(l + 1), C0 = c0(l + 1), mjc = P.mj[l + 1];
+    for (int q = tid; q < ni(l) * nj(l); q += CTA_THREADS) {
+      const int li = q / nj(l), lj = q - li * nj(l), s = li * mj + lj;
+      const int i = r0(l) + li, j = c0(l) + lj;
+      const float2 v = fmul4(D[s], b[s]);
+      const float2 c = zc[(i / ax - R0) * mjc + (j / ay - C0)];
+      x[s] = make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+    }
+    cluster.sync();
+    const LevelView L = S.lev[S.first + l];
+    for (int q = tid; q < ni(l) * nj(l); q += CTA_THREADS) {
+      const int li = q / nj(l), lj = q - li * nj(l), s = li * mj + lj;
+      const int i = r0(l) + li, j = c0(l) + lj;
+      const float2 xk = x[s];
+      const float2 y = small_apply(A, cp, s, i, j, Mx, My, [&](int ii, int jj) { return fetch(l, 2, ii, jj); });
+      const float2 bk = b[s];
+      const float2 d = fmul4(D[s], make_float2(bk.x - y.x, bk.y - y.y));
+      const float2 zk = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+      z[s] = zk;
+      if (l == 0) L.x[i * My + j] = zk;
+    }
+    __syncthreads();
+  }
+  // no CTA leaves while another may still read its shared memory; after a staging wait
+  // that gave up, the copies still in flight are waited for once more (bounded) first
+  if (!staged) mbar_wait_bounded(bar_a, 0);
+  cluster.sync();
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -605,6 +845,22 @@ int mg_plan(int Mx, int My, MGHierarchy &H) {
   H.small_first = H.nlev - 1;
   while (H.small_first > 0 && H.lev[H.small_first - 1].N <= MG_CTA_CELLS) --H.small_first;
   H.small_smem = (int)sizeof(float2) * H.lev[H.small_first].N;   // every CTA stages a whole level
+  // the shared-memory cycle when every small level's block fits (ssa_small_plan.h)
+  {
+    int mx[SC_MAX_LEV], my[SC_MAX_LEV], ax[SC_MAX_LEV], ay[SC_MAX_LEV];
+    const int ns = H.nlev - H.small_first;
+    H.small_dsmem = false;
+    if (ns <= SC_MAX_LEV) {
+      for (int l = 0; l < ns; ++l) {
+        const MGLevel &L = H.lev[H.small_first + l];
+        mx[l] = L.Mx;
+        my[l] = L.My;
+        ax[l] = L.ax;
+        ay[l] = L.ay;
+      }
+      H.small_dsmem = small_plan(ns, mx, my, ax, ay, SMALL_DSMEM_MAX_BYTES, H.small_plan);
+    }
+  }
   return H.nlev;
 }
 
@@ -649,6 +905,14 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
     if (cudaMemcpy(H.views, v, sizeof(LevelView) * H.nlev, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
   }
   if (raise_dynamic_smem((const void *)k_mg_small_cycle, H.small_smem) != 0) return 1;
+  if (H.small_dsmem) {
+    if (cudaMalloc(&H.small_plan_dev, sizeof(SmallPlan)) != cudaSuccess) return 1;
+    if (cudaMemcpy(H.small_plan_dev, &H.small_plan, sizeof(SmallPlan), cudaMemcpyHostToDevice) != cudaSuccess)
+      return 1;
+    if (cudaMalloc(&H.small_timeout, sizeof(int)) != cudaSuccess) return 1;
+    if (cudaMemset(H.small_timeout, 0, sizeof(int)) != cudaSuccess) return 1;
+    if (raise_dynamic_smem((const void *)k_mg_small_dsmem, H.small_plan.smem) != 0) return 1;
+  }
   if (raise_dynamic_smem((const void *)k_mg_coarse_invert, (int)(sizeof(double) * n * n)) != 0) return 1;
   if (raise_dynamic_smem((const void *)k_mg_build1, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
   if (raise_dynamic_smem((const void *)k_mg_build, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
@@ -672,6 +936,10 @@ void mg_free(MGHierarchy &H) {
   cudaFree(H.cinv);
   cudaFree(H.singular);
   cudaFree(H.views);
+  cudaFree(H.small_plan_dev);
+  cudaFree(H.small_timeout);
+  H.small_plan_dev = nullptr;
+  H.small_timeout = nullptr;
   H.views = nullptr;
   H.nuHf = nullptr;
   H.betaf = nullptr;
@@ -772,8 +1040,18 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
 #undef MGCR
     ++launches;
   }
-  // the small levels in one CTA
-  {
+  // the small levels on one thread-block cluster
+  if (H.small_dsmem && H.small_kernel == 0) {
+    SmallDs S;
+    S.plan = reinterpret_cast<const SmallPlan *>(H.small_plan_dev);
+    S.lev = reinterpret_cast<const LevelView *>(H.views);
+    S.first = H.small_first;
+    S.invT = H.cinv;
+    S.n = 2 * H.lev[H.nlev - 1].N;
+    S.stage_timeout = H.small_timeout;
+    k_mg_small_dsmem<<<SMALL_CLUSTER, CTA_THREADS, H.small_plan.smem, Lc.stream>>>(S, omega, corr, st);
+    ++launches;
+  } else {
     SmallLevels S;
     S.first = H.small_first;
     S.last = H.nlev - 1;

@@ -1,0 +1,100 @@
+// ssa_small_plan.h — how the small multigrid levels are split over the CTAs of one
+// thread-block cluster (the shared-memory cycle of ssa_mg.cu), as plain C++ so that the host
+// compiler can check the split too.
+//
+// The coarsest level's rows and columns are cut into a Pr x Pc grid of blocks, one block per
+// CTA (Pr * Pc <= cluster size); every finer small level takes the blocks of the level below
+// it expanded by the aggregation factors, so the fine cells of a coarse cell's aggregate
+// always live on the coarse cell's CTA.  Each CTA keeps its block of every level in its own
+// shared memory, in arrays shaped by the largest block of that level (the same offsets on
+// every CTA, so a neighbour's value is read from the same offset in the neighbour's shared
+// memory).
+#pragma once
+
+namespace pism_gpu {
+
+constexpr int SC_CTAS = 8;       // CTAs of the cluster
+constexpr int SC_MAX_LEV = 12;   // small levels handled by the shared-memory cycle
+
+// (plain members only: the cycle kernel copies the plan into a __shared__ variable)
+struct SmallPlan {
+  int nlev;                            // small levels first .. first + nlev - 1
+  int Pr, Pc;                          // CTA grid
+  int Mx[SC_MAX_LEV], My[SC_MAX_LEV];  // level sizes
+  int ax[SC_MAX_LEV], ay[SC_MAX_LEV];  // aggregation towards the next (coarser) level
+  int rb[SC_MAX_LEV][SC_CTAS + 1];     // row boundaries: CTA row p owns rows [rb[p], rb[p+1])
+  int cb[SC_MAX_LEV][SC_CTAS + 1];     // column boundaries
+  int mi[SC_MAX_LEV], mj[SC_MAX_LEV];  // largest block: the shape of every CTA's arrays
+  int off4[SC_MAX_LEV];                // byte offset of the level's float4 arrays (9 blocks of A, D^-1)
+  int off2[SC_MAX_LEV];                // byte offset of the level's float2 arrays (b, x0, x, z)
+  int smem;                            // bytes of dynamic shared memory per CTA
+};
+
+// bytes per cell slot: 10 float4 (the nine 2 x 2 blocks and D^-1) + 4 float2 (b, x0, x, z)
+constexpr int SC_BYTES_PER_CELL = 10 * 16 + 4 * 8;
+
+// Plan the split of levels (Mx[l], My[l], ax[l], ay[l]), l = 0 .. nlev-1 from fine to
+// coarse (level l+1 has ceil(Mx[l] / ax[l]) x ceil(My[l] / ay[l]) cells).  Returns false
+// when the levels do not fit (too many, or more shared memory than max_smem per CTA).
+inline bool small_plan(int nlev, const int *Mx, const int *My, const int *ax, const int *ay, int max_smem,
+                       SmallPlan &P) {
+  if (nlev < 1 || nlev > SC_MAX_LEV) return false;
+  P = SmallPlan{};
+  P.nlev = nlev;
+  for (int l = 0; l < nlev; ++l) {
+    P.Mx[l] = Mx[l];
+    P.My[l] = My[l];
+    P.ax[l] = ax[l];
+    P.ay[l] = ay[l];
+    if (Mx[l] < 1 || My[l] < 1) return false;
+    if (l + 1 < nlev &&
+        (Mx[l + 1] != (Mx[l] + ax[l] - 1) / ax[l] || My[l + 1] != (My[l] + ay[l] - 1) / ay[l]))
+      return false;
+  }
+  const int c = nlev - 1;
+  // the CTA grid over the coarsest level: as many rows as allowed, then columns
+  P.Pr = Mx[c] < SC_CTAS ? Mx[c] : SC_CTAS;
+  P.Pc = SC_CTAS / P.Pr;
+  if (P.Pc > My[c]) P.Pc = My[c];
+  for (int p = 0; p <= P.Pr; ++p) P.rb[c][p] = (int)((long long)p * Mx[c] / P.Pr);
+  for (int q = 0; q <= P.Pc; ++q) P.cb[c][q] = (int)((long long)q * My[c] / P.Pc);
+  for (int l = c - 1; l >= 0; --l) {
+    for (int p = 0; p <= P.Pr; ++p) {
+      const int r = P.rb[l + 1][p] * ax[l];
+      P.rb[l][p] = r < Mx[l] ? r : Mx[l];
+    }
+    for (int q = 0; q <= P.Pc; ++q) {
+      const int r = P.cb[l + 1][q] * ay[l];
+      P.cb[l][q] = r < My[l] ? r : My[l];
+    }
+  }
+  int bytes = 0;
+  for (int l = 0; l < nlev; ++l) {
+    int mi = 0, mj = 0;
+    for (int p = 0; p < P.Pr; ++p) mi = P.rb[l][p + 1] - P.rb[l][p] > mi ? P.rb[l][p + 1] - P.rb[l][p] : mi;
+    for (int q = 0; q < P.Pc; ++q) mj = P.cb[l][q + 1] - P.cb[l][q] > mj ? P.cb[l][q + 1] - P.cb[l][q] : mj;
+    P.mi[l] = mi;
+    P.mj[l] = mj;
+    const int cells = mi * mj;
+    P.off4[l] = bytes;
+    bytes += 10 * 16 * cells;
+    P.off2[l] = bytes;
+    bytes += 4 * 8 * cells;
+    bytes = (bytes + 127) / 128 * 128;
+  }
+  P.smem = bytes;
+  return bytes <= max_smem;
+}
+
+// the CTA row / column block that holds row i (column j) of level l
+inline
+#if defined(__CUDACC__)
+    __host__ __device__
+#endif
+    int small_owner(const int *bounds, int parts, int i) {
+  int p = parts - 1;
+  while (p > 0 && bounds[p] > i) --p;
+  return p;
+}
+
+}  // namespace pism_gpu

@@ -408,3 +408,25 @@ def test_lagged_coarse_levels_meet_the_same_tolerance(precision):
     assert abs(st["picard_iterations"] - o.stats.picard_iterations) <= 1
     assert 1 <= st["mg_rebuilds"] < st["picard_iterations"]
     assert rel(vel, ref) < 1e-7
+
+
+@pytest.mark.parametrize("shape,precision", [((201, 201), "mixed"), ((64, 64), "fp64"), ((45, 44), "mixed"),
+                                              ("test_i", "fp64")])
+def test_small_level_cycles_agree_bitwise(shape, precision):
+    """The multigrid's small levels cycled with every CTA holding its block of every level in
+    shared memory (mg_small_kernel 0) and staged from L2 at every step (1): the same
+    arithmetic per cell in the same order, so the same velocities and counts, bit for bit."""
+    if shape == "test_i":
+        g, c, f = V.build_test_i(My=201)
+        c.ssafd_relative_convergence = 5e-7
+        c.ksp_rtol = 1e-12
+    else:
+        g, c, f, _ = S.build_synthetic(shape[0], 4000e3 / (shape[0] - 1), seed=6)
+        c.ksp_rtol = 1e-8
+    c = c.copy(pc_type="mg", precision=precision)
+    out = {}
+    for k in (0, 1):
+        vel, st = _solve_case(g, c.copy(mg_small_kernel=k), f)
+        out[k] = (vel, st["picard_iterations"], st["ksp_iterations"], st["refinement_steps"])
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert out[0][1:] == out[1][1:]
