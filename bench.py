@@ -618,9 +618,9 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = sampler.stop()
     vel_mode = out.clone()
     if args.profile:
+        sampler.stop()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": ms_per_step_local(total_ms, args.steps), "unit": "ms",
                               "profile": True, "solver": {"picard_iterations": picard, "ksp_iterations": ksp}}))
@@ -702,6 +702,7 @@ def main():
         torch.cuda.synchronize()
         e2e_ms += (time.perf_counter() - t0) * 1e3
     e2e_ms /= max(1, args.steps)
+    clocks = sampler.stop()   # sampled over the timed steps and the end-to-end steps alike
     e2e_value = job_time_per_solve(max_over_ranks(e2e_ms, dev), world)
     e2e_same = bool(torch.equal(hout, vel_mode.cpu()))
 

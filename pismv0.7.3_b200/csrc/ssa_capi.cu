@@ -988,7 +988,7 @@ int pism_gpu_ssa_create(const pism_gpu_grid *grid, const pism_gpu_ssa_config *cf
   AL(h->K.r, N); AL(h->K.rhat, N); AL(h->K.p, N); AL(h->K.v, N); AL(h->K.s, N); AL(h->K.t, N);
   AL(h->K.phat, N); AL(h->K.shat, N); AL(h->K.dinv, N); AL(h->K.st, 1);
   AL(h->K32.rhs, N); AL(h->K32.r, N); AL(h->K32.rhat, N); AL(h->K32.p, N); AL(h->K32.v, N);
-  AL(h->K32.s, N); AL(h->K32.t, N); AL(h->K32.phat, N); AL(h->K32.shat, N); AL(h->K32.d, N); AL(h->K32.st, 1);
+  AL(h->K32.t, N); AL(h->K32.phat, N); AL(h->K32.shat, N); AL(h->K32.d, N); AL(h->K32.st, 1);
   AL(h->res_dev, 2);
   h->L.max_blocks = sms * 4;   // persistent grids: one wave at the tile kernels' 4 blocks per SM
   if (mg_plan(grid->Mx, grid->My, h->mg) > 0) {
@@ -1029,7 +1029,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->enthalpy, h->z_dev, h->mask, h->bc, h->bcv, h->taud, h->rhs, h->hardness, h->nuH, h->vel,
                  h->vel_old, h->beta, h->bfrict, h->flags, h->K.r, h->K.rhat, h->K.p, h->K.v, h->K.s, h->K.t,
                  h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev,
-                 h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.s, h->K32.t, h->K32.phat,
+                 h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
                  h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G};
   for (void *p : dev)

@@ -89,4 +89,25 @@ __device__ __forceinline__ float2 from_f2<float2>(const float2 &v) { return v; }
 
 FineF fine_view(const GridDev &g, const Fields &f, const MGHierarchy &H);
 
+// right-hand side accessors of the fine-level multigrid passes: b(q) is the value at cell q.
+// A kernel calls bind() once at its start (after the early exit of a finished solve).
+template <class V>
+struct VecAcc {   // a stored vector
+  const V *p;
+  __device__ __forceinline__ VecAcc bind() const { return *this; }
+  __device__ __forceinline__ float2 operator()(int q) const { return to_f2(p[q]); }
+};
+// BiCGStab's s = r - alpha v, formed where it is read instead of stored (alpha from the
+// device-side Krylov state, as the iteration's other kernels read it)
+struct SAcc {
+  const float2 *r, *v;
+  const KState *st;
+  float al;
+  __device__ __forceinline__ SAcc bind() const { return SAcc{r, v, st, (float)st->alpha}; }
+  __device__ __forceinline__ float2 operator()(int q) const {
+    const float2 rk = r[q], vk = v[q];
+    return make_float2(rk.x - al * vk.x, rk.y - al * vk.y);
+  }
+};
+
 }  // namespace pism_gpu

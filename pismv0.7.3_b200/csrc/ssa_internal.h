@@ -51,7 +51,7 @@ struct Gmres {
 
 // FP32 work vectors of the inner solve of the mixed-precision path
 struct Krylov32 {
-  float2 *rhs, *r, *rhat, *p, *v, *s, *t, *phat, *shat, *d;
+  float2 *rhs, *r, *rhat, *p, *v, *t, *phat, *shat, *d;   // s = r - alpha v is never stored
   KState *st;
 };
 
@@ -140,6 +140,9 @@ void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHiera
                double2 *z, const KState *st);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
                const KState *st);
+// the V-cycle with right-hand side s = r - st->alpha v, formed on the fly (BiCGStab's s)
+void mg_vcycle_s(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
+                 const float2 *v, float2 *z, const KState *st);
 // ---- line block-Jacobi preconditioner (ssa_line.cu) ----
 void line_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const LinePC &lp);
 void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const double2 *b, double2 *z, const KState *st);

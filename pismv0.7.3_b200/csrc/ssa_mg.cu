@@ -323,10 +323,11 @@ __device__ __forceinline__ void store_aggregates(float2 (&rsh)[TILE_I][TILE_J], 
 }
 
 // fine level: b_1 = R (b - A x0), x0 = omega D^-1 b
-template <int AX, int AY, class BV>
-__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const BV *__restrict__ b, float omega, int Mxc,
+template <int AX, int AY, class BA>
+__global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, BA b_in, float omega, int Mxc,
                                                       int Myc, TileM tm, float2 *__restrict__ bc, const KState *st) {
   if (st && st->done) return;
+  const auto b = b_in.bind();
   __shared__ HaloTile<float2> xT, nT;
   __shared__ float2 rsh[TILE_I][TILE_J];
   const GridDev &g = F.g;
@@ -338,11 +339,11 @@ __global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const BV *__restr
     const int k = inside ? i * g.My + j : 0;
     const uint32_t f = F.flags[k];   // issued with the tile loads: one round trip per tile
     const float bta = F.beta[k];
-    const float2 bk = to_f2(b[k]);
+    const float2 bk = b(k);
     __syncthreads();
     load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int ii, int jj) {
       const int q = ii * g.My + jj;
-      const float2 v = fmul4(F.dinv[q], to_f2(b[q]));
+      const float2 v = fmul4(F.dinv[q], b(q));
       return make_float2(omega * v.x, omega * v.y);
     });
     load_halo_tile<float2>(nT, i0, j0, g.Mx, g.My, [&](int ii, int jj) { return F.nuH[ii * g.My + jj]; });
@@ -359,11 +360,12 @@ __global__ void __launch_bounds__(NTm) k_mg0_restrict(FineF F, const BV *__restr
 }
 
 // fine level: x = omega D^-1 b + s P x_1;  z = x + omega D^-1 (b - A x)
-template <int AX, int AY, class BV, class ZV>
-__global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const BV *__restrict__ b, float omega, float corr,
+template <int AX, int AY, class BA, class ZV>
+__global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, BA b_in, float omega, float corr,
                                                   int Myc, const float2 *__restrict__ xc, TileM tm,
                                                   ZV *__restrict__ z, const KState *st) {
   if (st && st->done) return;
+  const auto b = b_in.bind();
   __shared__ HaloTile<float2> xT, nT;
   const GridDev &g = F.g;
   const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
@@ -374,12 +376,12 @@ __global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, const BV *__restrict_
     const int k = inside ? i * g.My + j : 0;
     const uint32_t f = F.flags[k];   // issued with the tile loads: one round trip per tile
     const float bta = F.beta[k];
-    const float2 bk = to_f2(b[k]);
+    const float2 bk = b(k);
     const float4 dk = F.dinv[k];
     __syncthreads();
     load_halo_tile<float2>(xT, i0, j0, g.Mx, g.My, [&](int ii, int jj) {
       const int q = ii * g.My + jj;
-      const float2 v = fmul4(F.dinv[q], to_f2(b[q]));
+      const float2 v = fmul4(F.dinv[q], b(q));
       const float2 c = xc[(ii / AX) * Myc + jj / AY];
       return make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
     });
@@ -647,20 +649,49 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   const int pr = (int)rank / P.Pc, pc = (int)rank % P.Pc;
   const bool active = (int)rank < P.Pr * P.Pc;
   auto cap = [&](int l) { return P.mi[l] * P.mj[l]; };
-  // arrays of level l: blocks 0..8 of A and D^-1 (float4); b, x0, x, z (float2)
+  // arrays of level l: blocks 0..8 of A and D^-1 (float4, cap slots each); b, z (float2, cap
+  // slots each); x0, x (float2, padded: (mi + 2) x (mj + 2) with the halo ring)
   auto A4 = [&](int l) { return reinterpret_cast<float4 *>(sm + P.off4[l]); };
   auto F2 = [&](int l, int a) { return reinterpret_cast<float2 *>(sm + P.off2[l]) + a * cap(l); };
+  auto PAD = [&](int l, int a) {
+    return reinterpret_cast<float2 *>(sm + P.offp[l]) + a * (P.mi[l] + 2) * (P.mj[l] + 2);
+  };
   auto r0 = [&](int l) { return active ? P.rb[l][pr] : 0; };
   auto c0 = [&](int l) { return active ? P.cb[l][pc] : 0; };
   auto ni = [&](int l) { return active ? P.rb[l][pr + 1] - P.rb[l][pr] : 0; };
   auto nj = [&](int l) { return active ? P.cb[l][pc + 1] - P.cb[l][pc] : 0; };
-  // array `a` of level l at cell (ii, jj), from whichever CTA holds it
-  auto fetch = [&](int l, int a, int ii, int jj) {
+  // value of cell (ii, jj) (wrapped indices) of level l in the padded array `a` or, with
+  // pad < 0, in the cap-slot array F2(l, -1 - pad), from whichever CTA holds it
+  auto fetch_pad = [&](int l, int a, int ii, int jj) {
     const int qp = small_owner(P.rb[l], P.Pr, ii), qc = small_owner(P.cb[l], P.Pc, jj);
-    const int s = (ii - P.rb[l][qp]) * P.mj[l] + (jj - P.cb[l][qc]);
-    float2 *base = F2(l, a);
+    const int s = (ii - P.rb[l][qp] + 1) * (P.mj[l] + 2) + (jj - P.cb[l][qc] + 1);
+    float2 *base = PAD(l, a);
     const unsigned owner = (unsigned)(qp * P.Pc + qc);
     return owner == rank ? base[s] : cluster.map_shared_rank(base, owner)[s];
+  };
+  // the halo ring of this CTA's padded array `a` of level l, from the neighbours' interiors
+  auto fill_ring = [&](int l, int a) {
+    const int n_i = ni(l), n_j = nj(l), w = P.mj[l] + 2;
+    const int top = n_j + 2, count = 2 * top + 2 * n_i;
+    float2 *x = PAD(l, a);
+    for (int t = tid; t < count; t += CTA_THREADS) {
+      int pa, pb;   // padded coordinates
+      if (t < top) {
+        pa = 0;
+        pb = t;
+      } else if (t < 2 * top) {
+        pa = n_i + 1;
+        pb = t - top;
+      } else if (t < 2 * top + n_i) {
+        pa = t - 2 * top + 1;
+        pb = 0;
+      } else {
+        pa = t - 2 * top - n_i + 1;
+        pb = n_j + 1;
+      }
+      const int ii = pmod(r0(l) + pa - 1, P.Mx[l]), jj = pmod(c0(l) + pb - 1, P.My[l]);
+      x[pa * w + pb] = fetch_pad(l, a, ii, jj);
+    }
   };
 
   // ---- staging: this CTA's block of every level's operator by bulk copies, b of the first ----
@@ -712,17 +743,20 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
 
   // ---- down: x0 = omega D^-1 b; b_{l+1} = R (b - A x0) ----
   for (int l = 0; l + 1 < P.nlev; ++l) {
-    const int Mx = P.Mx[l], My = P.My[l], mj = P.mj[l], cp = cap(l);
+    const int Mx = P.Mx[l], My = P.My[l], mj = P.mj[l], w = mj + 2, cp = cap(l);
     const float4 *A = A4(l), *D = A4(l) + 9 * cp;
     const float2 *b = F2(l, 0);
-    float2 *x0 = F2(l, 1);
+    float2 *x0 = PAD(l, 0);
     for (int q = tid; q < ni(l) * nj(l); q += CTA_THREADS) {
-      const int li = q / nj(l), s = li * mj + (q - li * nj(l));
+      const int li = q / nj(l), lj = q - li * nj(l), s = li * mj + lj;
       const float2 v = fmul4(D[s], b[s]);
-      x0[s] = make_float2(omega * v.x, omega * v.y);
+      x0[(li + 1) * w + lj + 1] = make_float2(omega * v.x, omega * v.y);
     }
     cluster.sync();
+    fill_ring(l, 0);
+    __syncthreads();
     const int ax = P.ax[l], ay = P.ay[l], R0 = r0(l + 1), C0 = c0(l + 1), ncj = nj(l + 1), nc = ni(l + 1) * ncj;
+    const int i0 = r0(l), j0 = c0(l);
     float2 *bc = F2(l + 1, 0);
     const int span = (4 * nc + 31) & ~31;   // whole warps take part in the shuffles
     for (int base = tid; base < span; base += CTA_THREADS) {
@@ -732,8 +766,11 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
         const int I = R0 + kc / ncj, J = C0 + kc % ncj;
         const int i = I * ax + pi, j = J * ay + pj;
         if (i < Mx && j < My) {
-          const int s = (i - r0(l)) * mj + (j - c0(l));
-          const float2 y = small_apply(A, cp, s, i, j, Mx, My, [&](int ii, int jj) { return fetch(l, 1, ii, jj); });
+          const int li = i - i0, lj = j - j0, s = li * mj + lj;
+          const float2 y = small_apply(A, cp, s, i, j, Mx, My, [&](int ii, int jj) {
+            // (ii, jj) is a neighbour of (i, j): its padded position from the offset
+            return x0[(li + 1 + wdiff(ii, i, Mx)) * w + (lj + 1 + wdiff(jj, j, My))];
+          });
           const float2 bk = b[s];
           ru = bk.x - y.x;
           rv = bk.y - y.y;
@@ -753,16 +790,21 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
     const int l = P.nlev - 1, Myc = P.My[l], Nc = P.Mx[l] * Myc;
     cluster.sync();
     for (int q = tid; q < Nc; q += CTA_THREADS) {
-      const float2 v = fetch(l, 0, q / Myc, q % Myc);
+      const int ii = q / Myc, jj = q % Myc;
+      const int qp = small_owner(P.rb[l], P.Pr, ii), qc = small_owner(P.cb[l], P.Pc, jj);
+      const int s = (ii - P.rb[l][qp]) * P.mj[l] + (jj - P.cb[l][qc]);
+      const unsigned owner = (unsigned)(qp * P.Pc + qc);
+      float2 *base = F2(l, 0);
+      const float2 v = owner == rank ? base[s] : cluster.map_shared_rank(base, owner)[s];
       bsh[2 * q] = v.x;
       bsh[2 * q + 1] = v.y;
     }
     __syncthreads();
     const int lane = tid & 31, warp = tid >> 5, nrows = 2 * ni(l) * nj(l);
-    float *z = reinterpret_cast<float *>(F2(l, 3));
+    float *z = reinterpret_cast<float *>(F2(l, 1));
     const LevelView Lc = S.lev[S.first + l];
-    for (int w = warp; w < nrows; w += CTA_THREADS / 32) {
-      const int q = w >> 1, comp = w & 1, li = q / nj(l), lj = q - li * nj(l);
+    for (int wv = warp; wv < nrows; wv += CTA_THREADS / 32) {
+      const int q = wv >> 1, comp = wv & 1, li = q / nj(l), lj = q - li * nj(l);
       const int r = 2 * ((r0(l) + li) * Myc + c0(l) + lj) + comp;
       double acc = 0.0;
       for (int c = lane; c < S.n; c += 32) acc += S.invT[c * S.n + r] * (double)bsh[c];
@@ -778,25 +820,29 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
 
   // ---- up: x = omega D^-1 b + s P z_{l+1}; z = x + omega D^-1 (b - A x) ----
   for (int l = P.nlev - 2; l >= 0; --l) {
-    const int Mx = P.Mx[l], My = P.My[l], mj = P.mj[l], cp = cap(l);
+    const int Mx = P.Mx[l], My = P.My[l], mj = P.mj[l], w = mj + 2, cp = cap(l);
     const float4 *A = A4(l), *D = A4(l) + 9 * cp;
-    const float2 *b = F2(l, 0), *zc = F2(l + 1, 3);
-    float2 *x = F2(l, 2), *z = F2(l, 3);
+    const float2 *b = F2(l, 0), *zc = F2(l + 1, 1);
+    float2 *x = PAD(l, 1), *z = F2(l, 1);
     const int ax = P.ax[l], ay = P.ay[l], R0 = r0(l + 1), C0 = c0(l + 1), mjc = P.mj[l + 1];
     for (int q = tid; q < ni(l) * nj(l); q += CTA_THREADS) {
       const int li = q / nj(l), lj = q - li * nj(l), s = li * mj + lj;
       const int i = r0(l) + li, j = c0(l) + lj;
       const float2 v = fmul4(D[s], b[s]);
       const float2 c = zc[(i / ax - R0) * mjc + (j / ay - C0)];
-      x[s] = make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+      x[(li + 1) * w + lj + 1] = make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
     }
     cluster.sync();
+    fill_ring(l, 1);
+    __syncthreads();
     const LevelView L = S.lev[S.first + l];
     for (int q = tid; q < ni(l) * nj(l); q += CTA_THREADS) {
       const int li = q / nj(l), lj = q - li * nj(l), s = li * mj + lj;
       const int i = r0(l) + li, j = c0(l) + lj;
-      const float2 xk = x[s];
-      const float2 y = small_apply(A, cp, s, i, j, Mx, My, [&](int ii, int jj) { return fetch(l, 2, ii, jj); });
+      const float2 xk = x[(li + 1) * w + lj + 1];
+      const float2 y = small_apply(A, cp, s, i, j, Mx, My, [&](int ii, int jj) {
+        return x[(li + 1 + wdiff(ii, i, Mx)) * w + (lj + 1 + wdiff(jj, j, My))];
+      });
       const float2 bk = b[s];
       const float2 d = fmul4(D[s], make_float2(bk.x - y.x, bk.y - y.y));
       const float2 zk = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
@@ -1013,8 +1059,8 @@ static void dispatch_ax(int ax, int ay, F22 f22, F21 f21, F12 f12, F11 f11) {
   else f11();
 }
 
-template <class BV, class ZV>
-static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const BV *b, ZV *z,
+template <class BA, class ZV>
+static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, BA b, ZV *z,
                    const KState *st) {
   const FineF F = fine_view(g, f, H);
   const float omega = H.omega, corr = H.correction;
@@ -1024,7 +1070,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(g.Mx, g.My);
     const int nb = blocks_for(Lc, tm.tiles);
-#define MG0R(AX, AY) [&] { k_mg0_restrict<AX, AY, BV><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, C.Mx, C.My, tm, C.b, st); }
+#define MG0R(AX, AY) [&] { k_mg0_restrict<AX, AY, BA><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, C.Mx, C.My, tm, C.b, st); }
     dispatch_ax(H.fine_ax, H.fine_ay, MG0R(2, 2), MG0R(2, 1), MG0R(1, 2), MG0R(1, 1));
 #undef MG0R
     ++launches;
@@ -1077,7 +1123,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(g.Mx, g.My);
     const int nb = blocks_for(Lc, tm.tiles);
-#define MG0P(AX, AY) [&] { k_mg0_post<AX, AY, BV, ZV><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, st); }
+#define MG0P(AX, AY) [&] { k_mg0_post<AX, AY, BA, ZV><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, st); }
     dispatch_ax(H.fine_ax, H.fine_ay, MG0P(2, 2), MG0P(2, 1), MG0P(1, 2), MG0P(1, 1));
 #undef MG0P
     ++launches;
@@ -1087,12 +1133,17 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
 
 void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b, double2 *z,
                const KState *st) {
-  vcycle(Lc, g, f, H, b, z, st);
+  vcycle(Lc, g, f, H, VecAcc<double2>{b}, z, st);
 }
 
 void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
                const KState *st) {
-  vcycle(Lc, g, f, H, b, z, st);
+  vcycle(Lc, g, f, H, VecAcc<float2>{b}, z, st);
+}
+
+void mg_vcycle_s(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
+                 const float2 *v, float2 *z, const KState *st) {
+  vcycle(Lc, g, f, H, SAcc{r, v, st, 0.0f}, z, st);
 }
 
 }  // namespace pism_gpu

@@ -139,20 +139,13 @@ __global__ void __launch_bounds__(NT32) k32_v(FineF F, Tile32 tm, const float2 *
   }
 }
 
-__global__ void __launch_bounds__(NT32) k32_s(int N, const float2 *__restrict__ r, const float2 *__restrict__ v,
-                                              float2 *__restrict__ s, const KState *st) {
+// t = A shat with the dots (t, s) and (t, t); s = r - alpha v is formed here, not stored
+__global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *__restrict__ shat,
+                                              const float2 *__restrict__ r, const float2 *__restrict__ v,
+                                              float2 *__restrict__ tv, double *partials, unsigned *ticket,
+                                              KState *st) {
   if (st->done) return;
   const float al = (float)st->alpha;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    const float2 rk = r[k], vk = v[k];
-    s[k] = make_float2(rk.x - al * vk.x, rk.y - al * vk.y);
-  }
-}
-
-__global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *__restrict__ shat,
-                                              const float2 *__restrict__ s, float2 *__restrict__ tv, double *partials,
-                                              unsigned *ticket, KState *st) {
-  if (st->done) return;
   __shared__ HaloTile<float2> xT, nT;
   double acc[2] = {0.0, 0.0};
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
@@ -160,15 +153,17 @@ __global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *
     float2 y;
     if (!apply32(F, tm, t, shat, xT, nT, k, y)) continue;
     tv[k] = y;
-    acc[0] += dotf(y, s[k]);
+    const float2 rk = r[k], vk = v[k];
+    acc[0] += dotf(y, make_float2(rk.x - al * vk.x, rk.y - al * vk.y));
     acc[1] += dotf(y, y);
   }
   double tot[2];
   if (grid_reduce<2>(acc, partials, ticket, tot)) st->omega = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
 }
 
+// d += alpha phat + omega shat; r = s - omega t with s = r - alpha v formed here
 __global__ void __launch_bounds__(NT32) k32_x(int N, const float2 *__restrict__ phat, const float2 *__restrict__ shat,
-                                              const float2 *__restrict__ s, const float2 *__restrict__ tv,
+                                              const float2 *__restrict__ v, const float2 *__restrict__ tv,
                                               const float2 *__restrict__ rhat, float2 *__restrict__ d,
                                               float2 *__restrict__ r, double *partials, unsigned *ticket,
                                               KState *st) {
@@ -176,7 +171,9 @@ __global__ void __launch_bounds__(NT32) k32_x(int N, const float2 *__restrict__ 
   const float al = (float)st->alpha, om = (float)st->omega;
   double acc[2] = {0.0, 0.0};
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    const float2 ph = phat[k], sh = shat[k], sk = s[k], tk = tv[k];
+    const float2 rk0 = r[k], vk = v[k];
+    const float2 sk = make_float2(rk0.x - al * vk.x, rk0.y - al * vk.y);
+    const float2 ph = phat[k], sh = shat[k], tk = tv[k];
     float2 dk = d[k];
     dk.x += al * ph.x + om * sh.x;
     dk.y += al * ph.y + om * sh.y;
@@ -234,11 +231,10 @@ void launch_mixed_iteration(const Launch &L, const GridDev &g, const Fields &f, 
   k32_p<<<bv, NT32, 0, L.stream>>>(N, K.r, K.v, K.p, K.st);
   mg_vcycle(L, g, f, H, K.p, K.phat, K.st);
   k32_v<<<bt, NT32, 0, L.stream>>>(F, tm, K.phat, K.rhat, K.v, L.partials, L.ticket, K.st);
-  k32_s<<<bv, NT32, 0, L.stream>>>(N, K.r, K.v, K.s, K.st);
-  mg_vcycle(L, g, f, H, K.s, K.shat, K.st);
-  k32_t<<<bt, NT32, 0, L.stream>>>(F, tm, K.shat, K.s, K.t, L.partials, L.ticket, K.st);
-  k32_x<<<bv, NT32, 0, L.stream>>>(N, K.phat, K.shat, K.s, K.t, K.rhat, K.d, K.r, L.partials, L.ticket, K.st);
-  L.tick(5);
+  mg_vcycle_s(L, g, f, H, K.r, K.v, K.shat, K.st);   // s = r - alpha v is not stored
+  k32_t<<<bt, NT32, 0, L.stream>>>(F, tm, K.shat, K.r, K.v, K.t, L.partials, L.ticket, K.st);
+  k32_x<<<bv, NT32, 0, L.stream>>>(N, K.phat, K.shat, K.v, K.t, K.rhat, K.d, K.r, L.partials, L.ticket, K.st);
+  L.tick(4);
 }
 
 }  // namespace pism_gpu

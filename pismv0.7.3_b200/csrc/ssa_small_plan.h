@@ -8,7 +8,8 @@
 // always live on the coarse cell's CTA.  Each CTA keeps its block of every level in its own
 // shared memory, in arrays shaped by the largest block of that level (the same offsets on
 // every CTA, so a neighbour's value is read from the same offset in the neighbour's shared
-// memory).
+// memory); the smoothed iterates x0 and x also carry a one-cell halo ring, filled from the
+// neighbours once per step.
 #pragma once
 
 namespace pism_gpu {
@@ -26,12 +27,11 @@ struct SmallPlan {
   int cb[SC_MAX_LEV][SC_CTAS + 1];     // column boundaries
   int mi[SC_MAX_LEV], mj[SC_MAX_LEV];  // largest block: the shape of every CTA's arrays
   int off4[SC_MAX_LEV];                // byte offset of the level's float4 arrays (9 blocks of A, D^-1)
-  int off2[SC_MAX_LEV];                // byte offset of the level's float2 arrays (b, x0, x, z)
+  int off2[SC_MAX_LEV];                // byte offset of the level's float2 arrays (b, z)
+  int offp[SC_MAX_LEV];                // byte offset of the padded float2 arrays (x0, x) with a halo ring
   int smem;                            // bytes of dynamic shared memory per CTA
 };
 
-// bytes per cell slot: 10 float4 (the nine 2 x 2 blocks and D^-1) + 4 float2 (b, x0, x, z)
-constexpr int SC_BYTES_PER_CELL = 10 * 16 + 4 * 8;
 
 // Plan the split of levels (Mx[l], My[l], ax[l], ay[l]), l = 0 .. nlev-1 from fine to
 // coarse (level l+1 has ceil(Mx[l] / ax[l]) x ceil(My[l] / ay[l]) cells).  Returns false
@@ -77,9 +77,11 @@ inline bool small_plan(int nlev, const int *Mx, const int *My, const int *ax, co
     P.mj[l] = mj;
     const int cells = mi * mj;
     P.off4[l] = bytes;
-    bytes += 10 * 16 * cells;
+    bytes += 10 * 16 * cells;   // the nine 2 x 2 blocks and D^-1
     P.off2[l] = bytes;
-    bytes += 4 * 8 * cells;
+    bytes += 2 * 8 * cells;     // b, z
+    P.offp[l] = bytes;
+    bytes += 2 * 8 * (mi + 2) * (mj + 2);   // x0, x with their halo rings
     bytes = (bytes + 127) / 128 * 128;
   }
   P.smem = bytes;

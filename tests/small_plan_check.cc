@@ -27,8 +27,8 @@ int main() {
     }
     printf("{\"ok\": true, \"Pr\": %d, \"Pc\": %d, \"smem\": %d, \"levels\": [", P.Pr, P.Pc, P.smem);
     for (int l = 0; l < P.nlev; ++l) {
-      printf("%s{\"mi\": %d, \"mj\": %d, \"off4\": %d, \"off2\": %d, \"rb\": [", l ? ", " : "", P.mi[l], P.mj[l],
-             P.off4[l], P.off2[l]);
+      printf("%s{\"mi\": %d, \"mj\": %d, \"off4\": %d, \"off2\": %d, \"offp\": %d, \"rb\": [", l ? ", " : "",
+             P.mi[l], P.mj[l], P.off4[l], P.off2[l], P.offp[l]);
       for (int p = 0; p <= P.Pr; ++p) printf("%s%d", p ? ", " : "", P.rb[l][p]);
       printf("], \"cb\": [");
       for (int q = 0; q <= P.Pc; ++q) printf("%s%d", q ? ", " : "", P.cb[l][q]);

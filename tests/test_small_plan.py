@@ -82,10 +82,12 @@ def test_plans_cover_nest_and_fit(driver):
             # the owner lookup
             assert L["row_owner"] == [next(p for p in range(Pr) if rb[p] <= i < rb[p + 1]) for i in range(mx)]
             assert L["col_owner"] == [next(q for q in range(Pc) if cb[q] <= j < cb[q + 1]) for j in range(my)]
-            # the arrays: 10 float4 then 4 float2 per slot, levels one after another
+            # the arrays: 10 float4 and 2 float2 per slot, then two padded float2 arrays with a
+            # halo ring, levels one after another
             assert L["off4"] >= end and L["off4"] % 128 == 0
             assert L["off2"] == L["off4"] + 160 * mi * mj
-            end = L["off2"] + 32 * mi * mj
+            assert L["offp"] == L["off2"] + 16 * mi * mj
+            end = L["offp"] + 16 * (mi + 2) * (mj + 2)
             assert end <= P["smem"]
             # nesting: a coarse cell's aggregate lives on its CTA
             if l + 1 < len(small):
