@@ -148,9 +148,10 @@ typedef struct pism_gpu_ssa_config {
      iteration counts, not the tolerance the solve meets */
   double mg_rebuild_rtol;
   /* the multigrid's small levels (<= 4096 cells each) in one thread-block cluster:
-     0 each CTA holds a block of every small level in its shared memory (operators staged by
-     bulk asynchronous copies, halos read from the neighbouring CTAs' shared memory), where the
-     blocks fit; 1 the levels are staged from L2 at every step.  Both give the same results;
+     0 every CTA stages each level from L2 at every step; 1 each CTA holds a block of every
+     small level in its shared memory (operators staged by bulk asynchronous copies, halos read
+     from the neighbouring CTAs' shared memory), where the blocks fit.  Both give the same
+     results, bit for bit, in the same time on a B200 (30.6 and 31.4 us per cycle at 801^2);
      a launch-shape knob for the autotuner */
   int    mg_small_kernel;
 } pism_gpu_ssa_config;
@@ -286,6 +287,12 @@ int pism_gpu_ssa_apply_preconditioner(pism_gpu_ssa *h, const double *r_dev, doub
  * initial guess on entry.  *iterations and *rel_residual may be NULL. */
 int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations,
                               double *rel_residual);
+
+/* The same linear solve for the caller's right-hand side b (device, 2N; not x_dev): PETSc's
+ * KSPSolve with any b (SSAFD.cc:1018 passes m_b).  Used to build the learned preconditioner's
+ * training pairs (pism_unet_gpu.h). */
+int pism_gpu_ssa_linear_solve_rhs(pism_gpu_ssa *h, const double *b_dev, double *x_dev, int *iterations,
+                                  double *rel_residual);
 
 /* ---- allocation-free entry point ------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:

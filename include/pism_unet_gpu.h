@@ -75,6 +75,25 @@ int pism_gpu_ssa_learned_features(pism_gpu_ssa *ssa, int stride, float *features
  * (as pism_gpu_ssa_set_initial_guess does). */
 int pism_gpu_ssa_learned_guess(pism_gpu_ssa *ssa, pism_gpu_unet *net, int stride);
 
+/* The learned preconditioner correction inside flexible GMRES (ksp_type PISM_KSP_GMRES; no
+ * reference counterpart: PETSc's PCSetUp / PCApply inside KSPSolve, SSAFD.cc:136-161, 1018,
+ * apply a fixed preconditioner).  With a network attached, every Arnoldi step of the handle's
+ * GMRES solves takes z = M^-1 v from the configured preconditioner and then
+ *   r = v - A z,   s = D^-1 r (D the 2 x 2 diagonal blocks),
+ *   z += rho * N(features, s / rho)   (rho = RMS of s at the network's resolution),
+ * the network N seeing the learned-guess features with channels 6, 7 (driving stress)
+ * replaced by the stride x stride block means of s / rho, its output interpolated back to
+ * the grid.  Right preconditioning lets the preconditioner vary from step to step; the
+ * Krylov solve's FP64 residual test decides every accepted answer as without the network.
+ * net = NULL detaches it.  The network must outlive its use by the handle. */
+int pism_gpu_ssa_set_learned_pc(pism_gpu_ssa *ssa, pism_gpu_unet *net, int stride);
+
+/* The correction's network input for a residual r (device, 2N) at the current nu*H and
+ * beta: a [height][width][8] FP32 device image as above (height, width >= the grid at
+ * `stride`), and rho (device, one double).  For building training data. */
+int pism_gpu_ssa_learned_pc_input(pism_gpu_ssa *ssa, int stride, const double *r_dev, float *image_dev, int height,
+                                  int width, double *rho_dev);
+
 #ifdef __cplusplus
 }
 #endif

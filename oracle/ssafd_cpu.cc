@@ -240,15 +240,16 @@ extern "C" {
 // order) holds the initial guess and receives the last iterate.  par: the Par fields in
 // order.  perm (2N): the oracle's unknown of each PETSc row; block_start (nranks + 1):
 // PETSc's rank blocks.  Per iteration k < *picard_its the arrays ksp_its, t_nuH, t_asm,
-// t_ksp (each max_iterations long, may be NULL) get the KSP iterations and the seconds
-// spent in nu*H + norms, drag + assembly, and the KSP solve.  Returns 0 converged,
+// t_ksp, rel_change (each max_iterations long, may be NULL) get the KSP iterations, the
+// seconds spent in nu*H + norms, drag + assembly and the KSP solve, and the relative nu*H
+// change of the Picard test.  Returns 0 converged,
 // 1 Picard limit reached, or the negative KSP reason of a failed solve.
 int ssafd_cpu_picard(int Mx, int My, const double *par, const double *H, const int *mask, const double *tauc,
                      const double *hardness, const int *bc, const double *b, double *vel, const int *perm,
                      int nranks, const int *block_start, int nthreads, int max_iterations, double picard_rtol,
                      double ksp_rtol, int ksp_maxit, int restart, double reg, double underrelax, int *picard_its,
                      double *norm_out, double *change_out, int *ksp_its, double *t_nuH, double *t_asm,
-                     double *t_ksp) {
+                     double *t_ksp, double *rel_change) {
   if (nthreads > 0) omp_set_num_threads(nthreads);
   Par p;
   std::memcpy(&p, par, sizeof(Par));
@@ -295,6 +296,7 @@ int ssafd_cpu_picard(int Mx, int My, const double *par, const double *H, const i
     if (t_nuH) t_nuH[k] = (t3 - t2) + (k == 0 ? t_pre : 0.0);
     if (t_asm) t_asm[k] = t1 - t0;
     if (t_ksp) t_ksp[k] = t2 - t1;
+    if (rel_change) rel_change[k] = norm > 0 ? change / norm : 0.0;
     *picard_its = k + 1;
     *norm_out = norm;
     *change_out = change;

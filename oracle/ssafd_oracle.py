@@ -1145,7 +1145,8 @@ def picard_native(grid: Grid, cfg: Config, inp: Inputs, hardness, b, vel0, reg, 
 
     Returns (velocity, info) with info = {"status": 0 converged / 1 Picard limit / < 0 KSP
     reason, "picard_iterations", "nuH_norm", "nuH_norm_change", "ksp_iterations" [per
-    iteration], "t_nuH", "t_assemble", "t_ksp" [seconds per iteration]}."""
+    iteration], "t_nuH", "t_assemble", "t_ksp" [seconds per iteration], "rel_change" [the
+    relative nu*H change of each Picard test]}."""
     import ctypes
     if cfg.calving_front_stress_boundary_condition or cfg.nu_bedrock_set or cfg.sub_groundingline:
         raise ValueError("picard_native: CFBC, nu_bedrock and sub_groundingline are not restated natively")
@@ -1155,7 +1156,7 @@ def picard_native(grid: Grid, cfg: Config, inp: Inputs, hardness, b, vel0, reg, 
         D, I = ctypes.c_double, ctypes.c_int
         lib.ssafd_cpu_picard.restype = I
         lib.ssafd_cpu_picard.argtypes = [I, I, P(D), P(D), P(I), P(D), P(D), P(I), P(D), P(D), P(I), I, P(I), I, I,
-                                         D, D, I, I, D, D, P(I), P(D), P(D), P(I), P(D), P(D), P(D)]
+                                         D, D, I, I, D, D, P(I), P(D), P(D), P(I), P(D), P(D), P(D), P(D)]
         lib._picard_bound = True
     Mx, My = grid.Mx, grid.My
     n_it = max_iterations if max_iterations is not None else cfg.max_iterations_ssafd
@@ -1178,7 +1179,7 @@ def picard_native(grid: Grid, cfg: Config, inp: Inputs, hardness, b, vel0, reg, 
     perm = np.ascontiguousarray(perm, dtype=np.int32)
     starts = np.ascontiguousarray(starts, dtype=np.int32)
     its = np.zeros(n_it, dtype=np.int32)
-    t_nuH, t_asm, t_ksp = np.zeros(n_it), np.zeros(n_it), np.zeros(n_it)
+    t_nuH, t_asm, t_ksp, relc = np.zeros(n_it), np.zeros(n_it), np.zeros(n_it), np.zeros(n_it)
     npic = ctypes.c_int(0)
     norm, change = ctypes.c_double(0), ctypes.c_double(0)
     P = ctypes.POINTER
@@ -1192,9 +1193,9 @@ def picard_native(grid: Grid, cfg: Config, inp: Inputs, hardness, b, vel0, reg, 
     st = lib.ssafd_cpu_picard(Mx, My, dp(par), dp(H), ip(mask), dp(tauc), dp(hard), ip(bc), dp(bb), dp(vel),
                               ip(perm), len(starts) - 1, ip(starts), nthreads, n_it, rtol, ksp_rtol, ksp_maxit,
                               restart, reg, underrelax, ctypes.byref(npic), ctypes.byref(norm),
-                              ctypes.byref(change), ip(its), dp(t_nuH), dp(t_asm), dp(t_ksp))
+                              ctypes.byref(change), ip(its), dp(t_nuH), dp(t_asm), dp(t_ksp), dp(relc))
     k = npic.value
     m = k if st >= 0 else k + 1
     return vel, {"status": st, "picard_iterations": k, "nuH_norm": norm.value, "nuH_norm_change": change.value,
                  "ksp_iterations": its[:m].tolist(), "t_nuH": t_nuH[:k].tolist(), "t_assemble": t_asm[:k].tolist(),
-                 "t_ksp": t_ksp[:k].tolist()}
+                 "t_ksp": t_ksp[:k].tolist(), "rel_change": relc[:k].tolist()}

@@ -26,6 +26,7 @@ EXPORTS = [
     "pism_gpu_ssa_set_initial_guess", "pism_gpu_ssa_solve", "pism_gpu_ssa_get_field",
     "pism_gpu_ssa_assemble_rhs", "pism_gpu_ssa_compute_hardness", "pism_gpu_ssa_compute_nuH",
     "pism_gpu_ssa_apply", "pism_gpu_ssa_apply_preconditioner", "pism_gpu_ssa_linear_solve",
+    "pism_gpu_ssa_linear_solve_rhs",
     "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch",
 ]
 # every symbol include/pism_unet_gpu.h declares
@@ -33,6 +34,7 @@ UNET_EXPORTS = [
     "pism_gpu_unet_param_count", "pism_gpu_unet_create", "pism_gpu_unet_destroy", "pism_gpu_unet_last_error",
     "pism_gpu_unet_set_stream", "pism_gpu_unet_set_params", "pism_gpu_unet_get_params", "pism_gpu_unet_forward",
     "pism_gpu_unet_backward", "pism_gpu_unet_adam", "pism_gpu_ssa_learned_features", "pism_gpu_ssa_learned_guess",
+    "pism_gpu_ssa_set_learned_pc", "pism_gpu_ssa_learned_pc_input",
 ]
 
 _lib = None
@@ -64,6 +66,7 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_apply": (I, [V, V, V]),
         "pism_gpu_ssa_apply_preconditioner": (I, [V, V, V]),
         "pism_gpu_ssa_linear_solve": (I, [V, V, P(I), P(D)]),
+        "pism_gpu_ssa_linear_solve_rhs": (I, [V, V, V, P(I), P(D)]),
         "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
         "pism_gpu_ssa_solve_batch": (I, [V, V, I, I, P(CMember), P(CStats)]),
         "pism_gpu_unet_param_count": (C.c_longlong, []),
@@ -78,6 +81,8 @@ def load() -> C.CDLL:
         "pism_gpu_unet_adam": (I, [V, C.c_float, C.c_float, C.c_float, C.c_float]),
         "pism_gpu_ssa_learned_features": (I, [V, I, V, I, I]),
         "pism_gpu_ssa_learned_guess": (I, [V, V, I]),
+        "pism_gpu_ssa_set_learned_pc": (I, [V, V, I]),
+        "pism_gpu_ssa_learned_pc_input": (I, [V, I, V, V, I, I, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

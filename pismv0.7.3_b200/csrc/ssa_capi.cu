@@ -88,6 +88,14 @@ struct pism_gpu_ssa {
   // the learned initial guess: feature image and network output
   float *lfeat = nullptr, *lout = nullptr;
   size_t lcap = 0;   // pixels allocated
+  // the learned preconditioner correction inside FGMRES (pism_gpu_ssa_set_learned_pc)
+  struct LearnedPC {
+    pism_gpu_unet *net = nullptr;
+    int stride = 1, height = 0, width = 0;
+    float *img = nullptr, *out = nullptr;
+    double2 *r = nullptr;
+    double *part = nullptr, *rho = nullptr;
+  } lpc;
   std::string err;
   pism_gpu_ssa_stats stats{};
 };
@@ -660,6 +668,32 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *st
   return PISM_GPU_SSA_OK;
 }
 
+// ---- the learned preconditioner correction ----
+// After z = M^-1 v: r = v - A z, the network's input from the solve's features and the
+// block-Jacobi-scaled residual D^-1 r (normalised by its RMS rho), and z += rho * its output
+// interpolated to the grid.  Right preconditioning in FGMRES allows a preconditioner that
+// changes from one step to the next, so the correction may be any function of v; the FP64
+// residual test of the Krylov solve decides every accepted answer as without it.
+int learned_correction(pism_gpu_ssa *h, const double2 *v, double2 *z, const int *done) {
+  auto &P = h->lpc;
+  const Fields f = fields_of(h);
+  launch_pc_residual(h->L, h->g, f, v, z, P.r, h->G.st);
+  pism_unet::launch_features(h->stream, h->g.Mx, h->g.My, P.stride, h->H, h->bed, h->tauc, h->hardness, h->mask,
+                             h->taud, P.img, P.height, P.width);
+  pism_unet::launch_pc_input(h->stream, h->g.Mx, h->g.My, P.stride, P.r, h->K.dinv, P.img, P.height, P.width, P.part,
+                             P.rho, done);
+  cudaStream_t ns = pism_unet::stream_of(P.net);
+  pism_gpu_unet_set_stream(P.net, h->stream);
+  const int rc = pism_gpu_unet_forward(P.net, P.img, 1, P.height, P.width, P.out);
+  pism_gpu_unet_set_stream(P.net, ns);
+  if (rc != PISM_GPU_SSA_OK)
+    return fail(h, rc, "learned preconditioner: network forward failed: %s", pism_gpu_unet_last_error(P.net));
+  pism_unet::launch_pc_correct(h->stream, P.out, P.height, P.width, P.stride, h->g.Mx, h->g.My, P.rho, z, done);
+  h->L.tick(22);   // features, input (2), network (18), correction; the residual ticks its own
+  CK(h, cudaGetLastError());
+  return PISM_GPU_SSA_OK;
+}
+
 // ---- one linear solve: restarted flexible GMRES(m) on the device (PETSc's default KSP
 // type, restart gmres_restart), right-preconditioned by the active preconditioner ----
 int linear_solve_gmres(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *status_out) {
@@ -689,7 +723,13 @@ int linear_solve_gmres(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, i
     const MGHierarchy *mg = active_mg(h);
     const LinePC *line = active_line(h);
     for (int q = 0; q < chunk; ++q) {
-      launch_gmres_step(h->L, g, f, h->G, h->K.dinv, mg, line, j);
+      if (h->lpc.net) {
+        launch_gmres_precondition(h->L, g, f, h->G, h->K.dinv, mg, line, j);
+        RET(learned_correction(h, h->G.V + (size_t)j * h->N, h->G.Z + (size_t)j * h->N, &h->G.st->done));
+        launch_gmres_orthogonalize(h->L, g, f, h->G, j);
+      } else {
+        launch_gmres_step(h->L, g, f, h->G, h->K.dinv, mg, line, j);
+      }
       if (j == m - 1) {   // end of a cycle: x += Z y, then a restart unless converged
         launch_gmres_update(h->L, g, h->G, x);
         launch_gmres_residual(h->L, g, f, h->G, h->rhs, x, 0);
@@ -1031,7 +1071,8 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->K.phat, h->K.shat, h->K.dinv, h->K.st, h->partials, h->ticket, h->norm_dev, h->zd_dev,
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
-                 h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G};
+                 h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G, h->lpc.img, h->lpc.out,
+                 h->lpc.r, h->lpc.part, h->lpc.rho};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -1249,6 +1290,18 @@ int pism_gpu_ssa_apply_preconditioner(pism_gpu_ssa *h, const double *r_dev, doub
   return PISM_GPU_SSA_OK;
 }
 
+int pism_gpu_ssa_linear_solve_rhs(pism_gpu_ssa *h, const double *b_dev, double *x_dev, int *iterations,
+                                  double *rel_residual) {
+  if (!h || !b_dev || !x_dev) return PISM_GPU_SSA_EINVAL;
+  if (b_dev == x_dev) return fail(h, PISM_GPU_SSA_EINVAL, "linear_solve_rhs: b and x must be different vectors");
+  // the solve reads its right-hand side through h->rhs (outside any captured graph)
+  double2 *keep = h->rhs;
+  h->rhs = const_cast<double2 *>(reinterpret_cast<const double2 *>(b_dev));
+  const int rc = pism_gpu_ssa_linear_solve(h, x_dev, iterations, rel_residual);
+  h->rhs = keep;
+  return rc;
+}
+
 int pism_gpu_ssa_linear_solve(pism_gpu_ssa *h, double *x_dev, int *iterations, double *rel_residual) {
   if (!h || !x_dev) return PISM_GPU_SSA_EINVAL;
   DeviceGuard dg(h->device);
@@ -1326,6 +1379,58 @@ int pism_gpu_ssa_learned_guess(pism_gpu_ssa *h, pism_gpu_unet *net, int stride) 
   pism_unet::launch_velocity(h->stream, h->lout, hh, ww, stride, h->g.Mx, h->g.My, 31556925.9747, h->vel);
   CK(h, cudaGetLastError());
   CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_set_learned_pc(pism_gpu_ssa *h, pism_gpu_unet *net, int stride) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  auto &P = h->lpc;
+  if (!net) {
+    P.net = nullptr;
+    return PISM_GPU_SSA_OK;
+  }
+  if (pism_unet::device_of(net) != h->device)
+    return fail(h, PISM_GPU_SSA_EINVAL, "network and solver on different devices");
+  if (stride < 1 || stride > 2) return fail(h, PISM_GPU_SSA_EINVAL, "stride must be 1 or 2");
+  const int hh = ((h->g.Mx + stride - 1) / stride + 7) / 8 * 8, ww = ((h->g.My + stride - 1) / stride + 7) / 8 * 8;
+  if (!P.r || hh != P.height || ww != P.width) {
+    for (void *q : {(void *)P.img, (void *)P.out, (void *)P.r, (void *)P.part, (void *)P.rho})
+      if (q) cudaFree(q);
+    P = {};
+    CK(h, cudaMalloc((void **)&P.img, (size_t)hh * ww * 8 * sizeof(float)));
+    CK(h, cudaMemset(P.img, 0, (size_t)hh * ww * 8 * sizeof(float)));
+    CK(h, cudaMalloc((void **)&P.out, (size_t)hh * ww * 2 * sizeof(float)));
+    CK(h, cudaMalloc((void **)&P.r, sizeof(double2) * h->N));
+    CK(h, cudaMalloc((void **)&P.part, sizeof(double) * pism_unet::pc_parts(hh, ww)));
+    CK(h, cudaMalloc((void **)&P.rho, sizeof(double)));
+  }
+  P.net = net;
+  P.stride = stride;
+  P.height = hh;
+  P.width = ww;
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_learned_pc_input(pism_gpu_ssa *h, int stride, const double *r_dev, float *image_dev, int height,
+                                  int width, double *rho_dev) {
+  if (!h || !r_dev || !image_dev || !rho_dev) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  int hh = 0, ww = 0;
+  RET(learned_image(h, stride, &hh, &ww));
+  if (height < (h->g.Mx + stride - 1) / stride || width < (h->g.My + stride - 1) / stride)
+    return fail(h, PISM_GPU_SSA_EINVAL, "image %d x %d is smaller than the grid at stride %d", height, width, stride);
+  RET(pc_setup(h));   // D^-1 at the current nu*H and beta
+  double *part = nullptr;
+  CK(h, cudaMalloc((void **)&part, sizeof(double) * pism_unet::pc_parts(height, width)));
+  pism_unet::launch_features(h->stream, h->g.Mx, h->g.My, stride, h->H, h->bed, h->tauc, h->hardness, h->mask,
+                             h->taud, image_dev, height, width);
+  pism_unet::launch_pc_input(h->stream, h->g.Mx, h->g.My, stride, (const double2 *)r_dev, h->K.dinv, image_dev,
+                             height, width, part, rho_dev, nullptr);
+  const cudaError_t e = cudaGetLastError();
+  cudaStreamSynchronize(h->stream);
+  cudaFree(part);
+  CK(h, e);
   return PISM_GPU_SSA_OK;
 }
 

@@ -132,6 +132,13 @@ void launch_gmres_residual(const Launch &L, const GridDev &g, const Fields &f, c
                            const double2 *x, int init);
 void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
                        const MGHierarchy *mg, const LinePC *line, int j);
+// the two halves of an Arnoldi step: z_j = M^-1 v_j, then w = A z_j orthogonalised
+void launch_gmres_precondition(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G,
+                               const double4 *dinv, const MGHierarchy *mg, const LinePC *line, int j);
+void launch_gmres_orthogonalize(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, int j);
+// r = v - A z (FP64), skipped once st->done
+void launch_pc_residual(const Launch &L, const GridDev &g, const Fields &f, const double2 *v, const double2 *z,
+                        double2 *r, const KState *st);
 void launch_gmres_update(const Launch &L, const GridDev &g, const Gmres &G, double2 *x);
 void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
 void mg_setup_fine(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);

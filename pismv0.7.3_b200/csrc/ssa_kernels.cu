@@ -1115,23 +1115,53 @@ void launch_gmres_residual(const Launch &L, const GridDev &g, const Fields &f, c
   k_gm_scale0<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.V, G.gs);
 }
 
-void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
-                       const MGHierarchy *mg, const LinePC *line, int j) {
-  L.tick(mg || line ? 3 : 4);
-  TileMap tm = make_tiles(g);
+void launch_gmres_precondition(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G,
+                               const double4 *dinv, const MGHierarchy *mg, const LinePC *line, int j) {
   const int N = g.Mx * g.My;
   const double2 *vj = G.V + (size_t)j * N;
-  double2 *zj = G.Z + (size_t)j * N, *w = G.V + (size_t)(j + 1) * N;
-  if (mg)
+  double2 *zj = G.Z + (size_t)j * N;
+  if (mg) {
     mg_vcycle(L, g, f, *mg, vj, zj, G.st);
-  else if (line)
+  } else if (line) {
     line_apply(L, g, *line, vj, zj, G.st);
-  else
+  } else {
+    L.tick();
     k_gm_jacobi<<<grid_for(L, N), NT, 0, L.stream>>>(N, vj, dinv, zj, G.st);
+  }
+}
+
+void launch_gmres_orthogonalize(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, int j) {
+  L.tick(3);
+  TileMap tm = make_tiles(g);
+  const int N = g.Mx * g.My;
+  double2 *zj = G.Z + (size_t)j * N, *w = G.V + (size_t)(j + 1) * N;
   k_gm_apply_dots<<<grid_for_tiles(L, tm.tiles), NT, 0, L.stream>>>(g, tm, stencil_const(g, f), f.flags, f.nuH, f.beta,
                                                                     zj, G.V, w, j, G.partials, L.ticket, G.st, G.gs);
   k_gm_orth<<<grid_for(L, N), NT, 0, L.stream>>>(N, G.V, w, j, G.m, G.partials, L.ticket, G.st, G.gs);
   k_gm_scale_next<<<grid_for(L, N), NT, 0, L.stream>>>(N, w, G.st, G.gs);
+}
+
+void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, const double4 *dinv,
+                       const MGHierarchy *mg, const LinePC *line, int j) {
+  launch_gmres_precondition(L, g, f, G, dinv, mg, line, j);
+  launch_gmres_orthogonalize(L, g, f, G, j);
+}
+
+// r = v - y where y = A z (the residual the learned correction sees); skipped once done
+__global__ void k_pc_residual(int N, const double2 *__restrict__ v, double2 *__restrict__ y, const KState *st) {
+  if (st && st->done) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 vk = v[k], yk = y[k];
+    y[k] = make_double2(vk.x - yk.x, vk.y - yk.y);
+  }
+}
+
+void launch_pc_residual(const Launch &L, const GridDev &g, const Fields &f, const double2 *v, const double2 *z,
+                        double2 *r, const KState *st) {
+  launch_apply(L, g, f, z, r);
+  L.tick();
+  const int N = g.Mx * g.My;
+  k_pc_residual<<<grid_for(L, N), NT, 0, L.stream>>>(N, v, r, st);
 }
 
 void launch_pc_apply(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const MGHierarchy *mg,

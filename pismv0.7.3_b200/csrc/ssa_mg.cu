@@ -1087,7 +1087,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     ++launches;
   }
   // the small levels on one thread-block cluster
-  if (H.small_dsmem && H.small_kernel == 0) {
+  if (H.small_dsmem && H.small_kernel == 1) {
     SmallDs S;
     S.plan = reinterpret_cast<const SmallPlan *>(H.small_plan_dev);
     S.lev = reinterpret_cast<const LevelView *>(H.views);

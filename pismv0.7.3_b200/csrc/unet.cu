@@ -607,6 +607,101 @@ __global__ void k_velocity(const float *__restrict__ y, int height, int width, i
   }
 }
 
+// ---- the learned preconditioner correction: the residual's image and the correction ----
+constexpr int PC_THREADS = 256;
+
+// channels 6, 7 of the image = the stride x stride block means of s = D^-1 r (the
+// block-Jacobi-scaled residual, in velocity units); per block the partial sum of their squares
+__global__ void __launch_bounds__(PC_THREADS) k_pc_image(int Mx, int My, int stride, const double2 *__restrict__ r,
+                                                          const double4 *__restrict__ dinv, float *__restrict__ img,
+                                                          int height, int width, double *__restrict__ part,
+                                                          const int *done) {
+  if (done && *done) return;
+  double acc = 0.0;
+  const long long n = (long long)height * width;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(q / width), J = (int)(q % width);
+    double su = 0.0, sv = 0.0;
+    int cnt = 0;
+    for (int a = 0; a < stride; ++a)
+      for (int b = 0; b < stride; ++b) {
+        const int i = I * stride + a, j = J * stride + b;
+        if (i < Mx && j < My) {
+          const size_t k = (size_t)i * My + j;
+          const double4 d = dinv[k];
+          const double2 rk = r[k];
+          su += d.x * rk.x + d.y * rk.y;
+          sv += d.z * rk.x + d.w * rk.y;
+          ++cnt;
+        }
+      }
+    if (cnt > 0) {
+      su /= cnt;
+      sv /= cnt;
+    }
+    img[q * 8 + 6] = (float)su;
+    img[q * 8 + 7] = (float)sv;
+    acc += su * su + sv * sv;
+  }
+  __shared__ double sh[PC_THREADS / 32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < PC_THREADS / 32; ++w) t += sh[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// rho = RMS of the residual channels (every block sums the partials in the same order);
+// channels 6, 7 scaled by 1 / rho; block 0 stores rho
+__global__ void __launch_bounds__(PC_THREADS) k_pc_scale(float *__restrict__ img, int height, int width,
+                                                          const double *__restrict__ part, int nparts,
+                                                          double *__restrict__ rho_out, const int *done) {
+  if (done && *done) return;
+  __shared__ double rho_sh;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < nparts; ++b) t += part[b];
+    rho_sh = sqrt(t / (2.0 * (double)height * width));
+    if (blockIdx.x == 0) *rho_out = rho_sh;
+  }
+  __syncthreads();
+  const double rho = rho_sh;
+  const float inv = rho > 0.0 ? (float)(1.0 / rho) : 0.0f;
+  const long long n = (long long)height * width;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    img[q * 8 + 6] *= inv;
+    img[q * 8 + 7] *= inv;
+  }
+}
+
+// z += rho * (the network's output interpolated to the grid, as k_velocity interpolates)
+__global__ void k_pc_correct(const float *__restrict__ y, int height, int width, int stride, int Mx, int My,
+                             const double *__restrict__ rho, double2 *__restrict__ z, const int *done) {
+  if (done && *done) return;
+  const double s = *rho;
+  const long long n = (long long)Mx * My;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / My), j = (int)(k % My);
+    const int I0 = i / stride, J0 = j / stride;
+    const int I1 = min(I0 + (i % stride ? 1 : 0), height - 1), J1 = min(J0 + (j % stride ? 1 : 0), width - 1);
+    double u = 0.0, v = 0.0;
+    const int Is[2] = {I0, I1}, Js[2] = {J0, J1};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const float2 o = reinterpret_cast<const float2 *>(y)[(size_t)Is[a] * width + Js[b]];
+        u += (double)o.x;
+        v += (double)o.y;
+      }
+    const double2 zk = z[k];
+    z[k] = make_double2(zk.x + 0.25 * s * u, zk.y + 0.25 * s * v);
+  }
+}
+
 }  // namespace pism_unet
 
 // ---------------------------------------------------------------------------
@@ -742,6 +837,20 @@ void launch_features(cudaStream_t s, int Mx, int My, int stride, const double *H
                      int height, int width) {
   k_features<<<grid_for((long long)height * width), 256, 0, s>>>(Mx, My, stride, H, bed, tauc, hardness, mask, taud,
                                                                   out, height, width);
+}
+
+int pc_parts(int height, int width) { return std::min(grid_for((long long)height * width, PC_THREADS), 592); }
+
+void launch_pc_input(cudaStream_t s, int Mx, int My, int stride, const double2 *r, const double4 *dinv, float *img,
+                     int height, int width, double *part, double *rho, const int *done) {
+  const int nb = pc_parts(height, width);
+  k_pc_image<<<nb, PC_THREADS, 0, s>>>(Mx, My, stride, r, dinv, img, height, width, part, done);
+  k_pc_scale<<<nb, PC_THREADS, 0, s>>>(img, height, width, part, nb, rho, done);
+}
+
+void launch_pc_correct(cudaStream_t s, const float *y, int height, int width, int stride, int Mx, int My,
+                       const double *rho, double2 *z, const int *done) {
+  k_pc_correct<<<grid_for((long long)Mx * My), 256, 0, s>>>(y, height, width, stride, Mx, My, rho, z, done);
 }
 
 void launch_velocity(cudaStream_t s, const float *y, int height, int width, int stride, int Mx, int My,

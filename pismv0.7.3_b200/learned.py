@@ -306,3 +306,84 @@ def evaluate(net: UNet, data):
         net.forward(x[None].contiguous())
         out.append(net.backward(t[None].contiguous(), w[None].contiguous()))
     return float(np.mean(out))
+
+
+# ---------------------------------------------------------------------------
+# the learned preconditioner correction inside flexible GMRES
+# ---------------------------------------------------------------------------
+PC_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_ssa_pc_10km.npz")
+
+
+def set_learned_pc(ssa, net, stride: int = 1):
+    """attach the correction network to the handle's GMRES solves (net None detaches it)"""
+    ssa._check(ssa.lib.pism_gpu_ssa_set_learned_pc(ssa._h, net._h if net is not None else None, stride),
+               "set_learned_pc")
+
+
+def pc_input(ssa, r, stride: int = 1):
+    """the correction network's input for a residual r (CUDA float64 [Mx, My, 2]) at the
+    handle's current nu*H and beta: (image [H8, W8, 8] float32, rho as a 0-d float64 tensor)"""
+    import torch
+    hh, ww = image_shape(*ssa.shape, stride)
+    img = torch.zeros((hh, ww, IN_CHANNELS), dtype=torch.float32, device=r.device)
+    rho = torch.zeros((), dtype=torch.float64, device=r.device)
+    rr = r.contiguous()
+    ssa._check(ssa.lib.pism_gpu_ssa_learned_pc_input(ssa._h, stride, _ptr(rr), _ptr(img), hh, ww, _ptr(rho)),
+               "learned_pc_input")
+    return img, rho
+
+
+def pc_config(c: SSAConfig) -> SSAConfig:
+    """the FP64 FGMRES(30) + multigrid set-up the correction works inside"""
+    return c.copy(pc_type="mg", precision="fp64", ksp_type="gmres", gmres_restart=30, graphs=2)
+
+
+def generate_pc(seeds, M: int = 401, samples: int = 4, picard_rtol: float = 1e-2, device: int = 0, log=None):
+    """Training pairs of the correction from seeded sheets: each sheet is solved to a Picard
+    tolerance of picard_rtol (an iterate on the way to the solution, where the operator has
+    the structure the linear solves see), then for `samples` random vectors v the residual
+    the multigrid cycle leaves, r = v - A M^-1 v, and the error that removes it, e = A^-1 r
+    (a linear solve to 1e-10).  Input: the network image of r (features + the block means
+    of D^-1 r / rho); target: e / rho at the cells.  Returns [(x, t, w)] on the device."""
+    import torch
+    from .ssa import SSAFD
+    dev = torch.device("cuda", device)
+    out = []
+    rng = torch.Generator(device=dev)
+    s = None
+    try:
+        for q, seed in enumerate(seeds):
+            g, c, f, _ = training_case(seed, M)
+            cfg = pc_config(c).copy(ssafd_relative_convergence=picard_rtol, ksp_rtol=1e-8)
+            if s is None:
+                s = SSAFD(g, cfg, device=device)
+            else:
+                s.set_config(cfg)
+            s.set_inputs(**{k: f[k] for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
+            s.set_initial_guess(torch.zeros((M, M, 2), dtype=torch.float64, device=dev))
+            s.solve(out=torch.empty((M, M, 2), dtype=torch.float64, device=dev))
+            s.set_config(cfg.copy(ksp_rtol=1e-10))
+            hh, ww = image_shape(M, M, 1)
+            mask = torch.tensor(f["mask"], device=dev)
+            w = torch.zeros((hh, ww), dtype=torch.float32, device=dev)
+            w[:M, :M] = torch.where((mask == 2) | (mask == 3), 1.0, 0.2).float()
+            rng.manual_seed(int(seed))
+            for _ in range(samples):
+                v = torch.randn((M, M, 2), dtype=torch.float64, device=dev, generator=rng)
+                z = torch.empty_like(v)
+                s.apply_preconditioner(v, z)
+                az = torch.empty_like(v)
+                s.apply(z, az)
+                r = v - az
+                img, rho = pc_input(s, r, 1)
+                e = torch.zeros_like(r)
+                s.linear_solve_rhs(r, e)
+                t = torch.zeros((hh, ww, 2), dtype=torch.float32, device=dev)
+                t[:M, :M] = (e / rho).float()
+                out.append((img, t, w))
+            if log:
+                log(f"pc case {q} seed {seed}: {samples} samples")
+    finally:
+        if s is not None:
+            s.close()
+    return out

@@ -287,6 +287,16 @@ class SSAFD:
         self._check(self.lib.pism_gpu_ssa_apply_preconditioner(self._h, C.c_void_p(r_dev.data_ptr()),
                                                                C.c_void_p(z_dev.data_ptr())), "PCApply")
 
+    def linear_solve_rhs(self, b_dev, x_dev):
+        """A x = b for a device right-hand side b ([Mx, My, 2] float64 CUDA); x holds the initial
+        guess and receives the solution.  Returns (iterations, relative residual)."""
+        its = C.c_int(0)
+        res = C.c_double(0)
+        self._check(self.lib.pism_gpu_ssa_linear_solve_rhs(self._h, C.c_void_p(b_dev.data_ptr()),
+                                                           C.c_void_p(x_dev.data_ptr()), C.byref(its), C.byref(res)),
+                    "KSPSolve")
+        return its.value, res.value
+
     def linear_solve(self, x_dev):
         its = C.c_int(0)
         res = C.c_double(0)

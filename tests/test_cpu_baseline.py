@@ -90,13 +90,15 @@ def test_native_picard_refuses_what_it_does_not_restate():
 
 
 def test_whole_solve_estimate_scales_the_sample_by_the_recorded_run():
+    """cost model: a Picard iteration costs (setup + GMRES iterations) GMRES iterations"""
     b = _bench()
-    full = {"threads": 8, "cumulative_s": [5.0, 9.0, 13.0], "total_s": {"1e-06": 1300.0, "0.0001": 650.0},
-            "picard_iterations": {"1e-06": 350, "0.0001": 180}}
-    est, how = b.cpu_estimate(6.5, 3, 1e-6, full=full)
-    assert est == pytest.approx(6.5 * 1300.0 / 13.0 * 1e3)
-    assert "x 100.00" in how
-    est4, _ = b.cpu_estimate(2.5, 1, 1e-4, full=full)
-    assert est4 == pytest.approx(2.5 * 650.0 / 5.0 * 1e3)
+    full = {"threads": 8, "picard_iterations": {"1e-06": 350, "0.0001": 180},
+            "ksp_iterations": {"1e-06": 10000, "0.0001": 8000}, "first_ksp_iterations": [100, 200, 300],
+            "setup_iterations": 10.0}
+    est, how = b.cpu_estimate(6.6, 3, 1e-6, full=full)
+    assert est == pytest.approx(6.6 * (10000 + 350 * 10.0) / (300 + 3 * 10.0) * 1e3)
+    assert "350 Picard iterations" in how
+    est4, _ = b.cpu_estimate(2.2, 1, 1e-4, full=full)
+    assert est4 == pytest.approx(2.2 * (8000 + 180 * 10.0) / (100 + 10.0) * 1e3)
     assert b.cpu_estimate(1.0, 3, 1e-7, full=full)[0] is None
     assert b.cpu_estimate(1.0, 4, 1e-6, full=full)[0] is None

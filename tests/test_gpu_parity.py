@@ -413,9 +413,9 @@ def test_lagged_coarse_levels_meet_the_same_tolerance(precision):
 @pytest.mark.parametrize("shape,precision", [((201, 201), "mixed"), ((64, 64), "fp64"), ((45, 44), "mixed"),
                                               ("test_i", "fp64")])
 def test_small_level_cycles_agree_bitwise(shape, precision):
-    """The multigrid's small levels cycled with every CTA holding its block of every level in
-    shared memory (mg_small_kernel 0) and staged from L2 at every step (1): the same
-    arithmetic per cell in the same order, so the same velocities and counts, bit for bit."""
+    """The multigrid's small levels staged from L2 at every step (mg_small_kernel 0) and held
+    by every CTA as a block of every level in shared memory (1): the same arithmetic per cell
+    in the same order, so the same velocities and counts, bit for bit."""
     if shape == "test_i":
         g, c, f = V.build_test_i(My=201)
         c.ssafd_relative_convergence = 5e-7
