@@ -610,7 +610,7 @@ def main():
     torch.cuda.synchronize()
     total_ms = 0.0
     launches = 0
-    picard, ksp, refine, rebuilds = [], [], [], []
+    picard, ksp, refine, rebuilds, step_ms = [], [], [], [], []
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -619,6 +619,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1)
+        step_ms.append(e0.elapsed_time(e1))
         st = s.stats()
         # the solver's own count, plus the learned guess: features, 18 network kernels, velocity
         launches += st["kernel_launches"] + (20 if net is not None else 0)
@@ -702,7 +703,7 @@ def main():
     hout = torch.empty((M, M, 2), dtype=torch.float64).pin_memory()
     h2d = sum(v.numel() * 8 for v in hfields.values()) + (0 if net is not None else hzero.numel() * 8)
     d2h = hout.numel() * 8
-    e2e_ms = 0.0
+    e2e_ms, e2e_steps = 0.0, []
     for _ in range(max(1, args.steps)):
         flush.fill_(1.0)
         torch.cuda.synchronize()
@@ -711,7 +712,8 @@ def main():
         prime(s, net is not None, hzero.numpy())
         s.solve(out=hout.numpy())
         torch.cuda.synchronize()
-        e2e_ms += (time.perf_counter() - t0) * 1e3
+        e2e_steps.append((time.perf_counter() - t0) * 1e3)
+        e2e_ms += e2e_steps[-1]
     e2e_ms /= max(1, args.steps)
     clocks = sampler.stop()   # sampled over the timed steps and the end-to-end steps alike
     e2e_value = job_time_per_solve(max_over_ranks(e2e_ms, dev), world)
@@ -768,7 +770,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "velocity_error_vs_fp64_oracle": headline_error,
         "solver": {"picard_iterations": picard, "ksp_iterations": ksp, "converged": st["converged"],
-                   "refinement_steps": refine, "mg_rebuilds": rebuilds,
+                   "refinement_steps": refine, "mg_rebuilds": rebuilds, "step_ms": step_ms,
                    "strategy": st["strategy"], "final_linear_residual": st["final_linear_residual"]},
         "comparison": {"other_mode": "plain" if args.mode == "fast" else "fast", "other_ms": other_ms,
                        "other_picard_iterations": st_other["picard_iterations"],
@@ -779,7 +781,7 @@ def main():
                        "accuracy": accuracy},
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": max(1, args.steps), "same_velocity_as_timed": e2e_same},
+                "steps": max(1, args.steps), "step_ms": e2e_steps, "same_velocity_as_timed": e2e_same},
         "gpu_launches": launches,
         "clocks": clocks,
     }

@@ -80,10 +80,12 @@ int pism_gpu_ssa_learned_guess(pism_gpu_ssa *ssa, pism_gpu_unet *net, int stride
  * apply a fixed preconditioner).  With a network attached, every Arnoldi step of the handle's
  * GMRES solves takes z = M^-1 v from the configured preconditioner and then
  *   r = v - A z,   s = D^-1 r (D the 2 x 2 diagonal blocks),
- *   z += rho * N(features, s / rho)   (rho = RMS of s at the network's resolution),
+ *   d = rho * N(features, s / rho)   (rho = RMS of s at the network's resolution),
+ *   z += gamma d,   gamma = (r, A d) / (A d, A d),
  * the network N seeing the learned-guess features with channels 6, 7 (driving stress)
  * replaced by the stride x stride block means of s / rho, its output interpolated back to
- * the grid.  Right preconditioning lets the preconditioner vary from step to step; the
+ * the grid; gamma makes the corrected step leave no larger a residual than the
+ * preconditioner alone.  Right preconditioning lets the preconditioner vary from step to step; the
  * Krylov solve's FP64 residual test decides every accepted answer as without the network.
  * net = NULL detaches it.  The network must outlive its use by the handle. */
 int pism_gpu_ssa_set_learned_pc(pism_gpu_ssa *ssa, pism_gpu_unet *net, int stride);

@@ -93,8 +93,8 @@ struct pism_gpu_ssa {
     pism_gpu_unet *net = nullptr;
     int stride = 1, height = 0, width = 0;
     float *img = nullptr, *out = nullptr;
-    double2 *r = nullptr;
-    double *part = nullptr, *rho = nullptr;
+    double2 *r = nullptr, *d = nullptr, *ad = nullptr;
+    double *part = nullptr, *rho = nullptr, *gamma = nullptr;
   } lpc;
   std::string err;
   pism_gpu_ssa_stats stats{};
@@ -670,10 +670,12 @@ int linear_solve(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, int *st
 
 // ---- the learned preconditioner correction ----
 // After z = M^-1 v: r = v - A z, the network's input from the solve's features and the
-// block-Jacobi-scaled residual D^-1 r (normalised by its RMS rho), and z += rho * its output
-// interpolated to the grid.  Right preconditioning in FGMRES allows a preconditioner that
-// changes from one step to the next, so the correction may be any function of v; the FP64
-// residual test of the Krylov solve decides every accepted answer as without it.
+// block-Jacobi-scaled residual D^-1 r (normalised by its RMS rho), d = rho * its output
+// interpolated to the grid, and z += gamma d with gamma = (r, A d) / (A d, A d), the step that
+// minimises ||v - A (z + gamma d)||: the corrected step never leaves a larger residual than
+// the preconditioner alone, whatever the network returns.  Right preconditioning in FGMRES
+// allows a preconditioner that changes from one step to the next; the FP64 residual test of
+// the Krylov solve decides every accepted answer as without it.
 int learned_correction(pism_gpu_ssa *h, const double2 *v, double2 *z, const int *done) {
   auto &P = h->lpc;
   const Fields f = fields_of(h);
@@ -688,8 +690,9 @@ int learned_correction(pism_gpu_ssa *h, const double2 *v, double2 *z, const int 
   pism_gpu_unet_set_stream(P.net, ns);
   if (rc != PISM_GPU_SSA_OK)
     return fail(h, rc, "learned preconditioner: network forward failed: %s", pism_gpu_unet_last_error(P.net));
-  pism_unet::launch_pc_correct(h->stream, P.out, P.height, P.width, P.stride, h->g.Mx, h->g.My, P.rho, z, done);
-  h->L.tick(22);   // features, input (2), network (18), correction; the residual ticks its own
+  pism_unet::launch_pc_expand(h->stream, P.out, P.height, P.width, P.stride, h->g.Mx, h->g.My, P.rho, P.d, done);
+  h->L.tick(22);   // features, input (2), network (18), expansion; the residual and line search tick their own
+  launch_pc_line_search(h->L, h->g, f, P.r, P.d, P.ad, P.gamma, z, h->G.st);
   CK(h, cudaGetLastError());
   return PISM_GPU_SSA_OK;
 }
@@ -1072,7 +1075,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
                  h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G, h->lpc.img, h->lpc.out,
-                 h->lpc.r, h->lpc.part, h->lpc.rho};
+                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -1395,13 +1398,17 @@ int pism_gpu_ssa_set_learned_pc(pism_gpu_ssa *h, pism_gpu_unet *net, int stride)
   if (stride < 1 || stride > 2) return fail(h, PISM_GPU_SSA_EINVAL, "stride must be 1 or 2");
   const int hh = ((h->g.Mx + stride - 1) / stride + 7) / 8 * 8, ww = ((h->g.My + stride - 1) / stride + 7) / 8 * 8;
   if (!P.r || hh != P.height || ww != P.width) {
-    for (void *q : {(void *)P.img, (void *)P.out, (void *)P.r, (void *)P.part, (void *)P.rho})
+    for (void *q : {(void *)P.img, (void *)P.out, (void *)P.r, (void *)P.d, (void *)P.ad, (void *)P.part,
+                     (void *)P.rho, (void *)P.gamma})
       if (q) cudaFree(q);
     P = {};
     CK(h, cudaMalloc((void **)&P.img, (size_t)hh * ww * 8 * sizeof(float)));
     CK(h, cudaMemset(P.img, 0, (size_t)hh * ww * 8 * sizeof(float)));
     CK(h, cudaMalloc((void **)&P.out, (size_t)hh * ww * 2 * sizeof(float)));
     CK(h, cudaMalloc((void **)&P.r, sizeof(double2) * h->N));
+    CK(h, cudaMalloc((void **)&P.d, sizeof(double2) * h->N));
+    CK(h, cudaMalloc((void **)&P.ad, sizeof(double2) * h->N));
+    CK(h, cudaMalloc((void **)&P.gamma, sizeof(double)));
     CK(h, cudaMalloc((void **)&P.part, sizeof(double) * pism_unet::pc_parts(hh, ww)));
     CK(h, cudaMalloc((void **)&P.rho, sizeof(double)));
   }

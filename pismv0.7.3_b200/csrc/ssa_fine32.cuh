@@ -57,24 +57,40 @@ __device__ __forceinline__ bool fine_rows_tile(const FineF &F, int i, int j, uin
   return true;
 }
 
+// y = A x at fine cell (i, j) from its flag word f, beta, the four staggered nu*H
+// coefficients (west, east, south, north faces) and x read through xr(di, dj)
+template <class XR>
+__device__ __forceinline__ float2 fine_apply_coef(const FineF &F, int i, int j, uint32_t f, float bta, float c_w,
+                                                  float c_e, float c_s, float c_n, const XR &xr) {
+  if ((f & (F_WEIGHTS | F_DIAG_ONLY | F_NB_ANY)) == F_WEIGHTS)
+    return apply_regular<float, float2>(F.rdx2, F.rdy2, F.r2, F.r4, c_w, c_e, c_s, c_n, bta, xr);
+  if (f & F_DIAG_ONLY) {
+    const float2 xc = xr(0, 0);
+    return make_float2(F.scaling * xc.x, F.scaling * xc.y);
+  }
+  if (f & F_NB_ANY) {   // nu_bedrock_set overrides, SSAFD.cc:561-585
+    const GridDev &g = F.g;
+    const int k = cell(g, i, j);
+    const double Hc = F.H[k], HE = F.H[nbr(g, i, j, 1, 0)];
+    if (f & F_NB_W) c_w = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, -1, 0)]));
+    if (f & F_NB_E) c_e = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
+    if (f & F_NB_N) c_n = (float)(F.nu_bedrock * 0.5 * (Hc + F.H[nbr(g, i, j, 0, 1)]));
+    if (f & F_NB_S) c_s = (float)(F.nu_bedrock * 0.5 * (Hc + HE));
+  }
+  Row2T<float> e1, e2;
+  stencil_rows_t<float>(F.rdx2, F.rdy2, F.r2, F.r4, f, c_w, c_e, c_s, c_n, bta, e1, e2);
+  return apply_rows_rel<float, float2>(e1, e2, xr);
+}
+
 // y = A x at fine cell (i, j) = tile position (ti, tj), x and nu*H from tiles
 // f and bta (the cell's flag word and beta) are loaded by the caller together with the
 // halo tiles, so that a tile costs one round trip to memory
 __device__ __forceinline__ float2 fine_apply_tile(const FineF &F, int i, int j, uint32_t f, float bta,
                                                   const HaloTile<float2> &xT, const HaloTile<float2> &nT, int ti,
                                                   int tj) {
-  if ((f & (F_WEIGHTS | F_DIAG_ONLY | F_NB_ANY)) == F_WEIGHTS) {
-    auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
-    return apply_regular<float, float2>(F.rdx2, F.rdy2, F.r2, F.r4, nT[ti][tj + 1].x, nT[ti + 1][tj + 1].x,
-                                        nT[ti + 1][tj].y, nT[ti + 1][tj + 1].y, bta, xr);
-  }
-  Row2T<float> e1, e2;
-  if (!fine_rows_tile(F, i, j, f, bta, nT, ti, tj, e1, e2)) {
-    const float2 xc = xT[ti + 1][tj + 1];
-    return make_float2(F.scaling * xc.x, F.scaling * xc.y);
-  }
   auto xr = [&](int di, int dj) { return xT[ti + 1 + di][tj + 1 + dj]; };
-  return apply_rows_rel<float, float2>(e1, e2, xr);
+  return fine_apply_coef(F, i, j, f, bta, nT[ti][tj + 1].x, nT[ti + 1][tj + 1].x, nT[ti + 1][tj].y,
+                         nT[ti + 1][tj + 1].y, xr);
 }
 
 

@@ -136,6 +136,9 @@ void launch_gmres_step(const Launch &L, const GridDev &g, const Fields &f, const
 void launch_gmres_precondition(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G,
                                const double4 *dinv, const MGHierarchy *mg, const LinePC *line, int j);
 void launch_gmres_orthogonalize(const Launch &L, const GridDev &g, const Fields &f, const Gmres &G, int j);
+// ad = A d; gamma = (r, ad) / (ad, ad); z += gamma d (skipped once st->done)
+void launch_pc_line_search(const Launch &L, const GridDev &g, const Fields &f, const double2 *r, const double2 *d,
+                           double2 *ad, double *gamma, double2 *z, const KState *st);
 // r = v - A z (FP64), skipped once st->done
 void launch_pc_residual(const Launch &L, const GridDev &g, const Fields &f, const double2 *v, const double2 *z,
                         double2 *r, const KState *st);

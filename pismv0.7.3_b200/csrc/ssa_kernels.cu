@@ -1156,6 +1156,40 @@ __global__ void k_pc_residual(int N, const double2 *__restrict__ v, double2 *__r
   }
 }
 
+// gamma = (r, Ad) / (Ad, Ad) (0 when Ad vanishes), the step along d that minimises
+// ||r - gamma A d||; then z += gamma d
+__global__ void k_pc_gamma(int N, const double2 *__restrict__ r, const double2 *__restrict__ ad, double *partials,
+                           unsigned *ticket, double *gamma, const KState *st) {
+  if (st && st->done) return;
+  double acc[2] = {0.0, 0.0};
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 rk = r[k], a = ad[k];
+    acc[0] += rk.x * a.x + rk.y * a.y;
+    acc[1] += a.x * a.x + a.y * a.y;
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, partials, ticket, tot)) *gamma = (tot[1] > 0.0 && isfinite(tot[0] / tot[1])) ? tot[0] / tot[1] : 0.0;
+}
+
+__global__ void k_pc_add(int N, const double2 *__restrict__ d, const double *__restrict__ gamma,
+                         double2 *__restrict__ z, const KState *st) {
+  if (st && st->done) return;
+  const double gm = *gamma;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double2 dk = d[k], zk = z[k];
+    z[k] = make_double2(zk.x + gm * dk.x, zk.y + gm * dk.y);
+  }
+}
+
+void launch_pc_line_search(const Launch &L, const GridDev &g, const Fields &f, const double2 *r, const double2 *d,
+                           double2 *ad, double *gamma, double2 *z, const KState *st) {
+  launch_apply(L, g, f, d, ad);
+  L.tick(2);
+  const int N = g.Mx * g.My;
+  k_pc_gamma<<<grid_for(L, N), NT, 0, L.stream>>>(N, r, ad, L.partials, L.ticket, gamma, st);
+  k_pc_add<<<grid_for(L, N), NT, 0, L.stream>>>(N, d, gamma, z, st);
+}
+
 void launch_pc_residual(const Launch &L, const GridDev &g, const Fields &f, const double2 *v, const double2 *z,
                         double2 *r, const KState *st) {
   launch_apply(L, g, f, z, r);

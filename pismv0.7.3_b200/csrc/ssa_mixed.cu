@@ -11,6 +11,7 @@
 // reads 32 B per cell (x 8, nu*H 8, beta 4, flags 4, y 8) instead of 60.
 #include "ssa_fine32.cuh"
 #include "ssa_reduce.cuh"
+#include "ssa_tma_tile.cuh"
 
 namespace pism_gpu {
 
@@ -115,19 +116,62 @@ __global__ void __launch_bounds__(NT32) k32_p(int N, const float2 *__restrict__ 
   }
 }
 
+// The tile loop of the two FP32 apply kernels: tiles whose rows can be staged by the bulk-copy
+// engine go through two shared-memory stages (the next tile's rows in flight while this one
+// computes); the rest (the first and last tile columns) load as before.  body(k, y) gets each
+// cell's y = A x.  The same tiles in the same order per block as the plain loop, so the same
+// sums.
+template <class BODY>
+__device__ __forceinline__ void tile_loop_staged(const FineF &F, const Tile32 &tm, const float2 *__restrict__ x,
+                                                 const BODY &body) {
+  __shared__ HaloTile<float2> xT, nT;
+  __shared__ TmaStage stg[2];
+  __shared__ unsigned long long bars[2];
+  if (threadIdx.x == 0) {
+    tma_bar_init(&bars[0]);
+    tma_bar_init(&bars[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int My = F.g.My;
+  unsigned parity[2] = {0u, 0u};
+  int t = blockIdx.x, s = 0;
+  if (t < tm.tiles) {
+    const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    if (tma_tile_ok(j0, My)) tma_issue(stg[0], &bars[0], x, F, i0, j0);
+  }
+  __syncthreads();   // the first staged tile's offsets
+  for (; t < tm.tiles; t += gridDim.x, s ^= 1) {
+    const int tn = t + gridDim.x;
+    if (tn < tm.tiles) {
+      const int i0n = (tn / tm.tiles_j) * TILE_I, j0n = (tn % tm.tiles_j) * TILE_J;
+      if (tma_tile_ok(j0n, My)) tma_issue(stg[s ^ 1], &bars[s ^ 1], x, F, i0n, j0n);
+    }
+    const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
+    int k = 0;
+    float2 y;
+    bool inside;
+    if (tma_tile_ok(j0, My)) {
+      tma_wait(&bars[s], parity[s]);   // bounded: a wait that gives up leaves this tile's values stale
+      parity[s] ^= 1u;
+      inside = tma_apply(F, stg[s], i0, j0, k, y);
+    } else {
+      inside = apply32(F, tm, t, x, xT, nT, k, y);
+    }
+    if (inside) body(k, y);
+    __syncthreads();   // stage s is free again; the next staged tile's offsets are visible
+  }
+}
+
 __global__ void __launch_bounds__(NT32) k32_v(FineF F, Tile32 tm, const float2 *__restrict__ phat,
                                               const float2 *__restrict__ rhat, float2 *__restrict__ v,
                                               double *partials, unsigned *ticket, KState *st) {
   if (st->done) return;
-  __shared__ HaloTile<float2> xT, nT;
   double acc[1] = {0.0};
-  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int k;
-    float2 y;
-    if (!apply32(F, tm, t, phat, xT, nT, k, y)) continue;
+  tile_loop_staged(F, tm, phat, [&](int k, const float2 &y) {
     v[k] = y;
     acc[0] += dotf(rhat[k], y);
-  }
+  });
   double tot[1];
   if (grid_reduce<1>(acc, partials, ticket, tot)) {
     if (tot[0] == 0.0 || !isfinite(tot[0])) {
@@ -146,17 +190,13 @@ __global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *
                                               KState *st) {
   if (st->done) return;
   const float al = (float)st->alpha;
-  __shared__ HaloTile<float2> xT, nT;
   double acc[2] = {0.0, 0.0};
-  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
-    int k;
-    float2 y;
-    if (!apply32(F, tm, t, shat, xT, nT, k, y)) continue;
+  tile_loop_staged(F, tm, shat, [&](int k, const float2 &y) {
     tv[k] = y;
     const float2 rk = r[k], vk = v[k];
     acc[0] += dotf(y, make_float2(rk.x - al * vk.x, rk.y - al * vk.y));
     acc[1] += dotf(y, y);
-  }
+  });
   double tot[2];
   if (grid_reduce<2>(acc, partials, ticket, tot)) st->omega = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
 }

@@ -677,9 +677,9 @@ __global__ void __launch_bounds__(PC_THREADS) k_pc_scale(float *__restrict__ img
   }
 }
 
-// z += rho * (the network's output interpolated to the grid, as k_velocity interpolates)
-__global__ void k_pc_correct(const float *__restrict__ y, int height, int width, int stride, int Mx, int My,
-                             const double *__restrict__ rho, double2 *__restrict__ z, const int *done) {
+// d = rho * (the network's output interpolated to the grid, as k_velocity interpolates)
+__global__ void k_pc_expand(const float *__restrict__ y, int height, int width, int stride, int Mx, int My,
+                            const double *__restrict__ rho, double2 *__restrict__ d, const int *done) {
   if (done && *done) return;
   const double s = *rho;
   const long long n = (long long)Mx * My;
@@ -697,8 +697,7 @@ __global__ void k_pc_correct(const float *__restrict__ y, int height, int width,
         u += (double)o.x;
         v += (double)o.y;
       }
-    const double2 zk = z[k];
-    z[k] = make_double2(zk.x + 0.25 * s * u, zk.y + 0.25 * s * v);
+    d[k] = make_double2(0.25 * s * u, 0.25 * s * v);
   }
 }
 
@@ -848,9 +847,9 @@ void launch_pc_input(cudaStream_t s, int Mx, int My, int stride, const double2 *
   k_pc_scale<<<nb, PC_THREADS, 0, s>>>(img, height, width, part, nb, rho, done);
 }
 
-void launch_pc_correct(cudaStream_t s, const float *y, int height, int width, int stride, int Mx, int My,
-                       const double *rho, double2 *z, const int *done) {
-  k_pc_correct<<<grid_for((long long)Mx * My), 256, 0, s>>>(y, height, width, stride, Mx, My, rho, z, done);
+void launch_pc_expand(cudaStream_t s, const float *y, int height, int width, int stride, int Mx, int My,
+                      const double *rho, double2 *d, const int *done) {
+  k_pc_expand<<<grid_for((long long)Mx * My), 256, 0, s>>>(y, height, width, stride, Mx, My, rho, d, done);
 }
 
 void launch_velocity(cudaStream_t s, const float *y, int height, int width, int stride, int Mx, int My,

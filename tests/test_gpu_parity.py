@@ -430,3 +430,32 @@ def test_small_level_cycles_agree_bitwise(shape, precision):
         out[k] = (vel, st["picard_iterations"], st["ksp_iterations"], st["refinement_steps"])
     np.testing.assert_array_equal(out[0][0], out[1][0])
     assert out[0][1:] == out[1][1:]
+
+
+@pytest.mark.parametrize("shape", [(161, 131), (130, 97)])
+def test_mixed_solve_on_grids_with_staged_tiles(shape):
+    """Grids wide enough for the FP32 apply kernels to stage interior tiles by bulk copies
+    (tile columns 32 .. My - 36) next to the plain-loaded edge columns: the mixed-precision
+    linear solve against a direct solve, and a whole solve against the oracle."""
+    Mx, My = shape
+    g, c, f, _ = S.build_synthetic(Mx, 4000e3 / (Mx - 1), seed=12)
+    g = GridDesc(Mx, My, g.Lx, g.Lx * (My - 1) / (Mx - 1), periodicity=0, z=g.z)
+    f = {k: (v[:Mx, :My] if isinstance(v, np.ndarray) else v) for k, v in f.items()}
+    c = c.copy(pc_type="mg", precision="mixed", ksp_rtol=1e-12, do_pseudo_plastic_till=True,
+               ssafd_relative_convergence=1e-7)
+    G, Cc, I = O.from_case(g, c, f)
+    s = make_solver(g, c, f)
+    s.assemble_rhs()
+    s.compute_hardav_staggered()
+    s.set_initial_guess(np.zeros((Mx, My, 2)))
+    s.compute_nuH_staggered(c.epsilon_ssa)
+    A = O.assemble_matrix(G, Cc, I, s.nuH(), s.beta())
+    x_ref = O.linear_solve(A, s.rhs().ravel(), None, "direct").reshape((Mx, My, 2))
+    xd = torch.zeros((Mx, My, 2), dtype=torch.float64, device="cuda")
+    its, res = s.linear_solve(xd)
+    assert res <= 1e-12
+    assert rel(xd.cpu().numpy(), x_ref) < 1e-8
+    s.close()
+    vel, st = _solve_case(g, c, f)
+    ref = O.SSAFDOracle(G, Cc, I).solve()
+    assert st["converged"] == 1 and rel(vel, ref) < 1e-8
