@@ -164,17 +164,18 @@ def tune_launch_mode(solver, config, prime, candidates=(2, 3), tuner: Optional[A
     return best["graphs"]
 
 
-def tune_mg_post_blocks(solver, config, prime, candidates=(0, 3, 2), tuner: Optional[Autotuner] = None,
-                        workload: Optional[dict] = None) -> int:
-    """The grid size of the coarse-level multigrid post-smoothing (resident blocks per SM it
-    is sized for; 0 = the tile kernels' 4): a launch shape that does not change the
-    arithmetic, so every candidate must give the first one's velocities bit for bit."""
+def tune_config_knob(solver, config, prime, name: str, candidates, tuner: Optional[Autotuner] = None,
+                     workload: Optional[dict] = None):
+    """The value of one launch-shape field of the solver configuration (`name`, e.g.
+    mg_post_blocks_per_sm or mg_small_kernel) for repeated solves of this workload.  Such a
+    field changes how the kernels are launched, not their arithmetic, so every candidate must
+    give the first one's velocities bit for bit; the first candidate is the default."""
     tuner = tuner or Autotuner()
-    wl = {"workload": "ssa solve, mg post blocks", "grid": list(solver.shape), "config": config_key(config),
+    wl = {"workload": f"ssa solve, {name}", "grid": list(solver.shape), "config": config_key(config),
           **(workload or {})}
 
     def run(cand):
-        solver.set_config(config.copy(mg_post_blocks_per_sm=cand["mg_post_blocks_per_sm"]))
+        solver.set_config(config.copy(**{name: cand[name]}))
         prime()
         return solver.solve()
 
@@ -183,7 +184,21 @@ def tune_mg_post_blocks(solver, config, prime, candidates=(0, 3, 2), tuner: Opti
         return out is not None and ref is not None and np.array_equal(np.asarray(out), np.asarray(ref))
 
     try:
-        best = tuner.choose(wl, [{"mg_post_blocks_per_sm": int(b)} for b in candidates], run, verify=same)
+        best = tuner.choose(wl, [{name: c} for c in candidates], run, verify=same)
     finally:
         solver.set_config(config)
-    return best["mg_post_blocks_per_sm"]
+    return best[name]
+
+
+def tune_mg_post_blocks(solver, config, prime, candidates=(0, 3, 2), tuner: Optional[Autotuner] = None,
+                        workload: Optional[dict] = None) -> int:
+    """The grid size of the coarse-level multigrid post-smoothing (resident blocks per SM it
+    is sized for; 0 = the tile kernels' 4)."""
+    return tune_config_knob(solver, config, prime, "mg_post_blocks_per_sm", candidates, tuner, workload)
+
+
+def tune_small_kernel(solver, config, prime, candidates=(0, 1), tuner: Optional[Autotuner] = None,
+                      workload: Optional[dict] = None) -> int:
+    """How the multigrid's small levels are cycled: staged from L2 at every step (0) or held
+    in the cluster's shared memory (1)."""
+    return tune_config_knob(solver, config, prime, "mg_small_kernel", candidates, tuner, workload)

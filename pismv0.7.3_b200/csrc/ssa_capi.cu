@@ -782,7 +782,10 @@ int linear_solve_mixed(pism_gpu_ssa *h, double2 *x, double rtol, int *its_out, i
     if (refine >= max_refine) { status = KSP_MAXIT; break; }
     inner_total += h->st_host->iter;
     h->stats.refinement_steps += 1;
-    if (h->st_host->status == KSP_NAN) { status = KSP_NAN; break; }
+    if (h->st_host->status == KSP_NAN || h->st_host->status == KSP_STALLED) {
+      status = h->st_host->status;
+      break;
+    }
     if (h->st_host->iter == 0) { status = KSP_BREAKDOWN; break; }   // no progress possible
     launch_axpy32(h->L, g.Mx * g.My, h->K32.d, x);
     launch_residual32(h->L, g, f, h->rhs, x, h->K32.rhs, h->res_dev);

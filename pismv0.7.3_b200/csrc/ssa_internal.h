@@ -90,7 +90,6 @@ struct MGHierarchy {
   int small_kernel = 0;                          // mg_small_kernel of the configuration
   SmallPlan small_plan{};                        // their split over the cluster's CTAs
   void *small_plan_dev = nullptr;                // device copy of small_plan
-  int *small_timeout = nullptr;                  // set when that cycle's staging wait gave up
   float omega = 0.9f;                            // damping of the block-Jacobi smoother
   float correction = 1.2f;                       // scaling of the coarse-grid correction
   int post_blocks = 0;                           // grid cap of the coarse post-smoothing (0: none)
@@ -147,12 +146,12 @@ void mg_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 
 void mg_setup_fine(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv0, MGHierarchy &H);
 void mg_setup_coarse(const Launch &L, const GridDev &g, const Fields &f, MGHierarchy &H);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b,
-               double2 *z, const KState *st);
+               double2 *z, KState *st);
 void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
-               const KState *st);
+               KState *st);
 // the V-cycle with right-hand side s = r - st->alpha v, formed on the fly (BiCGStab's s)
 void mg_vcycle_s(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
-                 const float2 *v, float2 *z, const KState *st);
+                 const float2 *v, float2 *z, KState *st);
 // ---- line block-Jacobi preconditioner (ssa_line.cu) ----
 void line_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const LinePC &lp);
 void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const double2 *b, double2 *z, const KState *st);

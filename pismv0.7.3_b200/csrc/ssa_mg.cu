@@ -593,7 +593,6 @@ struct SmallDs {
   int first;               // index of the first small level
   const double *invT;      // dense inverse of the coarsest operator (transposed)
   int n;                   // unknowns of the coarsest level
-  int *stage_timeout;      // set when the staging wait gave up (the cycle then runs on what arrived)
 };
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -634,7 +633,7 @@ __device__ __forceinline__ float2 small_apply(const float4 *__restrict__ A0, int
 }
 
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THREADS)
-    k_mg_small_dsmem(SmallDs S, float omega, float corr, const KState *st) {
+    k_mg_small_dsmem(SmallDs S, float omega, float corr, KState *st) {
   if (st && st->done) return;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(128) unsigned char sm[];
@@ -737,7 +736,10 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   bool staged = true;
   if (total > 0) {
     staged = mbar_wait_bounded(bar_a, 0);
-    if (!staged && tid == 0) *S.stage_timeout = 1;
+    if (!staged && tid == 0 && st) {   // the Krylov solve stops: this cycle ran on what had arrived
+      st->done = 1;
+      st->status = KSP_STALLED;
+    }
   }
   __syncthreads();
 
@@ -955,8 +957,6 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
     if (cudaMalloc(&H.small_plan_dev, sizeof(SmallPlan)) != cudaSuccess) return 1;
     if (cudaMemcpy(H.small_plan_dev, &H.small_plan, sizeof(SmallPlan), cudaMemcpyHostToDevice) != cudaSuccess)
       return 1;
-    if (cudaMalloc(&H.small_timeout, sizeof(int)) != cudaSuccess) return 1;
-    if (cudaMemset(H.small_timeout, 0, sizeof(int)) != cudaSuccess) return 1;
     if (raise_dynamic_smem((const void *)k_mg_small_dsmem, H.small_plan.smem) != 0) return 1;
   }
   if (raise_dynamic_smem((const void *)k_mg_coarse_invert, (int)(sizeof(double) * n * n)) != 0) return 1;
@@ -983,9 +983,7 @@ void mg_free(MGHierarchy &H) {
   cudaFree(H.singular);
   cudaFree(H.views);
   cudaFree(H.small_plan_dev);
-  cudaFree(H.small_timeout);
   H.small_plan_dev = nullptr;
-  H.small_timeout = nullptr;
   H.views = nullptr;
   H.nuHf = nullptr;
   H.betaf = nullptr;
@@ -1061,7 +1059,7 @@ static void dispatch_ax(int ax, int ay, F22 f22, F21 f21, F12 f12, F11 f11) {
 
 template <class BA, class ZV>
 static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, BA b, ZV *z,
-                   const KState *st) {
+                   KState *st) {
   const FineF F = fine_view(g, f, H);
   const float omega = H.omega, corr = H.correction;
   int launches = 0;
@@ -1094,7 +1092,6 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     S.first = H.small_first;
     S.invT = H.cinv;
     S.n = 2 * H.lev[H.nlev - 1].N;
-    S.stage_timeout = H.small_timeout;
     k_mg_small_dsmem<<<SMALL_CLUSTER, CTA_THREADS, H.small_plan.smem, Lc.stream>>>(S, omega, corr, st);
     ++launches;
   } else {
@@ -1132,17 +1129,17 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
 }
 
 void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const double2 *b, double2 *z,
-               const KState *st) {
+               KState *st) {
   vcycle(Lc, g, f, H, VecAcc<double2>{b}, z, st);
 }
 
 void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b, float2 *z,
-               const KState *st) {
+               KState *st) {
   vcycle(Lc, g, f, H, VecAcc<float2>{b}, z, st);
 }
 
 void mg_vcycle_s(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
-                 const float2 *v, float2 *z, const KState *st) {
+                 const float2 *v, float2 *z, KState *st) {
   vcycle(Lc, g, f, H, SAcc{r, v, st, 0.0f}, z, st);
 }
 

@@ -120,9 +120,11 @@ __global__ void __launch_bounds__(NT32) k32_p(int N, const float2 *__restrict__ 
 // engine go through two shared-memory stages (the next tile's rows in flight while this one
 // computes); the rest (the first and last tile columns) load as before.  body(k, y) gets each
 // cell's y = A x.  The same tiles in the same order per block as the plain loop, so the same
-// sums.
+// sums.  A stage whose bounded wait gives up is computed from global memory instead, staging
+// stops for the rest of the block's tiles, and the late copies are waited for (bounded) before
+// the block exits; the return value then tells the caller to stop the solve.
 template <class BODY>
-__device__ __forceinline__ void tile_loop_staged(const FineF &F, const Tile32 &tm, const float2 *__restrict__ x,
+__device__ __forceinline__ bool tile_loop_staged(const FineF &F, const Tile32 &tm, const float2 *__restrict__ x,
                                                  const BODY &body) {
   __shared__ HaloTile<float2> xT, nT;
   __shared__ TmaStage stg[2];
@@ -134,33 +136,53 @@ __device__ __forceinline__ void tile_loop_staged(const FineF &F, const Tile32 &t
   }
   __syncthreads();
   const int My = F.g.My;
-  unsigned parity[2] = {0u, 0u};
+  // block-uniform state: the phase parity of each stage's mbarrier (bit q for stage q);
+  // stages whose copies came late (never reused); staging on; the current tile's rows were
+  // issued into stage s
+  unsigned parity = 0u, lost = 0u;
+  bool staging = true, cur = false;
   int t = blockIdx.x, s = 0;
   if (t < tm.tiles) {
     const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
-    if (tma_tile_ok(j0, My)) tma_issue(stg[0], &bars[0], x, F, i0, j0);
+    if (tma_tile_ok(j0, My)) {
+      tma_issue(stg[0], &bars[0], x, F, i0, j0);
+      cur = true;
+    }
   }
   __syncthreads();   // the first staged tile's offsets
   for (; t < tm.tiles; t += gridDim.x, s ^= 1) {
     const int tn = t + gridDim.x;
-    if (tn < tm.tiles) {
+    bool next = false;
+    if (staging && tn < tm.tiles) {
       const int i0n = (tn / tm.tiles_j) * TILE_I, j0n = (tn % tm.tiles_j) * TILE_J;
-      if (tma_tile_ok(j0n, My)) tma_issue(stg[s ^ 1], &bars[s ^ 1], x, F, i0n, j0n);
+      if (tma_tile_ok(j0n, My)) {
+        tma_issue(stg[s ^ 1], &bars[s ^ 1], x, F, i0n, j0n);
+        next = true;
+      }
     }
     const int i0 = (t / tm.tiles_j) * TILE_I, j0 = (t % tm.tiles_j) * TILE_J;
     int k = 0;
     float2 y;
-    bool inside;
-    if (tma_tile_ok(j0, My)) {
-      tma_wait(&bars[s], parity[s]);   // bounded: a wait that gives up leaves this tile's values stale
-      parity[s] ^= 1u;
-      inside = tma_apply(F, stg[s], i0, j0, k, y);
+    bool inside, late = false;
+    if (cur) {
+      late = !tma_wait(&bars[s], (parity >> s) & 1u);
+      inside = late ? tma_apply_direct(F, x, i0, j0, k, y) : tma_apply(F, stg[s], i0, j0, k, y);
     } else {
       inside = apply32(F, tm, t, x, xT, nT, k, y);
     }
     if (inside) body(k, y);
-    __syncthreads();   // stage s is free again; the next staged tile's offsets are visible
+    // stage s is free again (and the next staged tile's offsets are visible) unless late
+    if (__syncthreads_or(late)) {
+      staging = false;
+      lost |= 1u << s;
+    } else if (cur) {
+      parity ^= 1u << s;
+    }
+    cur = next;
   }
+  for (int q = 0; q < 2; ++q)
+    if ((lost >> q) & 1u) tma_wait(&bars[q], (parity >> q) & 1u);
+  return lost != 0u;
 }
 
 __global__ void __launch_bounds__(NT32) k32_v(FineF F, Tile32 tm, const float2 *__restrict__ phat,
@@ -168,10 +190,14 @@ __global__ void __launch_bounds__(NT32) k32_v(FineF F, Tile32 tm, const float2 *
                                               double *partials, unsigned *ticket, KState *st) {
   if (st->done) return;
   double acc[1] = {0.0};
-  tile_loop_staged(F, tm, phat, [&](int k, const float2 &y) {
+  const bool stalled = tile_loop_staged(F, tm, phat, [&](int k, const float2 &y) {
     v[k] = y;
     acc[0] += dotf(rhat[k], y);
   });
+  if (stalled && threadIdx.x == 0) {
+    st->done = 1;
+    st->status = KSP_STALLED;
+  }
   double tot[1];
   if (grid_reduce<1>(acc, partials, ticket, tot)) {
     if (tot[0] == 0.0 || !isfinite(tot[0])) {
@@ -191,12 +217,16 @@ __global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *
   if (st->done) return;
   const float al = (float)st->alpha;
   double acc[2] = {0.0, 0.0};
-  tile_loop_staged(F, tm, shat, [&](int k, const float2 &y) {
+  const bool stalled = tile_loop_staged(F, tm, shat, [&](int k, const float2 &y) {
     tv[k] = y;
     const float2 rk = r[k], vk = v[k];
     acc[0] += dotf(y, make_float2(rk.x - al * vk.x, rk.y - al * vk.y));
     acc[1] += dotf(y, y);
   });
+  if (stalled && threadIdx.x == 0) {
+    st->done = 1;
+    st->status = KSP_STALLED;
+  }
   double tot[2];
   if (grid_reduce<2>(acc, partials, ticket, tot)) st->omega = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
 }

@@ -16,8 +16,10 @@
 
 namespace pism_gpu {
 
-// Krylov status codes written by the device (KSPConvergedReason analogues)
-enum : int { KSP_OK = 0, KSP_MAXIT = -3, KSP_BREAKDOWN = -5, KSP_NAN = -7 };
+// Krylov status codes written by the device (KSPConvergedReason analogues); KSP_STALLED: a
+// kernel's bounded wait for data staged by the bulk-copy engine gave up (the solve stops
+// rather than go on with a preconditioner or operator that may have used late data)
+enum : int { KSP_OK = 0, KSP_MAXIT = -3, KSP_BREAKDOWN = -5, KSP_NAN = -7, KSP_STALLED = -11 };
 constexpr int KSP_OUTER_DONE = 1;   // mixed precision: the outer residual already meets the tolerance
 
 // scalars of one Krylov solve, owned by the device
@@ -124,8 +126,8 @@ PISM_HD void refine_end(PState &P, const KState &st, int max_refine) {
   } else {
     P.ksp_its += st.iter;
     P.refine_steps += 1;
-    if (st.status == KSP_NAN) {
-      status = KSP_NAN;
+    if (st.status == KSP_NAN || st.status == KSP_STALLED) {
+      status = st.status;
       stop = 1;
     } else if (st.iter == 0) {
       status = KSP_BREAKDOWN;

@@ -115,4 +115,18 @@ __device__ __forceinline__ bool tma_apply(const FineF &F, const TmaStage &S, int
   return true;
 }
 
+// y = A x at this thread's cell of a tile that could be staged (tma_tile_ok), read straight
+// from global memory: for a staged tile whose copies did not arrive in time.  The same
+// operands as tma_apply, so the same bits.
+__device__ __forceinline__ bool tma_apply_direct(const FineF &F, const float2 *__restrict__ x, int i0, int j0, int &k,
+                                                 float2 &y) {
+  const int Mx = F.g.Mx, My = F.g.My, i = i0 + (threadIdx.x >> 5), j = j0 + (threadIdx.x & 31);
+  if (i >= Mx) return false;
+  k = i * My + j;
+  const int rm = pmod(i - 1, Mx) * My + j, rp = pmod(i + 1, Mx) * My + j;
+  auto xr = [&](int di, int dj) { return x[(di < 0 ? rm : di > 0 ? rp : k) + dj]; };
+  y = fine_apply_coef(F, i, j, F.flags[k], F.beta[k], F.nuH[rm].x, F.nuH[k].x, F.nuH[k - 1].y, F.nuH[k].y, xr);
+  return true;
+}
+
 }  // namespace pism_gpu

@@ -163,3 +163,27 @@ def test_launch_mode_through_the_solver_interface(tmp_path):
     base = SSAConfig(pc_type="mg", precision="mixed")
     assert tune_launch_mode(s, base, prime=lambda: None, tuner=tuner) == 3
     assert s.log == [2, 3] and s.cfg is base
+
+
+def test_small_kernel_through_the_solver_interface(tmp_path):
+    """tune_small_kernel: both small-level cycles give the same bits; the faster is chosen"""
+    import numpy as np
+    from pism_b200.autotune import tune_small_kernel
+    from pism_b200.config import SSAConfig
+    tuner, clock = make(tmp_path, repeats=1, warmup=0)
+
+    class Solver:
+        shape = (401, 401)
+        cfg = None
+
+        def set_config(self, c):
+            self.cfg = c
+
+        def solve(self):
+            clock.cost = {0: 50.0, 1: 48.0}[self.cfg.mg_small_kernel]
+            return np.ones(3)
+
+    s = Solver()
+    base = SSAConfig(pc_type="mg")
+    assert tune_small_kernel(s, base, prime=lambda: None, tuner=tuner) == 1
+    assert s.cfg is base

@@ -454,8 +454,16 @@ def test_mixed_solve_on_grids_with_staged_tiles(shape):
     xd = torch.zeros((Mx, My, 2), dtype=torch.float64, device="cuda")
     its, res = s.linear_solve(xd)
     assert res <= 1e-12
-    assert rel(xd.cpu().numpy(), x_ref) < 1e-8
+    x = xd.cpu().numpy()
+    b = s.rhs().ravel()
+    res_gpu = np.linalg.norm(b - A @ x.ravel()) / np.linalg.norm(b)
+    # the first Picard step's system (plastic drag at zero velocity) has a condition number
+    # near 1e5 on these grids: the true residual is the sharp check, the error follows it
+    assert res_gpu < 1e-11, res_gpu
+    assert rel(x, x_ref) < 1e-6, (rel(x, x_ref), res_gpu)
     s.close()
     vel, st = _solve_case(g, c, f)
-    ref = O.SSAFDOracle(G, Cc, I).solve()
-    assert st["converged"] == 1 and rel(vel, ref) < 1e-8
+    o = O.SSAFDOracle(G, Cc, I)
+    ref = o.solve()
+    assert st["converged"] == 1 and abs(st["picard_iterations"] - o.stats.picard_iterations) <= 1
+    assert rel(vel, ref) < 1e-7

@@ -16,7 +16,7 @@ import pytest
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 OK, EKSP, EPICARD, EZERODIAG, ENAN = 0, 4, 5, 6, 7
-KSP_OK, KSP_MAXIT, KSP_BREAKDOWN, KSP_NAN, KSP_OUTER_DONE = 0, -3, -5, -7, 1
+KSP_OK, KSP_MAXIT, KSP_BREAKDOWN, KSP_NAN, KSP_STALLED, KSP_OUTER_DONE = 0, -3, -5, -7, -11, 1
 
 
 def _header_codes():
@@ -63,8 +63,8 @@ def host_mixed(records, max_refine):
             break
         inner += it
         steps += 1
-        if st == KSP_NAN:
-            status = KSP_NAN
+        if st in (KSP_NAN, KSP_STALLED):
+            status = st
             break
         if it == 0:
             status = KSP_BREAKDOWN
@@ -145,7 +145,7 @@ def scenario(seed, mixed):
                 if v < 0.25:
                     recs.append((0, KSP_OUTER_DONE, r2, b2))
                 elif v < 0.27:
-                    recs.append((int(rng.integers(1, 9)), KSP_NAN, r2, b2))
+                    recs.append((int(rng.integers(1, 9)), KSP_NAN if v < 0.26 else KSP_STALLED, r2, b2))
                 elif v < 0.29:
                     recs.append((0, KSP_OK, r2, b2))
                 elif v < 0.30:
@@ -158,7 +158,7 @@ def scenario(seed, mixed):
             rec["refine"] = recs
         else:
             rec["iter"] = int(rng.integers(0, 200))
-            rec["status"] = KSP_OK if clean else int(rng.choice([KSP_OK] * 30 + [KSP_MAXIT, KSP_NAN, KSP_BREAKDOWN]))
+            rec["status"] = KSP_OK if clean else int(rng.choice([KSP_OK] * 30 + [KSP_MAXIT, KSP_NAN, KSP_BREAKDOWN, KSP_STALLED]))
             rec["r2"], rec["b2"] = float(rng.uniform(0, 1e-12)), float(rng.uniform(1, 10))
         iters.append(rec)
     return c, max_refine, iters
