@@ -252,46 +252,49 @@ def large_roofline(c, stream, flush, dev, peak, M=1601):
 # The host-core cost of the whole reference solve is sampled: the first CPU_SAMPLE_PICARD
 # Picard iterations of the native restatement (oracle/ssafd_cpu.cc: nu*H, drag, 18-column
 # assembly, PETSc-style GMRES(30) + block Jacobi / ILU(0), norms) run on the host cores, and
-# the whole solve is that time scaled by a cost model: a Picard iteration costs
-# (setup + GMRES iterations) x the cost of one GMRES iteration, with the GMRES iteration
-# counts of one complete run of the same restatement on this sheet (KSP rtol 1e-8 from a zero
-# guess; the tolerance-1e-4 solve is the prefix of the tolerance-1e-6 one) and the per-Picard
-# setup (ILU(0) factorisation, assembly) in units of GMRES iterations fitted on a complete
-# 401^2 run (profiles/cpu_baseline_native.md).
+# the whole solve is estimated by a cost model: Picard iteration k costs (c + its_k) units, its_k
+# its GMRES iterations and c the per-Picard set-up (ILU(0) factorisation, assembly) in GMRES
+# iterations.  The unit is the median over the sampled iterations of t_k / (c + its_k) (one
+# iteration slowed by another process does not move it); the whole solve costs
+# (n c + sum its_k) units with n and sum its_k from one complete run of the same restatement on
+# this sheet (KSP rtol 1e-8 from a zero guess; the tolerance-1e-4 solve is the prefix of the
+# tolerance-1e-6 one), c fitted on that run (least squares with 4-MAD outlier rejection).
 CPU_FULL_RUN_801 = {
     "threads": 8,
     "picard_iterations": {"1e-06": 359, "0.0001": 184},
-    "ksp_iterations": {"1e-06": 27936, "0.0001": 22647},
-    "first_ksp_iterations": [221, 442, 665],   # cumulative after Picard iterations 1, 2, 3
-    "setup_iterations": 36.6,
+    "ksp_iterations": {"1e-06": 27936, "0.0001": 22646},
+    "setup_iterations": 13.6,
 }
 CPU_SAMPLE_PICARD = 3
 
 
-def cpu_estimate(sample_s, k, picard_rtol, full=None):
-    """(estimated ms of the whole CPU solve, how) from the first k iterations' seconds"""
+def cpu_estimate(prepare_s, sample, picard_rtol, full=None):
+    """(estimated ms of the whole CPU solve, how) from the set-up seconds and the sampled
+    Picard iterations' (seconds, GMRES iterations)"""
     full = full if full is not None else CPU_FULL_RUN_801
-    if full is None or k < 1 or k > len(full["first_ksp_iterations"]):
+    if full is None or not sample:
         return None, "no complete CPU run on record"
     key = f"{picard_rtol:g}"
     if key not in full["ksp_iterations"]:
         return None, f"no complete CPU run at Picard tolerance {key}"
     c = full["setup_iterations"]
     n, its = full["picard_iterations"][key], full["ksp_iterations"][key]
-    ratio = (its + n * c) / (full["first_ksp_iterations"][k - 1] + k * c)
-    how = (f"first {k} Picard iterations timed on the host cores ({sample_s:.1f} s), x {ratio:.2f}: the whole "
-           f"solve's {n} Picard iterations and {its} GMRES iterations (one complete run of the same restatement "
-           f"on this sheet at Picard tolerance {key}) against the sample's, each Picard iteration costing "
-           f"{c:g} GMRES iterations of set-up")
-    return sample_s * ratio * 1e3, how
+    unit = float(np.median([t / (c + k) for t, k in sample]))
+    est = prepare_s + unit * (its + n * c)
+    how = (f"first {len(sample)} Picard iterations timed on the host cores "
+           f"({sum(t for t, _ in sample):.1f} s, {sum(k for _, k in sample)} GMRES iterations): median cost "
+           f"{unit * 1e3:.2f} ms per GMRES iteration with {c:g} iterations of set-up per Picard iteration, "
+           f"times the {n} Picard and {its} GMRES iterations of one complete run of the same restatement on "
+           f"this sheet at Picard tolerance {key}")
+    return est * 1e3, how
 
 
 def cpu_reference_sample(M, picard_sample, nthreads, picard_rtol):
     """The native CPU restatement of the reference's Picard loop (oracle/ssafd_cpu.cc) on the
     host cores: driving stress / right-hand side / hardness (oracle.prepare), then
     `picard_sample` Picard iterations from a zero guess (nu*H, drag, assembly, PETSc-style
-    GMRES(30) + block Jacobi ILU(0) with one block per thread, norms).  Returns (seconds,
-    Picard iterations done)."""
+    GMRES(30) + block Jacobi ILU(0) with one block per thread, norms).  Returns (set-up
+    seconds, [(seconds, GMRES iterations) per Picard iteration])."""
     sys.path.insert(0, REPO)
     from oracle import ssafd_oracle as O
     g, c, f, _ = build_case(M)
@@ -300,20 +303,25 @@ def cpu_reference_sample(M, picard_sample, nthreads, picard_rtol):
     t0 = time.perf_counter()
     o = O.SSAFDOracle(G, Cc, I)
     o.prepare()
+    t1 = time.perf_counter()
     _, info = O.picard_native(G, Cc, I, o.hardness, o.b, np.zeros((M, M, 2)), Cc.epsilon_ssa, nranks=nthreads,
                               nthreads=nthreads, ksp_rtol=c.ksp_rtol, max_iterations=picard_sample,
                               picard_rtol=picard_rtol)
-    return time.perf_counter() - t0, info["picard_iterations"]
+    total = time.perf_counter() - t1
+    per = [a + b + d for a, b, d in zip(info["t_nuH"], info["t_assemble"], info["t_ksp"])]
+    rest = (total - sum(per)) / max(1, len(per))   # norms, tests and the copies around them
+    return t1 - t0, [(t + rest, int(k)) for t, k in zip(per, info["ksp_iterations"])]
 
 
 def cpu_baseline(M, picard_rtol, nthreads, picard_gpu=None):
     """the cpu_baseline object: the host-core sample and its whole-solve estimate"""
-    dt, done = cpu_reference_sample(M, CPU_SAMPLE_PICARD, nthreads, picard_rtol)
-    est, how = (cpu_estimate(dt, done, picard_rtol) if M == 801 else (None, "no complete CPU run at this size"))
-    if est is None and picard_gpu:
-        est = dt * 1e3 / max(1, done) * picard_gpu
-        how = (f"first {done} Picard iterations timed on the host cores ({dt:.1f} s), scaled by the iteration count "
-               f"of the plain GPU solve ({picard_gpu}; {how})")
+    prep, sample = cpu_reference_sample(M, CPU_SAMPLE_PICARD, nthreads, picard_rtol)
+    est, how = (cpu_estimate(prep, sample, picard_rtol) if M == 801 else (None, "no complete CPU run at this size"))
+    if est is None and picard_gpu and sample:
+        dt = sum(t for t, _ in sample)
+        est = (prep + dt / len(sample) * picard_gpu) * 1e3
+        how = (f"first {len(sample)} Picard iterations timed on the host cores ({dt:.1f} s), scaled by the "
+               f"iteration count of the plain GPU solve ({picard_gpu}; {how})")
     return {"value": est, "unit": "ms", "cores": nthreads, "kind": "port", "sample": how}
 
 
@@ -504,6 +512,9 @@ def main():
     ap.add_argument("--ksp-max", type=float, default=1e-1, help="fast set-up: loosest KSP rtol of a Picard iteration")
     ap.add_argument("--mg-small-kernel", type=int, default=0, choices=[0, 1],
                     help="multigrid small levels: 0 staged from L2 per step, 1 held in the cluster's shared memory")
+    ap.add_argument("--apply-kernel", type=int, default=1, choices=[0, 1, 2],
+                    help="mixed precision, the FP32 operator apply after each V-cycle: 0 plain tile loads, "
+                         "1 bulk-copy staged tiles, 2 fused into the V-cycle's fine-level pass")
     ap.add_argument("--mg-lag", type=float, default=FAST_MG_LAG,
                     help="fast set-up: rebuild the multigrid coarse levels once the summed relative nu*H change "
                          "reaches this (0: every Picard iteration)")
@@ -537,6 +548,7 @@ def main():
     if args.mg_post_blocks is not None:
         c_plain.mg_post_blocks_per_sm = args.mg_post_blocks
     c_plain.mg_small_kernel = args.mg_small_kernel
+    c_plain.mixed_apply_kernel = args.apply_kernel
     c_fast = fast_config(c_plain, factor=args.ksp_factor, rtol_max=args.ksp_max, mg_lag=args.mg_lag)
     if args.inner_rtol is not None:
         c_fast.mixed_inner_rtol = args.inner_rtol
@@ -765,6 +777,7 @@ def main():
                    "ksp_rtol": c.ksp_rtol, "ksp_rtol_adaptive": bool(c.ksp_rtol_adaptive),
                    "picard_rtol": c.ssafd_relative_convergence, "graphs": c.graphs,
                    "mg_rebuild_rtol": c.mg_rebuild_rtol, "mg_small_kernel": c.mg_small_kernel,
+                   "mixed_apply_kernel": c.mixed_apply_kernel,
                    "warm_start": (f"learned (U-Net, features at stride {stride})" if net is not None else "zero"),
                    "l2": "flushed (256 MB write) between steps",
                    "parallelism": f"replicas x{world}"},

@@ -154,6 +154,13 @@ typedef struct pism_gpu_ssa_config {
      results, bit for bit, in the same time on a B200 (30.6 and 31.4 us per cycle at 801^2);
      a launch-shape knob for the autotuner */
   int    mg_small_kernel;
+  /* mixed precision with multigrid, the FP32 operator apply that BiCGStab performs on each
+     V-cycle's result: 0 a kernel of its own loading each tile with plain loads; 1 the same
+     kernel with interior tiles staged by bulk asynchronous copies, the next tile in flight;
+     2 fused into the V-cycle's fine-level pass (one kernel per V-cycle fewer, the halo of the
+     smoothed iterate recomputed instead of read back).  All give the same results, bit for
+     bit: a launch-shape knob */
+  int    mixed_apply_kernel;
 } pism_gpu_ssa_config;
 
 /* ---- input fields (SSA::init_impl, SSA.cc:134-184; SSAFD::update) -------- */

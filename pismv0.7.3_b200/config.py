@@ -97,6 +97,7 @@ class SSAConfig:
     mg_post_blocks_per_sm: int = 0
     mg_rebuild_rtol: float = 0.0
     mg_small_kernel: int = 0
+    mixed_apply_kernel: int = 1
     # geometry helpers (not part of the C struct)
     mask_icefree_thickness_standard: float = 0.01
     mask_is_floating_thickness_standard: float = 1.0
@@ -152,7 +153,7 @@ class CConfig(C.Structure):
         ("ksp_max_it", _I), ("gmres_restart", _I), ("precision", _I), ("mixed_inner_rtol", _D),
         ("mg_omega", _D), ("mg_correction", _D), ("ksp_rtol_adaptive", _I), ("ksp_rtol_max", _D),
         ("ksp_rtol_factor", _D), ("graphs", _I), ("verbosity", _I), ("mg_post_blocks_per_sm", _I),
-        ("mg_rebuild_rtol", _D), ("mg_small_kernel", _I),
+        ("mg_rebuild_rtol", _D), ("mg_small_kernel", _I), ("mixed_apply_kernel", _I),
     ]
 
 

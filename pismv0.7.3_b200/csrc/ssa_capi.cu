@@ -182,6 +182,7 @@ int pc_setup(pism_gpu_ssa *h, bool rebuild_coarse = true) {
   h->mg.correction = (float)h->cfg.mg_correction;
   h->mg.post_blocks = h->cfg.mg_post_blocks_per_sm > 0 ? h->L.max_blocks / 4 * h->cfg.mg_post_blocks_per_sm : 0;
   h->mg.small_kernel = h->cfg.mg_small_kernel;
+  h->mg.apply_kernel = h->cfg.mixed_apply_kernel;
   if (active_mg(h)) {
     mg_setup_fine(h->L, h->g, f, h->K.dinv, h->mg);
     if (rebuild_coarse) {
@@ -224,6 +225,8 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
     return fail(h, PISM_GPU_SSA_EINVAL, "mg_post_blocks_per_sm must be in [0, 4]");
   if (c->mg_small_kernel < 0 || c->mg_small_kernel > 1)
     return fail(h, PISM_GPU_SSA_EINVAL, "mg_small_kernel must be 0 or 1");
+  if (c->mixed_apply_kernel < 0 || c->mixed_apply_kernel > 2)
+    return fail(h, PISM_GPU_SSA_EINVAL, "mixed_apply_kernel must be 0, 1 or 2");
   if (!(c->mg_rebuild_rtol >= 0.0)) return fail(h, PISM_GPU_SSA_EINVAL, "mg_rebuild_rtol must be >= 0");
   if (!(c->ksp_rtol > 0.0) || c->ksp_max_it < 1 || c->max_iterations_ssafd < 1)
     return fail(h, PISM_GPU_SSA_EINVAL, "ksp_rtol, ksp_max_it and max_iterations_ssafd must be positive");
@@ -464,6 +467,7 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   h->mg.correction = (float)c.mg_correction;
   h->mg.post_blocks = c.mg_post_blocks_per_sm > 0 ? h->L.max_blocks / 4 * c.mg_post_blocks_per_sm : 0;
   h->mg.small_kernel = c.mg_small_kernel;
+  h->mg.apply_kernel = c.mixed_apply_kernel;
   PicardConst pc{c.ksp_rtol, c.ksp_rtol_max, c.ksp_rtol_factor, c.ssafd_relative_convergence,
                  c.ksp_rtol_adaptive ? 1 : 0, c.max_iterations_ssafd, c.mg_rebuild_rtol};
   PState *P = h->pstate;
@@ -985,6 +989,7 @@ int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *c) {
   c->ksp_rtol_factor = 1.0e-2;
   c->graphs = 2;
   c->verbosity = 0;
+  c->mixed_apply_kernel = 1;
   return PISM_GPU_SSA_OK;
 }
 

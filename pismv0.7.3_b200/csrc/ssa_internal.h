@@ -88,6 +88,7 @@ struct MGHierarchy {
   int small_smem = 0;                            // its per-CTA staging buffer (bytes)
   bool small_dsmem = false;                      // the small levels fit the cluster's shared memory
   int small_kernel = 0;                          // mg_small_kernel of the configuration
+  int apply_kernel = 1;                          // mixed_apply_kernel of the configuration
   SmallPlan small_plan{};                        // their split over the cluster's CTAs
   void *small_plan_dev = nullptr;                // device copy of small_plan
   float omega = 0.9f;                            // damping of the block-Jacobi smoother
@@ -152,6 +153,14 @@ void mg_vcycle(const Launch &L, const GridDev &g, const Fields &f, const MGHiera
 // the V-cycle with right-hand side s = r - st->alpha v, formed on the fly (BiCGStab's s)
 void mg_vcycle_s(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
                  const float2 *v, float2 *z, KState *st);
+// the FP32 V-cycles of BiCGStab with the operator apply that follows each fused into the
+// fine-level pass: z = M^-1 b, then y = A z handed to the epilogue (ssa_krylov32.cuh)
+struct EpiV;
+struct EpiT;
+void mg_vcycle_apply(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b,
+                     float2 *z, const EpiV &e);
+void mg_vcycle_s_apply(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
+                       const float2 *v, float2 *z, const EpiT &e);
 // ---- line block-Jacobi preconditioner (ssa_line.cu) ----
 void line_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const LinePC &lp);
 void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const double2 *b, double2 *z, const KState *st);

@@ -27,14 +27,17 @@
 #include <cstdio>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 #include <cooperative_groups.h>
 
 #include "ssa_fine32.cuh"
+#include "ssa_krylov32.cuh"
 #include "ssa_small_plan.h"
 
 namespace pism_gpu {
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -163,125 +166,158 @@ __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, co
   }
 }
 
+// Galerkin operator and D^-1 of coarse cell (I, J) of the level below F, accumulated in FP64
+// in acc[q * NTm] (q < 36: the nine 2 x 2 blocks)
+__device__ __forceinline__ void galerkin_cell(const LevelView &F, int Mxc, int Myc, int I, int J, double *acc,
+                                              float4 *Ac, float4 *dinvc) {
+  const int Nc = Mxc * Myc, ax = F.ax, ay = F.ay;
+  for (int q = 0; q < 36; ++q) acc[q * NTm] = 0.0;
+  for (int pi = 0; pi < ax; ++pi)
+    for (int pj = 0; pj < ay; ++pj) {
+      const int i = I * ax + pi, j = J * ay + pj;
+      if (i >= F.Mx || j >= F.My) continue;
+      const int k = i * F.My + j;
+#pragma unroll
+      for (int b = 0; b < 9; ++b) {
+        const int di = (b % 3) - 1, dj = 1 - (b / 3);
+        const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
+        const int cb = blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc));
+        const float4 a = F.A[b * F.N + k];
+        acc[(4 * cb + 0) * NTm] += (double)a.x;
+        acc[(4 * cb + 1) * NTm] += (double)a.y;
+        acc[(4 * cb + 2) * NTm] += (double)a.z;
+        acc[(4 * cb + 3) * NTm] += (double)a.w;
+      }
+    }
+  const int kc = I * Myc + J;
+  for (int b = 0; b < 9; ++b)
+    Ac[b * Nc + kc] = make_float4((float)acc[(4 * b) * NTm], (float)acc[(4 * b + 1) * NTm],
+                                  (float)acc[(4 * b + 2) * NTm], (float)acc[(4 * b + 3) * NTm]);
+  dinvc[kc] = inv2x2((float)acc[16 * NTm], (float)acc[17 * NTm], (float)acc[18 * NTm], (float)acc[19 * NTm]);
+}
+
 // level l+1 from the stored operator of level l
 __global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc, TileM tm, float4 *Ac, float4 *dinvc) {
   extern __shared__ double acc_sh[];
-  double *acc = acc_sh + threadIdx.x;
-  const int Nc = Mxc * Myc, ax = F.ax, ay = F.ay;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int I, J;
     if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
-    for (int q = 0; q < 36; ++q) acc[q * NTm] = 0.0;
-    for (int pi = 0; pi < ax; ++pi)
-      for (int pj = 0; pj < ay; ++pj) {
-        const int i = I * ax + pi, j = J * ay + pj;
-        if (i >= F.Mx || j >= F.My) continue;
-        const int k = i * F.My + j;
-#pragma unroll
-        for (int b = 0; b < 9; ++b) {
-          const int di = (b % 3) - 1, dj = 1 - (b / 3);
-          const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
-          const int cb = blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc));
-          const float4 a = F.A[b * F.N + k];
-          acc[(4 * cb + 0) * NTm] += (double)a.x;
-          acc[(4 * cb + 1) * NTm] += (double)a.y;
-          acc[(4 * cb + 2) * NTm] += (double)a.z;
-          acc[(4 * cb + 3) * NTm] += (double)a.w;
-        }
-      }
-    const int kc = I * Myc + J;
-    for (int b = 0; b < 9; ++b)
-      Ac[b * Nc + kc] = make_float4((float)acc[(4 * b) * NTm], (float)acc[(4 * b + 1) * NTm],
-                                    (float)acc[(4 * b + 2) * NTm], (float)acc[(4 * b + 3) * NTm]);
-    dinvc[kc] = inv2x2((float)acc[16 * NTm], (float)acc[17 * NTm], (float)acc[18 * NTm], (float)acc[19 * NTm]);
+    galerkin_cell(F, Mxc, Myc, I, J, acc_sh + threadIdx.x, Ac, dinvc);
   }
 }
 
-// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial
-// pivoting, in place in shared memory (n <= 2 * 16), one CTA; written transposed so
-// that the per-cycle product reads it coalesced.  Rows are spread over 8-lane groups.
-__global__ void __launch_bounds__(CTA_THREADS) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
-  extern __shared__ double a[];   // n * n, row-major
-  const int n = 2 * L.N;
-  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
-  __shared__ int piv_row;
-  const int t = threadIdx.x, lane8 = t & 7, grp = t >> 3, ngrp = CTA_THREADS >> 3;
-  for (int q = t; q < n * n; q += CTA_THREADS) a[q] = 0.0;
-  __syncthreads();
-  if (t < L.N) {   // each cell's two rows are written by one thread
+// Dense inverse of the coarsest operator (n = 2 N <= 32 unknowns) by Gauss-Jordan elimination
+// with partial pivoting, in place in shared memory, by one warp: lane r owns row r (rows
+// padded to 33 entries, so a column's entries of consecutive rows sit in different banks)
+// and every step is ordered by __syncwarp alone.  Written transposed, so that the per-cycle
+// product reads it coalesced.
+constexpr int CI_PAD = 2 * MG_MAX_COARSE_CELLS + 1;
+static_assert(2 * MG_MAX_COARSE_CELLS <= 32, "one lane per row of the coarsest operator");
+
+__device__ void coarse_invert_warp(const LevelView &L, double (*a)[CI_PAD], int *perm, double *invT_out,
+                                   int *singular) {
+  const int t = threadIdx.x & 31, n = 2 * L.N;
+  for (int r = 0; r < n; ++r)
+    if (t < n) a[r][t] = 0.0;
+  __syncwarp();
+  if (t < L.N) {   // each cell's two rows are written by one lane
     const int k = t, i = k / L.My, j = k % L.My;
     for (int b = 0; b < 9; ++b) {
       const int di = (b % 3) - 1, dj = 1 - (b / 3);
       const int kn = wrap(i + di, L.Mx) * L.My + wrap(j + dj, L.My);
       const float4 v = L.A[b * L.N + k];
-      a[(2 * k + 0) * n + 2 * kn + 0] += (double)v.x;
-      a[(2 * k + 0) * n + 2 * kn + 1] += (double)v.y;
-      a[(2 * k + 1) * n + 2 * kn + 0] += (double)v.z;
-      a[(2 * k + 1) * n + 2 * kn + 1] += (double)v.w;
+      a[2 * k + 0][2 * kn + 0] += (double)v.x;
+      a[2 * k + 0][2 * kn + 1] += (double)v.y;
+      a[2 * k + 1][2 * kn + 0] += (double)v.z;
+      a[2 * k + 1][2 * kn + 1] += (double)v.w;
     }
   }
-  __syncthreads();
+  __syncwarp();
   for (int col = 0; col < n; ++col) {
-    if (t < 32) {   // pivot search by warp 0
-      double best = -1.0;
-      int bi = col;
-      for (int r = col + t; r < n; r += 32) {
-        const double v = fabs(a[r * n + col]);
-        if (v > best) { best = v; bi = r; }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (t == 0) {
-        piv_row = bi;
-        perm[col] = bi;
-        if (!(best > 0.0)) *singular = 1;
+    double best = -1.0;
+    int bi = col;
+    if (col + t < n) {
+      best = fabs(a[col + t][col]);
+      bi = col + t;
+    }
+    for (int o = 16; o > 0; o >>= 1) {   // every lane ends with the same (largest, lowest row)
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
       }
     }
-    __syncthreads();
-    const int p = piv_row;
-    if (p != col)
-      for (int q = t; q < n; q += CTA_THREADS) {
-        const double tmp = a[col * n + q];
-        a[col * n + q] = a[p * n + q];
-        a[p * n + q] = tmp;
-      }
-    __syncthreads();
-    const double pv = a[col * n + col];
+    if (t == 0) {
+      perm[col] = bi;
+      if (!(best > 0.0)) *singular = 1;
+    }
+    const int p = bi;
+    if (p != col && t < n) {   // lane t swaps column t of the two rows
+      const double tmp = a[col][t];
+      a[col][t] = a[p][t];
+      a[p][t] = tmp;
+    }
+    __syncwarp();
+    const double pv = a[col][col];
     const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    __syncthreads();
+    __syncwarp();
     // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
-    for (int q = t; q < n; q += CTA_THREADS) a[col * n + q] = (q == col ? 1.0 : a[col * n + q]) * pinv;
-    __syncthreads();
+    if (t < n) a[col][t] = (t == col ? 1.0 : a[col][t]) * pinv;
+    __syncwarp();
     // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
-    for (int r = grp; r < n; r += ngrp) {
-      if (r == col) continue;
-      const double f = a[r * n + col];
-      for (int q = lane8; q < n; q += 8)
-        if (q != col) a[r * n + q] -= f * a[col * n + q];
+    if (t < n && t != col) {
+      const double f = a[t][col];
+      for (int q = 0; q < n; ++q)
+        if (q != col) a[t][q] -= f * a[col][q];
+      a[t][col] = -a[t][col] * a[col][col];
     }
-    __syncthreads();
-    for (int r = t; r < n; r += CTA_THREADS)
-      if (r != col) a[r * n + col] = -a[r * n + col] * a[col * n + col];
-    __syncthreads();
+    __syncwarp();
   }
   // undo the row interchanges as column interchanges, in reverse order
   for (int col = n - 1; col >= 0; --col) {
     const int p = perm[col];
-    if (p != col)
-      for (int r = t; r < n; r += CTA_THREADS) {
-        const double tmp = a[r * n + col];
-        a[r * n + col] = a[r * n + p];
-        a[r * n + p] = tmp;
-      }
-    __syncthreads();
+    if (p != col && t < n) {
+      const double tmp = a[t][col];
+      a[t][col] = a[t][p];
+      a[t][p] = tmp;
+    }
+    __syncwarp();
   }
-  for (int q = t; q < n * n; q += CTA_THREADS) {
-    const int r = q / n, c = q - r * n;
-    invT_out[c * n + r] = a[q];
+  for (int q = t; q < n * n; q += 32) {
+    const int c = q / n, r = q - c * n;
+    invT_out[q] = a[r][c];   // invT[c][r] = inverse[r][c]
   }
+}
+
+// the coarsest inverse alone (a hierarchy whose only coarse level is built from the fine grid)
+__global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
+  __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
+  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
+  coarse_invert_warp(L, a, perm, invT_out, singular);
+}
+
+// The small levels' Galerkin operators (levels first .. nlev - 1, each from the level above it,
+// all of <= MG_CTA_CELLS cells) and the coarsest inverse in one launch on one thread-block
+// cluster: one cluster barrier (release / acquire at cluster scope) between levels, then warp 0
+// of CTA 0 inverts the coarsest operator.  The arithmetic of every cell is k_mg_build's.
+__global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
+    k_mg_build_small(const LevelView *__restrict__ lev, int first, int nlev, double *invT_out, int *singular) {
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ double acc_sh[];
+  __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
+  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
+  const int rank = cluster.block_rank() * NTm + threadIdx.x, nthr = SMALL_CLUSTER * NTm;
+  for (int c = first; c < nlev; ++c) {
+    const LevelView F = lev[c - 1], C = lev[c];
+    for (int kc = rank; kc < C.N; kc += nthr) {
+      const int I = kc / C.My, J = kc - I * C.My;
+      galerkin_cell(F, C.Mx, C.My, I, J, acc_sh + threadIdx.x, const_cast<float4 *>(C.A),
+                    const_cast<float4 *>(C.dinv));
+    }
+    cluster.sync();
+  }
+  if (cluster.block_rank() == 0 && threadIdx.x < 32) coarse_invert_warp(lev[nlev - 1], a, perm, invT_out, singular);
 }
 
 // ---------------------------------------------------------------------------
@@ -396,6 +432,61 @@ __global__ void __launch_bounds__(NTm) k_mg0_post(FineF F, BA b_in, float omega,
   }
 }
 
+// The fine-level pass fused with the FP32 operator apply that follows the V-cycle in
+// BiCGStab.  Per tile: x = omega D^-1 b + corr P x_1 on the tile and a two-cell halo;
+// z = x + omega D^-1 (b - A x) on the tile and a one-cell halo (the halo's z recomputed here
+// rather than read back from the tiles that own it); z stored on the tile; y = A z on the
+// tile handed to the epilogue.  Every value comes from the same arithmetic as k_mg0_post
+// followed by the apply kernel, over the same tiles in the same order per block, so the
+// results and the epilogue's sums are the same bits.
+constexpr int H2I = TIm + 4, H2J = TJm + 4;   // the two-cell-halo region of a tile
+
+template <int AX, int AY, class BA, class EPI>
+__global__ void __launch_bounds__(NTm) k_mg0_post_apply(FineF F, BA b_in, float omega, float corr, int Myc,
+                                                        const float2 *__restrict__ xc, TileM tm,
+                                                        float2 *__restrict__ z, EPI e) {
+  if (e.st->done) return;
+  e.begin();
+  const auto b = b_in.bind();
+  __shared__ float2 xs[H2I][H2J], ns[H2I][H2J], zs[TIm + 2][TJm + 2];
+  const int Mx = F.g.Mx, My = F.g.My;
+  const int ti = threadIdx.x >> 5, tj = threadIdx.x & 31;
+  for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+    const int i0 = (t / tm.tiles_j) * TIm, j0 = (t % tm.tiles_j) * TJm;
+    __syncthreads();   // the previous tile's readers are done
+    for (int q = threadIdx.x; q < H2I * H2J; q += NTm) {   // cell (i0 - 2 + a, j0 - 2 + c), wrapped
+      const int a = q / H2J, c = q - a * H2J;
+      const int ii = pmod(i0 - 2 + a, Mx), jj = pmod(j0 - 2 + c, My), kq = ii * My + jj;
+      const float2 v = fmul4(F.dinv[kq], b(kq));
+      const float2 cc = xc[(ii / AX) * Myc + jj / AY];
+      xs[a][c] = make_float2(omega * v.x + corr * cc.x, omega * v.y + corr * cc.y);
+      ns[a][c] = F.nuH[kq];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < (TIm + 2) * (TJm + 2); q += NTm) {   // cell (i0 - 1 + a, j0 - 1 + c)
+      const int a = q / (TJm + 2), c = q - a * (TJm + 2);
+      const int ii = pmod(i0 - 1 + a, Mx), jj = pmod(j0 - 1 + c, My), kq = ii * My + jj;
+      auto xr = [&](int di, int dj) { return xs[a + 1 + di][c + 1 + dj]; };
+      const float2 y = fine_apply_coef(F, ii, jj, F.flags[kq], F.beta[kq], ns[a][c + 1].x, ns[a + 1][c + 1].x,
+                                       ns[a + 1][c].y, ns[a + 1][c + 1].y, xr);
+      const float2 xk = xs[a + 1][c + 1], bk = b(kq);
+      const float2 d = fmul4(F.dinv[kq], make_float2(bk.x - y.x, bk.y - y.y));
+      zs[a][c] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+    }
+    __syncthreads();
+    const int i = i0 + ti, j = j0 + tj;
+    if (i < Mx && j < My) {
+      const int k = i * My + j;
+      z[k] = zs[ti + 1][tj + 1];
+      auto zr = [&](int di, int dj) { return zs[ti + 1 + di][tj + 1 + dj]; };
+      const float2 y = fine_apply_coef(F, i, j, F.flags[k], F.beta[k], ns[ti + 1][tj + 2].x, ns[ti + 2][tj + 2].x,
+                                       ns[ti + 2][tj + 1].y, ns[ti + 2][tj + 2].y, zr);
+      e.body(k, y);
+    }
+  }
+  e.finish();
+}
+
 // coarse level l: b_{l+1} = R (b_l - A_l x0), x0 = omega D^-1 b_l
 template <int AX, int AY>
 __global__ void __launch_bounds__(NTm) k_mgc_restrict(LevelView L, float omega, int Mxc, int Myc, TileM tm,
@@ -477,7 +568,6 @@ struct SmallLevels {
 // The small levels run on one thread-block cluster of SMALL_CLUSTER CTAs: every CTA
 // stages the whole level's x in its shared memory, computes its share of the cells, and the
 // cluster barrier (release / acquire at cluster scope) orders the steps.
-namespace cg = cooperative_groups;
 
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THREADS)
     k_mg_small_cycle(SmallLevels S, float omega, float corr, const KState *st) {
@@ -959,7 +1049,7 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
       return 1;
     if (raise_dynamic_smem((const void *)k_mg_small_dsmem, H.small_plan.smem) != 0) return 1;
   }
-  if (raise_dynamic_smem((const void *)k_mg_coarse_invert, (int)(sizeof(double) * n * n)) != 0) return 1;
+  if (raise_dynamic_smem((const void *)k_mg_build_small, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
   if (raise_dynamic_smem((const void *)k_mg_build1, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
   if (raise_dynamic_smem((const void *)k_mg_build, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
   return 0;
@@ -1038,15 +1128,21 @@ void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHier
     k_mg_build1<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(g, s, f.flags, f.nuH, f.beta, H.fine_ax,
                                                                      H.fine_ay, C.Mx, C.My, tm, C.A, C.dinv);
   }
-  for (int l = 0; l + 1 < H.nlev; ++l) {
+  // levels 1 .. cfirst - 1 by tiled passes; cfirst .. nlev - 1 (the cluster-cycled small
+  // levels) and the coarsest inverse by one cluster launch
+  const int cfirst = H.nlev > 1 ? std::max(1, H.small_first) : H.nlev;
+  for (int l = 0; l + 1 < cfirst; ++l) {
     const MGLevel &F = H.lev[l], &C = H.lev[l + 1];
     const TileM tm = tiles_of(C.Mx, C.My);
     k_mg_build<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(view(F), C.Mx, C.My, tm, C.A, C.dinv);
   }
-  const MGLevel &C = H.lev[H.nlev - 1];
-  const int n = 2 * C.N;
-  k_mg_coarse_invert<<<1, CTA_THREADS, sizeof(double) * n * n, Lc.stream>>>(view(C), H.cinv, H.singular);
-  Lc.tick(H.nlev + 1);
+  if (cfirst < H.nlev) {
+    k_mg_build_small<<<SMALL_CLUSTER, NTm, smem, Lc.stream>>>(reinterpret_cast<const LevelView *>(H.views), cfirst,
+                                                             H.nlev, H.cinv, H.singular);
+  } else {
+    k_mg_coarse_invert<<<1, 32, 0, Lc.stream>>>(view(H.lev[H.nlev - 1]), H.cinv, H.singular);
+  }
+  Lc.tick(cfirst + 1);
 }
 
 template <class F22, class F21, class F12, class F11>
@@ -1057,9 +1153,13 @@ static void dispatch_ax(int ax, int ay, F22 f22, F21 f21, F12 f12, F11 f11) {
   else f11();
 }
 
-template <class BA, class ZV>
+struct NoEpi {};
+
+// One V-cycle z = M^-1 b; with an epilogue EPI (EpiV, EpiT) the fine-level pass also applies A
+// to z and hands y = A z to it (k_mg0_post_apply)
+template <class BA, class ZV, class EPI = NoEpi>
 static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, BA b, ZV *z,
-                   KState *st) {
+                   KState *st, const EPI &epi = EPI{}) {
   const FineF F = fine_view(g, f, H);
   const float omega = H.omega, corr = H.correction;
   int launches = 0;
@@ -1120,9 +1220,16 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(g.Mx, g.My);
     const int nb = blocks_for(Lc, tm.tiles);
+    if constexpr (std::is_same<EPI, NoEpi>::value) {
 #define MG0P(AX, AY) [&] { k_mg0_post<AX, AY, BA, ZV><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, st); }
-    dispatch_ax(H.fine_ax, H.fine_ay, MG0P(2, 2), MG0P(2, 1), MG0P(1, 2), MG0P(1, 1));
+      dispatch_ax(H.fine_ax, H.fine_ay, MG0P(2, 2), MG0P(2, 1), MG0P(1, 2), MG0P(1, 1));
 #undef MG0P
+    } else {
+      static_assert(std::is_same<ZV, float2>::value, "the fused pass produces FP32 iterates");
+#define MG0PA(AX, AY) [&] { k_mg0_post_apply<AX, AY, BA, EPI><<<nb, NTm, 0, Lc.stream>>>(F, b, omega, corr, C.My, C.x, tm, z, epi); }
+      dispatch_ax(H.fine_ax, H.fine_ay, MG0PA(2, 2), MG0PA(2, 1), MG0PA(1, 2), MG0PA(1, 1));
+#undef MG0PA
+    }
     ++launches;
   }
   Lc.tick(launches);
@@ -1141,6 +1248,16 @@ void mg_vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MGHier
 void mg_vcycle_s(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
                  const float2 *v, float2 *z, KState *st) {
   vcycle(Lc, g, f, H, SAcc{r, v, st, 0.0f}, z, st);
+}
+
+void mg_vcycle_apply(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *b,
+                     float2 *z, const EpiV &e) {
+  vcycle(Lc, g, f, H, VecAcc<float2>{b}, z, e.st, e);
+}
+
+void mg_vcycle_s_apply(const Launch &Lc, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
+                       const float2 *v, float2 *z, const EpiT &e) {
+  vcycle(Lc, g, f, H, SAcc{r, v, e.st, 0.0f}, z, e.st, e);
 }
 
 }  // namespace pism_gpu

@@ -10,7 +10,7 @@
 // answer meets the same ||b - A x|| <= rtol ||b|| as the plain FP64 solve; the FP32 stencil
 // reads 32 B per cell (x 8, nu*H 8, beta 4, flags 4, y 8) instead of 60.
 #include "ssa_fine32.cuh"
-#include "ssa_reduce.cuh"
+#include "ssa_krylov32.cuh"
 #include "ssa_tma_tile.cuh"
 
 namespace pism_gpu {
@@ -48,10 +48,6 @@ __device__ __forceinline__ bool apply32(const FineF &F, const Tile32 &tm, int t,
   if (!inside) return false;
   y = fine_apply_tile(F, i, j, f, bta, xT, nT, ti, tj);
   return true;
-}
-
-__device__ __forceinline__ double dotf(const float2 &a, const float2 &b) {
-  return (double)a.x * (double)b.x + (double)a.y * (double)b.y;
 }
 
 // start of an inner solve with d0 = 0: r = rhat = rhs, p = v = d = 0.  The outer test
@@ -185,50 +181,27 @@ __device__ __forceinline__ bool tile_loop_staged(const FineF &F, const Tile32 &t
   return lost != 0u;
 }
 
-__global__ void __launch_bounds__(NT32) k32_v(FineF F, Tile32 tm, const float2 *__restrict__ phat,
-                                              const float2 *__restrict__ rhat, float2 *__restrict__ v,
-                                              double *partials, unsigned *ticket, KState *st) {
-  if (st->done) return;
-  double acc[1] = {0.0};
-  const bool stalled = tile_loop_staged(F, tm, phat, [&](int k, const float2 &y) {
-    v[k] = y;
-    acc[0] += dotf(rhat[k], y);
-  });
-  if (stalled && threadIdx.x == 0) {
-    st->done = 1;
-    st->status = KSP_STALLED;
-  }
-  double tot[1];
-  if (grid_reduce<1>(acc, partials, ticket, tot)) {
-    if (tot[0] == 0.0 || !isfinite(tot[0])) {
-      st->done = 1;
-      st->status = isfinite(tot[0]) ? KSP_BREAKDOWN : KSP_NAN;
-    } else {
-      st->alpha = st->rho / tot[0];
+// y = A x over the tiles with the BiCGStab epilogue e (EpiV: v = A phat; EpiT: t = A shat);
+// STAGED: interior tiles through the bulk-copy stages, else every tile by plain loads
+template <class EPI, bool STAGED>
+__global__ void __launch_bounds__(NT32) k32_apply(FineF F, Tile32 tm, const float2 *__restrict__ x, EPI e) {
+  if (e.st->done) return;
+  e.begin();
+  auto body = [&](int k, const float2 &y) { e.body(k, y); };
+  if constexpr (STAGED) {
+    if (tile_loop_staged(F, tm, x, body) && threadIdx.x == 0) {
+      e.st->done = 1;
+      e.st->status = KSP_STALLED;
+    }
+  } else {
+    __shared__ HaloTile<float2> xT, nT;
+    for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
+      int k = 0;
+      float2 y;
+      if (apply32(F, tm, t, x, xT, nT, k, y)) body(k, y);
     }
   }
-}
-
-// t = A shat with the dots (t, s) and (t, t); s = r - alpha v is formed here, not stored
-__global__ void __launch_bounds__(NT32) k32_t(FineF F, Tile32 tm, const float2 *__restrict__ shat,
-                                              const float2 *__restrict__ r, const float2 *__restrict__ v,
-                                              float2 *__restrict__ tv, double *partials, unsigned *ticket,
-                                              KState *st) {
-  if (st->done) return;
-  const float al = (float)st->alpha;
-  double acc[2] = {0.0, 0.0};
-  const bool stalled = tile_loop_staged(F, tm, shat, [&](int k, const float2 &y) {
-    tv[k] = y;
-    const float2 rk = r[k], vk = v[k];
-    acc[0] += dotf(y, make_float2(rk.x - al * vk.x, rk.y - al * vk.y));
-    acc[1] += dotf(y, y);
-  });
-  if (stalled && threadIdx.x == 0) {
-    st->done = 1;
-    st->status = KSP_STALLED;
-  }
-  double tot[2];
-  if (grid_reduce<2>(acc, partials, ticket, tot)) st->omega = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
+  e.finish();
 }
 
 // d += alpha phat + omega shat; r = s - omega t with s = r - alpha v formed here
@@ -298,13 +271,24 @@ void launch_mixed_iteration(const Launch &L, const GridDev &g, const Fields &f, 
   const FineF F = fine_view(g, f, H);
   const Tile32 tm = tiles32(g);
   const int bv = blocks_n(L, N), bt = std::min(tm.tiles, L.max_blocks);
+  const EpiV ev{K.rhat, K.v, L.partials, L.ticket, K.st, {0.0}};
+  const EpiT et{K.r, K.v, K.t, L.partials, L.ticket, K.st, {0.0, 0.0}, 0.0f};
   k32_p<<<bv, NT32, 0, L.stream>>>(N, K.r, K.v, K.p, K.st);
-  mg_vcycle(L, g, f, H, K.p, K.phat, K.st);
-  k32_v<<<bt, NT32, 0, L.stream>>>(F, tm, K.phat, K.rhat, K.v, L.partials, L.ticket, K.st);
-  mg_vcycle_s(L, g, f, H, K.r, K.v, K.shat, K.st);   // s = r - alpha v is not stored
-  k32_t<<<bt, NT32, 0, L.stream>>>(F, tm, K.shat, K.r, K.v, K.t, L.partials, L.ticket, K.st);
+  if (H.apply_kernel == 2) {   // the V-cycles' fine-level passes apply A to their results
+    mg_vcycle_apply(L, g, f, H, K.p, K.phat, ev);
+    mg_vcycle_s_apply(L, g, f, H, K.r, K.v, K.shat, et);   // s = r - alpha v is not stored
+  } else {
+    const bool staged = H.apply_kernel == 1;
+    mg_vcycle(L, g, f, H, K.p, K.phat, K.st);
+    if (staged) k32_apply<EpiV, true><<<bt, NT32, 0, L.stream>>>(F, tm, K.phat, ev);
+    else k32_apply<EpiV, false><<<bt, NT32, 0, L.stream>>>(F, tm, K.phat, ev);
+    mg_vcycle_s(L, g, f, H, K.r, K.v, K.shat, K.st);   // s = r - alpha v is not stored
+    if (staged) k32_apply<EpiT, true><<<bt, NT32, 0, L.stream>>>(F, tm, K.shat, et);
+    else k32_apply<EpiT, false><<<bt, NT32, 0, L.stream>>>(F, tm, K.shat, et);
+    L.tick(2);
+  }
   k32_x<<<bv, NT32, 0, L.stream>>>(N, K.phat, K.shat, K.v, K.t, K.rhat, K.d, K.r, L.partials, L.ticket, K.st);
-  L.tick(4);
+  L.tick(2);
 }
 
 }  // namespace pism_gpu

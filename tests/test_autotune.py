@@ -187,3 +187,28 @@ def test_small_kernel_through_the_solver_interface(tmp_path):
     base = SSAConfig(pc_type="mg")
     assert tune_small_kernel(s, base, prime=lambda: None, tuner=tuner) == 1
     assert s.cfg is base
+
+
+def test_apply_kernel_through_the_solver_interface(tmp_path):
+    """the three BiCGStab apply kernels are timed like any other knob, the fastest chosen and
+    the caller's configuration left as it was"""
+    import numpy as np
+    from pism_b200.autotune import tune_apply_kernel
+    from pism_b200.config import SSAConfig
+    tuner, clock = make(tmp_path, repeats=1, warmup=0)
+
+    class Solver:
+        shape = (801, 801)
+        cfg = None
+
+        def set_config(self, c):
+            self.cfg = c
+
+        def solve(self):
+            clock.cost = {0: 230.0, 1: 228.0, 2: 200.0}[self.cfg.mixed_apply_kernel]
+            return np.ones(3)
+
+    s = Solver()
+    base = SSAConfig(pc_type="mg", precision="mixed")
+    assert tune_apply_kernel(s, base, prime=lambda: None, tuner=tuner) == 2
+    assert s.cfg is base

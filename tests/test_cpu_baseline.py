@@ -90,15 +90,28 @@ def test_native_picard_refuses_what_it_does_not_restate():
 
 
 def test_whole_solve_estimate_scales_the_sample_by_the_recorded_run():
-    """cost model: a Picard iteration costs (setup + GMRES iterations) GMRES iterations"""
+    """cost model: a Picard iteration costs (setup + GMRES iterations) units; the unit is the
+    sample's median, so one slowed iteration does not move the estimate"""
     b = _bench()
     full = {"threads": 8, "picard_iterations": {"1e-06": 350, "0.0001": 180},
-            "ksp_iterations": {"1e-06": 10000, "0.0001": 8000}, "first_ksp_iterations": [100, 200, 300],
-            "setup_iterations": 10.0}
-    est, how = b.cpu_estimate(6.6, 3, 1e-6, full=full)
-    assert est == pytest.approx(6.6 * (10000 + 350 * 10.0) / (300 + 3 * 10.0) * 1e3)
-    assert "350 Picard iterations" in how
-    est4, _ = b.cpu_estimate(2.2, 1, 1e-4, full=full)
-    assert est4 == pytest.approx(2.2 * (8000 + 180 * 10.0) / (100 + 10.0) * 1e3)
-    assert b.cpu_estimate(1.0, 3, 1e-7, full=full)[0] is None
-    assert b.cpu_estimate(1.0, 4, 1e-6, full=full)[0] is None
+            "ksp_iterations": {"1e-06": 10000, "0.0001": 8000}, "setup_iterations": 10.0}
+    sample = [(2.2, 100), (4.4, 100), (2.2, 100)]   # 20 ms per unit, the second iteration slowed
+    est, how = b.cpu_estimate(0.5, sample, 1e-6, full=full)
+    assert est == pytest.approx((0.5 + 0.02 * (10000 + 350 * 10.0)) * 1e3)
+    assert "350 Picard" in how and "10000 GMRES" in how
+    est4, _ = b.cpu_estimate(0.0, sample[:1], 1e-4, full=full)
+    assert est4 == pytest.approx(0.02 * (8000 + 180 * 10.0) * 1e3)
+    assert b.cpu_estimate(1.0, sample, 1e-7, full=full)[0] is None
+    assert b.cpu_estimate(1.0, [], 1e-6, full=full)[0] is None
+
+
+def test_recorded_run_predicts_itself():
+    """the recorded complete 801^2 run's totals are consistent with its own cost model: a
+    sample whose iterations cost exactly the model's unit reproduces n c + sum its"""
+    b = _bench()
+    full = b.CPU_FULL_RUN_801
+    c = full["setup_iterations"]
+    u = 0.05
+    est, _ = b.cpu_estimate(0.0, [(u * (c + 221), 221), (u * (c + 223), 223)], 1e-6)
+    assert est == pytest.approx(u * (full["ksp_iterations"]["1e-06"] + 359 * c) * 1e3)
+    assert full["ksp_iterations"]["0.0001"] < full["ksp_iterations"]["1e-06"]

@@ -432,6 +432,36 @@ def test_small_level_cycles_agree_bitwise(shape, precision):
     assert out[0][1:] == out[1][1:]
 
 
+@pytest.mark.parametrize("shape,graphs", [((201, 201), 3), ((161, 131), 2), ((130, 97), 0), ((45, 44), 3),
+                                           ("test_i", 3)])
+def test_apply_kernels_agree_bitwise(shape, graphs):
+    """Each FP32 V-cycle's fine-level pass fused with the operator apply that follows it
+    (mixed_apply_kernel 2: the halo of the smoothed iterate recomputed per tile) against the
+    apply kernel of its own with plain (0) and bulk-copy staged (1) tile loads: the same
+    arithmetic per cell and the same sums in the same order, so the same velocities and counts,
+    bit for bit -- on ragged tiles, periodic wrap at the grid's edges and Dirichlet rows."""
+    if shape == "test_i":
+        g, c, f = V.build_test_i(My=201)
+        c.ssafd_relative_convergence = 5e-7
+        c.ksp_rtol = 1e-12
+    else:
+        Mx, My = shape
+        g, c, f, _ = S.build_synthetic(Mx, 4000e3 / (Mx - 1), seed=6)
+        if My != Mx:
+            g = GridDesc(Mx, My, g.Lx, g.Lx * (My - 1) / (Mx - 1), periodicity=0, z=g.z)
+            f = {k: (v[:Mx, :My] if isinstance(v, np.ndarray) else v) for k, v in f.items()}
+        c.ksp_rtol = 1e-8
+        c.do_pseudo_plastic_till = True
+    c = c.copy(pc_type="mg", precision="mixed", graphs=graphs)
+    out = {}
+    for k in (0, 1, 2):
+        vel, st = _solve_case(g, c.copy(mixed_apply_kernel=k), f)
+        out[k] = (vel, st["picard_iterations"], st["ksp_iterations"], st["refinement_steps"])
+    for k in (1, 2):
+        np.testing.assert_array_equal(out[0][0], out[k][0])
+        assert out[0][1:] == out[k][1:]
+
+
 @pytest.mark.parametrize("shape", [(161, 131), (130, 97)])
 def test_mixed_solve_on_grids_with_staged_tiles(shape):
     """Grids wide enough for the FP32 apply kernels to stage interior tiles by bulk copies
