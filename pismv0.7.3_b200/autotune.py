@@ -204,7 +204,7 @@ def tune_small_kernel(solver, config, prime, candidates=(0, 1), tuner: Optional[
     return tune_config_knob(solver, config, prime, "mg_small_kernel", candidates, tuner, workload)
 
 
-def tune_apply_kernel(solver, config, prime, candidates=(0, 1, 2), tuner: Optional[Autotuner] = None,
+def tune_apply_kernel(solver, config, prime, candidates=(2, 0, 1), tuner: Optional[Autotuner] = None,
                       workload: Optional[dict] = None) -> int:
     """How BiCGStab's FP32 operator apply after each V-cycle runs: its own kernel with plain
     (0) or bulk-copy staged (1) tile loads, or fused into the V-cycle's fine-level pass (2)."""

@@ -97,7 +97,7 @@ class SSAConfig:
     mg_post_blocks_per_sm: int = 0
     mg_rebuild_rtol: float = 0.0
     mg_small_kernel: int = 0
-    mixed_apply_kernel: int = 1
+    mixed_apply_kernel: int = 2
     # geometry helpers (not part of the C struct)
     mask_icefree_thickness_standard: float = 0.01
     mask_is_floating_thickness_standard: float = 1.0

@@ -989,7 +989,7 @@ int pism_gpu_ssa_config_defaults(pism_gpu_ssa_config *c) {
   c->ksp_rtol_factor = 1.0e-2;
   c->graphs = 2;
   c->verbosity = 0;
-  c->mixed_apply_kernel = 1;
+  c->mixed_apply_kernel = 2;
   return PISM_GPU_SSA_OK;
 }
 

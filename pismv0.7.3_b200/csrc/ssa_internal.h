@@ -88,7 +88,7 @@ struct MGHierarchy {
   int small_smem = 0;                            // its per-CTA staging buffer (bytes)
   bool small_dsmem = false;                      // the small levels fit the cluster's shared memory
   int small_kernel = 0;                          // mg_small_kernel of the configuration
-  int apply_kernel = 1;                          // mixed_apply_kernel of the configuration
+  int apply_kernel = 2;                          // mixed_apply_kernel of the configuration
   SmallPlan small_plan{};                        // their split over the cluster's CTAs
   void *small_plan_dev = nullptr;                // device copy of small_plan
   float omega = 0.9f;                            // damping of the block-Jacobi smoother
