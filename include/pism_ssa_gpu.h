@@ -273,6 +273,23 @@ enum {
 };
 int pism_gpu_ssa_get_field(pism_gpu_ssa *h, int field, double *out, int where);
 
+/* The consumers of the SSA velocity in StressBalance::update with a full update
+ * (PISMStressBalance.cc:79-116, fast == false), from the handle's current velocity (the last
+ * solve's, or the initial guess), mask, thickness and enthalpy:
+ *   u3, v3          ConstantInColumn::update (SSB_Modifier.cc:126-152): every level of the
+ *                   3-D horizontal velocity is the column's SSA velocity
+ *   strain_heating  StressBalance::compute_volumetric_strain_heating
+ *                   (PISMStressBalance.cc:369-499), zero above kBelowHeight(H)
+ *   w3              StressBalance::compute_vertical_velocity (PISMStressBalance.cc:192-287),
+ *                   w(0) = -basal_melt_rate (Mx*My, m/s) or 0 when basal_melt_rate is NULL
+ *                   (include_bmr_in_continuity false)
+ * Each output is Mx*My*Mz doubles, [i][j][k] (IceModelVec3's column order); any may be NULL.
+ * All pointers are host or device per `where`.  Needs a grid with Mz >= 2 levels and, for
+ * the strain heating under an enthalpy-dependent flow law, the inputs' enthalpy.  Blocks
+ * until done. */
+int pism_gpu_ssa_stress_balance_3d(pism_gpu_ssa *h, const double *basal_melt_rate, double *u3, double *v3,
+                                   double *w3, double *strain_heating, int where);
+
 /* Stage entry points, each the device restatement of one reference method, for
  * stage-by-stage checking:
  *   assemble_rhs       -> SSA::compute_driving_stress + SSAFD::assemble_rhs

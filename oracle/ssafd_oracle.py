@@ -1019,6 +1019,93 @@ def basal_frictional_heating(cfg: Config, inp: Inputs, vel):
     return np.where(m_ocean(M), 0.0, -bx * u - by * v)
 
 
+# ---------------------------------------------------------------------------
+# the consumers of the SSA velocity in StressBalance::update (full update)
+# ---------------------------------------------------------------------------
+def _margin_differences(grid: Grid, M):
+    """The one-sided / centred difference weights at ice margins shared by the vertical
+    velocity and the strain heating (PISMStressBalance.cc:229-257, 414-442): (west, east,
+    D_x, south, north, D_y) per cell."""
+    icy, free = m_icy(M), m_ice_free(M)
+
+    def cut(di, dj):
+        Mn_icy, Mn_free = nb(icy, di, dj), nb(free, di, dj)
+        return np.where((icy & Mn_free) | (free & Mn_icy), 0.0, 1.0)
+
+    east, west, north, south = cut(1, 0), cut(-1, 0), cut(0, 1), cut(0, -1)
+    D_x = np.where(east + west > 0, 1.0 / (grid.dx * np.maximum(east + west, 1.0)), 0.0)
+    D_y = np.where(north + south > 0, 1.0 / (grid.dy * np.maximum(north + south, 1.0)), 0.0)
+    return west, east, D_x, south, north, D_y
+
+
+def constant_in_column(vel, Mz: int):
+    """ConstantInColumn::update, SSB_Modifier.cc:126-152: every level of the 3-D horizontal
+    velocity is the column's SSA velocity.  Returns (u3, v3), (Mx, My, Mz)."""
+    u3 = np.repeat(vel[..., 0:1], Mz, axis=2)
+    v3 = np.repeat(vel[..., 1:2], Mz, axis=2)
+    return u3, v3
+
+
+def vertical_velocity(grid: Grid, inp: Inputs, u3, v3, basal_melt_rate=None):
+    """StressBalance::compute_vertical_velocity, PISMStressBalance.cc:192-287: the trapezoid
+    rule integral of -(u_x + v_y) up each column from w(0) = -basal melt rate (or 0), with
+    one-sided differences at ice margins."""
+    M = as_int(inp.mask)
+    west, east, D_x, south, north, D_y = _margin_differences(grid, M)
+    z = np.asarray(grid.z, dtype=np.float64)
+    Mz = len(z)
+    w = np.zeros(u3.shape)
+    w[..., 0] = 0.0 if basal_melt_rate is None else -np.asarray(basal_melt_rate, dtype=np.float64)
+
+    def integrand(k):
+        u_x = D_x * (west * (u3[..., k] - nb(u3[..., k], -1, 0)) + east * (nb(u3[..., k], 1, 0) - u3[..., k]))
+        v_y = D_y * (south * (v3[..., k] - nb(v3[..., k], 0, -1)) + north * (nb(v3[..., k], 0, 1) - v3[..., k]))
+        return u_x + v_y
+
+    old = integrand(0)
+    for k in range(1, Mz):
+        new = integrand(k)
+        w[..., k] = w[..., k - 1] - 0.5 * (new + old) * (z[k] - z[k - 1])
+        old = new
+    return w
+
+
+def volumetric_strain_heating(grid: Grid, cfg: Config, inp: Inputs, u3, v3):
+    """StressBalance::compute_volumetric_strain_heating, PISMStressBalance.cc:369-499:
+    Sigma = 2 e^(-1/n) B(E, p) D^(1/n + 1) with the shallow approximation of D^2 (D2,
+    PISMStressBalance.cc:309-311) at the levels k <= kBelowHeight(H), zero above."""
+    M = as_int(inp.mask)
+    west, east, D_x, south, north, D_y = _margin_differences(grid, M)
+    z = np.asarray(grid.z, dtype=np.float64)
+    Mz = len(z)
+    H = np.asarray(inp.thickness, dtype=np.float64)
+    ks = k_below_height(z, H)
+    n = cfg.ssa_Glen_exponent
+    exponent = 0.5 * (1.0 / n + 1.0)
+    e_to_a_power = cfg.ssa_enhancement_factor ** (-1.0 / n)
+    # an isothermal flow law reads no enthalpy
+    E = np.zeros(u3.shape) if inp.enthalpy is None else np.asarray(inp.enthalpy, dtype=np.float64)
+    sigma = np.zeros(u3.shape)
+    for k in range(Mz - 1):
+        uk, vk = u3[..., k], v3[..., k]
+        u_x = D_x * (west * (uk - nb(uk, -1, 0)) + east * (nb(uk, 1, 0) - uk))
+        u_y = D_y * (south * (uk - nb(uk, 0, -1)) + north * (nb(uk, 0, 1) - uk))
+        v_x = D_x * (west * (vk - nb(vk, -1, 0)) + east * (nb(vk, 1, 0) - vk))
+        v_y = D_y * (south * (vk - nb(vk, 0, -1)) + north * (nb(vk, 0, 1) - vk))
+        if k > 0:
+            dz = z[k + 1] - z[k - 1]
+            u_z = (u3[..., k + 1] - u3[..., k - 1]) / dz
+            v_z = (v3[..., k + 1] - v3[..., k - 1]) / dz
+        else:
+            dz = z[1] - z[0]
+            u_z = (u3[..., 1] - u3[..., 0]) / dz
+            v_z = (v3[..., 1] - v3[..., 0]) / dz
+        B = hardness_parameter(cfg, E[..., k], ec_pressure(cfg, H - z[k]))
+        D2 = 0.5 * ((u_x + v_y) ** 2 + u_x * u_x + v_y * v_y + 0.5 * ((u_y + v_x) ** 2 + u_z * u_z + v_z * v_z))
+        sigma[..., k] = np.where(k <= ks, 2.0 * e_to_a_power * B * np.power(D2, exponent), 0.0)
+    return sigma
+
+
 def residual_rel(grid, cfg, inp, vel, reg, hardness, b):
     """||b - A(u) u||_2 / ||b||_2 with A built at the velocity itself (a nonlinear residual)."""
     nuH = compute_nuH(grid, cfg, inp, hardness, vel, reg)

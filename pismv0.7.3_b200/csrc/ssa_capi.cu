@@ -36,6 +36,7 @@ struct pism_gpu_ssa {
   // derived / state
   double2 *taud = nullptr, *rhs = nullptr, *hardness = nullptr, *nuH = nullptr, *vel = nullptr, *vel_old = nullptr;
   double *beta = nullptr, *bfrict = nullptr;
+  double *sb3d = nullptr;   // host-destination staging of pism_gpu_ssa_stress_balance_3d
   uint32_t *flags = nullptr;
   Krylov K{};
   Krylov32 K32{};
@@ -1083,7 +1084,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
                  h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G, h->lpc.img, h->lpc.out,
-                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma};
+                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma, h->sb3d};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -1247,6 +1248,37 @@ int pism_gpu_ssa_get_field(pism_gpu_ssa *h, int field, double *out, int where) {
     case PISM_FIELD_BFRICT: return copy_out(h, out, h->bfrict, 8 * N, where);
     default: return fail(h, PISM_GPU_SSA_EINVAL, "unknown field %d", field);
   }
+}
+
+int pism_gpu_ssa_stress_balance_3d(pism_gpu_ssa *h, const double *basal_melt_rate, double *u3, double *v3,
+                                   double *w3, double *strain_heating, int where) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (where != PISM_MEM_HOST && where != PISM_MEM_DEVICE) return fail(h, PISM_GPU_SSA_EINVAL, "bad memory kind");
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  const int Mz = (int)h->z_host.size();
+  if (Mz < 2) return fail(h, PISM_GPU_SSA_EINVAL, "the 3-D fields need a grid with Mz >= 2 levels");
+  if (strain_heating && h->cfg.flow_law != PISM_FLOW_LAW_ISOTHERMAL_GLEN && !h->have_enthalpy)
+    return fail(h, PISM_GPU_SSA_EINVAL, "the strain heating's flow law needs enthalpy");
+  const size_t N3 = (size_t)h->N * Mz;
+  double *out[4] = {u3, v3, w3, strain_heating};
+  double *dev[4] = {u3, v3, w3, strain_heating};
+  const double *bmr = basal_melt_rate;
+  if (where == PISM_MEM_HOST) {   // device staging: the four fields and the melt rate
+    if (!h->sb3d) RET(dalloc(h, &h->sb3d, 4 * N3 + h->N));
+    for (int q = 0; q < 4; ++q) dev[q] = out[q] ? h->sb3d + q * N3 : nullptr;
+    if (basal_melt_rate) {
+      RET(copy_in(h, h->sb3d + 4 * N3, basal_melt_rate, sizeof(double) * h->N, PISM_MEM_HOST));
+      bmr = h->sb3d + 4 * N3;
+    }
+  }
+  launch_stress_balance_3d(h->L, h->g, h->cfg, Mz, fields_of(h), h->z_dev, bmr, dev[0], dev[1], dev[2], dev[3]);
+  CK(h, cudaGetLastError());
+  if (where == PISM_MEM_HOST)
+    for (int q = 0; q < 4; ++q)
+      if (out[q]) RET(copy_out(h, out[q], dev[q], sizeof(double) * N3, PISM_MEM_HOST));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
 }
 
 int pism_gpu_ssa_assemble_rhs(pism_gpu_ssa *h) {

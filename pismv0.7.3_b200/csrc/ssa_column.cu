@@ -1,0 +1,129 @@
+// ssa_column.cu — the consumers of the SSA velocity in StressBalance::update with a full
+// update (PISMStressBalance.cc:79-116), on the device, from the handle's velocity, mask,
+// thickness and enthalpy columns:
+//
+//   u3, v3  ConstantInColumn::update (SSB_Modifier.cc:126-152): every level of the 3-D
+//           horizontal velocity is the column's SSA velocity
+//   sigma   StressBalance::compute_volumetric_strain_heating (PISMStressBalance.cc:369-499)
+//   w3      StressBalance::compute_vertical_velocity (PISMStressBalance.cc:192-287)
+//
+// The 3-D fields are [i][j][k] (a column's Mz levels contiguous).  One thread per (column,
+// level), consecutive threads on consecutive levels, so every load of an enthalpy column and
+// every store of the four outputs is coalesced.  The horizontal velocity is constant in each
+// column, so u_z = v_z = 0 exactly and the horizontal derivatives are the column's; each
+// thread recomputes them (the neighbours' velocities and masks come from L1) and the
+// trapezoid sum of w up to its level, in the reference's order of operations.
+#include <algorithm>
+#include <cmath>
+
+#include "ssa_internal.h"
+
+namespace pism_gpu {
+
+namespace {
+
+constexpr int NTC = 256;
+
+__device__ __forceinline__ bool icy(int m) { return m == 2 || m == 3; }   // Mask.hh:46-48
+
+// the margin-aware difference weights of one column (PISMStressBalance.cc:229-257): (west,
+// east, D_x), (south, north, D_y)
+struct ColumnDiff {
+  double west, east, D_x, south, north, D_y;
+};
+
+__device__ __forceinline__ ColumnDiff column_diff(const GridDev &g, const int8_t *__restrict__ mask, int i, int j) {
+  const int m = mask[cell(g, i, j)];
+  auto cut = [&](int di, int dj) {
+    const int n = mask[nbr(g, i, j, di, dj)];
+    return ((icy(m) && !icy(n)) || (!icy(m) && icy(n))) ? 0.0 : 1.0;
+  };
+  ColumnDiff d;
+  d.east = cut(1, 0);
+  d.west = cut(-1, 0);
+  d.north = cut(0, 1);
+  d.south = cut(0, -1);
+  d.D_x = d.east + d.west > 0 ? 1.0 / (g.dx * (d.east + d.west)) : 0.0;
+  d.D_y = d.north + d.south > 0 ? 1.0 / (g.dy * (d.north + d.south)) : 0.0;
+  return d;
+}
+
+// IceGrid::kBelowHeight through gsl_interp_accel_find: the largest k in [0, Mz - 2] with
+// z[k] <= height (GSL's bisection, lo = 0, hi = Mz - 1)
+__device__ __forceinline__ int k_below_height(const double *__restrict__ z, int Mz, double height) {
+  int lo = 0, hi = Mz - 1;
+  while (hi > lo + 1) {
+    const int mid = (lo + hi) / 2;
+    if (z[mid] > height) hi = mid;
+    else lo = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(NTC) k_stress_balance_3d(GridDev g, pism_gpu_ssa_config c, int Mz,
+                                                           double e_to_a_power, double exponent,
+                                                           const double2 *__restrict__ vel,
+                                                           const int8_t *__restrict__ mask,
+                                                           const double *__restrict__ H,
+                                                           const double *__restrict__ E,
+                                                           const double *__restrict__ z,
+                                                           const double *__restrict__ bmr, double *__restrict__ u3,
+                                                           double *__restrict__ v3, double *__restrict__ w3,
+                                                           double *__restrict__ sigma) {
+  const long long total = (long long)g.Mx * g.My * Mz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(q / Mz), k = (int)(q - (long long)col * Mz);
+    const int i = col / g.My, j = col - i * g.My;
+    const double2 U = vel[col];
+    if (u3) u3[q] = U.x;
+    if (v3) v3[q] = U.y;
+    if (!w3 && !sigma) continue;
+    const ColumnDiff d = column_diff(g, mask, i, j);
+    const double2 Uw = vel[nbr(g, i, j, -1, 0)], Ue = vel[nbr(g, i, j, 1, 0)], Us = vel[nbr(g, i, j, 0, -1)],
+                  Un = vel[nbr(g, i, j, 0, 1)];
+    const double u_x = d.D_x * (d.west * (U.x - Uw.x) + d.east * (Ue.x - U.x));
+    const double v_y = d.D_y * (d.south * (U.y - Us.y) + d.north * (Un.y - U.y));
+    if (w3) {
+      // w(0) = -bmr (or 0); w(k) = w(k-1) - (integrand(k) + integrand(k-1)) / 2 dz, the
+      // integrand u_x + v_y the same at every level; the products and sums in that order
+      const double integrand = __dadd_rn(u_x, v_y);
+      double w = bmr ? -bmr[col] : 0.0;
+      for (int kk = 1; kk <= k; ++kk)
+        w = __dsub_rn(w, __dmul_rn(__dmul_rn(0.5, __dadd_rn(integrand, integrand)), __dsub_rn(z[kk], z[kk - 1])));
+      w3[q] = w;
+    }
+    if (sigma) {
+      const double Hc = H[col];
+      const int ks = k_below_height(z, Mz, Hc);
+      double s = 0.0;
+      if (k <= ks) {
+        const double u_y = d.D_y * (d.south * (U.x - Us.x) + d.north * (Un.x - U.x));
+        const double v_x = d.D_x * (d.west * (U.y - Uw.y) + d.east * (Ue.y - U.y));
+        const double B = hardness_parameter(c, E ? E[q] : 0.0, ec_pressure(c, Hc - z[k]));
+        const double a = u_x + v_y, b = u_y + v_x;   // u_z = v_z = 0
+        // D2(), PISMStressBalance.cc:309-311
+        const double D2 = 0.5 * (a * a + u_x * u_x + v_y * v_y + 0.5 * (b * b));
+        s = 2.0 * e_to_a_power * B * pow(D2, exponent);
+      }
+      sigma[q] = s;
+    }
+  }
+}
+
+}  // namespace
+
+void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int Mz,
+                              const Fields &f, const double *z, const double *bmr, double *u3, double *v3,
+                              double *w3, double *sigma) {
+  const long long total = (long long)g.Mx * g.My * Mz;
+  const int blocks = (int)std::min<long long>((total + NTC - 1) / NTC, 2LL * L.max_blocks);
+  // PISMStressBalance.cc:384-387: the flow law's exponent and enhancement factor
+  const double n = c.ssa_Glen_exponent, exponent = 0.5 * (1.0 / n + 1.0);
+  const double e_to_a_power = std::pow(c.ssa_enhancement_factor, -1.0 / n);
+  L.tick();
+  k_stress_balance_3d<<<blocks, NTC, 0, L.stream>>>(g, c, Mz, e_to_a_power, exponent, f.vel, f.mask, f.H, f.enthalpy,
+                                                    z, bmr, u3, v3, w3, sigma);
+}
+
+}  // namespace pism_gpu

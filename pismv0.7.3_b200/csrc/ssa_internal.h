@@ -161,6 +161,10 @@ void mg_vcycle_apply(const Launch &L, const GridDev &g, const Fields &f, const M
                      float2 *z, const EpiV &e);
 void mg_vcycle_s_apply(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
                        const float2 *v, float2 *z, const EpiT &e);
+// ---- the consumers of the SSA velocity (ssa_column.cu) ----
+void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int Mz,
+                              const Fields &f, const double *z, const double *bmr, double *u3, double *v3,
+                              double *w3, double *sigma);
 // ---- line block-Jacobi preconditioner (ssa_line.cu) ----
 void line_setup(const Launch &L, const GridDev &g, const Fields &f, const double4 *dinv, const LinePC &lp);
 void line_apply(const Launch &L, const GridDev &g, const LinePC &lp, const double2 *b, double2 *z, const KState *st);

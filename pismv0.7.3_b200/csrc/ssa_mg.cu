@@ -120,17 +120,39 @@ __global__ void k_mg0_compact(int N, const double2 *__restrict__ nuH, const doub
 // set-up: Galerkin coarse operators
 // ---------------------------------------------------------------------------
 // level 1 from the fine operator (FP64 rows, FP64 accumulation in shared memory)
+// acc[4 cb .. 4 cb + 3] += (x, y, z, w) for a block index cb known only at run time: the
+// accumulators stay in registers (every index below is static once unrolled), so the
+// operator loads of the next fine cell need not wait behind shared-memory updates
+__device__ __forceinline__ void acc_block(double (&acc)[36], int cb, double x, double y, double z, double w) {
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    if (cb == c) {
+      acc[4 * c + 0] += x;
+      acc[4 * c + 1] += y;
+      acc[4 * c + 2] += z;
+      acc[4 * c + 3] += w;
+    }
+}
+
+// the coarse cell's nine blocks (FP32) and its D^-1 from the FP64 sums
+__device__ __forceinline__ void store_coarse(const double (&acc)[36], int Nc, int kc, float4 *Ac, float4 *dinvc) {
+#pragma unroll
+  for (int b = 0; b < 9; ++b)
+    Ac[b * Nc + kc] = make_float4((float)acc[4 * b], (float)acc[4 * b + 1], (float)acc[4 * b + 2], (float)acc[4 * b + 3]);
+  dinvc[kc] = inv2x2((float)acc[16], (float)acc[17], (float)acc[18], (float)acc[19]);
+}
+
 __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, const uint32_t *__restrict__ flags,
                                                    const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                                    int ax, int ay, int Mxc, int Myc, TileM tm, float4 *Ac,
                                                    float4 *dinvc) {
-  extern __shared__ double acc_sh[];   // [36][NTm]
-  double *acc = acc_sh + threadIdx.x;
   const int Nc = Mxc * Myc;
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int I, J;
     if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
-    for (int q = 0; q < 36; ++q) acc[q * NTm] = 0.0;
+    double acc[36];
+#pragma unroll
+    for (int q = 0; q < 36; ++q) acc[q] = 0.0;
     for (int pi = 0; pi < ax; ++pi)
       for (int pj = 0; pj < ay; ++pj) {
         const int i = I * ax + pi, j = J * ay + pj;
@@ -138,9 +160,8 @@ __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, co
         const uint32_t f = flags[cell(g, i, j)];
         Row2 e1, e2;
         if (!cell_rows(g, s, i, j, f, nuH, beta, e1, e2)) {
-          const int cb = blk_of(0, 0);
-          acc[(4 * cb + 0) * NTm] += s.scaling;
-          acc[(4 * cb + 3) * NTm] += s.scaling;
+          acc[4 * blk_of(0, 0) + 0] += s.scaling;
+          acc[4 * blk_of(0, 0) + 3] += s.scaling;
           continue;
         }
         const double r1u[9] = {e1.uNW, e1.uN, e1.uNE, e1.uW, e1.uC, e1.uE, e1.uSW, e1.uS, e1.uSE};
@@ -151,58 +172,53 @@ __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, co
         for (int b = 0; b < 9; ++b) {
           const int di = (b % 3) - 1, dj = 1 - (b / 3);
           const int ni = wrap(i + di, g.Mx), nj = wrap(j + dj, g.My);
-          const int cb = blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc));
-          acc[(4 * cb + 0) * NTm] += r1u[b];
-          acc[(4 * cb + 1) * NTm] += r1v[b];
-          acc[(4 * cb + 2) * NTm] += r2u[b];
-          acc[(4 * cb + 3) * NTm] += r2v[b];
+          acc_block(acc, blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc)), r1u[b], r1v[b], r2u[b], r2v[b]);
         }
       }
-    const int kc = I * Myc + J;
-    for (int b = 0; b < 9; ++b)
-      Ac[b * Nc + kc] = make_float4((float)acc[(4 * b) * NTm], (float)acc[(4 * b + 1) * NTm],
-                                    (float)acc[(4 * b + 2) * NTm], (float)acc[(4 * b + 3) * NTm]);
-    dinvc[kc] = inv2x2((float)acc[16 * NTm], (float)acc[17 * NTm], (float)acc[18 * NTm], (float)acc[19 * NTm]);
+    store_coarse(acc, Nc, I * Myc + J, Ac, dinvc);
   }
 }
 
-// Galerkin operator and D^-1 of coarse cell (I, J) of the level below F, accumulated in FP64
-// in acc[q * NTm] (q < 36: the nine 2 x 2 blocks)
-__device__ __forceinline__ void galerkin_cell(const LevelView &F, int Mxc, int Myc, int I, int J, double *acc,
-                                              float4 *Ac, float4 *dinvc) {
-  const int Nc = Mxc * Myc, ax = F.ax, ay = F.ay;
-  for (int q = 0; q < 36; ++q) acc[q * NTm] = 0.0;
-  for (int pi = 0; pi < ax; ++pi)
-    for (int pj = 0; pj < ay; ++pj) {
-      const int i = I * ax + pi, j = J * ay + pj;
-      if (i >= F.Mx || j >= F.My) continue;
-      const int k = i * F.My + j;
+// Galerkin operator and D^-1 of coarse cell (I, J) of the level below F, summed in FP64 in
+// registers: the nine blocks of every fine cell of the aggregate are loaded first (one round
+// of loads per coarse cell), then added in the order fine cell, block
+__device__ __forceinline__ void galerkin_cell(const LevelView &F, int Mxc, int Myc, int I, int J, float4 *Ac,
+                                              float4 *dinvc) {
+  const int ax = F.ax, ay = F.ay;
+  float4 a[4][9];
+  bool ok[4];
 #pragma unroll
-      for (int b = 0; b < 9; ++b) {
-        const int di = (b % 3) - 1, dj = 1 - (b / 3);
-        const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
-        const int cb = blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc));
-        const float4 a = F.A[b * F.N + k];
-        acc[(4 * cb + 0) * NTm] += (double)a.x;
-        acc[(4 * cb + 1) * NTm] += (double)a.y;
-        acc[(4 * cb + 2) * NTm] += (double)a.z;
-        acc[(4 * cb + 3) * NTm] += (double)a.w;
-      }
+  for (int p = 0; p < 4; ++p) {
+    const int pi = p >> 1, pj = p & 1, i = I * ax + pi, j = J * ay + pj;
+    ok[p] = pi < ax && pj < ay && i < F.Mx && j < F.My;
+    const int k = ok[p] ? i * F.My + j : 0;
+#pragma unroll
+    for (int b = 0; b < 9; ++b) a[p][b] = F.A[b * F.N + k];
+  }
+  double acc[36];
+#pragma unroll
+  for (int q = 0; q < 36; ++q) acc[q] = 0.0;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    if (!ok[p]) continue;
+    const int i = I * ax + (p >> 1), j = J * ay + (p & 1);
+#pragma unroll
+    for (int b = 0; b < 9; ++b) {
+      const int di = (b % 3) - 1, dj = 1 - (b / 3);
+      const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
+      acc_block(acc, blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc)), a[p][b].x, a[p][b].y, a[p][b].z,
+                a[p][b].w);
     }
-  const int kc = I * Myc + J;
-  for (int b = 0; b < 9; ++b)
-    Ac[b * Nc + kc] = make_float4((float)acc[(4 * b) * NTm], (float)acc[(4 * b + 1) * NTm],
-                                  (float)acc[(4 * b + 2) * NTm], (float)acc[(4 * b + 3) * NTm]);
-  dinvc[kc] = inv2x2((float)acc[16 * NTm], (float)acc[17 * NTm], (float)acc[18 * NTm], (float)acc[19 * NTm]);
+  }
+  store_coarse(acc, Mxc * Myc, I * Myc + J, Ac, dinvc);
 }
 
 // level l+1 from the stored operator of level l
 __global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc, TileM tm, float4 *Ac, float4 *dinvc) {
-  extern __shared__ double acc_sh[];
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int I, J;
     if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
-    galerkin_cell(F, Mxc, Myc, I, J, acc_sh + threadIdx.x, Ac, dinvc);
+    galerkin_cell(F, Mxc, Myc, I, J, Ac, dinvc);
   }
 }
 
@@ -304,7 +320,6 @@ __global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *in
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
     k_mg_build_small(const LevelView *__restrict__ lev, int first, int nlev, double *invT_out, int *singular) {
   cg::cluster_group cluster = cg::this_cluster();
-  extern __shared__ double acc_sh[];
   __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
   __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
   const int rank = cluster.block_rank() * NTm + threadIdx.x, nthr = SMALL_CLUSTER * NTm;
@@ -312,8 +327,7 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
     const LevelView F = lev[c - 1], C = lev[c];
     for (int kc = rank; kc < C.N; kc += nthr) {
       const int I = kc / C.My, J = kc - I * C.My;
-      galerkin_cell(F, C.Mx, C.My, I, J, acc_sh + threadIdx.x, const_cast<float4 *>(C.A),
-                    const_cast<float4 *>(C.dinv));
+      galerkin_cell(F, C.Mx, C.My, I, J, const_cast<float4 *>(C.A), const_cast<float4 *>(C.dinv));
     }
     cluster.sync();
   }
@@ -1049,9 +1063,6 @@ int mg_allocate(MGHierarchy &H, int fine_cells) {
       return 1;
     if (raise_dynamic_smem((const void *)k_mg_small_dsmem, H.small_plan.smem) != 0) return 1;
   }
-  if (raise_dynamic_smem((const void *)k_mg_build_small, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
-  if (raise_dynamic_smem((const void *)k_mg_build1, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
-  if (raise_dynamic_smem((const void *)k_mg_build, (int)(sizeof(double) * 36 * NTm)) != 0) return 1;
   return 0;
 }
 
@@ -1121,11 +1132,10 @@ void mg_setup_fine(const Launch &Lc, const GridDev &g, const Fields &f, const do
 // the coarse levels: Galerkin operators and D^-1 of every level, the coarsest inverse
 void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHierarchy &H) {
   const StencilConst s = stencil_const(g, f);
-  const size_t smem = sizeof(double) * 36 * NTm;
   {
     const MGLevel &C = H.lev[0];
     const TileM tm = tiles_of(C.Mx, C.My);
-    k_mg_build1<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(g, s, f.flags, f.nuH, f.beta, H.fine_ax,
+    k_mg_build1<<<blocks_for(Lc, tm.tiles), NTm, 0, Lc.stream>>>(g, s, f.flags, f.nuH, f.beta, H.fine_ax,
                                                                      H.fine_ay, C.Mx, C.My, tm, C.A, C.dinv);
   }
   // levels 1 .. cfirst - 1 by tiled passes; cfirst .. nlev - 1 (the cluster-cycled small
@@ -1134,10 +1144,10 @@ void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHier
   for (int l = 0; l + 1 < cfirst; ++l) {
     const MGLevel &F = H.lev[l], &C = H.lev[l + 1];
     const TileM tm = tiles_of(C.Mx, C.My);
-    k_mg_build<<<blocks_for(Lc, tm.tiles), NTm, smem, Lc.stream>>>(view(F), C.Mx, C.My, tm, C.A, C.dinv);
+    k_mg_build<<<blocks_for(Lc, tm.tiles), NTm, 0, Lc.stream>>>(view(F), C.Mx, C.My, tm, C.A, C.dinv);
   }
   if (cfirst < H.nlev) {
-    k_mg_build_small<<<SMALL_CLUSTER, NTm, smem, Lc.stream>>>(reinterpret_cast<const LevelView *>(H.views), cfirst,
+    k_mg_build_small<<<SMALL_CLUSTER, NTm, 0, Lc.stream>>>(reinterpret_cast<const LevelView *>(H.views), cfirst,
                                                              H.nlev, H.cinv, H.singular);
   } else {
     k_mg_coarse_invert<<<1, 32, 0, Lc.stream>>>(view(H.lev[H.nlev - 1]), H.cinv, H.singular);

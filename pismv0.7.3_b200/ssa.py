@@ -266,6 +266,36 @@ class SSAFD:
     def basal_frictional_heating(self, out=None):
         return self._get(_capi.FIELD_BFRICT, self.shape, out)
 
+    def stress_balance_3d(self, basal_melt_rate=None, out=None, device: bool = False) -> dict:
+        """The consumers of the velocity in StressBalance::update with a full update
+        (PISMStressBalance.cc:79-116): ConstantInColumn's 3-D horizontal velocity "u", "v"
+        (SSB_Modifier.cc:126-152), the vertical velocity "w" (PISMStressBalance.cc:192-287; w at
+        the base = -basal_melt_rate, or 0 without one) and the volumetric strain heating
+        "strain_heating" (PISMStressBalance.cc:369-499), each [Mx, My, Mz], from the current
+        velocity.  `out` may give preallocated host arrays or CUDA tensors (all of one kind)
+        for any of the four; the others are created (CUDA tensors when device=True)."""
+        Mz = 0 if self.grid.z is None else len(self.grid.z)
+        shape = (*self.shape, Mz)
+        names = ("u", "v", "w", "strain_heating")
+        out = dict(out or {})
+        on_device = device or any(_is_device(a) for a in out.values())
+        for k in names:
+            if k not in out:
+                if on_device:
+                    import torch
+                    out[k] = torch.empty(shape, dtype=torch.float64, device=f"cuda:{self.device}")
+                else:
+                    out[k] = np.empty(shape)
+        bufs = {k: _Buf(out[k], shape) for k in names}
+        bmr = _Buf(basal_melt_rate, self.shape) if basal_melt_rate is not None else None
+        if bmr is not None and bmr.device != on_device:
+            raise ValueError("basal_melt_rate must be where the outputs are (host or device)")
+        where = _capi.MEM_DEVICE if on_device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_stress_balance_3d(
+            self._h, bmr.ptr if bmr is not None else None, *(bufs[k].ptr for k in names), where),
+            "stress_balance_3d")
+        return {k: (bufs[k].keep if on_device else out[k]) for k in names}
+
     # ---- stage methods (one reference method each) ----
     def assemble_rhs(self):
         self._check(self.lib.pism_gpu_ssa_assemble_rhs(self._h), "assemble_rhs")
@@ -308,3 +338,52 @@ class SSAFD:
 def SSAFD_GPUFactory(grid: GridDesc, config: SSAConfig | None = None) -> SSAFD:
     """The SSAFactory of this solver (typedef SSAFactory, SSA.hh:77; SSAFDFactory SSAFD.cc:47-49)."""
     return SSAFD(grid, config)
+
+
+class StressBalance:
+    """StressBalance (PISMStressBalance.hh) over this SSAFD with the ConstantInColumn modifier
+    (SSB_Modifier.hh:71-74): update() runs the SSA solve and, unless fast, the 3-D fields
+    its consumers read (PISMStressBalance.cc:79-116), all on the device; the getters return
+    the last update's fields."""
+
+    def __init__(self, ssa: SSAFD, device_outputs: bool = False):
+        self.ssa = ssa
+        self.device_outputs = device_outputs
+        self._bmr = None
+        self._fields = None
+
+    def set_basal_melt_rate(self, bmr_input):
+        """StressBalance::set_basal_melt_rate (PISMStressBalance.cc:73-76)."""
+        self._bmr = bmr_input
+
+    def set_boundary_conditions(self, locations, velocities):
+        self.ssa.set_boundary_conditions(locations, velocities)
+
+    def update(self, fast: bool = False, melange_back_pressure=None):
+        """StressBalance::update (PISMStressBalance.cc:79-116)."""
+        self.ssa.update(fast, melange_back_pressure)
+        if not fast:
+            self._fields = self.ssa.stress_balance_3d(self._bmr, device=self.device_outputs)
+
+    def advective_velocity(self):
+        return self.ssa.velocity()
+
+    def basal_frictional_heating(self):
+        return self.ssa.basal_frictional_heating()
+
+    def _field(self, name):
+        if self._fields is None:
+            raise SSAError("StressBalance::update(fast=False) has not run")
+        return self._fields[name]
+
+    def velocity_u(self):
+        return self._field("u")
+
+    def velocity_v(self):
+        return self._field("v")
+
+    def velocity_w(self):
+        return self._field("w")
+
+    def volumetric_strain_heating(self):
+        return self._field("strain_heating")
