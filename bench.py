@@ -249,6 +249,47 @@ def large_roofline(c, stream, flush, dev, peak, M=1601):
     return r
 
 
+def column_roofline(vel, stream, flush, dev, peak, M=801, Mz=41, reps=20):
+    """StressBalance::update's 3-D fields (pism_gpu_ssa_stress_balance_3d: ConstantInColumn's
+    u and v, the vertical velocity, the volumetric strain heating) on the benchmark sheet with
+    Mz levels through 4000 m, from the solved velocity, device outputs.  Algorithmic bytes per
+    call: the four [M, M, Mz] FP64 outputs written once plus the velocity, mask, thickness and
+    basal melt rate read once (the flow law is isothermal: no enthalpy is read)."""
+    import torch
+    from pism_b200.config import GridDesc
+    from pism_b200.ssa import SSAFD
+    g0, cl, f, _ = build_case(M)
+    g = GridDesc(g0.Mx, g0.My, g0.Lx, g0.Ly, periodicity=0, z=np.linspace(0.0, 4000.0, Mz))
+    s = SSAFD(g, cl, device=dev.index)
+    try:
+        s.set_stream(stream.cuda_stream)
+        s.set_inputs(**{k: torch.tensor(f[k], dtype=torch.float64, device=dev)
+                        for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
+        s.set_initial_guess(vel)
+        bmr = torch.full((M, M), 1e-9, dtype=torch.float64, device=dev)
+        out = {k: torch.empty((M, M, Mz), dtype=torch.float64, device=dev)
+               for k in ("u", "v", "w", "strain_heating")}
+        s.stress_balance_3d(bmr, out=out)
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.stress_balance_3d(bmr, out=out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+    finally:
+        s.close()
+    ms = float(np.median(ts))
+    nbytes = 4 * 8 * M * M * Mz + M * M * (16 + 1 + 8 + 8)
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"grid": [M, M, Mz], "ms": ms, "bytes_per_call": nbytes, "achieved": achieved, "unit": "GB/s",
+            "peak": peak, "frac": achieved / peak, "bound": "hbm",
+            "kernel": "k_stress_balance_3d (one thread per column level; the call's time includes its "
+                      "argument checks and one stream synchronisation)"}
+
+
 # The host-core cost of the whole reference solve is sampled: the first CPU_SAMPLE_PICARD
 # Picard iterations of the native restatement (oracle/ssafd_cpu.cc: nu*H, drag, 18-column
 # assembly, PETSc-style GMRES(30) + block Jacobi / ILU(0), norms) run on the host cores, and
@@ -825,6 +866,12 @@ def main():
             line["roofline"]["large"] = large_roofline(c, stream, flush, dev, peak)
         except Exception as e:   # noqa: BLE001 - reported in the line
             line["roofline"]["large"] = {"error": str(e)[:200]}
+    # the stress balance's 3-D fields from the timed solve's velocity
+    if not args.no_large and M == 801:
+        try:
+            line["stress_balance_3d"] = column_roofline(vel_mode, stream, flush, dev, peak)
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["stress_balance_3d"] = {"error": str(e)[:200]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
         plain_picard = st_other["picard_iterations"] if args.mode == "fast" else picard[-1]

@@ -142,6 +142,38 @@ __device__ __forceinline__ void store_coarse(const double (&acc)[36], int Nc, in
   dinvc[kc] = inv2x2((float)acc[16], (float)acc[17], (float)acc[18], (float)acc[19]);
 }
 
+// Whether the coarse blocks of a fine cell's nine blocks follow from its place in a 2 x 2
+// aggregate alone: floor((p + d) / 2) for fine offset p in {0, 1} and stencil offset d.
+// That holds for 2 x 2 aggregation with >= 3 coarse cells each way (the periodic wrap then
+// only links the first and last aggregates, at offset -1 / +1 as in the interior), except
+// that on a level with an odd number of cells the last aggregate is one cell wide and its
+// wrapped east (north) neighbour is the first aggregate, one further (ex, ey).
+__device__ __forceinline__ bool static_blocks(int ax, int ay, int Mxc, int Myc) {
+  return ax == 2 && ay == 2 && Mxc >= 3 && Myc >= 3;
+}
+
+// acc += the nine blocks v(b) of fine cell (PI, PJ) of its aggregate, each to its coarse
+// block (static_blocks); the additions in block order, as acc_block would make them
+template <int PI, int PJ, class V>
+__device__ __forceinline__ void acc_fine_static(double (&acc)[36], bool ex, bool ey, const V &v) {
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const int di = (b % 3) - 1, dj = 1 - (b / 3);
+    const int ci = (PI + di + 2) / 2 - 1, cj = (PJ + dj + 2) / 2 - 1;   // floor((p + d) / 2)
+    const bool wx = PI == 0 && di == 1, wy = PJ == 0 && dj == 1;       // may cross the odd edge
+    const double4 x = v(b);
+    if (wx || wy) {
+      acc_block(acc, blk_of(ci + (wx && ex ? 1 : 0), cj + (wy && ey ? 1 : 0)), x.x, x.y, x.z, x.w);
+    } else {
+      const int cb = blk_of(ci, cj);
+      acc[4 * cb + 0] += x.x;
+      acc[4 * cb + 1] += x.y;
+      acc[4 * cb + 2] += x.z;
+      acc[4 * cb + 3] += x.w;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, const uint32_t *__restrict__ flags,
                                                    const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                                    int ax, int ay, int Mxc, int Myc, TileM tm, float4 *Ac,
@@ -153,21 +185,28 @@ __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, co
     double acc[36];
 #pragma unroll
     for (int q = 0; q < 36; ++q) acc[q] = 0.0;
-    for (int pi = 0; pi < ax; ++pi)
-      for (int pj = 0; pj < ay; ++pj) {
-        const int i = I * ax + pi, j = J * ay + pj;
-        if (i >= g.Mx || j >= g.My) continue;
-        const uint32_t f = flags[cell(g, i, j)];
-        Row2 e1, e2;
-        if (!cell_rows(g, s, i, j, f, nuH, beta, e1, e2)) {
-          acc[4 * blk_of(0, 0) + 0] += s.scaling;
-          acc[4 * blk_of(0, 0) + 3] += s.scaling;
-          continue;
-        }
-        const double r1u[9] = {e1.uNW, e1.uN, e1.uNE, e1.uW, e1.uC, e1.uE, e1.uSW, e1.uS, e1.uSE};
-        const double r1v[9] = {e1.vNW, e1.vN, e1.vNE, e1.vW, e1.vC, e1.vE, e1.vSW, e1.vS, e1.vSE};
-        const double r2u[9] = {e2.uNW, e2.uN, e2.uNE, e2.uW, e2.uC, e2.uE, e2.uSW, e2.uS, e2.uSE};
-        const double r2v[9] = {e2.vNW, e2.vN, e2.vNE, e2.vW, e2.vC, e2.vE, e2.vSW, e2.vS, e2.vSE};
+    const bool fast = static_blocks(ax, ay, Mxc, Myc);
+    const bool ex = (g.Mx & 1) && I == Mxc - 1, ey = (g.My & 1) && J == Myc - 1;
+    // the two rows of fine cell (pi, pj), added to its coarse blocks
+    auto fine = [&](auto PI, auto PJ) {
+      const int pi = decltype(PI)::value, pj = decltype(PJ)::value;
+      const int i = I * ax + pi, j = J * ay + pj;
+      if (pi >= ax || pj >= ay || i >= g.Mx || j >= g.My) return;
+      const uint32_t f = flags[cell(g, i, j)];
+      Row2 e1, e2;
+      if (!cell_rows(g, s, i, j, f, nuH, beta, e1, e2)) {
+        acc[4 * blk_of(0, 0) + 0] += s.scaling;
+        acc[4 * blk_of(0, 0) + 3] += s.scaling;
+        return;
+      }
+      const double r1u[9] = {e1.uNW, e1.uN, e1.uNE, e1.uW, e1.uC, e1.uE, e1.uSW, e1.uS, e1.uSE};
+      const double r1v[9] = {e1.vNW, e1.vN, e1.vNE, e1.vW, e1.vC, e1.vE, e1.vSW, e1.vS, e1.vSE};
+      const double r2u[9] = {e2.uNW, e2.uN, e2.uNE, e2.uW, e2.uC, e2.uE, e2.uSW, e2.uS, e2.uSE};
+      const double r2v[9] = {e2.vNW, e2.vN, e2.vNE, e2.vW, e2.vC, e2.vE, e2.vSW, e2.vS, e2.vSE};
+      auto v = [&](int b) { return make_double4(r1u[b], r1v[b], r2u[b], r2v[b]); };
+      if (fast) {
+        acc_fine_static<decltype(PI)::value, decltype(PJ)::value>(acc, ex, ey, v);
+      } else {
 #pragma unroll
         for (int b = 0; b < 9; ++b) {
           const int di = (b % 3) - 1, dj = 1 - (b / 3);
@@ -175,46 +214,56 @@ __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, co
           acc_block(acc, blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc)), r1u[b], r1v[b], r2u[b], r2v[b]);
         }
       }
+    };
+    fine(std::integral_constant<int, 0>{}, std::integral_constant<int, 0>{});
+    fine(std::integral_constant<int, 0>{}, std::integral_constant<int, 1>{});
+    fine(std::integral_constant<int, 1>{}, std::integral_constant<int, 0>{});
+    fine(std::integral_constant<int, 1>{}, std::integral_constant<int, 1>{});
     store_coarse(acc, Nc, I * Myc + J, Ac, dinvc);
   }
 }
 
 // Galerkin operator and D^-1 of coarse cell (I, J) of the level below F, summed in FP64 in
-// registers: the nine blocks of every fine cell of the aggregate are loaded first (one round
-// of loads per coarse cell), then added in the order fine cell, block
+// registers, fine cell by fine cell of the aggregate and block by block (no stores between
+// the loads, so the compiler may issue them all at once)
 __device__ __forceinline__ void galerkin_cell(const LevelView &F, int Mxc, int Myc, int I, int J, float4 *Ac,
                                               float4 *dinvc) {
   const int ax = F.ax, ay = F.ay;
-  float4 a[4][9];
-  bool ok[4];
-#pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    const int pi = p >> 1, pj = p & 1, i = I * ax + pi, j = J * ay + pj;
-    ok[p] = pi < ax && pj < ay && i < F.Mx && j < F.My;
-    const int k = ok[p] ? i * F.My + j : 0;
-#pragma unroll
-    for (int b = 0; b < 9; ++b) a[p][b] = F.A[b * F.N + k];
-  }
   double acc[36];
 #pragma unroll
   for (int q = 0; q < 36; ++q) acc[q] = 0.0;
+  const bool fast = static_blocks(ax, ay, Mxc, Myc);
+  const bool ex = (F.Mx & 1) && I == Mxc - 1, ey = (F.My & 1) && J == Myc - 1;
+  auto fine = [&](auto PI, auto PJ) {
+    constexpr int pi = decltype(PI)::value, pj = decltype(PJ)::value;
+    const int i = I * ax + pi, j = J * ay + pj;
+    if (pi >= ax || pj >= ay || i >= F.Mx || j >= F.My) return;
+    const int k = i * F.My + j;
+    auto v = [&](int b) {
+      const float4 a = F.A[b * F.N + k];
+      return make_double4(a.x, a.y, a.z, a.w);
+    };
+    if (fast) {
+      acc_fine_static<pi, pj>(acc, ex, ey, v);
+    } else {
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    if (!ok[p]) continue;
-    const int i = I * ax + (p >> 1), j = J * ay + (p & 1);
-#pragma unroll
-    for (int b = 0; b < 9; ++b) {
-      const int di = (b % 3) - 1, dj = 1 - (b / 3);
-      const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
-      acc_block(acc, blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc)), a[p][b].x, a[p][b].y, a[p][b].z,
-                a[p][b].w);
+      for (int b = 0; b < 9; ++b) {
+        const int di = (b % 3) - 1, dj = 1 - (b / 3);
+        const int ni = wrap(i + di, F.Mx), nj = wrap(j + dj, F.My);
+        const double4 x = v(b);
+        acc_block(acc, blk_of(wdiff(ni / ax, I, Mxc), wdiff(nj / ay, J, Myc)), x.x, x.y, x.z, x.w);
+      }
     }
-  }
+  };
+  fine(std::integral_constant<int, 0>{}, std::integral_constant<int, 0>{});
+  fine(std::integral_constant<int, 0>{}, std::integral_constant<int, 1>{});
+  fine(std::integral_constant<int, 1>{}, std::integral_constant<int, 0>{});
+  fine(std::integral_constant<int, 1>{}, std::integral_constant<int, 1>{});
   store_coarse(acc, Mxc * Myc, I * Myc + J, Ac, dinvc);
 }
 
 // level l+1 from the stored operator of level l
-__global__ void __launch_bounds__(NTm) k_mg_build(LevelView F, int Mxc, int Myc, TileM tm, float4 *Ac, float4 *dinvc) {
+__global__ void __launch_bounds__(NTm, 2) k_mg_build(LevelView F, int Mxc, int Myc, TileM tm, float4 *Ac, float4 *dinvc) {
   for (int t = blockIdx.x; t < tm.tiles; t += gridDim.x) {
     int I, J;
     if (!tile_cell(tm, Mxc, Myc, t, I, J)) continue;
@@ -281,11 +330,17 @@ __device__ void coarse_invert_warp(const LevelView &L, double (*a)[CI_PAD], int 
     // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
     if (t < n) a[col][t] = (t == col ? 1.0 : a[col][t]) * pinv;
     __syncwarp();
-    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
+    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot.  The pivot
+    // row is read into registers first, so a lane's updates of its own row do not wait on
+    // reads that might alias them
+    double prow[2 * MG_MAX_COARSE_CELLS];
+#pragma unroll
+    for (int q = 0; q < 2 * MG_MAX_COARSE_CELLS; ++q) prow[q] = a[col][q];
     if (t < n && t != col) {
       const double f = a[t][col];
-      for (int q = 0; q < n; ++q)
-        if (q != col) a[t][q] -= f * a[col][q];
+#pragma unroll
+      for (int q = 0; q < 2 * MG_MAX_COARSE_CELLS; ++q)
+        if (q < n && q != col) a[t][q] -= f * prow[q];
       a[t][col] = -a[t][col] * a[col][col];
     }
     __syncwarp();
