@@ -59,9 +59,9 @@ FAST_MG_LAG = 0.0
 # tolerance 1e-6 took 224 ms with 3 and 236 ms with 2); the other one is timed beside it
 DEFAULT_GRAPHS = 3
 # In-solve DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control
-# none) of one inner iteration's kernels on the 801^2 sheet, per (grid, precision)
-# (profiles/inner_iteration_traffic_801.md: the per-launch averages of the 23 kernels)
-INNER_ITERATION_TRAFFIC = {(801, "mixed"): 96.7e6}
+# none) of one inner iteration's kernels on the 801^2 sheet, per (grid, precision, FP32 apply
+# kernel) (profiles/inner_iteration_traffic_801.md: the per-launch averages of the kernels)
+INNER_ITERATION_TRAFFIC = {}
 
 
 def _package():
@@ -178,22 +178,31 @@ def mg_levels(M):
     return out
 
 
-def iteration_bytes(M, precision):
+def iteration_bytes(M, precision, apply_kernel=2):
     """Algorithmic HBM bytes of one inner BiCGStab iteration with two V(1,1) cycles: every
-    array a kernel reads or writes, once per kernel (halo neighbours counted once).
-    FP32 Krylov (mixed): v, t 40 B/cell (x 8, nu*H 8, beta 4, flags 4, dot operand 8, out 8),
-    x 64, p 32, s 24.  FP64 Krylov: v, t 76, x 128, p 64, s 48.  Per V-cycle, fine level:
-    restrict b + D^-1 + nu*H + beta + flags (40 / 48 B), post the same + z (50 / 64 B), plus
-    the first coarse vector written and read (16 B per coarse cell); coarse levels: the
-    nine 2 x 2 blocks, D^-1 and b read by both passes and x written (344 B per cell)."""
+    array a kernel reads or writes, once per kernel (halo neighbours counted once), per fine
+    cell.  FP32 Krylov (mixed), s = r - alpha v formed where it is read:
+      p update: r, v, p read, p written                                      32
+      x update: phat, shat, v, t, rhat read; d, r read and written           72
+      V-cycle on p, fine restrict: p, D^-1, nu*H, beta, flags                40
+      V-cycle on s, fine restrict: r, v, D^-1, nu*H, beta, flags             48
+      apply_kernel 2 (fine post-smoothing fused with the apply):
+        on p: p, D^-1, nu*H, beta, flags read, phat written; rhat read, v written   64
+        on s: r, v, D^-1, nu*H, beta, flags read, shat written; t written           64
+      apply_kernel 0 / 1 (separate kernels):
+        posts 48 (on p) and 56 (on s); applies: phat, nu*H, beta, flags, rhat read,
+        v written 40; shat, nu*H, beta, flags, r, v read, t written 48
+    FP64 Krylov: 392 B per cell in the Krylov kernels and 112 per V-cycle on the fine level.
+    Every V-cycle adds the first coarse vector written and read (16 B per level-1 cell) and,
+    per coarse cell, the nine 2 x 2 blocks, D^-1 and b read by both passes and x written
+    (344 B)."""
     N0 = M * M
     lev = mg_levels(M)
-    if precision == "mixed":
-        krylov, fine = 200, 90
-    else:
-        krylov, fine = 392, 112
-    vcycle = fine * N0 + 16 * lev[0] + 344 * sum(lev)
-    return krylov * N0 + 2 * vcycle
+    coarse = 2 * (16 * lev[0] + 344 * sum(lev))
+    if precision != "mixed":
+        return 392 * N0 + 2 * 112 * N0 + coarse
+    fine = 32 + 72 + 40 + 48 + (64 + 64 if apply_kernel == 2 else 48 + 56 + 40 + 48)
+    return fine * N0 + coarse
 
 
 def iteration_roofline(s, c, M, stream, flush, dev):
@@ -213,7 +222,7 @@ def iteration_roofline(s, c, M, stream, flush, dev):
     torch.cuda.synchronize()
     lin_ms = ev[0].elapsed_time(ev[1])
     it_ms = lin_ms / max(1, lin_its)
-    it_bytes = iteration_bytes(M, c.precision)
+    it_bytes = iteration_bytes(M, c.precision, c.mixed_apply_kernel)
     return {"achieved": it_bytes / (it_ms * 1e-3) / 1e9, "unit": "GB/s", "bytes_per_launch": it_bytes,
             "launch_ms": it_ms, "timed": f"linear solve to rtol 1e-10: {lin_its} iterations in {lin_ms:.2f} ms"}
 
@@ -778,10 +787,9 @@ def main():
     roof = iteration_roofline(s, c, M, stream, flush, dev)
     s.set_config(c)
     roof.update(peak=peak, frac=roof["achieved"] / peak, peak_kind=peak_kind, bound="hbm",
-                traffic=INNER_ITERATION_TRAFFIC.get((M, c.precision)))
-    roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the iteration's 23 kernels, "
-                              "in-solve (--cache-control none), profiles/inner_iteration_traffic_801.md: the working "
-                              "set stays in L2, so DRAM traffic is a quarter of the algorithmic bytes"
+                traffic=INNER_ITERATION_TRAFFIC.get((M, c.precision, c.mixed_apply_kernel)))
+    roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the iteration's kernels, "
+                              "in-solve (--cache-control none), profiles/inner_iteration_traffic_801.md"
                               if roof["traffic"] is not None else None)
     roof["kernel"] = ("one inner BiCGStab + V(1,1) multigrid iteration: k32_p/v/s/t/x + 2 x (k_mg0_restrict, "
                       "k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, k_mg0_post)"

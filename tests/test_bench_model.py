@@ -21,12 +21,17 @@ def test_levels_of_the_801_grid():
 
 
 def test_iteration_bytes():
+    """per fine cell: p 32 + x 72 + restricts 40 + 48, then the fused post + apply 64 + 64
+    (apply_kernel 2) or posts 48 + 56 and applies 40 + 48 (0, 1); per V-cycle 16 B per
+    level-1 cell and 344 B per coarse cell"""
     b = _bench()
     N0, lev = 801 ** 2, b.mg_levels(801)
-    mixed = 200 * N0 + 2 * (90 * N0 + 16 * lev[0] + 344 * sum(lev))
-    assert b.iteration_bytes(801, "mixed") == mixed
-    assert b.iteration_bytes(801, "fp64") > mixed
-    assert 390e6 < mixed < 400e6
+    coarse = 2 * (16 * lev[0] + 344 * sum(lev))
+    fused = 320 * N0 + coarse
+    assert b.iteration_bytes(801, "mixed") == fused
+    assert b.iteration_bytes(801, "mixed", 0) == b.iteration_bytes(801, "mixed", 1) == 384 * N0 + coarse
+    assert b.iteration_bytes(801, "fp64") > b.iteration_bytes(801, "mixed", 0)
+    assert 350e6 < fused < 365e6
 
 
 def test_fast_config_keeps_the_accepted_tolerance():
