@@ -7,12 +7,13 @@
 //   sigma   StressBalance::compute_volumetric_strain_heating (PISMStressBalance.cc:369-499)
 //   w3      StressBalance::compute_vertical_velocity (PISMStressBalance.cc:192-287)
 //
-// The 3-D fields are [i][j][k] (a column's Mz levels contiguous).  One thread per (column,
-// level), consecutive threads on consecutive levels, so every load of an enthalpy column and
-// every store of the four outputs is coalesced.  The horizontal velocity is constant in each
-// column, so u_z = v_z = 0 exactly and the horizontal derivatives are the column's; each
-// thread recomputes them (the neighbours' velocities and masks come from L1) and the
-// trapezoid sum of w up to its level, in the reference's order of operations.
+// The 3-D fields are [i][j][k] (a column's Mz levels contiguous).  One thread per column:
+// the horizontal velocity is constant in each column, so u_z = v_z = 0 exactly and the
+// horizontal derivatives, D^2 and its power are the column's, computed once; the thread then
+// walks up its column, summing w by the trapezoid rule in the reference's order of operations
+// and scaling the strain heating by each level's hardness.  A warp's stores at one level hit
+// 32 sectors, each filled by four consecutive levels of one thread, so L2 merges them before
+// they reach HBM.
 #include <algorithm>
 #include <cmath>
 
@@ -61,7 +62,7 @@ __device__ __forceinline__ int k_below_height(const double *__restrict__ z, int 
 }
 
 __global__ void __launch_bounds__(NTC) k_stress_balance_3d(GridDev g, pism_gpu_ssa_config c, int Mz,
-                                                           double e_to_a_power, double exponent,
+                                                           double e_to_a_power, double exponent, double B_iso,
                                                            const double2 *__restrict__ vel,
                                                            const int8_t *__restrict__ mask,
                                                            const double *__restrict__ H,
@@ -70,14 +71,16 @@ __global__ void __launch_bounds__(NTC) k_stress_balance_3d(GridDev g, pism_gpu_s
                                                            const double *__restrict__ bmr, double *__restrict__ u3,
                                                            double *__restrict__ v3, double *__restrict__ w3,
                                                            double *__restrict__ sigma) {
-  const long long total = (long long)g.Mx * g.My * Mz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int col = (int)(q / Mz), k = (int)(q - (long long)col * Mz);
+  const int N = g.Mx * g.My;
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < N; col += gridDim.x * blockDim.x) {
     const int i = col / g.My, j = col - i * g.My;
     const double2 U = vel[col];
-    if (u3) u3[q] = U.x;
-    if (v3) v3[q] = U.y;
+    double *const uc = u3 ? u3 + (size_t)col * Mz : nullptr;
+    double *const vc = v3 ? v3 + (size_t)col * Mz : nullptr;
+    for (int k = 0; k < Mz; ++k) {
+      if (uc) uc[k] = U.x;
+      if (vc) vc[k] = U.y;
+    }
     if (!w3 && !sigma) continue;
     const ColumnDiff d = column_diff(g, mask, i, j);
     const double2 Uw = vel[nbr(g, i, j, -1, 0)], Ue = vel[nbr(g, i, j, 1, 0)], Us = vel[nbr(g, i, j, 0, -1)],
@@ -87,26 +90,35 @@ __global__ void __launch_bounds__(NTC) k_stress_balance_3d(GridDev g, pism_gpu_s
     if (w3) {
       // w(0) = -bmr (or 0); w(k) = w(k-1) - (integrand(k) + integrand(k-1)) / 2 dz, the
       // integrand u_x + v_y the same at every level; the products and sums in that order
+      double *const wc = w3 + (size_t)col * Mz;
       const double integrand = __dadd_rn(u_x, v_y);
+      const double half_sum = __dmul_rn(0.5, __dadd_rn(integrand, integrand));
       double w = bmr ? -bmr[col] : 0.0;
-      for (int kk = 1; kk <= k; ++kk)
-        w = __dsub_rn(w, __dmul_rn(__dmul_rn(0.5, __dadd_rn(integrand, integrand)), __dsub_rn(z[kk], z[kk - 1])));
-      w3[q] = w;
+      wc[0] = w;
+      for (int k = 1; k < Mz; ++k) {
+        w = __dsub_rn(w, __dmul_rn(half_sum, __dsub_rn(z[k], z[k - 1])));
+        wc[k] = w;
+      }
     }
     if (sigma) {
+      double *const sc = sigma + (size_t)col * Mz;
       const double Hc = H[col];
       const int ks = k_below_height(z, Mz, Hc);
-      double s = 0.0;
-      if (k <= ks) {
-        const double u_y = d.D_y * (d.south * (U.x - Us.x) + d.north * (Un.x - U.x));
-        const double v_x = d.D_x * (d.west * (U.y - Uw.y) + d.east * (Ue.y - U.y));
-        const double B = hardness_parameter(c, E ? E[q] : 0.0, ec_pressure(c, Hc - z[k]));
-        const double a = u_x + v_y, b = u_y + v_x;   // u_z = v_z = 0
-        // D2(), PISMStressBalance.cc:309-311
-        const double D2 = 0.5 * (a * a + u_x * u_x + v_y * v_y + 0.5 * (b * b));
-        s = 2.0 * e_to_a_power * B * pow(D2, exponent);
+      const double u_y = d.D_y * (d.south * (U.x - Us.x) + d.north * (Un.x - U.x));
+      const double v_x = d.D_x * (d.west * (U.y - Uw.y) + d.east * (Ue.y - U.y));
+      const double a = u_x + v_y, b = u_y + v_x;   // u_z = v_z = 0
+      // D2(), PISMStressBalance.cc:309-311
+      const double D2 = 0.5 * (a * a + u_x * u_x + v_y * v_y + 0.5 * (b * b));
+      const double two_e = 2.0 * e_to_a_power, D2e = pow(D2, exponent);
+      const double *const Ec = E ? E + (size_t)col * Mz : nullptr;
+      for (int k = 0; k < Mz; ++k) {
+        double s = 0.0;
+        if (k <= ks) {
+          const double B = Ec ? hardness_parameter(c, Ec[k], ec_pressure(c, Hc - z[k])) : B_iso;
+          s = two_e * B * D2e;   // the reference's order: (2 e^(-1/n) B) D^(1/n + 1)
+        }
+        sc[k] = s;
       }
-      sigma[q] = s;
     }
   }
 }
@@ -116,14 +128,17 @@ __global__ void __launch_bounds__(NTC) k_stress_balance_3d(GridDev g, pism_gpu_s
 void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int Mz,
                               const Fields &f, const double *z, const double *bmr, double *u3, double *v3,
                               double *w3, double *sigma) {
-  const long long total = (long long)g.Mx * g.My * Mz;
-  const int blocks = (int)std::min<long long>((total + NTC - 1) / NTC, 2LL * L.max_blocks);
-  // PISMStressBalance.cc:384-387: the flow law's exponent and enhancement factor
+  const int N = g.Mx * g.My;
+  const int blocks = std::min((N + NTC - 1) / NTC, 4 * L.max_blocks);
+  // PISMStressBalance.cc:384-387: the flow law's exponent and enhancement factor; an
+  // isothermal flow law's hardness A^(-1/n) is the same at every level
   const double n = c.ssa_Glen_exponent, exponent = 0.5 * (1.0 / n + 1.0);
   const double e_to_a_power = std::pow(c.ssa_enhancement_factor, -1.0 / n);
+  const bool iso = c.flow_law == PISM_FLOW_LAW_ISOTHERMAL_GLEN;
+  const double B_iso = iso ? std::pow(c.ice_softness, -1.0 / n) : 0.0;
   L.tick();
-  k_stress_balance_3d<<<blocks, NTC, 0, L.stream>>>(g, c, Mz, e_to_a_power, exponent, f.vel, f.mask, f.H, f.enthalpy,
-                                                    z, bmr, u3, v3, w3, sigma);
+  k_stress_balance_3d<<<blocks, NTC, 0, L.stream>>>(g, c, Mz, e_to_a_power, exponent, B_iso, f.vel, f.mask, f.H,
+                                                    iso ? nullptr : f.enthalpy, z, bmr, u3, v3, w3, sigma);
 }
 
 }  // namespace pism_gpu
