@@ -290,6 +290,28 @@ int pism_gpu_ssa_get_field(pism_gpu_ssa *h, int field, double *out, int where);
 int pism_gpu_ssa_stress_balance_3d(pism_gpu_ssa *h, const double *basal_melt_rate, double *u3, double *v3,
                                    double *w3, double *strain_heating, int where);
 
+/* Mass transport consuming the SSA velocity: IceModel::massContExplicitStep
+ * (iMgeometry.cc:497-819) over dt seconds on the handle's velocity, mask, thickness and (with
+ * ssa_dirichlet_bc) Dirichlet data, with the ConstantInColumn modifier (no diffusive flux) and
+ * part_grid off: the upwinded SSA flux divergence (face velocities of cell_interface_fluxes,
+ * iMgeometry.cc:309-410), the climatic mass balance (kg m-2 s-1) and, when
+ * basal_melt_rate != NULL (include_bmr_in_continuity), the basal melt rate (m s-1) as sources
+ * (neither on ice-free ocean nor at Dirichlet locations), the non-negativity rule; then
+ * updateSurfaceElevationAndMask (iMgeometry.cc:56-68) on the new thickness with the
+ * GeometryCalculator thresholds mask_icefree_thickness_standard and
+ * mask_is_floating_thickness_standard (dry simulation off).  cell_area may be NULL (dx dy).
+ * Outputs (Mx*My each; only thickness_out is required): the new thickness, mask (as
+ * doubles) and surface, and the flux divergence (m s-1); totals (host, 8 doubles, may be
+ * NULL) gets the step's grounded basal, non-negativity, sub-shelf, surface, SIA and SSA
+ * divergence, Href-to-H and H-to-Href fluxes in kg (iMgeometry.cc:778-787 order).  The
+ * handle's own fields are not changed: pass the new ones to pism_gpu_ssa_set_inputs for
+ * the next solve.  Arrays are host or device per `where`.  Blocks until done. */
+int pism_gpu_ssa_mass_continuity_step(pism_gpu_ssa *h, double dt, const double *climatic_mass_balance,
+                                      const double *basal_melt_rate, const double *cell_area,
+                                      double icefree_thickness, double is_floating_thickness, double *thickness_out,
+                                      double *mask_out, double *surface_out, double *flux_divergence,
+                                      double *totals, int where);
+
 /* Stage entry points, each the device restatement of one reference method, for
  * stage-by-stage checking:
  *   assemble_rhs       -> SSA::compute_driving_stress + SSAFD::assemble_rhs

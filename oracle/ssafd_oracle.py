@@ -1106,6 +1106,86 @@ def volumetric_strain_heating(grid: Grid, cfg: Config, inp: Inputs, u3, v3):
     return sigma
 
 
+# ---------------------------------------------------------------------------
+# mass transport consuming the SSA velocity: IceModel::massContExplicitStep
+# ---------------------------------------------------------------------------
+MASS_TOTALS = ("grounded_basal_ice_flux", "nonneg_rule_flux", "sub_shelf_ice_flux", "surface_ice_flux",
+               "sum_divQ_SIA", "sum_divQ_SSA", "Href_to_H_flux", "H_to_Href_flux")
+
+
+def cell_interface_velocities(cfg: Config, inp: Inputs, vel):
+    """IceModel::cell_interface_fluxes, iMgeometry.cc:309-410 (the SSA part): the normal
+    velocity at the four faces of each cell, (e, w, n, s), by the icy / ice-free cases of the
+    two cells and, with ssa_dirichlet_bc, the boundary-condition cases."""
+    M = as_int(inp.mask)
+    icy = m_icy(M)
+    u, v = vel[..., 0], vel[..., 1]
+    out = {}
+    for name, di, dj, comp in (("e", 1, 0, u), ("w", -1, 0, u), ("n", 0, 1, v), ("s", 0, -1, v)):
+        icy_n = nb(icy, di, dj)
+        comp_n = nb(comp, di, dj)
+        f = np.where(icy & icy_n, 0.5 * (comp + comp_n),
+                     np.where(icy & ~icy_n, comp, np.where(~icy & icy_n, comp_n, 0.0)))
+        if cfg.ssa_dirichlet_bc and inp.bc_mask is not None:
+            bm = as_int(inp.bc_mask)
+            bm_n = nb(bm, di, dj)
+            bv = inp.bc_values[..., 0 if comp is u else 1]
+            bv_n = nb(bv, di, dj)
+            f = np.where((bm == 1) & (bm_n == 1), 0.5 * (bv + bv_n),
+                         np.where((bm == 1) & (bm_n == 0), bv, np.where((bm == 0) & (bm_n == 1), bv_n, f)))
+        out[name] = f
+    return out
+
+
+def mass_continuity_step(grid: Grid, cfg: Config, inp: Inputs, vel, dt, climatic_mass_balance,
+                         basal_melt_rate=None, cell_area=None):
+    """IceModel::massContExplicitStep, iMgeometry.cc:497-819, with the ConstantInColumn
+    modifier (no diffusive flux: divQ_SIA = 0), part_grid off and no residual redistribution:
+    upwinded SSA flux divergence, surface and basal mass balance (zero on ice-free ocean and at
+    Dirichlet locations), the non-negativity rule, and the eight flux totals in kg.  Returns
+    (new thickness, flux divergence, totals)."""
+    M = as_int(inp.mask)
+    H = np.asarray(inp.thickness, dtype=np.float64)
+    dx, dy = grid.dx, grid.dy
+    rho = cfg.ice_density
+    area = np.full(H.shape, dx * dy) if cell_area is None else np.asarray(cell_area, dtype=np.float64)
+    meter_to_kg = area * rho
+    meter_per_s_to_kg = meter_to_kg * dt
+    f = cell_interface_velocities(cfg, inp, vel)
+    divQ_SIA = np.zeros(H.shape)   # (Q.e - Q.w) / dx + (Q.n - Q.s) / dy with Q = 0
+    divQ_SSA = 0.0 + (f["e"] * np.where(f["e"] > 0, H, nb(H, 1, 0))
+                      - f["w"] * np.where(f["w"] > 0, nb(H, -1, 0), H)) / dx
+    divQ_SSA = divQ_SSA + (f["n"] * np.where(f["n"] > 0, H, nb(H, 0, 1))
+                           - f["s"] * np.where(f["s"] > 0, nb(H, 0, -1), H)) / dy
+    smb = np.asarray(climatic_mass_balance, dtype=np.float64) / rho
+    bmr = np.zeros(H.shape) if basal_melt_rate is None else np.asarray(basal_melt_rate, dtype=np.float64)
+    free_ocean = m_ice_free_ocean(M)
+    smb = np.where(free_ocean, 0.0, smb)
+    bmr = np.where(free_ocean, 0.0, bmr)
+    href_to_h = np.zeros(H.shape)
+    if cfg.ssa_dirichlet_bc and inp.bc_mask is not None:
+        bc = as_int(inp.bc_mask) == 1
+        smb, bmr = np.where(bc, 0.0, smb), np.where(bc, 0.0, bmr)
+        href_to_h = np.where(bc, 0.0, href_to_h)
+        divQ_SIA, divQ_SSA = np.where(bc, 0.0, divQ_SIA), np.where(bc, 0.0, divQ_SSA)
+    flux_divergence = divQ_SIA + divQ_SSA
+    Hnew = H + (dt * (smb - bmr - (divQ_SIA + divQ_SSA)) + href_to_h)
+    nonneg = np.where(Hnew < 0.0, -Hnew, 0.0)
+    Hnew = np.where(Hnew < 0.0, 0.0, Hnew)
+    grounded = m_grounded(M)
+    totals = {
+        "grounded_basal_ice_flux": float(np.sum(np.where(grounded, -bmr * meter_per_s_to_kg, 0.0))),
+        "nonneg_rule_flux": float(np.sum(nonneg * meter_to_kg)),
+        "sub_shelf_ice_flux": float(np.sum(np.where(grounded, 0.0, -bmr * meter_per_s_to_kg))),
+        "surface_ice_flux": float(np.sum(smb * meter_per_s_to_kg)),
+        "sum_divQ_SIA": float(np.sum(-divQ_SIA * meter_per_s_to_kg)),
+        "sum_divQ_SSA": float(np.sum(-divQ_SSA * meter_per_s_to_kg)),
+        "Href_to_H_flux": float(np.sum(href_to_h * meter_to_kg)),
+        "H_to_Href_flux": 0.0,
+    }
+    return Hnew, flux_divergence, totals
+
+
 def residual_rel(grid, cfg, inp, vel, reg, hardness, b):
     """||b - A(u) u||_2 / ||b||_2 with A built at the velocity itself (a nonlinear residual)."""
     nuH = compute_nuH(grid, cfg, inp, hardness, vel, reg)

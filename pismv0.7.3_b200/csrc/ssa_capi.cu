@@ -37,6 +37,7 @@ struct pism_gpu_ssa {
   double2 *taud = nullptr, *rhs = nullptr, *hardness = nullptr, *nuH = nullptr, *vel = nullptr, *vel_old = nullptr;
   double *beta = nullptr, *bfrict = nullptr;
   double *sb3d = nullptr;   // host-destination staging of pism_gpu_ssa_stress_balance_3d
+  double *mc = nullptr;     // staging of pism_gpu_ssa_mass_continuity_step: 7 fields and 8 totals
   uint32_t *flags = nullptr;
   Krylov K{};
   Krylov32 K32{};
@@ -1084,7 +1085,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
                  h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G, h->lpc.img, h->lpc.out,
-                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma, h->sb3d};
+                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma, h->sb3d, h->mc};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -1277,6 +1278,41 @@ int pism_gpu_ssa_stress_balance_3d(pism_gpu_ssa *h, const double *basal_melt_rat
   if (where == PISM_MEM_HOST)
     for (int q = 0; q < 4; ++q)
       if (out[q]) RET(copy_out(h, out[q], dev[q], sizeof(double) * N3, PISM_MEM_HOST));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_mass_continuity_step(pism_gpu_ssa *h, double dt, const double *climatic_mass_balance,
+                                      const double *basal_melt_rate, const double *cell_area,
+                                      double icefree_thickness, double is_floating_thickness, double *thickness_out,
+                                      double *mask_out, double *surface_out, double *flux_divergence,
+                                      double *totals, int where) {
+  if (!h || !climatic_mass_balance || !thickness_out) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (where != PISM_MEM_HOST && where != PISM_MEM_DEVICE) return fail(h, PISM_GPU_SSA_EINVAL, "bad memory kind");
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  if (!(dt >= 0.0)) return fail(h, PISM_GPU_SSA_EINVAL, "dt must be >= 0");
+  const size_t N = h->N;
+  if (!h->mc) RET(dalloc(h, &h->mc, 7 * N + 8));
+  const double *in[3] = {climatic_mass_balance, basal_melt_rate, cell_area};
+  double *out[4] = {thickness_out, mask_out, surface_out, flux_divergence};
+  const double *din[3];
+  double *dout[4];
+  for (int q = 0; q < 3; ++q) {
+    din[q] = in[q];
+    if (in[q] && where == PISM_MEM_HOST) {
+      RET(copy_in(h, h->mc + q * N, in[q], sizeof(double) * N, PISM_MEM_HOST));
+      din[q] = h->mc + q * N;
+    }
+  }
+  for (int q = 0; q < 4; ++q) dout[q] = (out[q] && where == PISM_MEM_HOST) ? h->mc + (3 + q) * N : out[q];
+  double *dtot = h->mc + 7 * N;
+  launch_mass_continuity(h->L, h->g, h->cfg, fields_of(h), dt, icefree_thickness, is_floating_thickness, din[0],
+                         din[1], din[2], dout[0], dout[3], dout[1], dout[2], dtot);
+  CK(h, cudaGetLastError());
+  for (int q = 0; q < 4; ++q)
+    if (out[q] && where == PISM_MEM_HOST) RET(copy_out(h, out[q], dout[q], sizeof(double) * N, PISM_MEM_HOST));
+  if (totals) RET(copy_out(h, totals, dtot, sizeof(double) * 8, PISM_MEM_HOST));
   CK(h, cudaStreamSynchronize(h->stream));
   return PISM_GPU_SSA_OK;
 }

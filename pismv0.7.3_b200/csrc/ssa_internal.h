@@ -161,7 +161,11 @@ void mg_vcycle_apply(const Launch &L, const GridDev &g, const Fields &f, const M
                      float2 *z, const EpiV &e);
 void mg_vcycle_s_apply(const Launch &L, const GridDev &g, const Fields &f, const MGHierarchy &H, const float2 *r,
                        const float2 *v, float2 *z, const EpiT &e);
-// ---- the consumers of the SSA velocity (ssa_column.cu) ----
+// ---- the consumers of the SSA velocity (ssa_column.cu, ssa_transport.cu) ----
+void launch_mass_continuity(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, const Fields &f,
+                            double dt, double icefree_thickness, double is_floating_thickness, const double *cmb,
+                            const double *bmr, const double *area, double *Hnew, double *fdiv, double *mask_new,
+                            double *surface_new, double *totals);
 void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int Mz,
                               const Fields &f, const double *z, const double *bmr, double *u3, double *v3,
                               double *w3, double *sigma);

@@ -296,6 +296,39 @@ class SSAFD:
             "stress_balance_3d")
         return {k: (bufs[k].keep if on_device else out[k]) for k in names}
 
+    MASS_TOTALS = ("grounded_basal_ice_flux", "nonneg_rule_flux", "sub_shelf_ice_flux", "surface_ice_flux",
+                   "sum_divQ_SIA", "sum_divQ_SSA", "Href_to_H_flux", "H_to_Href_flux")
+
+    def mass_continuity_step(self, dt: float, climatic_mass_balance, basal_melt_rate=None, cell_area=None,
+                             device: bool = False) -> dict:
+        """IceModel::massContExplicitStep (iMgeometry.cc:497-819) over dt seconds from the
+        current velocity (ConstantInColumn: no diffusive flux; part_grid off), then
+        updateSurfaceElevationAndMask: returns the new "thickness", "mask", "surface", the
+        "flux_divergence" and the step's flux "totals" (kg).  Inputs host arrays or CUDA
+        tensors (all of one kind); outputs of the same kind."""
+        on_device = device or _is_device(climatic_mass_balance)
+        shape = self.shape
+        if on_device:
+            import torch
+            out = {k: torch.empty(shape, dtype=torch.float64, device=f"cuda:{self.device}")
+                   for k in ("thickness", "mask", "surface", "flux_divergence")}
+        else:
+            out = {k: np.empty(shape) for k in ("thickness", "mask", "surface", "flux_divergence")}
+        ins = [_Buf(a, shape) if a is not None else None for a in (climatic_mass_balance, basal_melt_rate, cell_area)]
+        if any(b is not None and b.device != on_device for b in ins):
+            raise ValueError("the inputs must all be host arrays or all CUDA tensors")
+        outs = {k: _Buf(v, shape) for k, v in out.items()}
+        totals = (C.c_double * 8)()
+        where = _capi.MEM_DEVICE if on_device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_mass_continuity_step(
+            self._h, float(dt), *(b.ptr if b is not None else None for b in ins),
+            float(self.config.mask_icefree_thickness_standard), float(self.config.mask_is_floating_thickness_standard),
+            outs["thickness"].ptr, outs["mask"].ptr, outs["surface"].ptr, outs["flux_divergence"].ptr,
+            C.cast(totals, _D), where), "massContExplicitStep")
+        res = {k: (outs[k].keep if on_device else out[k]) for k in out}
+        res["totals"] = dict(zip(self.MASS_TOTALS, list(totals)))
+        return res
+
     # ---- stage methods (one reference method each) ----
     def assemble_rhs(self):
         self._check(self.lib.pism_gpu_ssa_assemble_rhs(self._h), "assemble_rhs")
