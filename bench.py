@@ -61,7 +61,7 @@ DEFAULT_GRAPHS = 3
 # In-solve DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control
 # none) of one inner iteration's kernels on the 801^2 sheet, per (grid, precision, FP32 apply
 # kernel) (profiles/inner_iteration_traffic_801.md: the per-launch averages of the kernels)
-INNER_ITERATION_TRAFFIC = {}
+INNER_ITERATION_TRAFFIC = {(801, "mixed", 2): 96.5e6}
 
 
 def _package():
@@ -295,8 +295,48 @@ def column_roofline(vel, stream, flush, dev, peak, M=801, Mz=41, reps=20):
     achieved = nbytes / (ms * 1e-3) / 1e9
     return {"grid": [M, M, Mz], "ms": ms, "bytes_per_call": nbytes, "achieved": achieved, "unit": "GB/s",
             "peak": peak, "frac": achieved / peak, "bound": "hbm",
-            "kernel": "k_stress_balance_3d (one thread per column level; the call's time includes its "
-                      "argument checks and one stream synchronisation)"}
+            "kernel": "k_stress_balance_3d (one thread per column, results staged per warp in shared memory and "
+                      "written coalesced; the call's time includes its argument checks and one stream "
+                      "synchronisation)"}
+
+
+def mass_roofline(vel, stream, flush, dev, peak, M=801, reps=20):
+    """The explicit mass-continuity step (pism_gpu_ssa_mass_continuity_step) on the benchmark
+    sheet from the solved velocity, one model year, device buffers.  Algorithmic bytes per
+    call and cell: velocity 16, mask 1, thickness 8, bed 8, climatic mass balance 8, basal
+    melt rate 8, cell area 8 read; thickness, mask, surface and flux divergence 8 each
+    written (97 B)."""
+    import torch
+    from pism_b200.ssa import SSAFD
+    g, cl, f, _ = build_case(M)
+    s = SSAFD(g, cl, device=dev.index)
+    try:
+        s.set_stream(stream.cuda_stream)
+        s.set_inputs(**{k: torch.tensor(f[k], dtype=torch.float64, device=dev)
+                        for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
+        s.set_initial_guess(vel)
+        cmb = torch.full((M, M), 1e-5, dtype=torch.float64, device=dev)
+        bmr = torch.full((M, M), 1e-9, dtype=torch.float64, device=dev)
+        area = torch.full((M, M), g.dx * g.dy, dtype=torch.float64, device=dev)
+        s.mass_continuity_step(3.15e7, cmb, bmr, area)
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.mass_continuity_step(3.15e7, cmb, bmr, area)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+    finally:
+        s.close()
+    ms = float(np.median(ts))
+    nbytes = 97 * M * M
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"grid": [M, M], "ms": ms, "bytes_per_call": nbytes, "achieved": achieved, "unit": "GB/s", "peak": peak,
+            "frac": achieved / peak, "bound": "hbm",
+            "kernel": "k_mass_continuity (one thread per cell, the eight flux totals reduced in the same launch; "
+                      "the call's time includes the read-back of the totals and one stream synchronisation)"}
 
 
 # The host-core cost of the whole reference solve is sampled: the first CPU_SAMPLE_PICARD
@@ -880,6 +920,10 @@ def main():
             line["stress_balance_3d"] = column_roofline(vel_mode, stream, flush, dev, peak)
         except Exception as e:   # noqa: BLE001 - reported in the line
             line["stress_balance_3d"] = {"error": str(e)[:200]}
+        try:
+            line["mass_continuity"] = mass_roofline(vel_mode, stream, flush, dev, peak)
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["mass_continuity"] = {"error": str(e)[:200]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
         plain_picard = st_other["picard_iterations"] if args.mode == "fast" else picard[-1]

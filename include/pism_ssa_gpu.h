@@ -284,7 +284,7 @@ int pism_gpu_ssa_get_field(pism_gpu_ssa *h, int field, double *out, int where);
  *                   w(0) = -basal_melt_rate (Mx*My, m/s) or 0 when basal_melt_rate is NULL
  *                   (include_bmr_in_continuity false)
  * Each output is Mx*My*Mz doubles, [i][j][k] (IceModelVec3's column order); any may be NULL.
- * All pointers are host or device per `where`.  Needs a grid with Mz >= 2 levels and, for
+ * All pointers are host or device per `where`.  Needs a grid with 2 <= Mz <= 800 levels and, for
  * the strain heating under an enthalpy-dependent flow law, the inputs' enthalpy.  Blocks
  * until done. */
 int pism_gpu_ssa_stress_balance_3d(pism_gpu_ssa *h, const double *basal_melt_rate, double *u3, double *v3,

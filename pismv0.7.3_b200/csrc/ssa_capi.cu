@@ -1258,7 +1258,9 @@ int pism_gpu_ssa_stress_balance_3d(pism_gpu_ssa *h, const double *basal_melt_rat
   if (where != PISM_MEM_HOST && where != PISM_MEM_DEVICE) return fail(h, PISM_GPU_SSA_EINVAL, "bad memory kind");
   if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
   const int Mz = (int)h->z_host.size();
-  if (Mz < 2) return fail(h, PISM_GPU_SSA_EINVAL, "the 3-D fields need a grid with Mz >= 2 levels");
+  if (Mz < 2 || Mz > SB3D_MAX_LEVELS)
+    return fail(h, PISM_GPU_SSA_EINVAL, "the 3-D fields need a grid with 2 <= Mz <= %d levels", SB3D_MAX_LEVELS);
+  if (stress_balance_3d_prepare(Mz) != 0) return fail(h, PISM_GPU_SSA_ECUDA, "shared memory for the 3-D fields");
   if (strain_heating && h->cfg.flow_law != PISM_FLOW_LAW_ISOTHERMAL_GLEN && !h->have_enthalpy)
     return fail(h, PISM_GPU_SSA_EINVAL, "the strain heating's flow law needs enthalpy");
   const size_t N3 = (size_t)h->N * Mz;

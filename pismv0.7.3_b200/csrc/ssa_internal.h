@@ -166,6 +166,8 @@ void launch_mass_continuity(const Launch &L, const GridDev &g, const pism_gpu_ss
                             double dt, double icefree_thickness, double is_floating_thickness, const double *cmb,
                             const double *bmr, const double *area, double *Hnew, double *fdiv, double *mask_new,
                             double *surface_new, double *totals);
+constexpr int SB3D_MAX_LEVELS = 800;   // the column kernel's shared-memory tile holds 32 columns
+int stress_balance_3d_prepare(int Mz);
 void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int Mz,
                               const Fields &f, const double *z, const double *bmr, double *u3, double *v3,
                               double *w3, double *sigma);

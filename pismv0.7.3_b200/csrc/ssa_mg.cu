@@ -272,27 +272,20 @@ __global__ void __launch_bounds__(NTm, 2) k_mg_build(LevelView F, int Mxc, int M
 }
 
 // Dense inverse of the coarsest operator (n = 2 N <= 32 unknowns) by Gauss-Jordan elimination
-// with partial pivoting, by one warp, written transposed so that the per-cycle product reads
-// it coalesced.  Lane r keeps row r in registers for the whole elimination (the column loop is
-// unrolled, so every index into the row is static) and a position: row interchanges swap
-// positions instead of moving rows.  The pivot of column col is the largest |a| among the
-// rows at positions >= col, the lowest position on ties, and every element sees the same
-// operations in the same order as the in-place algorithm that moves rows; the rows are laid
-// out by position in shared memory at the end, where the interchanges are undone as column
-// interchanges.
-constexpr int CI_N = 2 * MG_MAX_COARSE_CELLS;
-constexpr int CI_PAD = CI_N + 1;
-static_assert(CI_N <= 32, "one lane per row of the coarsest operator");
+// with partial pivoting, in place in shared memory, by one warp: lane r owns row r (rows
+// padded to 33 entries, so a column's entries of consecutive rows sit in different banks)
+// and every step is ordered by __syncwarp alone.  Written transposed, so that the per-cycle
+// product reads it coalesced.
+constexpr int CI_PAD = 2 * MG_MAX_COARSE_CELLS + 1;
+static_assert(2 * MG_MAX_COARSE_CELLS <= 32, "one lane per row of the coarsest operator");
 
-// a: CI_N + 1 rows of CI_PAD doubles in shared memory
 __device__ void coarse_invert_warp(const LevelView &L, double (*a)[CI_PAD], int *perm, double *invT_out,
                                    int *singular) {
-  const unsigned full = 0xffffffffu;
   const int t = threadIdx.x & 31, n = 2 * L.N;
   for (int r = 0; r < n; ++r)
     if (t < n) a[r][t] = 0.0;
   __syncwarp();
-  if (t < L.N) {   // each cell's two rows are assembled by one lane
+  if (t < L.N) {   // each cell's two rows are written by one lane
     const int k = t, i = k / L.My, j = k % L.My;
     for (int b = 0; b < 9; ++b) {
       const int di = (b % 3) - 1, dj = 1 - (b / 3);
@@ -305,61 +298,54 @@ __device__ void coarse_invert_warp(const LevelView &L, double (*a)[CI_PAD], int 
     }
   }
   __syncwarp();
-  double row[CI_N];
-#pragma unroll
-  for (int q = 0; q < CI_N; ++q) row[q] = (t < n && q < n) ? a[t][q] : 0.0;
-  int pos = t;
-  __syncwarp();
-  double *prow = a[CI_N];   // the spare row: the scaled pivot row, read by every lane
-#pragma unroll
-  for (int col = 0; col < CI_N; ++col) {
-    if (col >= n) break;
-    const bool cand = t < n && pos >= col;
-    double best = cand ? fabs(row[col]) : -1.0;
-    int bp = cand ? pos : col;
-    for (int o = 16; o > 0; o >>= 1) {   // every lane ends with the same (largest, lowest position)
-      const double ob = __shfl_xor_sync(full, best, o);
-      const int op = __shfl_xor_sync(full, bp, o);
-      if (ob > best || (ob == best && op < bp)) {
+  for (int col = 0; col < n; ++col) {
+    double best = -1.0;
+    int bi = col;
+    if (col + t < n) {
+      best = fabs(a[col + t][col]);
+      bi = col + t;
+    }
+    for (int o = 16; o > 0; o >>= 1) {   // every lane ends with the same (largest, lowest row)
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
         best = ob;
-        bp = op;
+        bi = oi;
       }
     }
     if (t == 0) {
-      perm[col] = bp;
+      perm[col] = bi;
       if (!(best > 0.0)) *singular = 1;
     }
-    const int pl = __ffs(__ballot_sync(full, t < n && pos == bp)) - 1;    // the pivot row's lane
-    const int lc = __ffs(__ballot_sync(full, t < n && pos == col)) - 1;   // the lane at position col
-    if (t == lc) pos = bp;
-    if (t == pl) pos = col;
-    const double pv = __shfl_sync(full, row[col], pl);
-    const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
-    if (t == pl) {
-#pragma unroll
-      for (int q = 0; q < CI_N; ++q)
-        if (q < n) {
-          row[q] = (q == col ? 1.0 : row[q]) * pinv;
-          prow[q] = row[q];
-        }
+    const int p = bi;
+    if (p != col && t < n) {   // lane t swaps column t of the two rows
+      const double tmp = a[col][t];
+      a[col][t] = a[p][t];
+      a[p][t] = tmp;
     }
     __syncwarp();
-    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
-    if (t < n && t != pl) {
-      const double f = row[col];
+    const double pv = a[col][col];
+    const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
+    __syncwarp();
+    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
+    if (t < n) a[col][t] = (t == col ? 1.0 : a[col][t]) * pinv;
+    __syncwarp();
+    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot.  The pivot
+    // row is read into registers first, so a lane's updates of its own row do not wait on
+    // reads that might alias them
+    double prow[2 * MG_MAX_COARSE_CELLS];
 #pragma unroll
-      for (int q = 0; q < CI_N; ++q)
-        if (q < n && q != col) row[q] -= f * prow[q];
-      row[col] = -row[col] * prow[col];
+    for (int q = 0; q < 2 * MG_MAX_COARSE_CELLS; ++q) prow[q] = a[col][q];
+    if (t < n && t != col) {
+      const double f = a[t][col];
+#pragma unroll
+      for (int q = 0; q < 2 * MG_MAX_COARSE_CELLS; ++q)
+        if (q < n && q != col) a[t][q] -= f * prow[q];
+      a[t][col] = -a[t][col] * a[col][col];
     }
     __syncwarp();
   }
-  // the rows by position, then the interchanges undone as column interchanges, in reverse order
-#pragma unroll
-  for (int q = 0; q < CI_N; ++q)
-    if (t < n && q < n) a[pos][q] = row[q];
-  __syncwarp();
+  // undo the row interchanges as column interchanges, in reverse order
   for (int col = n - 1; col >= 0; --col) {
     const int p = perm[col];
     if (p != col && t < n) {
@@ -377,7 +363,7 @@ __device__ void coarse_invert_warp(const LevelView &L, double (*a)[CI_PAD], int 
 
 // the coarsest inverse alone (a hierarchy whose only coarse level is built from the fine grid)
 __global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
-  __shared__ double a[CI_N + 1][CI_PAD];   // the matrix and a spare row
+  __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
   __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
   coarse_invert_warp(L, a, perm, invT_out, singular);
 }
@@ -389,7 +375,7 @@ __global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *in
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
     k_mg_build_small(const LevelView *__restrict__ lev, int first, int nlev, double *invT_out, int *singular) {
   cg::cluster_group cluster = cg::this_cluster();
-  __shared__ double a[CI_N + 1][CI_PAD];   // the coarsest inverse's matrix and a spare row
+  __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
   __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
   const int rank = cluster.block_rank() * NTm + threadIdx.x, nthr = SMALL_CLUSTER * NTm;
   for (int c = first; c < nlev; ++c) {
