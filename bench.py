@@ -462,6 +462,48 @@ def ensemble_member(q, M=401):
     return g, c, f, {"T": T, "tauc_median": med}
 
 
+def ensemble_point(stream, flush, dev, members=16, steps=2):
+    """members/s of pism_gpu_ssa_solve_batch on `members` seeded 401^2 sheets (the ensemble
+    workload's members 0 .. members-1, fast set-up, learned guess), device-timed, L2 flushed
+    before each batch: the ensemble configuration in the default bench line"""
+    import torch
+    from pism_b200 import learned as Lrn
+    from pism_b200.ssa import SSAFD
+    M = 401
+    names = ("thickness", "surface", "bed", "mask", "tauc", "melange")
+    cases = [ensemble_member(q, M) for q in range(members)]
+    g, c0 = cases[0][0], cases[0][1]
+    mem = [{**{k: torch.tensor(f[k], dtype=torch.float64, device=dev) for k in names},
+            "ice_softness": c.ice_softness, "velocity": torch.zeros((M, M, 2), dtype=torch.float64, device=dev)}
+           for _, c, f, _ in cases]
+    hh, ww = Lrn.image_shape(M, M, 1)
+    net = Lrn.UNet(1, hh, ww, device=dev.index, params=np.load(Lrn.DEFAULT_WEIGHTS)["params"])
+    net.set_stream(stream.cuda_stream)
+    s = SSAFD(g, fast_config(c0), device=dev.index)
+    try:
+        s.set_stream(stream.cuda_stream)
+        s.solve_batch(mem[:2], net=net, stride=1)   # warm-up
+        ts, stats = [], None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, stats = s.solve_batch(mem, net=net, stride=1)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+    finally:
+        s.close()
+        net.close()
+    ms = float(np.mean(ts))
+    return {"members": members, "grid": [M, M], "ms_per_batch": ms, "members_per_s": members / (ms * 1e-3),
+            "converged": int(sum(st["converged"] for st in stats)),
+            "picard_iterations": [st["picard_iterations"] for st in stats],
+            "how": "pism_gpu_ssa_solve_batch, members in turn on one handle (bench.py --workload ensemble "
+                   "runs the 64-member configuration with its accuracy check)"}
+
+
 def run_ensemble(args):
     """--workload ensemble: pism_gpu_ssa_solve_batch over the members of this rank (the
     fast set-up with the learned guess), members/s of the whole job; each member's
@@ -924,6 +966,10 @@ def main():
             line["mass_continuity"] = mass_roofline(vel_mode, stream, flush, dev, peak)
         except Exception as e:   # noqa: BLE001 - reported in the line
             line["mass_continuity"] = {"error": str(e)[:200]}
+        try:
+            line["ensemble"] = ensemble_point(stream, flush, dev)
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["ensemble"] = {"error": str(e)[:200]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
         plain_picard = st_other["picard_iterations"] if args.mode == "fast" else picard[-1]
