@@ -14,6 +14,7 @@
 // and scaling the strain heating by each level's hardness.
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
 
 #include "ssa_internal.h"
@@ -181,19 +182,22 @@ void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_
                                                                v3, w3, sigma);
 }
 
-// the kernel's dynamic shared-memory limit for Mz levels: a function attribute shared by
-// every handle of the process, so it is only ever raised, under a lock
+// the kernel's dynamic shared-memory limit for Mz levels on the current device: a function
+// attribute shared by every handle on that device, so it is only ever raised, under a lock
 int stress_balance_3d_prepare(int Mz) {
   static std::mutex lock;
-  static int raised = 48 * 1024;
-  int warps = 0;
+  static std::map<int, int> raised;   // device -> bytes granted
+  int warps = 0, dev = 0;
   const int smem = stress_balance_3d_smem(Mz, &warps);
+  if (smem <= 48 * 1024) return 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
   std::lock_guard<std::mutex> guard(lock);
-  if (smem <= raised) return 0;
+  auto it = raised.find(dev);
+  if (it != raised.end() && smem <= it->second) return 0;
   if (cudaFuncSetAttribute((const void *)k_stress_balance_3d, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return 1;
-  raised = smem;
+  raised[dev] = smem;
   return 0;
 }
 
