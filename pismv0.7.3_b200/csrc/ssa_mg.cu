@@ -658,10 +658,18 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
   __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
   // Each step below costs one dependent round trip to L2: the staging loops are unrolled so
   // a thread's loads issue together, and the restriction gives every fine cell of an
-  // aggregate its own thread (four per coarse cell, summed by shuffles).
+  // aggregate its own thread (four per coarse cell, summed by shuffles).  A step whose work
+  // items all fall in CTA 0 (ranks below CTA_THREADS: the restrictions to levels of at most
+  // CTA_THREADS / 4 cells, the coarsest solve, the post-smoothing of levels of at most
+  // CTA_THREADS cells) is that CTA's alone and ends with a CTA barrier instead of the
+  // cluster's; the other CTAs wait at one cluster barrier for the first up step that needs
+  // them.  Which thread computes what is unchanged, so the results are too.
+  const bool lead = cluster.block_rank() == 0;
   // down
   for (int l = S.first; l < S.last; ++l) {
     const LevelView L = S.lev[l], C = S.lev[l + 1];
+    const bool local = ((4 * C.N + 31) & ~31) <= CTA_THREADS;
+    if (local && !lead) break;
 #pragma unroll 4
     for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
       const float2 v = fmul4(L.dinv[q], L.b[q]);
@@ -689,10 +697,11 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
       rv += __shfl_xor_sync(0xffffffffu, rv, 2);
       if (kc < C.N && (base & 3) == 0) C.b[kc] = make_float2(ru, rv);
     }
-    cluster.sync();
+    if (local) __syncthreads();
+    else cluster.sync();
   }
-  // coarsest: x = A^-1 b
-  {
+  // coarsest: x = A^-1 b (S.n <= 32 rows: CTA 0's warps)
+  if (lead) {
     const LevelView C = S.lev[S.last];
     for (int q = threadIdx.x; q < C.N; q += CTA_THREADS) {
       const float2 v = C.b[q];
@@ -710,11 +719,18 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0) reinterpret_cast<float *>(C.x)[r] = (float)acc;
     }
-    cluster.sync();
+    __syncthreads();
   }
   // up
+  bool joined = false;   // the other CTAs are back (after CTA 0's levels)
   for (int l = S.last - 1; l >= S.first; --l) {
     const LevelView L = S.lev[l], C = S.lev[l + 1];
+    const bool local = L.N <= CTA_THREADS;
+    if (local && !lead) continue;
+    if (!local && !joined) {
+      cluster.sync();   // CTA 0's coarse levels are written
+      joined = true;
+    }
 #pragma unroll 4
     for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
       const int i = q / L.My, j = q - i * L.My;
@@ -732,7 +748,8 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
       const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
       L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
     }
-    cluster.sync();
+    if (local) __syncthreads();
+    else cluster.sync();
   }
 }
 
