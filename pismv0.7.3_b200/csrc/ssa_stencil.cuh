@@ -148,6 +148,11 @@ template <class T>
 using HaloTile = T[TILE_I + 2][TILE_J + 2];
 
 __device__ __forceinline__ int pmod(int a, int n) {
+  // the halo indices of a tile are at most one period out of range except on grids narrower
+  // than a tile: those take the integer remainder, the rest a compare and an add
+  if (a >= 0 && a < n) return a;
+  if (a < 0 && a >= -n) return a + n;
+  if (a >= n && a < 2 * n) return a - n;
   a %= n;
   return a < 0 ? a + n : a;
 }
