@@ -642,8 +642,9 @@ def main():
     ap.add_argument("--ksp-factor", type=float, default=1.0,
                     help="fast set-up: KSP rtol of a Picard iteration = factor x the last relative nu*H change")
     ap.add_argument("--ksp-max", type=float, default=1e-1, help="fast set-up: loosest KSP rtol of a Picard iteration")
-    ap.add_argument("--mg-small-kernel", type=int, default=0, choices=[0, 1],
-                    help="multigrid small levels: 0 staged from L2 per step, 1 held in the cluster's shared memory")
+    ap.add_argument("--mg-small-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="multigrid small levels: 0 staged from L2 per step, 1 held in the cluster's shared memory, "
+                         "2 as 0 from the first level of <= 16384 cells")
     ap.add_argument("--apply-kernel", type=int, default=2, choices=[0, 1, 2],
                     help="mixed precision, the FP32 operator apply after each V-cycle: 0 plain tile loads, "
                          "1 bulk-copy staged tiles, 2 fused into the V-cycle's fine-level pass")

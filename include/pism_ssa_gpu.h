@@ -147,12 +147,14 @@ typedef struct pism_gpu_ssa_config {
      Krylov operator always use the current nu*H, so a lagged coarse level changes the
      iteration counts, not the tolerance the solve meets */
   double mg_rebuild_rtol;
-  /* the multigrid's small levels (<= 4096 cells each) in one thread-block cluster:
-     0 every CTA stages each level from L2 at every step; 1 each CTA holds a block of every
-     small level in its shared memory (operators staged by bulk asynchronous copies, halos read
-     from the neighbouring CTAs' shared memory), where the blocks fit.  Both give the same
-     results, bit for bit, in the same time on a B200 (30.6 and 31.4 us per cycle at 801^2);
-     a launch-shape knob for the autotuner */
+  /* the multigrid's small levels in one thread-block cluster: 0 the levels of <= 4096
+     cells, every CTA staging from L2 the rows its share of each step reads; 1 the same levels
+     with each CTA holding a block of every level in its shared memory (operators staged by
+     bulk asynchronous copies, halos read from the neighbouring CTAs' shared memory), where
+     the blocks fit; 0 and 1 give the same results, bit for bit (a launch-shape knob).  2 as 0
+     but from the first level of <= 16384 cells (the 101^2 level of an 801^2 grid joins the
+     cluster instead of two tiled passes); its residual sums at that level are added in
+     another order, so its results differ in the last bits */
   int    mg_small_kernel;
   /* mixed precision with multigrid, the FP32 operator apply that BiCGStab performs on each
      V-cycle's result: 0 a kernel of its own loading each tile with plain loads; 1 the same

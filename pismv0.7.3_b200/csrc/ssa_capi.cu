@@ -225,8 +225,8 @@ int check_config(pism_gpu_ssa *h, const pism_gpu_ssa_config *c) {
   if (c->graphs < 0 || c->graphs > 3) return fail(h, PISM_GPU_SSA_EINVAL, "graphs must be 0, 1, 2 or 3");
   if (c->mg_post_blocks_per_sm < 0 || c->mg_post_blocks_per_sm > 4)
     return fail(h, PISM_GPU_SSA_EINVAL, "mg_post_blocks_per_sm must be in [0, 4]");
-  if (c->mg_small_kernel < 0 || c->mg_small_kernel > 1)
-    return fail(h, PISM_GPU_SSA_EINVAL, "mg_small_kernel must be 0 or 1");
+  if (c->mg_small_kernel < 0 || c->mg_small_kernel > 2)
+    return fail(h, PISM_GPU_SSA_EINVAL, "mg_small_kernel must be 0, 1 or 2");
   if (c->mixed_apply_kernel < 0 || c->mixed_apply_kernel > 2)
     return fail(h, PISM_GPU_SSA_EINVAL, "mixed_apply_kernel must be 0, 1 or 2");
   if (!(c->mg_rebuild_rtol >= 0.0)) return fail(h, PISM_GPU_SSA_EINVAL, "mg_rebuild_rtol must be >= 0");

@@ -71,6 +71,7 @@ constexpr int MG_MAX_LEVELS = 16;
 constexpr int MG_COARSE_DIM = 4;                 // the coarsest level has <= 4 x 4 cells
 constexpr int MG_MAX_COARSE_CELLS = MG_COARSE_DIM * MG_COARSE_DIM;
 constexpr int MG_CTA_CELLS = 4096;               // levels this small are cycled by one thread-block cluster
+constexpr int MG_CTA_CELLS_WIDE = 16384;         // ... with mg_small_kernel 2
 
 struct MGLevel {
   int Mx = 0, My = 0, N = 0;
@@ -85,6 +86,7 @@ struct MGHierarchy {
   int fine_ax = 1, fine_ay = 1;                  // aggregation of the fine grid
   MGLevel lev[MG_MAX_LEVELS];
   int small_first = 0;                           // first level cycled by the cluster
+  int small_first_wide = 0;                      // the same with mg_small_kernel 2
   int small_smem = 0;                            // its per-CTA staging buffer (bytes)
   bool small_dsmem = false;                      // the small levels fit the cluster's shared memory
   int small_kernel = 0;                          // mg_small_kernel of the configuration

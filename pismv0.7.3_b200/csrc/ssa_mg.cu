@@ -625,8 +625,8 @@ __global__ void __launch_bounds__(NTm) k_mgc_post(LevelView L, float omega, floa
   }
 }
 
-// The small levels (first .. last, <= MG_CTA_CELLS cells each) in one launch: restrictions
-// down, the dense solve, post-smoothing up; __syncthreads between the steps.
+// The small levels (first .. last) in one launch: restrictions down, the dense solve,
+// post-smoothing up.
 struct SmallLevels {
   int first, last;        // level indices into lev[]
   const LevelView *lev;   // device array of the level views (read through L1, no local copy)
@@ -634,8 +634,68 @@ struct SmallLevels {
   int n;                  // unknowns of the coarsest level
 };
 
+// Work split of the small-level cycle, shared by the kernel and the host's sizing of its
+// staging buffer.  A down step from a level to the next coarser one (Nc cells) has
+// span(Nc) restriction items, four per coarse cell (one per fine cell of a 2 x 2 aggregate);
+// an up step has one post-smoothing item per cell.  Each of `parts` CTAs takes a contiguous
+// chunk of items (whole warps for the restriction's shuffles) and stages the fine rows those
+// items read: a window of rows, wrapped periodically, or the whole level once the window would
+// reach every row.
+__host__ __device__ inline int small_span(int Nc) { return (4 * Nc + 31) & ~31; }
+
+__host__ __device__ inline void small_chunk(int items, int parts, int c, int align, int &b0, int &b1) {
+  const int chunk = ((items + parts - 1) / parts + align - 1) / align * align;
+  b0 = c * chunk < items ? c * chunk : items;
+  b1 = b0 + chunk < items ? b0 + chunk : items;
+}
+
+// the fine rows [w0, w0 + nrows) read by the cells of rows r0 .. r1 of a level with Mx rows
+// (one halo row each side)
+__host__ __device__ inline void small_window(int Mx, int r0, int r1, int &w0, int &nrows) {
+  w0 = r0 - 1;
+  nrows = r1 - r0 + 3;
+  if (nrows >= Mx) {
+    w0 = 0;
+    nrows = Mx;
+  }
+}
+
+// the rows of a down step's restriction items b0 .. b1 - 1 (b1 > b0): the fine rows of the
+// aggregates of coarse rows I0 .. I1
+__host__ __device__ inline void small_down_rows(int ax, int Myc, int Nc, int b0, int b1, int &r0, int &r1) {
+  const int k0 = (b0 >> 2) < Nc ? (b0 >> 2) : Nc - 1, k1 = ((b1 - 1) >> 2) < Nc ? ((b1 - 1) >> 2) : Nc - 1;
+  r0 = (k0 / Myc) * ax;
+  r1 = (k1 / Myc) * ax + ax - 1;
+}
+
+// the largest window (cells) any CTA stages in a cycle over levels first .. nlev - 1
+inline int small_window_cells(const MGLevel *lev, int first, int nlev, int parts, int local_items) {
+  int most = 0;
+  for (int l = first; l + 1 < nlev; ++l) {
+    const MGLevel &L = lev[l], &C = lev[l + 1];
+    const int span = small_span(C.N), pd = span <= local_items ? 1 : parts;
+    for (int c = 0; c < pd; ++c) {
+      int b0, b1, r0, r1, w0, nr;
+      small_chunk(span, pd, c, 32, b0, b1);
+      if (b1 <= b0) continue;
+      small_down_rows(L.ax, C.My, C.N, b0, b1, r0, r1);
+      small_window(L.Mx, r0, r1, w0, nr);
+      most = nr * L.My > most ? nr * L.My : most;
+    }
+    const int pu = L.N <= local_items ? 1 : parts;
+    for (int c = 0; c < pu; ++c) {
+      int k0, k1, w0, nr;
+      small_chunk(L.N, pu, c, 32, k0, k1);
+      if (k1 <= k0) continue;
+      small_window(L.Mx, k0 / L.My, (k1 - 1) / L.My, w0, nr);
+      most = nr * L.My > most ? nr * L.My : most;
+    }
+  }
+  return most;
+}
+
 // The small levels run on one thread-block cluster of SMALL_CLUSTER CTAs: every CTA
-// stages the whole level's x in its shared memory, computes its share of the cells, and the
+// stages the rows its chunk of a step reads in its shared memory, computes its chunk, and the
 // cluster barrier (release / acquire at cluster scope) orders the steps.
 
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THREADS)
@@ -654,48 +714,66 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
       asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }
   }
-  extern __shared__ float2 xs[];   // the largest small level (H.small_smem bytes)
+  extern __shared__ float2 xs[];   // the largest window a CTA stages (H.small_smem bytes)
   __shared__ float bsh[2 * MG_MAX_COARSE_CELLS];
   // Each step below costs one dependent round trip to L2: the staging loops are unrolled so
   // a thread's loads issue together, and the restriction gives every fine cell of an
-  // aggregate its own thread (four per coarse cell, summed by shuffles).  A step whose work
-  // items all fall in CTA 0 (ranks below CTA_THREADS: the restrictions to levels of at most
-  // CTA_THREADS / 4 cells, the coarsest solve, the post-smoothing of levels of at most
-  // CTA_THREADS cells) is that CTA's alone and ends with a CTA barrier instead of the
-  // cluster's; the other CTAs wait at one cluster barrier for the first up step that needs
-  // them.  Which thread computes what is unchanged, so the results are too.
-  const bool lead = cluster.block_rank() == 0;
+  // aggregate its own thread (four per coarse cell, summed by shuffles).  A step whose items
+  // fit in one CTA (restrictions to levels of at most CTA_THREADS / 4 cells, the coarsest
+  // solve, the post-smoothing of levels of at most CTA_THREADS cells) is CTA 0's alone and
+  // ends with a CTA barrier instead of the cluster's; the other CTAs wait at one cluster
+  // barrier for the first up step that needs them.  Every item is computed by the same
+  // arithmetic whichever thread takes it, so the split does not change the results.
+  const int part = cluster.block_rank();
+  const bool lead = part == 0;
+  // x at wrapped fine row ii of the staged window [w0, w0 + nrows)
+  auto window = [&](int Mx, int My, int w0, int nrows) {
+    return [=](int ii, int jj) {
+      int r = ii - w0;
+      if (r < 0) r += Mx;
+      else if (r >= nrows) r -= Mx;
+      return xs[r * My + jj];
+    };
+  };
   // down
   for (int l = S.first; l < S.last; ++l) {
     const LevelView L = S.lev[l], C = S.lev[l + 1];
-    const bool local = ((4 * C.N + 31) & ~31) <= CTA_THREADS;
+    const int span = small_span(C.N);
+    const bool local = span <= CTA_THREADS;
     if (local && !lead) break;
+    int b0, b1;
+    small_chunk(span, local ? 1 : SMALL_CLUSTER, local ? 0 : part, 32, b0, b1);
+    if (b1 > b0) {
+      int r0, r1, w0, nrows;
+      small_down_rows(L.ax, C.My, C.N, b0, b1, r0, r1);
+      small_window(L.Mx, r0, r1, w0, nrows);
 #pragma unroll 4
-    for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
-      const float2 v = fmul4(L.dinv[q], L.b[q]);
-      xs[q] = make_float2(omega * v.x, omega * v.y);
-    }
-    __syncthreads();
-    auto xa = [&](int ii, int jj) { return xs[ii * L.My + jj]; };
-    const int span = (4 * C.N + 31) & ~31;   // whole warps take part in the shuffles
-    for (int base = rank; base < span; base += nthr) {
-      const int kc = base >> 2, pi = (base >> 1) & 1, pj = base & 1;
-      float ru = 0.0f, rv = 0.0f;
-      if (kc < C.N && pi < L.ax && pj < L.ay) {
-        const int I = kc / C.My, J = kc - I * C.My;
-        const int i = I * L.ax + pi, j = J * L.ay + pj;
-        if (i < L.Mx && j < L.My) {
-          const float2 y = coarse_apply(L, i, j, xa);
-          const float2 bk = L.b[i * L.My + j];
-          ru = bk.x - y.x;
-          rv = bk.y - y.y;
-        }
+      for (int q = threadIdx.x; q < nrows * L.My; q += CTA_THREADS) {
+        const int r = q / L.My, j = q - r * L.My, k = pmod(w0 + r, L.Mx) * L.My + j;
+        const float2 v = fmul4(L.dinv[k], L.b[k]);
+        xs[q] = make_float2(omega * v.x, omega * v.y);
       }
-      ru += __shfl_xor_sync(0xffffffffu, ru, 1);
-      rv += __shfl_xor_sync(0xffffffffu, rv, 1);
-      ru += __shfl_xor_sync(0xffffffffu, ru, 2);
-      rv += __shfl_xor_sync(0xffffffffu, rv, 2);
-      if (kc < C.N && (base & 3) == 0) C.b[kc] = make_float2(ru, rv);
+      __syncthreads();
+      const auto xa = window(L.Mx, L.My, w0, nrows);
+      for (int base = b0 + threadIdx.x; base < b1; base += CTA_THREADS) {
+        const int kc = base >> 2, pi = (base >> 1) & 1, pj = base & 1;
+        float ru = 0.0f, rv = 0.0f;
+        if (kc < C.N && pi < L.ax && pj < L.ay) {
+          const int I = kc / C.My, J = kc - I * C.My;
+          const int i = I * L.ax + pi, j = J * L.ay + pj;
+          if (i < L.Mx && j < L.My) {
+            const float2 y = coarse_apply(L, i, j, xa);
+            const float2 bk = L.b[i * L.My + j];
+            ru = bk.x - y.x;
+            rv = bk.y - y.y;
+          }
+        }
+        ru += __shfl_xor_sync(0xffffffffu, ru, 1);
+        rv += __shfl_xor_sync(0xffffffffu, rv, 1);
+        ru += __shfl_xor_sync(0xffffffffu, ru, 2);
+        rv += __shfl_xor_sync(0xffffffffu, rv, 2);
+        if (kc < C.N && (base & 3) == 0) C.b[kc] = make_float2(ru, rv);
+      }
     }
     if (local) __syncthreads();
     else cluster.sync();
@@ -711,7 +789,7 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
     __syncthreads();
     // one warp per row, the lanes split the columns (the row-major transpose keeps a
     // column's entries of consecutive rows adjacent; here each lane reads its own column)
-    const int lane = threadIdx.x & 31, warp = rank >> 5, nwarp = nthr >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = CTA_THREADS >> 5;
     for (int r = warp; r < S.n; r += nwarp) {
       double acc = 0.0;
       for (int c = lane; c < S.n; c += 32) acc += S.invT[c * S.n + r] * (double)bsh[c];
@@ -731,22 +809,28 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(CTA_THRE
       cluster.sync();   // CTA 0's coarse levels are written
       joined = true;
     }
+    int k0, k1;
+    small_chunk(L.N, local ? 1 : SMALL_CLUSTER, local ? 0 : part, 32, k0, k1);
+    if (k1 > k0) {
+      int w0, nrows;
+      small_window(L.Mx, k0 / L.My, (k1 - 1) / L.My, w0, nrows);
 #pragma unroll 4
-    for (int q = threadIdx.x; q < L.N; q += CTA_THREADS) {
-      const int i = q / L.My, j = q - i * L.My;
-      const float2 v = fmul4(L.dinv[q], L.b[q]);
-      const float2 c = C.x[(i / L.ax) * C.My + j / L.ay];
-      xs[q] = make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
-    }
-    __syncthreads();
-    auto xa = [&](int ii, int jj) { return xs[ii * L.My + jj]; };
-    for (int k = rank; k < L.N; k += nthr) {
-      const int i = k / L.My, j = k - i * L.My;
-      const float2 xk = xs[k];
-      const float2 y = coarse_apply(L, i, j, xa);
-      const float2 bk = L.b[k];
-      const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
-      L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+      for (int q = threadIdx.x; q < nrows * L.My; q += CTA_THREADS) {
+        const int r = q / L.My, j = q - r * L.My, i = pmod(w0 + r, L.Mx), k = i * L.My + j;
+        const float2 v = fmul4(L.dinv[k], L.b[k]);
+        const float2 c = C.x[(i / L.ax) * C.My + j / L.ay];
+        xs[q] = make_float2(omega * v.x + corr * c.x, omega * v.y + corr * c.y);
+      }
+      __syncthreads();
+      const auto xa = window(L.Mx, L.My, w0, nrows);
+      for (int k = k0 + threadIdx.x; k < k1; k += CTA_THREADS) {
+        const int i = k / L.My, j = k - i * L.My;
+        const float2 xk = xa(i, j);
+        const float2 y = coarse_apply(L, i, j, xa);
+        const float2 bk = L.b[k];
+        const float2 d = fmul4(L.dinv[k], make_float2(bk.x - y.x, bk.y - y.y));
+        L.x[k] = make_float2(xk.x + omega * d.x, xk.y + omega * d.y);
+      }
     }
     if (local) __syncthreads();
     else cluster.sync();
@@ -1068,7 +1152,13 @@ int mg_plan(int Mx, int My, MGHierarchy &H) {
   // the levels cycled by the cluster kernel: the trailing run of levels with <= MG_CTA_CELLS cells
   H.small_first = H.nlev - 1;
   while (H.small_first > 0 && H.lev[H.small_first - 1].N <= MG_CTA_CELLS) --H.small_first;
-  H.small_smem = (int)sizeof(float2) * H.lev[H.small_first].N;   // every CTA stages a whole level
+  // mg_small_kernel 2: the trailing run of levels with <= MG_CTA_CELLS_WIDE cells
+  H.small_first_wide = H.small_first;
+  while (H.small_first_wide > 0 && H.lev[H.small_first_wide - 1].N <= MG_CTA_CELLS_WIDE) --H.small_first_wide;
+  // every CTA stages the rows its share of a step reads
+  H.small_smem = (int)sizeof(float2) *
+                 std::max(small_window_cells(H.lev, H.small_first, H.nlev, SMALL_CLUSTER, CTA_THREADS),
+                          small_window_cells(H.lev, H.small_first_wide, H.nlev, SMALL_CLUSTER, CTA_THREADS));
   // the shared-memory cycle when every small level's block fits (ssa_small_plan.h)
   {
     int mx[SC_MAX_LEV], my[SC_MAX_LEV], ax[SC_MAX_LEV], ay[SC_MAX_LEV];
@@ -1256,7 +1346,10 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     ++launches;
   }
   // down through the large coarse levels
-  for (int l = 0; l < H.small_first; ++l) {
+  // the first level the cluster cycles (mg_small_kernel 2: the wider set)
+  const bool dsmem = H.small_dsmem && H.small_kernel == 1;
+  const int first = H.small_kernel == 2 ? H.small_first_wide : H.small_first;
+  for (int l = 0; l < first; ++l) {
     const MGLevel &L = H.lev[l], &C = H.lev[l + 1];
     const LevelView V = view(L);
     const TileM tm = tiles_of(L.Mx, L.My);
@@ -1267,7 +1360,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     ++launches;
   }
   // the small levels on one thread-block cluster
-  if (H.small_dsmem && H.small_kernel == 1) {
+  if (dsmem) {
     SmallDs S;
     S.plan = reinterpret_cast<const SmallPlan *>(H.small_plan_dev);
     S.lev = reinterpret_cast<const LevelView *>(H.views);
@@ -1278,7 +1371,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     ++launches;
   } else {
     SmallLevels S;
-    S.first = H.small_first;
+    S.first = first;
     S.last = H.nlev - 1;
     S.lev = reinterpret_cast<const LevelView *>(H.views);
     S.invT = H.cinv;
@@ -1287,7 +1380,7 @@ static void vcycle(const Launch &Lc, const GridDev &g, const Fields &f, const MG
     ++launches;
   }
   // up through the large coarse levels
-  for (int l = H.small_first - 1; l >= 0; --l) {
+  for (int l = first - 1; l >= 0; --l) {
     const MGLevel &L = H.lev[l], &C = H.lev[l + 1];
     const LevelView V = view(L);
     const TileM tm = tiles_of(L.Mx, L.My);

@@ -432,6 +432,23 @@ def test_small_level_cycles_agree_bitwise(shape, precision):
     assert out[0][1:] == out[1][1:]
 
 
+@pytest.mark.parametrize("shape,precision", [((201, 201), "mixed"), ((401, 401), "mixed"), ((201, 201), "fp64")])
+def test_wide_cluster_cycle_meets_the_same_tolerances(shape, precision):
+    """mg_small_kernel 2 (the cluster also cycles the level of <= 16384 cells) against 0: the
+    same preconditioner up to the order of one sum, so the same Picard count, Krylov counts
+    within a few, and answers that agree far inside the solve's tolerance"""
+    g, c, f, _ = S.build_synthetic(shape[0], 4000e3 / (shape[0] - 1), seed=6)
+    c = c.copy(pc_type="mg", precision=precision, ksp_rtol=1e-8)
+    out = {}
+    for k in (0, 2):
+        vel, st = _solve_case(g, c.copy(mg_small_kernel=k), f)
+        assert st["converged"] == 1
+        out[k] = (vel, st)
+    assert out[0][1]["picard_iterations"] == out[2][1]["picard_iterations"]
+    assert abs(out[0][1]["ksp_iterations"] - out[2][1]["ksp_iterations"]) <= 0.05 * out[0][1]["ksp_iterations"] + 3
+    assert rel(out[2][0], out[0][0]) < 1e-6
+
+
 @pytest.mark.parametrize("shape,graphs", [((201, 201), 3), ((161, 131), 2), ((130, 97), 0), ((45, 44), 3),
                                            ("test_i", 3)])
 def test_apply_kernels_agree_bitwise(shape, graphs):
