@@ -634,40 +634,6 @@ struct SmallLevels {
   int n;                  // unknowns of the coarsest level
 };
 
-// Work split of the small-level cycle, shared by the kernel and the host's sizing of its
-// staging buffer.  A down step from a level to the next coarser one (Nc cells) has
-// span(Nc) restriction items, four per coarse cell (one per fine cell of a 2 x 2 aggregate);
-// an up step has one post-smoothing item per cell.  Each of `parts` CTAs takes a contiguous
-// chunk of items (whole warps for the restriction's shuffles) and stages the fine rows those
-// items read: a window of rows, wrapped periodically, or the whole level once the window would
-// reach every row.
-__host__ __device__ inline int small_span(int Nc) { return (4 * Nc + 31) & ~31; }
-
-__host__ __device__ inline void small_chunk(int items, int parts, int c, int align, int &b0, int &b1) {
-  const int chunk = ((items + parts - 1) / parts + align - 1) / align * align;
-  b0 = c * chunk < items ? c * chunk : items;
-  b1 = b0 + chunk < items ? b0 + chunk : items;
-}
-
-// the fine rows [w0, w0 + nrows) read by the cells of rows r0 .. r1 of a level with Mx rows
-// (one halo row each side)
-__host__ __device__ inline void small_window(int Mx, int r0, int r1, int &w0, int &nrows) {
-  w0 = r0 - 1;
-  nrows = r1 - r0 + 3;
-  if (nrows >= Mx) {
-    w0 = 0;
-    nrows = Mx;
-  }
-}
-
-// the rows of a down step's restriction items b0 .. b1 - 1 (b1 > b0): the fine rows of the
-// aggregates of coarse rows I0 .. I1
-__host__ __device__ inline void small_down_rows(int ax, int Myc, int Nc, int b0, int b1, int &r0, int &r1) {
-  const int k0 = (b0 >> 2) < Nc ? (b0 >> 2) : Nc - 1, k1 = ((b1 - 1) >> 2) < Nc ? ((b1 - 1) >> 2) : Nc - 1;
-  r0 = (k0 / Myc) * ax;
-  r1 = (k1 / Myc) * ax + ax - 1;
-}
-
 // the largest window (cells) any CTA stages in a cycle over levels first .. nlev - 1
 inline int small_window_cells(const MGLevel *lev, int first, int nlev, int parts, int local_items) {
   int most = 0;

@@ -1,6 +1,6 @@
 // ssa_small_plan.h — how the small multigrid levels are split over the CTAs of one
-// thread-block cluster (the shared-memory cycle of ssa_mg.cu), as plain C++ so that the host
-// compiler can check the split too.
+// thread-block cluster (the shared-memory cycle of ssa_mg.cu, and the work split of the
+// L2-staged cycle), as plain C++ so that the host compiler can check the split too.
 //
 // The coarsest level's rows and columns are cut into a Pr x Pc grid of blocks, one block per
 // CTA (Pr * Pc <= cluster size); every finer small level takes the blocks of the level below
@@ -11,6 +11,12 @@
 // memory); the smoothed iterates x0 and x also carry a one-cell halo ring, filled from the
 // neighbours once per step.
 #pragma once
+
+#if defined(__CUDACC__)
+#define SMALL_HD __host__ __device__ inline
+#else
+#define SMALL_HD inline
+#endif
 
 namespace pism_gpu {
 
@@ -97,6 +103,40 @@ inline
   int p = parts - 1;
   while (p > 0 && bounds[p] > i) --p;
   return p;
+}
+
+// Work split of the small-level cycle, shared by the kernel and the host's sizing of its
+// staging buffer.  A down step from a level to the next coarser one (Nc cells) has
+// span(Nc) restriction items, four per coarse cell (one per fine cell of a 2 x 2 aggregate);
+// an up step has one post-smoothing item per cell.  Each of `parts` CTAs takes a contiguous
+// chunk of items (whole warps for the restriction's shuffles) and stages the fine rows those
+// items read: a window of rows, wrapped periodically, or the whole level once the window would
+// reach every row.
+SMALL_HD int small_span(int Nc) { return (4 * Nc + 31) & ~31; }
+
+SMALL_HD void small_chunk(int items, int parts, int c, int align, int &b0, int &b1) {
+  const int chunk = ((items + parts - 1) / parts + align - 1) / align * align;
+  b0 = c * chunk < items ? c * chunk : items;
+  b1 = b0 + chunk < items ? b0 + chunk : items;
+}
+
+// the fine rows [w0, w0 + nrows) read by the cells of rows r0 .. r1 of a level with Mx rows
+// (one halo row each side)
+SMALL_HD void small_window(int Mx, int r0, int r1, int &w0, int &nrows) {
+  w0 = r0 - 1;
+  nrows = r1 - r0 + 3;
+  if (nrows >= Mx) {
+    w0 = 0;
+    nrows = Mx;
+  }
+}
+
+// the rows of a down step's restriction items b0 .. b1 - 1 (b1 > b0): the fine rows of the
+// aggregates of coarse rows I0 .. I1
+SMALL_HD void small_down_rows(int ax, int Myc, int Nc, int b0, int b1, int &r0, int &r1) {
+  const int k0 = (b0 >> 2) < Nc ? (b0 >> 2) : Nc - 1, k1 = ((b1 - 1) >> 2) < Nc ? ((b1 - 1) >> 2) : Nc - 1;
+  r0 = (k0 / Myc) * ax;
+  r1 = (k1 / Myc) * ax + ax - 1;
 }
 
 }  // namespace pism_gpu
