@@ -368,6 +368,23 @@ class SSAFD:
         return its.value, res.value
 
 
+class _StrengthExtension:
+    """SSAStrengthExtension (SSA.hh:39-58) of a solver: its parameters are configuration fields."""
+
+    def __init__(self, ssa):
+        self._ssa = ssa
+
+    def set_min_thickness(self, thickness):
+        self._ssa.set_config(self._ssa.config.copy(min_thickness_strength_extension_ssa=float(thickness)))
+
+    def get_min_thickness(self):
+        return self._ssa.config.min_thickness_strength_extension_ssa
+
+
+SSAFD.strength_extension = property(lambda self: _StrengthExtension(self),
+                                    doc="SSA::strength_extension (SSA.hh:111): its minimum thickness")
+
+
 def SSAFD_GPUFactory(grid: GridDesc, config: SSAConfig | None = None) -> SSAFD:
     """The SSAFactory of this solver (typedef SSAFactory, SSA.hh:77; SSAFDFactory SSAFD.cc:47-49)."""
     return SSAFD(grid, config)
