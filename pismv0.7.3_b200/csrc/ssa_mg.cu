@@ -18,7 +18,9 @@
 //   ...  x_L = A_L^-1 b_L                        (dense inverse)
 //   x_l <- x_l + s P x_{l+1};  x_l <- x_l + omega D_l^-1 (b_l - A_l x_l)   (post kernel)
 // so each level costs two stencil passes.  Levels of <= MG_CTA_CELLS cells are cycled by
-// one CTA in one launch (their kernels would be launch- and latency-bound).
+// one thread-block cluster in one launch (their kernels would be launch- and
+// latency-bound), and their Galerkin operators and the coarsest inverse are built by one
+// cluster launch per Picard iteration.
 // The defaults omega = 0.9 and s = 1.2 (mg_omega, mg_correction; s > 1 over-corrects to
 // compensate the piecewise-constant interpolation) come from a sweep of whole 801^2
 // synthetic solves: 7115 BiCGStab iterations against 9558 at (0.7, 1.5) and 8042 at
@@ -119,7 +121,6 @@ __global__ void k_mg0_compact(int N, const double2 *__restrict__ nuH, const doub
 // ---------------------------------------------------------------------------
 // set-up: Galerkin coarse operators
 // ---------------------------------------------------------------------------
-// level 1 from the fine operator (FP64 rows, FP64 accumulation in shared memory)
 // acc[4 cb .. 4 cb + 3] += (x, y, z, w) for a block index cb known only at run time: the
 // accumulators stay in registers (every index below is static once unrolled), so the
 // operator loads of the next fine cell need not wait behind shared-memory updates
@@ -174,6 +175,7 @@ __device__ __forceinline__ void acc_fine_static(double (&acc)[36], bool ex, bool
   }
 }
 
+// level 1 from the fine operator (FP64 rows, FP64 accumulation in registers)
 __global__ void __launch_bounds__(NTm) k_mg_build1(GridDev g, StencilConst s, const uint32_t *__restrict__ flags,
                                                    const double2 *__restrict__ nuH, const double *__restrict__ beta,
                                                    int ax, int ay, int Mxc, int Myc, TileM tm, float4 *Ac,
