@@ -75,8 +75,10 @@ def test_plug_flow_through_the_front_end(capsys):
         vel = case.ssa.velocity()
         assert np.linalg.norm(vel - ref) / np.linalg.norm(ref) < 1e-8
         ref_table = report(ref, case.exact_velocity())
+        # the table prints m/year to 4 decimals (SSATestCase::report); the two velocities agree
+        # to 1e-8 of a 1400 m/year flow, so the printed errors agree to those digits
         for k in ("maxvector", "maxu", "avu"):
-            assert table[k] == pytest.approx(ref_table[k], rel=1e-6, abs=1e-9), k
+            assert table[k] == pytest.approx(ref_table[k], abs=1e-4), k
         errs[M] = table["maxvector"]
         case.ssa.close()
     assert 3.5 < errs[31] / errs[61] < 4.5   # second order
