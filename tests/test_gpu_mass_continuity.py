@@ -97,3 +97,13 @@ def test_step_after_an_ssa_solve():
     ref = oracle_step(g, c, f, vel, 3.15e7, cmb, None, None)
     assert relmax(out["thickness"], ref["thickness"]) < RTOL
     np.testing.assert_array_equal(out["mask"], ref["mask"])
+
+
+def test_a_zero_step_changes_nothing():
+    """dt = 0: the thickness is returned unchanged (no cell goes negative) and every total is 0"""
+    g, c, f, vel, cmb, bmr, area = random_step(11, dirichlet=True)
+    f = dict(f, thickness=np.where(f["thickness"] < 0.01, 0.0, f["thickness"]))
+    out = gpu_step(g, c, f, vel, 0.0, cmb, bmr, area, device=False)
+    np.testing.assert_array_equal(out["thickness"], f["thickness"])
+    assert all(v == 0.0 for k, v in out["totals"].items() if k not in ("sum_divQ_SSA",))
+    assert out["totals"]["sum_divQ_SSA"] == 0.0

@@ -106,3 +106,15 @@ def test_refuses_without_levels_or_enthalpy():
             s.stress_balance_3d()
     finally:
         s.close()
+
+
+def test_two_levels_and_the_top_level():
+    """Mz = 2 (the fewest the strain heating's one-sided z difference needs) with thicknesses
+    at 0 and at the top level: kBelowHeight is 0 for both, so only level 0 heats"""
+    g, c, f, vel = random_columns(9, Mz=2, flow_law="isothermal_glen")
+    f = dict(f, thickness=np.where(np.arange(g.Mx)[:, None] % 2 == 0, 0.0, g.z[-1]) * np.ones((g.Mx, g.My)))
+    ref = oracle_fields(g, c, f, vel, None)
+    got = gpu_fields(g, c, f, vel, None, device=False)
+    assert relmax(got["w"], ref["w"]) < RTOL
+    assert relmax(got["strain_heating"], ref["strain_heating"]) < RTOL
+    assert np.all(got["strain_heating"][..., 1] == 0.0)
