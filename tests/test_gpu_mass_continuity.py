@@ -46,8 +46,7 @@ def random_step(seed, Mx=29, My=23, dirichlet=False, periodicity=0):
 def oracle_step(g, c, f, vel, dt, cmb, bmr, area):
     G, Cc, I = O.from_case(g, c, f)
     Hn, fdiv, tot = O.mass_continuity_step(G, Cc, I, vel, dt, cmb, bmr, area)
-    Cc2 = Cc
-    mask, surface = O.geometry_mask_surface(Cc2, I.bed, Hn)
+    mask, surface = O.geometry_mask_surface(Cc, I.bed, Hn)
     return {"thickness": Hn, "flux_divergence": fdiv, "mask": mask, "surface": surface, "totals": tot}
 
 
@@ -102,8 +101,6 @@ def test_step_after_an_ssa_solve():
 def test_a_zero_step_changes_nothing():
     """dt = 0: the thickness is returned unchanged (no cell goes negative) and every total is 0"""
     g, c, f, vel, cmb, bmr, area = random_step(11, dirichlet=True)
-    f = dict(f, thickness=np.where(f["thickness"] < 0.01, 0.0, f["thickness"]))
     out = gpu_step(g, c, f, vel, 0.0, cmb, bmr, area, device=False)
     np.testing.assert_array_equal(out["thickness"], f["thickness"])
-    assert all(v == 0.0 for k, v in out["totals"].items() if k not in ("sum_divQ_SSA",))
-    assert out["totals"]["sum_divQ_SSA"] == 0.0
+    assert all(v == 0.0 for v in out["totals"].values())
