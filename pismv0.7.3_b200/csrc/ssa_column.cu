@@ -89,9 +89,14 @@ __global__ void __launch_bounds__(NTC) k_stress_balance_3d(GridDev g, pism_gpu_s
       __syncwarp();
       const int n = ncol * Mz;
       double *const out = dst + (size_t)c0 * Mz;
+      int r = lane / Mz, k = lane - r * Mz;   // (column, level) of element e, advanced by 32
       for (int e = lane; e < n; e += 32) {
-        const int r = e / Mz, k = e - r * Mz;
         out[e] = tile[r * S + k];
+        k += 32;
+        while (k >= Mz) {
+          k -= Mz;
+          ++r;
+        }
       }
       __syncwarp();
     };
