@@ -874,8 +874,11 @@ def main():
     roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the iteration's kernels, "
                               "in-solve (--cache-control none), profiles/inner_iteration_traffic_801.md"
                               if roof["traffic"] is not None else None)
-    roof["kernel"] = ("one inner BiCGStab + V(1,1) multigrid iteration: k32_p/v/s/t/x + 2 x (k_mg0_restrict, "
-                      "k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, k_mg0_post)"
+    fine_last = {2: "k_mg0_post_apply (the post-smoothing fused with the FP32 apply)",
+                 1: "k_mg0_post, then k32_apply with bulk-copy-staged tiles",
+                 0: "k_mg0_post, then k32_apply"}[c.mixed_apply_kernel]
+    roof["kernel"] = (f"one inner BiCGStab + V(1,1) multigrid iteration: k32_p, k32_x + 2 x (k_mg0_restrict, "
+                      f"k_mgc_restrict x3, k_mg_small_cycle, k_mgc_post x3, {fine_last})"
                       if c.precision == "mixed" else "one BiCGStab + V(1,1) multigrid iteration (FP64 Krylov vectors)")
     # the FP64 matrix-free apply alone, each launch timed with L2 flushed before it (HBM-bound)
     x = torch.randn((M, M, 2), dtype=torch.float64, device=dev) * 1e-5
