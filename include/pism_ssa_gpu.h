@@ -314,6 +314,38 @@ int pism_gpu_ssa_mass_continuity_step(pism_gpu_ssa *h, double dt, const double *
                                       double *mask_out, double *surface_out, double *flux_divergence,
                                       double *totals, int where);
 
+/* The strain rates and 2-D stresses of the handle's velocity:
+ *   edot      ShallowStressBalance::compute_2D_principal_strain_rates
+ *             (ShallowStressBalance.cc:224-305): the eigenvalues (max, min) of the vertically
+ *             integrated horizontal strain rate tensor (1/s), Mx*My*2, [i][j][2]
+ *   stresses  ShallowStressBalance::compute_2D_stresses (:308-386): nu (u_x, v_y,
+ *             (u_y + v_x) / 2) with nu the effective viscosity of the constant hardness
+ *             ice_softness^(-1/ssa_Glen_exponent) (Pa), Mx*My*3, [i][j][3]
+ * Differences are one-sided next to ice-free cells; both are zero on ice-free cells.  mask
+ * (Mx*My doubles, PISM's mask values) may be NULL for the handle's mask.  Either output may
+ * be NULL.  Arrays are host or device per `where`.  Blocks until done. */
+int pism_gpu_ssa_strain_rates(pism_gpu_ssa *h, const double *mask, double *edot, double *stresses, int where);
+
+/* EigenCalving::update (PISMEigenCalving.cc:77-235) over dt seconds with the constant K
+ * (eigen_calving_K, m s) on the handle's velocity: at each ice-free ocean cell next to
+ * floating ice the calving rate K e1 e2 H_average / dx (e1, e2 the principal strain rates
+ * averaged over the floating, non-margin cells two cells away) lowers Href; where Href goes
+ * negative the rest is shared among the floating neighbours, which are cut (thickness 0,
+ * ice-free ocean, Href = max(H - loss, 0)); then remove_narrow_tongues (:420-493) in the
+ * reference's (i, j) order.  mask (as doubles), Href and thickness (Mx*My each) are read and
+ * overwritten, host or device per `where`.  The grid is taken as one process's: a strain
+ * rate two cells across the grid's edge reads 0 (the reference's never-refreshed ghosts).
+ * Blocks until done. */
+int pism_gpu_ssa_eigen_calving(pism_gpu_ssa *h, double dt, double K, double *mask, double *Href, double *thickness,
+                               int where);
+
+/* EigenCalving::max_timestep (PISMEigenCalving.cc:249-341) on the handle's velocity and this
+ * mask: result (host, 4 doubles) = {the time step allowed (s), the maximum horizontal
+ * calving rate (m/s), their mean, the number of cells where the calving law applies}.  The
+ * caller applies it only with cfl_eigen_calving.  mask is host or device per `where`. */
+int pism_gpu_ssa_eigen_calving_max_timestep(pism_gpu_ssa *h, double K, const double *mask, double *result,
+                                            int where);
+
 /* Stage entry points, each the device restatement of one reference method, for
  * stage-by-stage checking:
  *   assemble_rhs       -> SSA::compute_driving_stress + SSAFD::assemble_rhs

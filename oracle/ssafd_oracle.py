@@ -1186,6 +1186,174 @@ def mass_continuity_step(grid: Grid, cfg: Config, inp: Inputs, vel, dt, climatic
     return Hnew, flux_divergence, totals
 
 
+# ---------------------------------------------------------------------------
+# strain rates and 2-D stresses of the SSA velocity; eigen-calving
+# ---------------------------------------------------------------------------
+def _velocity_gradient(grid: Grid, M, vel):
+    """u_x, u_y, v_x, v_y of ShallowStressBalance.cc:249-293 (and :330-371): centred
+    differences written as weighted one-sided ones, a side dropped where that neighbour is
+    ice-free, the derivative zero where both are."""
+    free = m_ice_free(M)
+    east, west = np.where(nb(free, 1, 0), 0.0, 1.0), np.where(nb(free, -1, 0), 0.0, 1.0)
+    north, south = np.where(nb(free, 0, 1), 0.0, 1.0), np.where(nb(free, 0, -1), 0.0, 1.0)
+    u, v = vel[..., 0], vel[..., 1]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rx = np.where(west + east > 0, 1.0 / (grid.dx * (west + east)), 0.0)
+        ry = np.where(south + north > 0, 1.0 / (grid.dy * (south + north)), 0.0)
+    u_x = np.where(west + east > 0, rx * (west * (u - nb(u, -1, 0)) + east * (nb(u, 1, 0) - u)), 0.0)
+    v_x = np.where(west + east > 0, rx * (west * (v - nb(v, -1, 0)) + east * (nb(v, 1, 0) - v)), 0.0)
+    u_y = np.where(south + north > 0, ry * (south * (u - nb(u, 0, -1)) + north * (nb(u, 0, 1) - u)), 0.0)
+    v_y = np.where(south + north > 0, ry * (south * (v - nb(v, 0, -1)) + north * (nb(v, 0, 1) - v)), 0.0)
+    return u_x, u_y, v_x, v_y
+
+
+def principal_strain_rates(grid: Grid, mask, vel):
+    """ShallowStressBalance::compute_2D_principal_strain_rates, ShallowStressBalance.cc:224-305:
+    the eigenvalues (max, min) of the vertically integrated horizontal strain rate tensor,
+    zero on ice-free cells.  Returns [Mx, My, 2] (1/s)."""
+    M = as_int(mask)
+    u_x, u_y, v_x, v_y = _velocity_gradient(grid, M, vel)
+    A = 0.5 * (u_x + v_y)
+    B = 0.5 * (u_x - v_y)
+    Dxy = 0.5 * (v_x + u_y)
+    q = np.sqrt(B * B + Dxy * Dxy)
+    free = m_ice_free(M)
+    return np.stack([np.where(free, 0.0, A + q), np.where(free, 0.0, A - q)], axis=-1)
+
+
+def deviatoric_stresses_2d(grid: Grid, cfg: Config, mask, vel):
+    """ShallowStressBalance::compute_2D_stresses, ShallowStressBalance.cc:308-386: the
+    effective viscosity of the constant hardness ice_softness^(-1/n) at the strain rate's
+    second invariant, times (u_x, v_y, (u_y + v_x) / 2).  Returns [Mx, My, 3] (Pa)."""
+    M = as_int(mask)
+    u_x, u_y, v_x, v_y = _velocity_gradient(grid, M, vel)
+    hardness = cfg.ice_softness ** (-1.0 / cfg.ssa_Glen_exponent)
+    nu = effective_viscosity(cfg, hardness, second_invariant_2d(u_x, u_y, v_x, v_y))
+    free = m_ice_free(M)
+    return np.stack([np.where(free, 0.0, nu * u_x), np.where(free, 0.0, nu * v_y),
+                     np.where(free, 0.0, 0.5 * nu * (u_y + v_x))], axis=-1)
+
+
+EIGEN_CALVING_OFFSET = 2   # EigenCalving::m_stencil_width, PISMEigenCalving.cc:33
+
+
+def _eigen_calving_front(grid: Grid, M, edot, K):
+    """The calving front cells of EigenCalving (ice-free ocean next to floating ice) and their
+    horizontal calving rate K eigen1 eigen2 (PISMEigenCalving.cc:115-176, 283-322): the
+    principal strain rates averaged over the floating, non-margin cells two cells away, in
+    the order (i-2, j), (i+2, j), (i, j-2), (i, j+2).  As one process runs it: a strain rate
+    read across the grid's edge is the ghost value 0; the mask wraps periodically (the
+    reference's mask ghosts are two wide, so a front cell within three cells of the edge
+    reads beyond them in ice_margin).  Returns (front, calving law applies, rate)."""
+    floating = m_floating_ice(M)
+    free = m_ice_free(M)
+    front = m_ice_free_ocean(M) & (nb(floating, 1, 0) | nb(floating, -1, 0) | nb(floating, 0, 1)
+                                   | nb(floating, 0, -1))
+    margin = m_icy(M) & (nb(free, 1, 0) | nb(free, -1, 0) | nb(free, 0, 1) | nb(free, 0, -1))
+    use = floating & ~margin
+    o = EIGEN_CALVING_OFFSET
+    Mx, My = M.shape
+    ii, jj = np.meshgrid(np.arange(Mx), np.arange(My), indexing="ij")
+    e1, e2, cnt = np.zeros(M.shape), np.zeros(M.shape), np.zeros(M.shape)
+    for di, dj in ((-o, 0), (o, 0), (0, -o), (0, o)):
+        take = nb(use, di, dj)
+        # the strain rates' ghosts are never refreshed after EigenCalving::init set them to 0
+        inside = (ii + di >= 0) & (ii + di < Mx) & (jj + dj >= 0) & (jj + dj < My)
+        e1 = e1 + np.where(take, np.where(inside, nb(edot[..., 0], di, dj), 0.0), 0.0)
+        e2 = e2 + np.where(take, np.where(inside, nb(edot[..., 1], di, dj), 0.0), 0.0)
+        cnt = cnt + take
+    e1 = np.where(cnt > 0, e1 / np.maximum(cnt, 1), e1)
+    e2 = np.where(cnt > 0, e2 / np.maximum(cnt, 1), e2)
+    law = front & (e2 > 0.0) & (e1 > 0.0)
+    return front, law, np.where(law, K * e1 * (e2 - 0.0), 0.0)
+
+
+def remove_narrow_tongues(M, H):
+    """EigenCalving::remove_narrow_tongues, PISMEigenCalving.cc:420-493, as one process runs it:
+    cells in (i, j) order with i outer (IceGrid.hh:335-345), the mask updated in place, so a
+    neighbour earlier in that order and inside the grid is read after its own update, while
+    one across the periodic edge is read from the ghost copy made before the loop.  Returns
+    the new (mask, thickness)."""
+    M0 = np.asarray(M, dtype=np.int64).copy()
+    live = M0.copy()
+    H = np.asarray(H, dtype=np.float64).copy()
+    Mx, My = M0.shape
+
+    def at(i, j):
+        if 0 <= i < Mx and 0 <= j < My:
+            return live[i, j]
+        return M0[i % Mx, j % My]
+
+    for i in range(Mx):
+        for j in range(My):
+            m = live[i, j]
+            if not (m == MASK_GROUNDED or m == MASK_FLOATING):
+                continue
+            if m == MASK_GROUNDED:
+                test = lambda a: a == MASK_ICE_FREE_OCEAN   # noqa: E731 (ice_free_ocean, Mask.hh:59-61)
+            else:
+                test = lambda a: not (a == MASK_GROUNDED or a == MASK_FLOATING)   # noqa: E731 (ice_free)
+            N, E, S, W = test(at(i, j + 1)), test(at(i + 1, j)), test(at(i, j - 1)), test(at(i - 1, j))
+            NE, NW, SE, SW = test(at(i + 1, j + 1)), test(at(i - 1, j + 1)), test(at(i + 1, j - 1)), test(at(i - 1, j - 1))
+            if ((not W and NW and SW and N and S and E) or (not N and NW and NE and W and E and S)
+                    or (not E and NE and SE and W and S and N) or (not S and SW and SE and W and E and N)):
+                live[i, j] = MASK_ICE_FREE_OCEAN
+                H[i, j] = 0.0
+    return live, H
+
+
+def eigen_calving(grid: Grid, mask, Href, thickness, vel, dt, K):
+    """EigenCalving::update, PISMEigenCalving.cc:77-235: the principal strain rates of the
+    velocity on this mask; at each calving front cell the calving rate K e1 e2 H_average / dx
+    lowers Href and, where Href goes negative, the loss is shared among the floating
+    neighbours, which are cut (thickness 0, ice-free ocean, Href = max(H - loss, 0)); then
+    remove_narrow_tongues.  Returns (mask, Href, thickness)."""
+    M = as_int(mask)
+    H = np.asarray(thickness, dtype=np.float64).copy()
+    Href = np.asarray(Href, dtype=np.float64).copy()
+    edot = principal_strain_rates(grid, M, vel)
+    front, _, rate_h = _eigen_calving_front(grid, M, edot, K)
+    floating = m_floating_ice(M)
+    nfl = np.zeros(M.shape)
+    hsum = np.zeros(M.shape)
+    for di, dj in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+        f = nb(floating, di, dj)
+        nfl = nfl + f
+        hsum = hsum + np.where(f, nb(H, di, dj), 0.0)
+    H_average = np.where(nfl > 0, hsum / np.maximum(nfl, 1), hsum)
+    calving_rate = rate_h * H_average / grid.dx
+    hit = front & (calving_rate > 0.0)
+    Href = np.where(hit, Href - calving_rate * dt, Href)
+    gone = hit & (Href < 0.0)
+    loss = np.where(gone, -Href, 0.0)
+    Href = np.where(gone, 0.0, Href)
+    loss = np.where(gone & (nfl > 0), loss / np.maximum(nfl, 1), loss)
+    ln = [nb(loss, 1, 0), nb(loss, -1, 0), nb(loss, 0, 1), nb(loss, 0, -1)]
+    cut = floating & ((ln[0] > 0.0) | (ln[1] > 0.0) | (ln[2] > 0.0) | (ln[3] > 0.0))
+    total = ln[0] + ln[1] + ln[2] + ln[3]
+    Href = np.where(cut, np.maximum(H - total, 0.0), Href)
+    H = np.where(cut, 0.0, H)
+    M = np.where(cut, MASK_ICE_FREE_OCEAN, M)
+    M, H = remove_narrow_tongues(M, H)
+    return M.astype(np.float64), Href, H
+
+
+def eigen_calving_max_timestep(grid: Grid, mask, vel, K):
+    """EigenCalving::max_timestep, PISMEigenCalving.cc:249-341: (dt, maximum rate, mean rate,
+    number of cells calving) from the calving rates K e1 e2 (m/s) at the front cells, dt =
+    max(1 / (max rate / dx + epsilon), 0.001 year)."""
+    M = as_int(mask)
+    edot = principal_strain_rates(grid, M, vel)
+    _, calving, rate = _eigen_calving_front(grid, M, edot, K)
+    count = float(np.count_nonzero(calving))
+    rmax = max(0.0, float(np.max(rate[calving]))) if count > 0 else 0.0
+    rmean = float(np.sum(rate[calving])) / count if count > 0 else 0.0
+    dt_min = 0.001 * SECPERA
+    epsilon = 0.001 / (grid.dx + grid.dy) / SECPERA
+    dt = 1.0 / (rmax / grid.dx + epsilon)
+    return max(dt, dt_min), rmax, rmean, count
+
+
 def residual_rel(grid, cfg, inp, vel, reg, hardness, b):
     """||b - A(u) u||_2 / ||b||_2 with A built at the velocity itself (a nonlinear residual)."""
     nuH = compute_nuH(grid, cfg, inp, hardness, vel, reg)

@@ -38,6 +38,8 @@ struct pism_gpu_ssa {
   double *beta = nullptr, *bfrict = nullptr;
   double *sb3d = nullptr;   // host-destination staging of pism_gpu_ssa_stress_balance_3d
   double *mc = nullptr;     // staging of pism_gpu_ssa_mass_continuity_step: 7 fields and 8 totals
+  double *ec = nullptr;     // staging of the strain rates and eigen-calving: 5 fields and 8 scalars
+  int8_t *ec_mask = nullptr;   // eigen-calving's mask before and during remove_narrow_tongues
   uint32_t *flags = nullptr;
   Krylov K{};
   Krylov32 K32{};
@@ -910,6 +912,18 @@ int prepare(pism_gpu_ssa *h) {
   return PISM_GPU_SSA_OK;
 }
 
+// staging of the strain rates and eigen-calving, in doubles from h->ec: strain rates 2 N at
+// EC_EDOT, stresses 3 N at EC_STRESS, the caller's mask N at EC_MASK; eigen-calving's Href,
+// thickness and per-cell loss N each at EC_HREF, EC_H, EC_LOSS (over the strain-rate slots,
+// which it does not use); 8 scalars at EC_SCALARS.  Plus 2 N bytes of masks in h->ec_mask.
+enum : size_t { EC_EDOT = 0, EC_STRESS = 2, EC_MASK = 5, EC_HREF = 0, EC_H = 1, EC_LOSS = 2, EC_SCALARS = 6 };
+
+int ec_buffers(pism_gpu_ssa *h) {
+  if (!h->ec) RET(dalloc(h, &h->ec, EC_SCALARS * (size_t)h->N + 8));
+  if (!h->ec_mask) RET(dalloc(h, &h->ec_mask, 2 * (size_t)h->N));
+  return PISM_GPU_SSA_OK;
+}
+
 int copy_in(pism_gpu_ssa *h, void *dst, const void *src, size_t bytes, int where) {
   CK(h, cudaMemcpyAsync(dst, src, bytes, where == PISM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                         h->stream));
@@ -1085,7 +1099,8 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->K32.rhs, h->K32.r, h->K32.rhat, h->K32.p, h->K32.v, h->K32.t, h->K32.phat,
                  h->K32.shat, h->K32.d, h->K32.st, h->res_dev, h->lfeat, h->lout, h->G.V, h->G.Z,
                  h->G.partials, h->G.gs, h->G.st, h->line.P, h->line.F, h->line.G, h->lpc.img, h->lpc.out,
-                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma, h->sb3d, h->mc};
+                 h->lpc.r, h->lpc.d, h->lpc.ad, h->lpc.part, h->lpc.rho, h->lpc.gamma, h->sb3d, h->mc,
+                 h->ec, h->ec_mask};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -1316,6 +1331,111 @@ int pism_gpu_ssa_mass_continuity_step(pism_gpu_ssa *h, double dt, const double *
     if (out[q] && where == PISM_MEM_HOST) RET(copy_out(h, out[q], dout[q], sizeof(double) * N, PISM_MEM_HOST));
   if (totals) RET(copy_out(h, totals, dtot, sizeof(double) * 8, PISM_MEM_HOST));
   CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_strain_rates(pism_gpu_ssa *h, const double *mask, double *edot, double *stresses, int where) {
+  if (!h) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (where != PISM_MEM_HOST && where != PISM_MEM_DEVICE) return fail(h, PISM_GPU_SSA_EINVAL, "bad memory kind");
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  const size_t N = h->N;
+  RET(ec_buffers(h));
+  const int8_t *m = h->mask;
+  if (mask) {
+    const double *dm = mask;
+    if (where == PISM_MEM_HOST) {
+      RET(copy_in(h, h->ec + EC_MASK * N, mask, sizeof(double) * N, PISM_MEM_HOST));
+      dm = h->ec + EC_MASK * N;
+    }
+    launch_mask_from_doubles(h->L, h->N, dm, h->ec_mask, nullptr);
+    m = h->ec_mask;
+  }
+  double *de = (edot && where == PISM_MEM_HOST) ? h->ec + EC_EDOT * N : edot;
+  double *ds = (stresses && where == PISM_MEM_HOST) ? h->ec + EC_STRESS * N : stresses;
+  launch_strain_rates(h->L, h->g, h->cfg, h->vel, m, de, ds);
+  CK(h, cudaGetLastError());
+  if (edot && where == PISM_MEM_HOST) RET(copy_out(h, edot, de, sizeof(double) * 2 * N, PISM_MEM_HOST));
+  if (stresses && where == PISM_MEM_HOST) RET(copy_out(h, stresses, ds, sizeof(double) * 3 * N, PISM_MEM_HOST));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_eigen_calving(pism_gpu_ssa *h, double dt, double K, double *mask, double *Href, double *thickness,
+                               int where) {
+  if (!h || !mask || !Href || !thickness) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (where != PISM_MEM_HOST && where != PISM_MEM_DEVICE) return fail(h, PISM_GPU_SSA_EINVAL, "bad memory kind");
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  if (!(dt >= 0.0) || !(K >= 0.0)) return fail(h, PISM_GPU_SSA_EINVAL, "dt and eigen_calving_K must be >= 0");
+  RET(ec_buffers(h));
+  const size_t N = h->N;
+  double *dm = mask, *dHref = Href, *dH = thickness;
+  if (where == PISM_MEM_HOST) {
+    dm = h->ec + EC_MASK * N;
+    dHref = h->ec + EC_HREF * N;
+    dH = h->ec + EC_H * N;
+    RET(copy_in(h, dm, mask, sizeof(double) * N, PISM_MEM_HOST));
+    RET(copy_in(h, dHref, Href, sizeof(double) * N, PISM_MEM_HOST));
+    RET(copy_in(h, dH, thickness, sizeof(double) * N, PISM_MEM_HOST));
+  }
+  int8_t *m0 = h->ec_mask, *live = h->ec_mask + N;
+  int *changed = reinterpret_cast<int *>(h->ec + EC_SCALARS * N + 3);
+  launch_mask_from_doubles(h->L, h->N, dm, m0, live);
+  launch_eigen_calving_passes(h->L, h->g, h->vel, K, dt, dH, dHref, h->ec + EC_LOSS * N, m0, live);
+  // remove_narrow_tongues: sweep until no cell changes; a chain of dependent cells is at
+  // most N long, so N + 1 sweeps always reach the fixed point
+  for (size_t sweep = 0;; ++sweep) {
+    if (sweep > N) return fail(h, PISM_GPU_SSA_ECUDA, "remove_narrow_tongues did not settle");
+    CK(h, cudaMemsetAsync(changed, 0, sizeof(int), h->stream));
+    launch_tongue_sweep(h->L, h->g, m0, live, changed);
+    CK(h, cudaGetLastError());
+    int flag = 0;
+    RET(copy_out(h, &flag, changed, sizeof(int), PISM_MEM_HOST));
+    if (!flag) break;
+  }
+  launch_eigen_calving_finish(h->L, h->N, m0, live, dH, dm);
+  CK(h, cudaGetLastError());
+  if (where == PISM_MEM_HOST) {
+    RET(copy_out(h, mask, dm, sizeof(double) * N, PISM_MEM_HOST));
+    RET(copy_out(h, Href, dHref, sizeof(double) * N, PISM_MEM_HOST));
+    RET(copy_out(h, thickness, dH, sizeof(double) * N, PISM_MEM_HOST));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  return PISM_GPU_SSA_OK;
+}
+
+int pism_gpu_ssa_eigen_calving_max_timestep(pism_gpu_ssa *h, double K, const double *mask, double *result,
+                                            int where) {
+  if (!h || !mask || !result) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (where != PISM_MEM_HOST && where != PISM_MEM_DEVICE) return fail(h, PISM_GPU_SSA_EINVAL, "bad memory kind");
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  if (!(K >= 0.0)) return fail(h, PISM_GPU_SSA_EINVAL, "eigen_calving_K must be >= 0");
+  RET(ec_buffers(h));
+  const size_t N = h->N;
+  const double *dm = mask;
+  if (where == PISM_MEM_HOST) {
+    RET(copy_in(h, h->ec + EC_MASK * N, mask, sizeof(double) * N, PISM_MEM_HOST));
+    dm = h->ec + EC_MASK * N;
+  }
+  double *stats = h->ec + EC_SCALARS * N;   // count, sum of rates, maximum rate (bits)
+  CK(h, cudaMemsetAsync(stats, 0, 3 * sizeof(double), h->stream));
+  launch_mask_from_doubles(h->L, h->N, dm, h->ec_mask, nullptr);
+  launch_eigen_calving_rates(h->L, h->g, h->vel, h->ec_mask, K, stats,
+                             reinterpret_cast<unsigned long long *>(stats + 2));
+  CK(h, cudaGetLastError());
+  double s[3];
+  RET(copy_out(h, s, stats, sizeof(s), PISM_MEM_HOST));
+  // PISMEigenCalving.cc:324-340, with units::convert's year of 31556925.9747 s
+  const double secpera = 31556925.9747, dx = h->grid.dx, dy = h->grid.dy;
+  const double count = s[0], rmax = s[2], mean = count > 0.0 ? s[1] / count : 0.0;
+  const double epsilon = 0.001 / (dx + dy) / secpera, dt_min = 0.001 * secpera;
+  const double dt = 1.0 / (rmax / dx + epsilon);
+  result[0] = std::max(dt, dt_min);
+  result[1] = rmax;
+  result[2] = mean;
+  result[3] = count;
   return PISM_GPU_SSA_OK;
 }
 

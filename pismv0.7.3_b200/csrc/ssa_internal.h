@@ -168,6 +168,17 @@ void launch_mass_continuity(const Launch &L, const GridDev &g, const pism_gpu_ss
                             double dt, double icefree_thickness, double is_floating_thickness, const double *cmb,
                             const double *bmr, const double *area, double *Hnew, double *fdiv, double *mask_new,
                             double *surface_new, double *totals);
+// ---- strain rates, 2-D stresses and eigen-calving (ssa_calving.cu) ----
+void launch_strain_rates(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, const double2 *vel,
+                         const int8_t *mask, double *edot, double *stress);
+void launch_mask_from_doubles(const Launch &L, int N, const double *in, int8_t *a, int8_t *b);
+void launch_eigen_calving_passes(const Launch &L, const GridDev &g, const double2 *vel, double K, double dt,
+                                 double *H, double *Href, double *loss, int8_t *m0, int8_t *live);
+void launch_tongue_sweep(const Launch &L, const GridDev &g, const int8_t *m0, int8_t *live, int *changed);
+void launch_eigen_calving_finish(const Launch &L, int N, const int8_t *m0, const int8_t *live, double *H,
+                                 double *mask_out);
+void launch_eigen_calving_rates(const Launch &L, const GridDev &g, const double2 *vel, const int8_t *mask, double K,
+                                double *out, unsigned long long *rmax);
 constexpr int SB3D_MAX_LEVELS = 800;   // the column kernel's shared-memory tile holds 32 columns
 int stress_balance_3d_prepare(int Mz);
 void launch_stress_balance_3d(const Launch &L, const GridDev &g, const pism_gpu_ssa_config &c, int Mz,

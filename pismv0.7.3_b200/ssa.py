@@ -329,6 +329,62 @@ class SSAFD:
         res["totals"] = dict(zip(self.MASS_TOTALS, list(totals)))
         return res
 
+    def strain_rates(self, mask=None, edot: bool = True, stresses: bool = True, device: bool = False) -> dict:
+        """ShallowStressBalance::compute_2D_principal_strain_rates and compute_2D_stresses
+        (ShallowStressBalance.cc:224-386) of the current velocity on `mask` (None: the
+        inputs' mask): "edot" [Mx, My, 2] (max, min; 1/s) and "stresses" [Mx, My, 3] (Pa)."""
+        on_device = device or _is_device(mask)
+        shape = self.shape
+        m = _Buf(mask, shape)
+        if m.device is not None and m.device != on_device:
+            raise ValueError("mask and outputs must both be on the host or both on the device")
+        want = {"edot": (edot, 2), "stresses": (stresses, 3)}
+        out = {}
+        for k, (on, d) in want.items():
+            if not on:
+                continue
+            if on_device:
+                import torch
+                out[k] = torch.empty((*shape, d), dtype=torch.float64, device=f"cuda:{self.device}")
+            else:
+                out[k] = np.empty((*shape, d))
+        bufs = {k: _Buf(v, v.shape) for k, v in out.items()}
+        where = _capi.MEM_DEVICE if on_device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_strain_rates(self._h, m.ptr, bufs["edot"].ptr if "edot" in bufs else None,
+                                                       bufs["stresses"].ptr if "stresses" in bufs else None, where),
+                    "compute_2D_principal_strain_rates")
+        return {k: (bufs[k].keep if on_device else out[k]) for k in out}
+
+    def eigen_calving(self, dt: float, K: float, mask, Href, thickness) -> dict:
+        """EigenCalving::update (PISMEigenCalving.cc:77-235) over dt seconds with constant K
+        (m s) on the current velocity: returns the new "mask", "Href" and "thickness" (the
+        caller's arrays are not changed).  Host arrays or CUDA tensors, all of one kind."""
+        shape = self.shape
+        kinds = {_is_device(a) for a in (mask, Href, thickness)}
+        if len(kinds) != 1:
+            raise ValueError("mask, Href and thickness must all be host arrays or all CUDA tensors")
+        on_device = kinds.pop()
+        # the library overwrites its arguments: hand it copies
+        if on_device:
+            import torch
+            bufs = [_Buf(a.to(torch.float64).reshape(shape).clone(), shape) for a in (mask, Href, thickness)]
+        else:
+            bufs = [_Buf(np.array(a, dtype=np.float64).reshape(shape), shape) for a in (mask, Href, thickness)]
+        where = _capi.MEM_DEVICE if on_device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_eigen_calving(self._h, float(dt), float(K), bufs[0].ptr, bufs[1].ptr,
+                                                        bufs[2].ptr, where), "EigenCalving::update")
+        return {k: b.keep for k, b in zip(("mask", "Href", "thickness"), bufs)}
+
+    def eigen_calving_max_timestep(self, K: float, mask) -> dict:
+        """EigenCalving::max_timestep (PISMEigenCalving.cc:249-341) on the current velocity:
+        "dt" (s), "max_rate", "mean_rate" (m/s) and "count" of calving cells."""
+        m = _Buf(mask, self.shape)
+        res = (C.c_double * 4)()
+        where = _capi.MEM_DEVICE if m.device else _capi.MEM_HOST
+        self._check(self.lib.pism_gpu_ssa_eigen_calving_max_timestep(self._h, float(K), m.ptr, C.cast(res, _D), where),
+                    "EigenCalving::max_timestep")
+        return dict(zip(("dt", "max_rate", "mean_rate", "count"), list(res)))
+
     # ---- stage methods (one reference method each) ----
     def assemble_rhs(self):
         self._check(self.lib.pism_gpu_ssa_assemble_rhs(self._h), "assemble_rhs")
@@ -437,3 +493,46 @@ class StressBalance:
 
     def volumetric_strain_heating(self):
         return self._field("strain_heating")
+
+    def compute_2D_principal_strain_rates(self, mask=None):
+        """ShallowStressBalance::compute_2D_principal_strain_rates (ShallowStressBalance.cc:224-305)
+        of the advective velocity: [Mx, My, 2], (max, min) eigenvalue (1/s)."""
+        return self.ssa.strain_rates(mask, edot=True, stresses=False, device=self.device_outputs)["edot"]
+
+    def compute_2D_stresses(self, mask=None):
+        """ShallowStressBalance::compute_2D_stresses (ShallowStressBalance.cc:308-386):
+        [Mx, My, 3] deviatoric stresses (Pa)."""
+        return self.ssa.strain_rates(mask, edot=False, stresses=True, device=self.device_outputs)["stresses"]
+
+
+class EigenCalving:
+    """calving::EigenCalving (PISMEigenCalving.hh) over a StressBalance: update() applies the
+    eigen-calving step to the model's mask, Href and thickness in place (numpy arrays or CUDA
+    tensors); max_timestep() returns the CFL time step, None unless cfl_eigen_calving."""
+
+    def __init__(self, stress_balance: StressBalance, K: float = 0.0, restrict_timestep: bool = False):
+        g = stress_balance.ssa.grid
+        if abs(g.dx - g.dy) / min(g.dx, g.dy) > 1e-2:   # EigenCalving::init, PISMEigenCalving.cc:63-69
+            raise SSAError("eigen_calving using a non-square grid cell is not implemented")
+        self.stress_balance = stress_balance
+        self.K = float(K)                         # eigen_calving_K (m s), pism_config.cdl:581-585
+        self.restrict_timestep = restrict_timestep   # cfl_eigen_calving
+        self.last_rates = None
+
+    def update(self, dt, pism_mask, Href, ice_thickness):
+        """EigenCalving::update(dt, pism_mask, Href, ice_thickness) (PISMEigenCalving.cc:77-235)."""
+        out = self.stress_balance.ssa.eigen_calving(dt, self.K, pism_mask, Href, ice_thickness)
+        for name, dst in (("mask", pism_mask), ("Href", Href), ("thickness", ice_thickness)):
+            if _is_device(dst):
+                dst.copy_(out[name].reshape(dst.shape))
+            else:
+                dst[...] = np.asarray(out[name]).reshape(dst.shape)
+
+    def max_timestep(self, mask):
+        """EigenCalving::max_timestep (PISMEigenCalving.cc:249-341) for the model's mask: the
+        allowed time step in seconds, or None (no restriction) unless cfl_eigen_calving; the
+        rates behind it are kept in last_rates."""
+        if not self.restrict_timestep:
+            return None
+        self.last_rates = self.stress_balance.ssa.eigen_calving_max_timestep(self.K, mask)
+        return self.last_rates["dt"]

@@ -238,6 +238,84 @@ def exact_velocity_v(grid: GridDesc):
     return out
 
 
+_LIN = {"L": 50.0e3, "H0": 500.0, "nu0": 30.0 * 1.0e6 * SECPERA, "tauc0": 1.0e4, "v0": 100.0 / SECPERA}
+
+
+def build_test_linear(Mx: int = 61, My: int = 61, cfg: SSAConfig | None = None):
+    """SSATestCaseExp (ssa_test_linear.cc:52-118): flat 500 m slab, linearly viscous till
+    (pseudo-plastic, q = 1), nu H fixed at nu0 H0 by the strength extension, exact
+    u = v0 exp(-alpha (x - L)) prescribed on the edges."""
+    L, H0, nu0, tauc0 = _LIN["L"], _LIN["H0"], _LIN["nu0"], _LIN["tauc0"]
+    grid = GridDesc.shallow(Mx, My, L, L, periodicity=0)
+    cfg = (cfg or SSAConfig()).copy()
+    cfg.do_pseudo_plastic_till = True
+    cfg.pseudo_plastic_q = 1.0
+    # the strength extension covers every thickness, so the hardness never enters: the
+    # isothermal law stands for the test case's flow law on its all-zero enthalpy
+    cfg.flow_law = "isothermal_glen"
+    # set_notional_strength(nu0 H0), then set_min_thickness(4000 * 10), which keeps nu H
+    cfg.min_thickness_strength_extension_ssa = 4000.0 * 10
+    cfg.constant_nu_strength_extension_ssa = nu0 * H0 / cfg.min_thickness_strength_extension_ssa
+    cfg.compute_surf_grad_inward_ssa = True
+    f = _empty_fields(Mx, My)
+    f["thickness"][:] = H0
+    f["surface"][:] = H0
+    f["tauc"][:] = tauc0
+    exact = exact_velocity_linear(grid, cfg)
+    I, J = np.meshgrid(np.arange(Mx), np.arange(My), indexing="ij")
+    edge = (J == 0) | (J == My - 1) | (I == 0) | (I == Mx - 1)
+    f["bc_mask"] = edge.astype(np.float64)
+    f["bc_values"] = np.where(edge[..., None], exact, 0.0)
+    return grid, cfg, f
+
+
+def exact_velocity_linear(grid: GridDesc, cfg: SSAConfig):
+    """SSATestCaseExp::exactSolution, ssa_test_linear.cc:120-130."""
+    alpha = math.sqrt((_LIN["tauc0"] / cfg.pseudo_plastic_uthreshold) / (4 * _LIN["nu0"] * _LIN["H0"]))
+    X, _ = np.meshgrid(grid.x_coords(), grid.y_coords(), indexing="ij")
+    out = np.zeros((grid.Mx, grid.My, 2))
+    out[..., 0] = _LIN["v0"] * np.exp(-alpha * (X - _LIN["L"]))
+    return out
+
+
+_PLUG = {"H0": 2000.0, "L": 50.0e3, "dhdx": 0.001, "B0": 3.7e8}
+
+
+def build_test_plug(Mx: int = 11, My: int = 61, glen_n: float = 3.0, cfg: SSAConfig | None = None):
+    """SSATestCasePlug (ssa_test_plug.cc:55-158): a 2000 m slab on a uniform slope, no basal
+    resistance, Dirichlet edges from the exact plug-flow speed."""
+    H0, L, dhdx, B0 = _PLUG["H0"], _PLUG["L"], _PLUG["dhdx"], _PLUG["B0"]
+    grid = GridDesc.shallow(Mx, My, L, L, periodicity=0)
+    cfg = (cfg or SSAConfig()).copy()
+    cfg.flow_law = "isothermal_glen"
+    cfg.ice_softness = B0 ** (-glen_n)
+    cfg.compute_surf_grad_inward_ssa = True
+    cfg.epsilon_ssa = 0.0
+    nuH = cfg.constant_nu_strength_extension_ssa * cfg.min_thickness_strength_extension_ssa
+    cfg.min_thickness_strength_extension_ssa = H0 / 2   # set_min_thickness keeps nu H
+    cfg.constant_nu_strength_extension_ssa = nuH / cfg.min_thickness_strength_extension_ssa
+    f = _empty_fields(Mx, My)
+    X, _ = np.meshgrid(grid.x_coords(), grid.y_coords(), indexing="ij")
+    f["thickness"][:] = H0
+    f["bed"] = -X * dhdx
+    f["surface"] = f["bed"] + H0
+    exact = exact_velocity_plug(grid, cfg)
+    I, J = np.meshgrid(np.arange(Mx), np.arange(My), indexing="ij")
+    edge = (J == 0) | (J == My - 1) | (I == 0) | (I == Mx - 1)
+    f["bc_mask"] = edge.astype(np.float64)
+    f["bc_values"] = np.where(edge[..., None], exact, 0.0)
+    return grid, cfg, f
+
+
+def exact_velocity_plug(grid: GridDesc, cfg: SSAConfig):
+    """SSATestCasePlug::exactSolution, ssa_test_plug.cc:160-168 (the cube is Glen's n = 3)."""
+    f = cfg.ice_density * cfg.standard_gravity * _PLUG["H0"] * _PLUG["dhdx"]
+    _, Y = np.meshgrid(grid.x_coords(), grid.y_coords(), indexing="ij")
+    out = np.zeros((grid.Mx, grid.My, 2))
+    out[..., 0] = 0.5 * f ** 3 * _PLUG["L"] ** 4 / (_PLUG["B0"] * _PLUG["H0"]) ** 3 * (1 - (Y / _PLUG["L"]) ** 4)
+    return out
+
+
 def report(velocity: np.ndarray, exact: np.ndarray) -> dict:
     """SSATestCase::report (SSATestCase.cc:173-253): error norms in m/year and percent."""
     uerr = np.abs(velocity[..., 0] - exact[..., 0])

@@ -9,8 +9,9 @@ What it records (nothing here is run at test time; the JSON is committed):
 
 * the verification-test error tables that the reference's regression scripts
   diff against (test/regression/ssa/ssa_testi_fd.sh, ssa_testj_fd.sh,
-  ssa_test_cfbc.sh), parsed from the scripts' heredocs, with the command-line
-  options each was produced with;
+  ssa_test_cfbc.sh; the SSAFEM scripts ssa_testi_fem.sh, ssa_testj_fem.sh,
+  ssafem_test_linear.sh, ssafem_test_plug.sh), parsed from the scripts' heredocs, with
+  the command-line options each was produced with;
 * the test-I error table of doc/verif/I_userman_may2012.nc (FD solver, Mx = 5);
 * the flow-law tables of test/regression/test_20.sh (gpbld), test_21.sh (pb),
   test_24.sh (hooke) and test_26.sh (arr);
@@ -78,6 +79,17 @@ def main(ref):
         "cases": [dict(Mx=M, My=3, **row) for M, row in zip((201, 401), parse_error_tables(
             os.path.join(ssa, "ssa_test_cfbc.sh")))],
     }
+    # the SSAFEM regression tables (ssa_method fem, -ksp_type cg, 2 ranks)
+    for key, script, sizes in (("test_i_fem", "ssa_testi_fem.sh", ((5, 61), (5, 121))),
+                               ("test_j_fem", "ssa_testj_fem.sh", ((61, 61), (121, 121))),
+                               ("linear_fem", "ssafem_test_linear.sh", ((61, 61), (121, 121))),
+                               ("plug_fem", "ssafem_test_plug.sh", ((22, 31), (61, 61)))):
+        out[key] = {
+            "script": "test/regression/ssa/" + script,
+            "options": {"ssa_method": "fem", "ksp_type": "cg", "mpi_ranks": 2},
+            "cases": [dict(Mx=Mx, My=My, **row) for (Mx, My), row in zip(sizes, parse_error_tables(
+                os.path.join(ssa, script)))],
+        }
     # verification table of the user manual
     from scipy.io import netcdf_file
     f = netcdf_file(os.path.join(ref, "doc/verif/I_userman_may2012.nc"), "r", mmap=False)
