@@ -346,6 +346,43 @@ int pism_gpu_ssa_eigen_calving(pism_gpu_ssa *h, double dt, double K, double *mas
 int pism_gpu_ssa_eigen_calving_max_timestep(pism_gpu_ssa *h, double K, const double *mask, double *result,
                                             int where);
 
+/* ---- SSAFEM: the Q1 finite-element SSA (SSAFEM.cc:151-840) on the same handle ----------- */
+
+/* The nonlinear and linear solver settings of SSAFEM::solve.  The reference hands F(u) = 0
+ * to PETSc's SNES (Newton with a line search); here Newton steps with a backtracking line
+ * search on ||F||, each linear solve by conjugate gradients preconditioned by the inverse
+ * 2 x 2 diagonal blocks (the regression tests' -ksp_type cg). */
+typedef struct pism_gpu_ssafem_options {
+  double snes_rtol;              /* converged when ||F|| <= snes_rtol ||F(u0)|| (PETSc 1e-8)    */
+  double snes_stol;              /* ... or when a step is below snes_stol ||u|| (PETSc 1e-8)    */
+  int snes_max_it;               /* Newton steps (200, SSAFEM.cc:91-95)                        */
+  double ksp_rtol;               /* linear solve: ||r|| <= ksp_rtol ||F|| (PETSc 1e-5)          */
+  int ksp_max_it;                /* CG iterations per Newton step (10000)                      */
+  double dirichlet_scale;        /* -ssa_fe_dirichlet_scale (1e9, SSAFEM.cc:128-131)           */
+  double icefree_thickness;      /* mask_icefree_thickness_standard (GeometryCalculator)       */
+  double is_floating_thickness;  /* mask_is_floating_thickness_standard                        */
+} pism_gpu_ssafem_options;
+
+typedef struct pism_gpu_ssafem_stats {
+  int converged;                 /* 1: ||F|| test, 2: step test; 0: not converged               */
+  int newton_iterations, ksp_iterations;
+  double fnorm0, fnorm;          /* ||F|| at the initial guess and at the answer                */
+} pism_gpu_ssafem_stats;
+
+void pism_gpu_ssafem_options_defaults(pism_gpu_ssafem_options *o);
+
+/* SSAFEM::solve (SSAFEM.cc:170-232): the coefficients at the quadrature points
+ * (cacheQuadPtValues, SSAFEM.cc:233-375: thickness, bed, tau_c, the driving stress
+ * -rho g H grad(surface), the GeometryCalculator mask and the column-averaged hardness), then
+ * Newton on the weak-form residual (compute_local_function, :441-532) with its Jacobian
+ * (compute_local_jacobian, :571-700), from the handle's current velocity (its initial guess or
+ * the last solve's answer) to the handle's velocity.  Inputs are those of
+ * pism_gpu_ssa_set_inputs (mask, melange and the CFBC are not used by this discretisation);
+ * Dirichlet data where bc_mask is 1.  stats may be NULL.  Returns PISM_GPU_SSA_EPICARD when
+ * the nonlinear solve does not converge ("SSAFEM solve failed to converge") and
+ * PISM_GPU_SSA_EKSP when a linear solve breaks down or reaches ksp_max_it. */
+int pism_gpu_ssafem_solve(pism_gpu_ssa *h, const pism_gpu_ssafem_options *o, pism_gpu_ssafem_stats *stats);
+
 /* Stage entry points, each the device restatement of one reference method, for
  * stage-by-stage checking:
  *   assemble_rhs       -> SSA::compute_driving_stress + SSAFD::assemble_rhs

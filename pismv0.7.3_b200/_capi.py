@@ -7,7 +7,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from .config import CConfig, CGrid, CInputs, CMember, CStats
+from .config import CConfig, CFemOptions, CFemStats, CGrid, CInputs, CMember, CStats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libpism_ssa_gpu.so")
@@ -28,6 +28,7 @@ EXPORTS = [
     "pism_gpu_ssa_apply", "pism_gpu_ssa_apply_preconditioner", "pism_gpu_ssa_linear_solve",
     "pism_gpu_ssa_linear_solve_rhs", "pism_gpu_ssa_stress_balance_3d", "pism_gpu_ssa_mass_continuity_step",
     "pism_gpu_ssa_strain_rates", "pism_gpu_ssa_eigen_calving", "pism_gpu_ssa_eigen_calving_max_timestep",
+    "pism_gpu_ssafem_options_defaults", "pism_gpu_ssafem_solve",
     "pism_gpu_ssa_nuH_noalloc", "pism_gpu_ssa_solve_batch",
 ]
 # every symbol include/pism_unet_gpu.h declares
@@ -73,6 +74,8 @@ def load() -> C.CDLL:
         "pism_gpu_ssa_strain_rates": (I, [V, P(D), P(D), P(D), I]),
         "pism_gpu_ssa_eigen_calving": (I, [V, D, D, P(D), P(D), P(D), I]),
         "pism_gpu_ssa_eigen_calving_max_timestep": (I, [V, D, P(D), P(D), I]),
+        "pism_gpu_ssafem_options_defaults": (None, [P(CFemOptions)]),
+        "pism_gpu_ssafem_solve": (I, [V, P(CFemOptions), P(CFemStats)]),
         "pism_gpu_ssa_nuH_noalloc": (I, [P(CGrid), P(CConfig), V, V, V, V, V, V, D, D, V, V, V, V]),
         "pism_gpu_ssa_solve_batch": (I, [V, V, I, I, P(CMember), P(CStats)]),
         "pism_gpu_unet_param_count": (C.c_longlong, []),

@@ -20,7 +20,8 @@ LIB = os.path.join(HERE, "lib")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 CU_SOURCES = ["ssa_kernels.cu", "ssa_mg.cu", "ssa_mixed.cu", "ssa_line.cu", "ssa_control.cu", "ssa_capi.cu", "ssa_noalloc.cu", "unet.cu",
-              "ssa_column.cu", "ssa_transport.cu", "ssa_calving.cu"]
+              "ssa_column.cu", "ssa_transport.cu", "ssa_calving.cu",
+              "ssa_fem.cu"]
 
 
 def _newer(target, sources):

@@ -182,6 +182,21 @@ class CStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class CFemOptions(C.Structure):
+    """pism_gpu_ssafem_options"""
+    _fields_ = [("snes_rtol", _D), ("snes_stol", _D), ("snes_max_it", _I), ("ksp_rtol", _D), ("ksp_max_it", _I),
+                ("dirichlet_scale", _D), ("icefree_thickness", _D), ("is_floating_thickness", _D)]
+
+
+class CFemStats(C.Structure):
+    """pism_gpu_ssafem_stats"""
+    _fields_ = [("converged", _I), ("newton_iterations", _I), ("ksp_iterations", _I), ("fnorm0", _D),
+                ("fnorm", _D)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 @dataclass
 class GridDesc:
     Mx: int

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +15,7 @@
 
 #include "pism_unet_gpu.h"
 #include "ssa_internal.h"
+#include "ssa_fem.h"
 #include "unet_internal.h"
 
 using namespace pism_gpu;
@@ -40,6 +42,7 @@ struct pism_gpu_ssa {
   double *mc = nullptr;     // staging of pism_gpu_ssa_mass_continuity_step: 7 fields and 8 totals
   double *ec = nullptr;     // staging of the strain rates and eigen-calving: 5 fields and 8 scalars
   int8_t *ec_mask = nullptr;   // eigen-calving's mask before and during remove_narrow_tongues
+  FemState fem{};              // the finite-element solve's state, allocated by its first call
   uint32_t *flags = nullptr;
   Krylov K{};
   Krylov32 K32{};
@@ -1103,6 +1106,7 @@ int pism_gpu_ssa_destroy(pism_gpu_ssa *h) {
                  h->ec, h->ec_mask};
   for (void *p : dev)
     if (p) cudaFree(p);
+  fem_free(h->fem);
   if (h->st_host) cudaFreeHost(h->st_host);
   if (h->norm_host) cudaFreeHost(h->norm_host);
   if (h->zd_host) cudaFreeHost(h->zd_host);
@@ -1437,6 +1441,123 @@ int pism_gpu_ssa_eigen_calving_max_timestep(pism_gpu_ssa *h, double K, const dou
   result[2] = mean;
   result[3] = count;
   return PISM_GPU_SSA_OK;
+}
+
+void pism_gpu_ssafem_options_defaults(pism_gpu_ssafem_options *o) {
+  if (!o) return;
+  o->snes_rtol = 1e-8;
+  o->snes_stol = 1e-8;
+  o->snes_max_it = 200;
+  o->ksp_rtol = 1e-5;
+  o->ksp_max_it = 10000;
+  o->dirichlet_scale = 1.0e9;
+  o->icefree_thickness = 0.01;       // pism_config.cdl mask_icefree_thickness_standard
+  o->is_floating_thickness = 1.0;    // pism_config.cdl mask_is_floating_thickness_standard
+}
+
+int pism_gpu_ssafem_solve(pism_gpu_ssa *h, const pism_gpu_ssafem_options *o, pism_gpu_ssafem_stats *stats) {
+  if (!h || !o) return PISM_GPU_SSA_EINVAL;
+  DeviceGuard dg(h->device);
+  if (!h->inputs_set) return fail(h, PISM_GPU_SSA_ESTATE, "pism_gpu_ssa_set_inputs was not called");
+  if (h->cfg.flow_law != PISM_FLOW_LAW_ISOTHERMAL_GLEN && !h->have_enthalpy)
+    return fail(h, PISM_GPU_SSA_EINVAL, "the flow law needs enthalpy");
+  if (h->grid.Mx < 2 || h->grid.My < 2) return fail(h, PISM_GPU_SSA_EINVAL, "SSAFEM needs Mx, My >= 2");
+  if (!(o->snes_rtol >= 0.0) || !(o->snes_stol >= 0.0) || o->snes_max_it < 0 || !(o->ksp_rtol > 0.0) ||
+      o->ksp_max_it < 1 || !(o->dirichlet_scale > 0.0))
+    return fail(h, PISM_GPU_SSA_EINVAL, "bad SSAFEM options");
+  FemState &S = h->fem;
+  if (fem_allocate(S, h->grid.Mx, h->grid.My, h->grid.periodicity) != 0)
+    return fail(h, PISM_GPU_SSA_ENOMEM, "SSAFEM buffers");
+  FemProblem P;
+  P.Mx = h->grid.Mx;
+  P.My = h->grid.My;
+  P.periodicity = h->grid.periodicity;
+  P.c = h->cfg;
+  P.W = fem_germs(h->grid.dx, h->grid.dy);
+  P.scale = o->dirichlet_scale;
+  P.notional_strength = h->cfg.constant_nu_strength_extension_ssa * h->cfg.min_thickness_strength_extension_ssa;
+  const Launch &L = h->L;
+  const int Mz = (int)h->z_host.size();
+  if (h->cfg.flow_law != PISM_FLOW_LAW_ISOTHERMAL_GLEN && Mz < 2)
+    return fail(h, PISM_GPU_SSA_EINVAL, "the column-averaged hardness needs a grid with Mz >= 2 levels");
+  launch_fem_coefficients(L, P, S, h->H, h->bed, h->tauc, h->srf, h->have_enthalpy ? h->enthalpy : nullptr,
+                          h->z_dev, Mz, o->icefree_thickness, o->is_floating_thickness);
+  CK(h, cudaMemsetAsync(S.zero_pivot, 0, sizeof(int), h->stream));
+  FemScalars sc{};
+  FemCG cg{};
+  pism_gpu_ssafem_stats st{};
+  double2 *vel = h->vel;
+  launch_fem_residual(L, P, S, vel, S.F, false, h->bc, h->bcv);
+  CK(h, cudaGetLastError());
+  RET(copy_out(h, &sc, S.sc, sizeof(sc), PISM_MEM_HOST));
+  double fn = sqrt(sc.f2);
+  st.fnorm0 = fn;
+  const double f0 = fn;
+  int rc = PISM_GPU_SSA_OK;
+  // SNES Newton (SNESNEWTONLS): the convergence tests of SNESConvergedDefault with atol 0
+  while (true) {
+    if (!std::isfinite(fn)) {
+      rc = fail(h, PISM_GPU_SSA_ENAN, "SSAFEM: non-finite residual");
+      break;
+    }
+    if (fn <= o->snes_rtol * f0 || fn == 0.0) {
+      st.converged = 1;
+      break;
+    }
+    if (st.newton_iterations >= o->snes_max_it) {
+      rc = fail(h, PISM_GPU_SSA_EPICARD, "SSAFEM solve failed to converge (%d Newton steps, ||F|| %g of %g)",
+                st.newton_iterations, fn, f0);
+      break;
+    }
+    // the Jacobian at the current iterate (its residual is the one already held)
+    launch_fem_residual(L, P, S, vel, S.F, true, h->bc, h->bcv);
+    launch_fem_cg_init(L, P, S, o->ksp_rtol, o->ksp_max_it);
+    CK(h, cudaGetLastError());
+    int zp = 0;
+    RET(copy_out(h, &zp, S.zero_pivot, sizeof(int), PISM_MEM_HOST));
+    if (zp) {
+      rc = fail(h, PISM_GPU_SSA_EZERODIAG, "SSAFEM: singular diagonal block at node %d", zp - 1);
+      break;
+    }
+    // conjugate gradients in batches; each iteration is skipped on the device once done
+    for (;;) {
+      launch_fem_cg_iterations(L, P, S, 16);
+      CK(h, cudaGetLastError());
+      RET(copy_out(h, &cg, S.cg, sizeof(cg), PISM_MEM_HOST));
+      if (cg.done) break;
+    }
+    st.ksp_iterations += cg.its;
+    if (cg.done != 1) {
+      rc = fail(h, PISM_GPU_SSA_EKSP, "SSAFEM: the linear solve %s after %d iterations",
+                cg.done == 2 ? "broke down (J not positive definite)" : "reached ksp_max_it", cg.its);
+      break;
+    }
+    // backtracking line search on ||F||
+    double lambda = 1.0, ft = 0.0;
+    for (;;) {
+      launch_fem_trial(L, S, vel, lambda);
+      launch_fem_residual(L, P, S, S.trial, S.Ft, false, h->bc, h->bcv);
+      CK(h, cudaGetLastError());
+      RET(copy_out(h, &sc, S.sc, sizeof(sc), PISM_MEM_HOST));
+      ft = sqrt(sc.f2);
+      if (ft < (1.0 - 1e-4 * lambda) * fn || lambda < 1e-6) break;
+      lambda *= 0.5;
+    }
+    // accept the step: the trial point becomes the iterate
+    CK(h, cudaMemcpyAsync(vel, S.trial, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(S.F, S.Ft, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
+    st.newton_iterations += 1;
+    const double prev = fn;
+    fn = ft;
+    if (sqrt(sc.step2) <= o->snes_stol * sqrt(sc.x2) && fn <= prev) {
+      st.converged = 2;
+      break;
+    }
+  }
+  st.fnorm = fn;
+  if (stats) *stats = st;
+  CK(h, cudaStreamSynchronize(h->stream));
+  return rc;
 }
 
 int pism_gpu_ssa_assemble_rhs(pism_gpu_ssa *h) {

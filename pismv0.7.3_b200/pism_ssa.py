@@ -59,8 +59,8 @@ class Config:
 
     def set_string(self, name, value):
         if name == "ssa_method":
-            if value not in ("fd", "gpu"):
-                raise ValueError("this solver restates SSAFD only (ssa_method fd)")
+            if value not in ("fd", "fem", "gpu"):
+                raise ValueError(f"unknown ssa_method {value} (fd or fem)")
             self.ssa_method = value
             return
         setattr(self.cfg, self._field(name), value)
@@ -229,8 +229,10 @@ class SSARun:
         raise NotImplementedError()
 
     def _constructSSA(self):
-        """SSAFD on the B200 (ssa_method "fd"; the reference's SSAFEM is not restated)."""
-        from .ssa import SSAFD
+        """SSAFD on the B200, or SSAFEM with ssa_method "fem" (PISM/ssa.py's SSAFactory choice)."""
+        from .ssa import SSAFD, SSAFEM
+        if self.config.get_string("ssa_method") == "fem":
+            return SSAFEM(self.grid.desc, self.config.cfg)
         return SSAFD(self.grid.desc, self.config.cfg)
 
     def _initSSA(self):

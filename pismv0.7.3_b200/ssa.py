@@ -20,7 +20,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from .config import CInputs, CMember, CStats, GridDesc, SSAConfig
+from .config import CFemOptions, CFemStats, CInputs, CMember, CStats, GridDesc, SSAConfig
 
 _D = C.POINTER(C.c_double)
 
@@ -536,3 +536,41 @@ class EigenCalving:
             return None
         self.last_rates = self.stress_balance.ssa.eigen_calving_max_timestep(self.K, mask)
         return self.last_rates["dt"]
+
+
+class SSAFEMFailure(SSAError):
+    """SSAFEM::solve's "SSAFEM solve failed to converge" (SSAFEM.cc:179-183)."""
+
+
+class SSAFEM(SSAFD):
+    """pism::stressbalance::SSAFEM (SSAFEM.hh) on the B200: the Q1 finite-element SSA, with the
+    inputs, boundary conditions, initial guess and getters of SSAFD; solve() runs Newton on
+    the weak form from the current velocity (SSAFEM::solve, SSAFEM.cc:170-232).  The
+    nonlinear and linear settings are `options` (pism_gpu_ssafem_options)."""
+
+    def __init__(self, grid: GridDesc, config: SSAConfig | None = None, device: int = 0, **options):
+        super().__init__(grid, config, device)
+        self.options = CFemOptions()
+        self.lib.pism_gpu_ssafem_options_defaults(C.byref(self.options))
+        self.options.icefree_thickness = self.config.mask_icefree_thickness_standard
+        self.options.is_floating_thickness = self.config.mask_is_floating_thickness_standard
+        for k, v in options.items():
+            setattr(self.options, k, v)
+        self._fem_stats = CFemStats()
+
+    def solve(self, out=None):
+        """SSAFEM::solve; returns the velocity ([Mx, My, 2])."""
+        rc = self.lib.pism_gpu_ssafem_solve(self._h, C.byref(self.options), C.byref(self._fem_stats))
+        if rc == _capi.EPICARD:
+            msg = self.lib.pism_gpu_ssa_last_error(self._h).decode()
+            raise SSAFEMFailure(f"SSAFEM solve failed to converge: {msg}")
+        self._check(rc, "SSAFEM::solve")
+        return self.velocity(out)
+
+    def stats(self) -> dict:
+        return self._fem_stats.as_dict()
+
+
+def SSAFEMFactory(grid: GridDesc, config: SSAConfig | None = None) -> SSAFEM:
+    """The SSAFactory of the finite-element solver (SSAFEMFactory, SSAFEM.cc:105-107)."""
+    return SSAFEM(grid, config)

@@ -16,7 +16,7 @@ HEADER = os.path.join(REPO, "include", "pism_ssa_gpu.h")
 
 def declared_functions():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^(?:int|const char \*)\s*(pism_gpu_ssa_\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|void|const char \*)\s*(pism_gpu_ssa(?:fem)?_\w+)\s*\(", txt, flags=re.M)))
 
 
 @pytest.fixture(scope="module")
@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol(lib):
     assert len(decl) >= 15
     assert sorted(_capi.EXPORTS) == decl
     out = subprocess.run(["nm", "-D", "--defined-only", _capi.LIB_PATH], capture_output=True, text=True).stdout
-    exported = set(re.findall(r" T (pism_gpu_ssa_\w+)", out))
+    exported = set(re.findall(r" T (pism_gpu_ssa(?:fem)?_\w+)", out))
     missing = [d for d in decl if d not in exported]
     assert not missing, missing
     for d in decl:

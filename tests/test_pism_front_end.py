@@ -94,8 +94,10 @@ def test_config_names_and_grid():
     cfg.set_boolean("ssa_dirichlet_bc", True)
     assert cfg.get_boolean("ssa_dirichlet_bc")
     assert cfg.get_string("ssa_method") == "fd"
+    cfg.set_string("ssa_method", "fem")   # SSAFEM, the finite-element solver
+    assert cfg.get_string("ssa_method") == "fem"
     with pytest.raises(ValueError):
-        cfg.set_string("ssa_method", "fem")
+        cfg.set_string("ssa_method", "spectral")
     with pytest.raises(KeyError):
         cfg.get_double("no_such_parameter")
     g = P.Grid.Shallow(10e3, 5e3, 0, 0, 11, 6)
