@@ -339,6 +339,85 @@ def mass_roofline(vel, stream, flush, dev, peak, M=801, reps=20):
                       "the call's time includes the read-back of the totals and one stream synchronisation)"}
 
 
+def calving_point(vel, stream, flush, dev, peak, M=801, reps=20):
+    """The calving front's consumers of the velocity on the benchmark sheet, device buffers:
+    pism_gpu_ssa_strain_rates (principal strain rates and 2-D stresses; algorithmic bytes per
+    cell: velocity 16 and mask 1 read, 16 + 24 written, 57 B) and one eigen-calving step
+    (pism_gpu_ssa_eigen_calving with K = 1e17 m s over a year, remove_narrow_tongues
+    included; its time counts every sweep and the flag read-back after each)."""
+    import torch
+    from pism_b200.ssa import SSAFD
+    g, cl, f, _ = build_case(M)
+    s = SSAFD(g, cl, device=dev.index)
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)   # noqa: E731
+    try:
+        s.set_stream(stream.cuda_stream)
+        s.set_inputs(**{k: t(f[k]) for k in ("thickness", "surface", "bed", "mask", "tauc", "melange")})
+        s.set_initial_guess(vel)
+        mask, H = t(f["mask"]), t(f["thickness"])
+        href = torch.zeros_like(H)
+
+        def timed(fn):
+            fn()
+            ts = []
+            for _ in range(reps):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return float(np.median(ts))
+
+        ms_sr = timed(lambda: s.strain_rates(mask, device=True))
+        ms_ec = timed(lambda: s.eigen_calving(3.15e7, 1e17, mask, href, H))
+        cut = s.eigen_calving(3.15e7, 1e17, mask, href, H)
+        changed = int((cut["mask"] != mask).sum().item())
+    finally:
+        s.close()
+    nbytes = 57 * M * M
+    achieved = nbytes / (ms_sr * 1e-3) / 1e9
+    return {"grid": [M, M], "strain_rates_ms": ms_sr, "bytes_per_call": nbytes, "achieved": achieved,
+            "unit": "GB/s", "peak": peak, "frac": achieved / peak, "bound": "hbm",
+            "eigen_calving_ms": ms_ec, "cells_cut": changed,
+            "kernel": "k_strain_rates (one thread per cell); eigen-calving: k_ec_front, k_ec_cut, k_ec_tongues "
+                      "sweeps to their fixed point, k_ec_finish"}
+
+
+def ssafem_point(dev, stream, reps=3):
+    """SSAFEM (pism_gpu_ssafem_solve) at the reference's solver settings on two verification
+    grids larger than its regression tests: test J's periodic shelf at 241^2 (one Newton step,
+    a linear problem) and test I's plastic-till stream at 5 x 481 (Newton from zero)."""
+    import torch
+    from pism_b200 import verification as Ver
+    from pism_b200.ssa import SSAFEM
+    out = {}
+    for name, (g, c, f), exact in (("test_j_241", Ver.build_test_j(241, 241), Ver.exact_velocity_j),
+                                   ("test_i_5x481", Ver.build_test_i(My=481), Ver.exact_velocity_i)):
+        s = SSAFEM(g, c, device=dev.index)
+        try:
+            s.set_stream(stream.cuda_stream)
+            s.set_inputs(**{k: f[k] for k in ("thickness", "surface", "bed", "mask", "tauc")},
+                         bc_mask=f["bc_mask"], bc_values=f["bc_values"])
+            ts = []
+            for _ in range(reps):
+                s.set_initial_guess(np.zeros((g.Mx, g.My, 2)))
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                vel = s.solve()
+                ts.append((time.perf_counter() - t0) * 1e3)
+            st = s.stats()
+        finally:
+            s.close()
+        err = Ver.report(vel, exact(g))
+        out[name] = {"ms": float(np.median(ts)), "newton_iterations": st["newton_iterations"],
+                     "cg_iterations": st["ksp_iterations"], "converged": st["converged"],
+                     "maxvector_error_m_per_year": err["maxvector"]}
+    out["note"] = "wall time of the call (host loop with a read-back per Newton step and CG batch)"
+    return out
+
+
 # The host-core cost of the whole reference solve is sampled: the first CPU_SAMPLE_PICARD
 # Picard iterations of the native restatement (oracle/ssafd_cpu.cc: nu*H, drag, 18-column
 # assembly, PETSc-style GMRES(30) + block Jacobi / ILU(0), norms) run on the host cores, and
@@ -970,6 +1049,14 @@ def main():
             line["mass_continuity"] = mass_roofline(vel_mode, stream, flush, dev, peak)
         except Exception as e:   # noqa: BLE001 - reported in the line
             line["mass_continuity"] = {"error": str(e)[:200]}
+        try:
+            line["calving_front"] = calving_point(vel_mode, stream, flush, dev, peak)
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["calving_front"] = {"error": str(e)[:200]}
+        try:
+            line["ssafem"] = ssafem_point(dev, stream)
+        except Exception as e:   # noqa: BLE001 - reported in the line
+            line["ssafem"] = {"error": str(e)[:200]}
         try:
             line["ensemble"] = ensemble_point(stream, flush, dev)
         except Exception as e:   # noqa: BLE001 - reported in the line
