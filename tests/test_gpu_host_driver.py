@@ -50,9 +50,16 @@ def test_driver_test_v(goldens, k):
 
 def test_driver_learned_warm_start(tmp_path):
     """SSAFD_GPU::set_warm_start: starting test I from the learned guess ends at the same
-    answer once the Picard tolerance is tight (the table agrees to its printed digits)."""
+    answer once the Picard tolerance is tight: the tables agree to within one unit of their
+    last printed digit (two answers 1e-9 apart may round either side of a printed digit)."""
+    import re
     params = np.load(os.path.join(REPO, "pismv0.7.3_b200", "weights", "unet_ssa_10km.npz"))["params"]
     f32 = tmp_path / "unet.f32"
     params.astype(np.float32).tofile(f32)
     args = ("-test", "I", "-My", "61", "-ssa_rtol", "1e-9", "-ssafd_ksp_rtol", "1e-12")
-    assert run(*args, "-learned", str(f32)) == run(*args)
+    a, b = run(*args, "-learned", str(f32)), run(*args)
+    na, nb = re.findall(r"-?\d+\.\d+", a), re.findall(r"-?\d+\.\d+", b)
+    assert len(na) == len(nb) > 0
+    for x, y in zip(na, nb):
+        unit = 10.0 ** -len(x.split(".")[1])
+        assert abs(float(x) - float(y)) <= 1.01 * unit, (x, y)
