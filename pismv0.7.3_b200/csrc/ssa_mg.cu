@@ -274,111 +274,120 @@ __global__ void __launch_bounds__(NTm, 2) k_mg_build(LevelView F, int Mxc, int M
 }
 
 // Dense inverse of the coarsest operator (n = 2 N <= 32 unknowns) by Gauss-Jordan elimination
-// with partial pivoting, in place in shared memory, by one warp: lane r owns row r (rows
-// padded to 33 entries, so a column's entries of consecutive rows sit in different banks)
-// and every step is ordered by __syncwarp alone.  Written transposed, so that the per-cycle
-// product reads it coalesced.
+// with partial pivoting, in place in shared memory, by one thread block (rows padded to 33
+// entries, so a column's entries of consecutive rows sit in different banks).  Warp 0 finds
+// each pivot; the elimination spreads the n x n element updates of a step over the block,
+// reading the step's multipliers from a copy of the pivot column, so each element is updated
+// with the same operands in the same order whatever thread does it.  Written transposed, so
+// that the per-cycle product reads it coalesced.
 constexpr int CI_PAD = 2 * MG_MAX_COARSE_CELLS + 1;
 static_assert(2 * MG_MAX_COARSE_CELLS <= 32, "one lane per row of the coarsest operator");
 
-__device__ void coarse_invert_warp(const LevelView &L, double (*a)[CI_PAD], int *perm, double *invT_out,
-                                   int *singular) {
-  const int t = threadIdx.x & 31, n = 2 * L.N;
-  for (int r = 0; r < n; ++r)
-    if (t < n) a[r][t] = 0.0;
-  __syncwarp();
-  if (t < L.N) {   // each cell's two rows are written by one lane
-    const int k = t, i = k / L.My, j = k % L.My;
+struct CoarseInvertSmem {
+  double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
+  double fcol[2 * MG_MAX_COARSE_CELLS];
+  int perm[2 * MG_MAX_COARSE_CELLS];
+  int pivot;
+};
+
+__device__ void coarse_invert_block(const LevelView &L, CoarseInvertSmem &S, double *invT_out, int *singular) {
+  const int tid = threadIdx.x, nth = blockDim.x, n = 2 * L.N;
+  for (int q = tid; q < n * CI_PAD; q += nth) (&S.a[0][0])[q] = 0.0;
+  __syncthreads();
+  if (tid < L.N) {   // each cell's two rows are written by one thread
+    const int k = tid, i = k / L.My, j = k % L.My;
     for (int b = 0; b < 9; ++b) {
       const int di = (b % 3) - 1, dj = 1 - (b / 3);
       const int kn = wrap(i + di, L.Mx) * L.My + wrap(j + dj, L.My);
       const float4 v = L.A[b * L.N + k];
-      a[2 * k + 0][2 * kn + 0] += (double)v.x;
-      a[2 * k + 0][2 * kn + 1] += (double)v.y;
-      a[2 * k + 1][2 * kn + 0] += (double)v.z;
-      a[2 * k + 1][2 * kn + 1] += (double)v.w;
+      S.a[2 * k + 0][2 * kn + 0] += (double)v.x;
+      S.a[2 * k + 0][2 * kn + 1] += (double)v.y;
+      S.a[2 * k + 1][2 * kn + 0] += (double)v.z;
+      S.a[2 * k + 1][2 * kn + 1] += (double)v.w;
     }
   }
-  __syncwarp();
+  __syncthreads();
   for (int col = 0; col < n; ++col) {
-    double best = -1.0;
-    int bi = col;
-    if (col + t < n) {
-      best = fabs(a[col + t][col]);
-      bi = col + t;
-    }
-    for (int o = 16; o > 0; o >>= 1) {   // every lane ends with the same (largest, lowest row)
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
+    if (tid < 32) {   // the pivot: the largest |a[r][col]|, r >= col, lowest row on ties
+      const int t = tid;
+      double best = -1.0;
+      int bi = col;
+      if (col + t < n) {
+        best = fabs(S.a[col + t][col]);
+        bi = col + t;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (t == 0) {
+        S.perm[col] = bi;
+        S.pivot = bi;
+        if (!(best > 0.0)) *singular = 1;
       }
     }
-    if (t == 0) {
-      perm[col] = bi;
-      if (!(best > 0.0)) *singular = 1;
+    __syncthreads();
+    const int p = S.pivot;
+    if (p != col && tid < n) {   // thread t swaps column t of the two rows
+      const double tmp = S.a[col][tid];
+      S.a[col][tid] = S.a[p][tid];
+      S.a[p][tid] = tmp;
     }
-    const int p = bi;
-    if (p != col && t < n) {   // lane t swaps column t of the two rows
-      const double tmp = a[col][t];
-      a[col][t] = a[p][t];
-      a[p][t] = tmp;
-    }
-    __syncwarp();
-    const double pv = a[col][col];
+    __syncthreads();
+    const double pv = S.a[col][col];
     const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    __syncwarp();
-    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot)
-    if (t < n) a[col][t] = (t == col ? 1.0 : a[col][t]) * pinv;
-    __syncwarp();
-    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot.  The pivot
-    // row is read into registers first, so a lane's updates of its own row do not wait on
-    // reads that might alias them
-    double prow[2 * MG_MAX_COARSE_CELLS];
-#pragma unroll
-    for (int q = 0; q < 2 * MG_MAX_COARSE_CELLS; ++q) prow[q] = a[col][q];
-    if (t < n && t != col) {
-      const double f = a[t][col];
-#pragma unroll
-      for (int q = 0; q < 2 * MG_MAX_COARSE_CELLS; ++q)
-        if (q < n && q != col) a[t][q] -= f * prow[q];
-      a[t][col] = -a[t][col] * a[col][col];
+    __syncthreads();
+    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot); the
+    // multipliers of the other rows are copied before any of them changes
+    if (tid < n) {
+      S.a[col][tid] = (tid == col ? 1.0 : S.a[col][tid]) * pinv;
+      S.fcol[tid] = S.a[tid][col];
     }
-    __syncwarp();
+    __syncthreads();
+    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
+    for (int e = tid; e < n * n; e += nth) {
+      const int r = e / n, q = e - r * n;
+      if (r == col) continue;
+      const double f = S.fcol[r];
+      if (q != col) S.a[r][q] -= f * S.a[col][q];
+      else S.a[r][col] = -f * S.a[col][col];
+    }
+    __syncthreads();
   }
   // undo the row interchanges as column interchanges, in reverse order
   for (int col = n - 1; col >= 0; --col) {
-    const int p = perm[col];
-    if (p != col && t < n) {
-      const double tmp = a[t][col];
-      a[t][col] = a[t][p];
-      a[t][p] = tmp;
+    const int p = S.perm[col];
+    if (p != col && tid < n) {
+      const double tmp = S.a[tid][col];
+      S.a[tid][col] = S.a[tid][p];
+      S.a[tid][p] = tmp;
     }
-    __syncwarp();
+    __syncthreads();
   }
-  for (int q = t; q < n * n; q += 32) {
+  for (int q = tid; q < n * n; q += nth) {
     const int c = q / n, r = q - c * n;
-    invT_out[q] = a[r][c];   // invT[c][r] = inverse[r][c]
+    invT_out[q] = S.a[r][c];   // invT[c][r] = inverse[r][c]
   }
 }
 
 // the coarsest inverse alone (a hierarchy whose only coarse level is built from the fine grid)
-__global__ void __launch_bounds__(32) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
-  __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
-  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
-  coarse_invert_warp(L, a, perm, invT_out, singular);
+__global__ void __launch_bounds__(NTm) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
+  __shared__ CoarseInvertSmem S;
+  coarse_invert_block(L, S, invT_out, singular);
 }
 
 // The small levels' Galerkin operators (levels first .. nlev - 1, each from the level above it,
 // all of <= MG_CTA_CELLS cells) and the coarsest inverse in one launch on one thread-block
-// cluster: one cluster barrier (release / acquire at cluster scope) between levels, then warp 0
-// of CTA 0 inverts the coarsest operator.  The arithmetic of every cell is k_mg_build's.
+// cluster: one cluster barrier (release / acquire at cluster scope) between levels, then CTA 0
+// inverts the coarsest operator.  The arithmetic of every cell is k_mg_build's.
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
     k_mg_build_small(const LevelView *__restrict__ lev, int first, int nlev, double *invT_out, int *singular) {
   cg::cluster_group cluster = cg::this_cluster();
-  __shared__ double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
-  __shared__ int perm[2 * MG_MAX_COARSE_CELLS];
+  __shared__ CoarseInvertSmem S;
   const int rank = cluster.block_rank() * NTm + threadIdx.x, nthr = SMALL_CLUSTER * NTm;
   for (int c = first; c < nlev; ++c) {
     const LevelView F = lev[c - 1], C = lev[c];
@@ -388,7 +397,7 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
     }
     cluster.sync();
   }
-  if (cluster.block_rank() == 0 && threadIdx.x < 32) coarse_invert_warp(lev[nlev - 1], a, perm, invT_out, singular);
+  if (cluster.block_rank() == 0) coarse_invert_block(lev[nlev - 1], S, invT_out, singular);   // uniform in CTA 0
 }
 
 // ---------------------------------------------------------------------------
@@ -1280,7 +1289,7 @@ void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHier
     k_mg_build_small<<<SMALL_CLUSTER, NTm, 0, Lc.stream>>>(reinterpret_cast<const LevelView *>(H.views), cfirst,
                                                              H.nlev, H.cinv, H.singular);
   } else {
-    k_mg_coarse_invert<<<1, 32, 0, Lc.stream>>>(view(H.lev[H.nlev - 1]), H.cinv, H.singular);
+    k_mg_coarse_invert<<<1, NTm, 0, Lc.stream>>>(view(H.lev[H.nlev - 1]), H.cinv, H.singular);
   }
   Lc.tick(cfirst + 1);
 }
