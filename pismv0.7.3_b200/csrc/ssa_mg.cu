@@ -276,7 +276,8 @@ __global__ void __launch_bounds__(NTm, 2) k_mg_build(LevelView F, int Mxc, int M
 // Dense inverse of the coarsest operator (n = 2 N <= 32 unknowns) by Gauss-Jordan elimination
 // with partial pivoting, in place in shared memory, by one thread block (rows padded to 33
 // entries, so a column's entries of consecutive rows sit in different banks).  Warp 0 finds
-// each pivot; the elimination spreads the n x n element updates of a step over the block,
+// each pivot, swaps and scales the pivot row (two block barriers per step in all); the
+// elimination spreads the n x n element updates of a step over the block,
 // reading the step's multipliers from a copy of the pivot column, so each element is updated
 // with the same operands in the same order whatever thread does it.  Written transposed, so
 // that the per-cycle product reads it coalesced.
@@ -287,7 +288,6 @@ struct CoarseInvertSmem {
   double a[2 * MG_MAX_COARSE_CELLS][CI_PAD];
   double fcol[2 * MG_MAX_COARSE_CELLS];
   int perm[2 * MG_MAX_COARSE_CELLS];
-  int pivot;
 };
 
 __device__ void coarse_invert_block(const LevelView &L, CoarseInvertSmem &S, double *invT_out, int *singular) {
@@ -308,7 +308,9 @@ __device__ void coarse_invert_block(const LevelView &L, CoarseInvertSmem &S, dou
   }
   __syncthreads();
   for (int col = 0; col < n; ++col) {
-    if (tid < 32) {   // the pivot: the largest |a[r][col]|, r >= col, lowest row on ties
+    // warp 0: the pivot (the largest |a[r][col]|, r >= col, lowest row on ties), the row
+    // interchange, the scaled pivot row and the copy of the multipliers, ordered by __syncwarp
+    if (tid < 32) {
       const int t = tid;
       double best = -1.0;
       int bi = col;
@@ -326,32 +328,31 @@ __device__ void coarse_invert_block(const LevelView &L, CoarseInvertSmem &S, dou
       }
       if (t == 0) {
         S.perm[col] = bi;
-        S.pivot = bi;
         if (!(best > 0.0)) *singular = 1;
+      }
+      const int p = bi;
+      if (p != col && t < n) {   // lane t swaps column t of the two rows
+        const double tmp = S.a[col][t];
+        S.a[col][t] = S.a[p][t];
+        S.a[p][t] = tmp;
+      }
+      __syncwarp();
+      const double pv = S.a[col][col];
+      const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
+      __syncwarp();
+      // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot); the
+      // multipliers of the other rows are copied before any of them changes
+      if (t < n) {
+        S.a[col][t] = (t == col ? 1.0 : S.a[col][t]) * pinv;
+        S.fcol[t] = S.a[t][col];
       }
     }
     __syncthreads();
-    const int p = S.pivot;
-    if (p != col && tid < n) {   // thread t swaps column t of the two rows
-      const double tmp = S.a[col][tid];
-      S.a[col][tid] = S.a[p][tid];
-      S.a[p][tid] = tmp;
-    }
-    __syncthreads();
-    const double pv = S.a[col][col];
-    const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
-    __syncthreads();
-    // pivot row: a[col][col] <- 1, then scaled by 1 / pivot (so it holds 1 / pivot); the
-    // multipliers of the other rows are copied before any of them changes
-    if (tid < n) {
-      S.a[col][tid] = (tid == col ? 1.0 : S.a[col][tid]) * pinv;
-      S.fcol[tid] = S.a[tid][col];
-    }
-    __syncthreads();
-    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot
-    for (int e = tid; e < n * n; e += nth) {
-      const int r = e / n, q = e - r * n;
-      if (r == col) continue;
+    // other rows: a[r][q] -= a[r][col] a[col][q]; a[r][col] <- -a[r][col] / pivot (element e
+    // is (r, q) = (e / 32, e % 32), those outside n x n idle)
+    for (int e = tid; e < 32 * 32; e += nth) {
+      const int r = e >> 5, q = e & 31;
+      if (r == col || r >= n || q >= n) continue;
       const double f = S.fcol[r];
       if (q != col) S.a[r][q] -= f * S.a[col][q];
       else S.a[r][col] = -f * S.a[col][col];
@@ -374,20 +375,21 @@ __device__ void coarse_invert_block(const LevelView &L, CoarseInvertSmem &S, dou
   }
 }
 
-// the coarsest inverse alone (a hierarchy whose only coarse level is built from the fine grid)
-__global__ void __launch_bounds__(NTm) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
+// the coarsest inverse, after the last level build (CI_THREADS threads: one element of the
+// 32 x 32 elimination each)
+constexpr int CI_THREADS = 1024;
+__global__ void __launch_bounds__(CI_THREADS) k_mg_coarse_invert(LevelView L, double *invT_out, int *singular) {
   __shared__ CoarseInvertSmem S;
   coarse_invert_block(L, S, invT_out, singular);
 }
 
 // The small levels' Galerkin operators (levels first .. nlev - 1, each from the level above it,
 // all of <= MG_CTA_CELLS cells) and the coarsest inverse in one launch on one thread-block
-// cluster: one cluster barrier (release / acquire at cluster scope) between levels, then CTA 0
-// inverts the coarsest operator.  The arithmetic of every cell is k_mg_build's.
+// cluster: one cluster barrier (release / acquire at cluster scope) between levels; the
+// coarsest inverse follows as its own launch.  The arithmetic of every cell is k_mg_build's.
 __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
-    k_mg_build_small(const LevelView *__restrict__ lev, int first, int nlev, double *invT_out, int *singular) {
+    k_mg_build_small(const LevelView *__restrict__ lev, int first, int nlev) {
   cg::cluster_group cluster = cg::this_cluster();
-  __shared__ CoarseInvertSmem S;
   const int rank = cluster.block_rank() * NTm + threadIdx.x, nthr = SMALL_CLUSTER * NTm;
   for (int c = first; c < nlev; ++c) {
     const LevelView F = lev[c - 1], C = lev[c];
@@ -397,7 +399,6 @@ __global__ void __cluster_dims__(SMALL_CLUSTER, 1, 1) __launch_bounds__(NTm)
     }
     cluster.sync();
   }
-  if (cluster.block_rank() == 0) coarse_invert_block(lev[nlev - 1], S, invT_out, singular);   // uniform in CTA 0
 }
 
 // ---------------------------------------------------------------------------
@@ -1278,7 +1279,7 @@ void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHier
                                                                      H.fine_ay, C.Mx, C.My, tm, C.A, C.dinv);
   }
   // levels 1 .. cfirst - 1 by tiled passes; cfirst .. nlev - 1 (the cluster-cycled small
-  // levels) and the coarsest inverse by one cluster launch
+  // levels) by one cluster launch; then the coarsest inverse
   const int cfirst = H.nlev > 1 ? std::max(1, H.small_first) : H.nlev;
   for (int l = 0; l + 1 < cfirst; ++l) {
     const MGLevel &F = H.lev[l], &C = H.lev[l + 1];
@@ -1287,10 +1288,10 @@ void mg_setup_coarse(const Launch &Lc, const GridDev &g, const Fields &f, MGHier
   }
   if (cfirst < H.nlev) {
     k_mg_build_small<<<SMALL_CLUSTER, NTm, 0, Lc.stream>>>(reinterpret_cast<const LevelView *>(H.views), cfirst,
-                                                             H.nlev, H.cinv, H.singular);
-  } else {
-    k_mg_coarse_invert<<<1, NTm, 0, Lc.stream>>>(view(H.lev[H.nlev - 1]), H.cinv, H.singular);
+                                                             H.nlev);
+    Lc.tick();
   }
+  k_mg_coarse_invert<<<1, CI_THREADS, 0, Lc.stream>>>(view(H.lev[H.nlev - 1]), H.cinv, H.singular);
   Lc.tick(cfirst + 1);
 }
 
