@@ -380,7 +380,8 @@ void pism_gpu_ssafem_options_defaults(pism_gpu_ssafem_options *o);
  * pism_gpu_ssa_set_inputs (mask, melange and the CFBC are not used by this discretisation);
  * Dirichlet data where bc_mask is 1.  stats may be NULL.  Returns PISM_GPU_SSA_EPICARD when
  * the nonlinear solve does not converge ("SSAFEM solve failed to converge") and
- * PISM_GPU_SSA_EKSP when a linear solve breaks down or reaches ksp_max_it. */
+ * PISM_GPU_SSA_EKSP when a linear solve breaks down or reaches ksp_max_it; after a failure the
+ * handle's velocity is the one the solve started from (SSAFEM.cc:215-228). */
 int pism_gpu_ssafem_solve(pism_gpu_ssa *h, const pism_gpu_ssafem_options *o, pism_gpu_ssafem_stats *stats);
 
 /* Stage entry points, each the device restatement of one reference method, for

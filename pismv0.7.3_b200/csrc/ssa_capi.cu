@@ -1487,6 +1487,8 @@ int pism_gpu_ssafem_solve(pism_gpu_ssa *h, const pism_gpu_ssafem_options *o, pis
   FemCG cg{};
   pism_gpu_ssafem_stats st{};
   double2 *vel = h->vel;
+  // SSAFEM::solve_nocache keeps the velocity of a failed solve (SSAFEM.cc:215-228)
+  CK(h, cudaMemcpyAsync(S.vel0, vel, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
   launch_fem_residual(L, P, S, vel, S.F, false, h->bc, h->bcv);
   CK(h, cudaGetLastError());
   RET(copy_out(h, &sc, S.sc, sizeof(sc), PISM_MEM_HOST));
@@ -1556,6 +1558,8 @@ int pism_gpu_ssafem_solve(pism_gpu_ssa *h, const pism_gpu_ssafem_options *o, pis
   }
   st.fnorm = fn;
   if (stats) *stats = st;
+  if (rc != PISM_GPU_SSA_OK)
+    CK(h, cudaMemcpyAsync(vel, S.vel0, sizeof(double2) * h->N, cudaMemcpyDeviceToDevice, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   return rc;
 }

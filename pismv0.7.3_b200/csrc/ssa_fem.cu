@@ -434,7 +434,7 @@ int fem_allocate(FemState &S, int Mx, int My, int periodicity) {
   const size_t Q = 4 * (size_t)S.Ne, N = S.N;
   int bad = alloc(&S.C.H, Q) | alloc(&S.C.tauc, Q) | alloc(&S.C.tdu, Q) | alloc(&S.C.tdv, Q) | alloc(&S.C.B, Q) |
             alloc(&S.C.mask, Q) | alloc(&S.J, 36 * N) | alloc(&S.dinv, N) | alloc(&S.F, N) | alloc(&S.Ft, N) |
-            alloc(&S.du, N) | alloc(&S.trial, N) | alloc(&S.r, N) | alloc(&S.z, N) | alloc(&S.p, N) |
+            alloc(&S.du, N) | alloc(&S.trial, N) | alloc(&S.vel0, N) | alloc(&S.r, N) | alloc(&S.z, N) | alloc(&S.p, N) |
             alloc(&S.q, N) | alloc(&S.cg, 1) | alloc(&S.sc, 1) | alloc(&S.zero_pivot, 1);
   if (bad) {
     fem_free(S);
@@ -445,7 +445,7 @@ int fem_allocate(FemState &S, int Mx, int My, int periodicity) {
 
 void fem_free(FemState &S) {
   void *ptrs[] = {S.C.H, S.C.tauc, S.C.tdu, S.C.tdv, S.C.B, S.C.mask, S.J, S.dinv, S.F, S.Ft,
-                  S.du, S.trial, S.r, S.z, S.p, S.q, S.cg, S.sc, S.zero_pivot};
+                  S.du, S.trial, S.vel0, S.r, S.z, S.p, S.q, S.cg, S.sc, S.zero_pivot};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   S = FemState{};

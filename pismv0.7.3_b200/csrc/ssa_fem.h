@@ -39,6 +39,7 @@ struct FemState {
   double *J = nullptr;                 // [36][N]: neighbour block (di+1)*3+(dj+1), row c, column d
   double4 *dinv = nullptr;             // inverse diagonal blocks
   double2 *F = nullptr, *Ft = nullptr, *du = nullptr, *trial = nullptr;
+  double2 *vel0 = nullptr;             // the velocity before the solve, put back if it fails
   double2 *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
   FemCG *cg = nullptr;
   FemScalars *sc = nullptr;

@@ -85,9 +85,19 @@ def test_enthalpy_hardness_at_the_quadrature_points():
 
 
 def test_failure_to_converge_raises():
+    """too few Newton steps: SSAFEMFailure, and the velocity is the one the solve started from"""
     g, c, f = V.build_test_i(My=61)
-    with pytest.raises(SSAFEMFailure):
-        gpu_solve(g, c, f, snes_max_it=1)
+    s = SSAFEM(g, c, snes_max_it=1)
+    try:
+        s.set_inputs(**{k: f[k] for k in ("thickness", "surface", "bed", "mask", "tauc")},
+                     bc_mask=f["bc_mask"], bc_values=f["bc_values"])
+        start = np.full((g.Mx, g.My, 2), 1e-6)
+        s.set_initial_guess(start)
+        with pytest.raises(SSAFEMFailure):
+            s.solve()
+        np.testing.assert_array_equal(s.velocity(), start)
+    finally:
+        s.close()
 
 
 def test_the_front_end_builds_ssafem():
