@@ -1521,9 +1521,33 @@ int pism_gpu_ssafem_solve(pism_gpu_ssa *h, const pism_gpu_ssafem_options *o, pis
       rc = fail(h, PISM_GPU_SSA_EZERODIAG, "SSAFEM: singular diagonal block at node %d", zp - 1);
       break;
     }
-    // conjugate gradients in batches; each iteration is skipped on the device once done
+    // conjugate gradients in batches of FEM_CG_BATCH iterations, each skipped on the device once
+    // done; the batch is captured into a CUDA graph on first use (its buffers never move) and
+    // replayed, with direct launches if the capture fails
+    if (!S.cg_batch && !S.cg_batch_failed && h->cfg.graphs >= 1) {
+      cudaGraph_t graph = nullptr;
+      const long long before = h->stats.kernel_launches;
+      bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        launch_fem_cg_iterations(L, P, S, FEM_CG_BATCH);
+        ok = cudaStreamEndCapture(h->stream, &graph) == cudaSuccess && graph != nullptr;
+      }
+      if (ok) ok = cudaGraphInstantiate(&S.cg_batch, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+      if (!ok) {
+        S.cg_batch = nullptr;
+        S.cg_batch_failed = true;
+        cudaGetLastError();   // clear the capture's error; the direct launches follow
+      }
+      h->stats.kernel_launches = before;   // nothing ran during the capture
+    }
     for (;;) {
-      launch_fem_cg_iterations(L, P, S, 16);
+      if (S.cg_batch) {
+        CK(h, cudaGraphLaunch(S.cg_batch, h->stream));
+        L.tick(3 * FEM_CG_BATCH);
+      } else {
+        launch_fem_cg_iterations(L, P, S, FEM_CG_BATCH);
+      }
       CK(h, cudaGetLastError());
       RET(copy_out(h, &cg, S.cg, sizeof(cg), PISM_MEM_HOST));
       if (cg.done) break;

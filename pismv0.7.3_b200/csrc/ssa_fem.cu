@@ -448,6 +448,7 @@ void fem_free(FemState &S) {
                   S.du, S.trial, S.vel0, S.r, S.z, S.p, S.q, S.cg, S.sc, S.zero_pivot};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (S.cg_batch) cudaGraphExecDestroy(S.cg_batch);
   S = FemState{};
 }
 

@@ -44,7 +44,10 @@ struct FemState {
   FemCG *cg = nullptr;
   FemScalars *sc = nullptr;
   int *zero_pivot = nullptr;
+  cudaGraphExec_t cg_batch = nullptr;  // FEM_CG_BATCH CG iterations captured once (all buffers fixed)
+  bool cg_batch_failed = false;
 };
+constexpr int FEM_CG_BATCH = 16;
 
 struct FemProblem {
   int Mx, My, periodicity;
