@@ -481,6 +481,23 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   const long long t0 = h->stats.kernel_launches;
   long long inc_picard = 0, inc_refine = 0, inc_inner = 0, inc_go = 0, inc_test = 0, inc_rebuild = 0, pre = 0;
   const bool lagged = mg && c.mg_rebuild_rtol > 0.0;
+  // a second capture stream for the per-Picard set-up that the coarse-level builds do not read
+  struct SideBranch {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~SideBranch() {
+      if (fork) cudaEventDestroy(fork);
+      if (join) cudaEventDestroy(join);
+      if (stream) cudaStreamDestroy(stream);
+    }
+  } side;
+  bool split = mixed && !lagged && !line;
+  if (split && (cudaStreamCreateWithFlags(&side.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&side.fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&side.join, cudaEventDisableTiming) != cudaSuccess)) {
+    cudaGetLastError();
+    split = false;
+  }
   if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
     S.failed = true;
@@ -495,8 +512,27 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
   bool ok = add_conditional(h, cudaGraphCondTypeWhile, not_done(&P->done), [&] {
     bool inner_ok = true, rebuild_ok = true;
     launch_picard_begin(h->L, P, pc, h->zd_dev);
-    launch_diag_setup(h->L, g, f, h->K.dinv, h->zd_dev);
-    if (lagged) {
+    bool residual_queued = false;
+    if (split) {
+      // The set-up in two branches of the graph. On the loop's stream: the coarse-level
+      // Galerkin builds and the coarsest inverse, which read nu*H, beta and the masks only.
+      // Beside them: the FP64 diagonal blocks, the FP32 fine-level copies and the first
+      // refinement residual. The small levels' builds run on one cluster and the inverse on
+      // one block, so most SMs are free for the second branch. Same kernels, same inputs:
+      // the results are those of the serial order.
+      cudaEventRecord(side.fork, h->L.stream);
+      cudaStreamWaitEvent(side.stream, side.fork, 0);
+      Launch Ls = h->L;
+      Ls.stream = side.stream;
+      launch_diag_setup(Ls, g, f, h->K.dinv, h->zd_dev);
+      mg_setup_fine(Ls, g, f, h->K.dinv, h->mg);
+      launch_residual32(Ls, g, f, h->rhs, h->vel, h->K32.rhs, h->res_dev);
+      cudaEventRecord(side.join, side.stream);
+      mg_setup_coarse(h->L, g, f, h->mg);
+      cudaStreamWaitEvent(h->L.stream, side.join, 0);
+      residual_queued = true;
+    } else if (lagged) {
+      launch_diag_setup(h->L, g, f, h->K.dinv, h->zd_dev);
       mg_setup_fine(h->L, g, f, h->K.dinv, h->mg);
       rebuild_ok = add_conditional(
           h, cudaGraphCondTypeIf,
@@ -506,12 +542,13 @@ int build_solve_graph(pism_gpu_ssa *h, double reg, double underrelax, bool *buil
             return true;
           },
           &inc_rebuild);
-    } else if (mg) {
-      mg_setup(h->L, g, f, h->K.dinv, h->mg);
+    } else {
+      launch_diag_setup(h->L, g, f, h->K.dinv, h->zd_dev);
+      if (mg) mg_setup(h->L, g, f, h->K.dinv, h->mg);
     }
     if (line) line_setup(h->L, g, f, h->K.dinv, h->line);
     if (mixed) {
-      launch_residual32(h->L, g, f, h->rhs, h->vel, h->K32.rhs, h->res_dev);
+      if (!residual_queued) launch_residual32(h->L, g, f, h->rhs, h->vel, h->K32.rhs, h->res_dev);
       inner_ok = add_conditional(h, cudaGraphCondTypeWhile, not_done(&P->refine_done), [&] {
         launch_mixed_init_dev(h->L, N, h->K32, h->res_dev, &P->rtol, c.mixed_inner_rtol, c.ksp_max_it);
         bool ok2 = add_conditional(
